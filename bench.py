@@ -1,0 +1,412 @@
+"""Benchmark of the B200 mapping + simulation path (one JSON line on rank 0).
+
+Workload (per GPU): the 40 x 40 x 10 m scene with 2000 boxes and 300 cylinders at 0.05 m, a
+640x480 frustum camera (87 x 58 deg, 10 m), a 100-frame seeded trajectory.  One step = one
+frame: simulated range image -> range noise (sigma 0.005 d^2, 2 % dropped) -> traversal and
+per-frame labels -> integration into the device map.  Inputs (sim map, poses) are resident
+when timing starts; L2 is flushed (256 MiB write) between steps, outside the per-step events.
+
+`e2e` repeats the metric through the reference-facing call (nm_map_insert_points with
+PointCloud2-style xyz records in pinned host memory, copied to the device inside the call,
+and a synchronous read-back of the frame status).
+
+`--impl reference` times the CPU path the reference runs (Handler::processPointCloudCPU,
+restated by the oracle, plus its simulated depth) on the host cores, rank 0 only.
+
+Multi-GPU (torchrun): each rank maps its own agent's trajectory into its own map (weak
+scaling, no collective on the data path); `value` = all ranks' voxel updates / max time.
+"""
+from __future__ import annotations
+
+import argparse
+import json
+import math
+import os
+import statistics
+import subprocess
+import sys
+import time
+from pathlib import Path
+
+import numpy as np
+
+ROOT = Path(__file__).resolve().parent
+sys.path.insert(0, str(ROOT))
+
+METRIC = "voxel updates/s"
+UNIT = "voxel updates/s"
+WORKLOAD = "sim_headline"
+
+
+def workload_config(spec):
+    return {
+        "workload": (f"sim+map frame: {spec.size[0]:.0f}x{spec.size[1]:.0f}x{spec.size[2]:.0f} m, "
+                     f"{spec.n_boxes} boxes + {spec.n_cyl} cylinders, {spec.width}x{spec.height} "
+                     f"{spec.hfov:.0f}x{spec.vfov:.0f} deg, {spec.max_range:.0f} m range, "
+                     f"{spec.map_res} m voxels, label mode, round-down policy"),
+        "frames_per_step": 1,
+        "pixels_per_frame": spec.width * spec.height,
+        "l2": "flushed between steps (256 MiB write outside the per-step CUDA events)",
+    }
+
+
+def dist_init():
+    ws = int(os.environ.get("WORLD_SIZE", "1"))
+    if ws <= 1:
+        return 0, 1, 0
+    import datetime
+
+    import torch
+    import torch.distributed as dist
+    rank = int(os.environ["RANK"])
+    local = int(os.environ.get("LOCAL_RANK", rank))
+    backend = "nccl" if torch.cuda.is_available() else "gloo"
+    if backend == "nccl":
+        torch.cuda.set_device(local)
+    dist.init_process_group(backend, timeout=datetime.timedelta(seconds=120))
+    return rank, ws, local
+
+
+def barrier():
+    import torch.distributed as dist
+    if dist.is_available() and dist.is_initialized():
+        dist.barrier()
+
+
+def allreduce_max(x: float) -> float:
+    import torch
+    import torch.distributed as dist
+    if not (dist.is_available() and dist.is_initialized()):
+        return x
+    dev = "cuda" if dist.get_backend() == "nccl" else "cpu"
+    t = torch.tensor([x], dtype=torch.float64, device=dev)
+    dist.all_reduce(t, op=dist.ReduceOp.MAX)
+    return float(t.item())
+
+
+def allreduce_sum(x: float) -> float:
+    import torch
+    import torch.distributed as dist
+    if not (dist.is_available() and dist.is_initialized()):
+        return x
+    dev = "cuda" if dist.get_backend() == "nccl" else "cpu"
+    t = torch.tensor([x], dtype=torch.float64, device=dev)
+    dist.all_reduce(t, op=dist.ReduceOp.SUM)
+    return float(t.item())
+
+
+class ClockSampler:
+    """nvidia-smi clock / throttle samples while the timed region runs."""
+
+    FIELDS = ("index,clocks.sm,clocks.max.sm,power.draw,clocks_event_reasons.active,"
+              "clocks_event_reasons.hw_slowdown,clocks_event_reasons.hw_thermal_slowdown,"
+              "clocks_event_reasons.sw_thermal_slowdown,clocks_event_reasons.sw_power_cap")
+
+    def __init__(self, device: int):
+        self.device = device
+        self.proc = None
+        self.path = Path(os.environ.get("TMPDIR", "/tmp")) / f"nm_clocks_{os.getpid()}.csv"
+
+    def start(self):
+        try:
+            self.fh = open(self.path, "w")
+            self.proc = subprocess.Popen(
+                ["nvidia-smi", f"--id={self.device}", f"--query-gpu={self.FIELDS}",
+                 "--format=csv,noheader,nounits", "-lms", "200"], stdout=self.fh,
+                stderr=subprocess.DEVNULL)
+        except (OSError, FileNotFoundError):
+            self.proc = None
+
+    def stop(self) -> dict:
+        if self.proc is None:
+            return {"sm_mhz": None, "sm_max_mhz": None, "reasons": ["nvidia-smi unavailable"]}
+        time.sleep(0.25)
+        self.proc.terminate()
+        try:
+            self.proc.wait(timeout=5)
+        except subprocess.TimeoutExpired:
+            self.proc.kill()
+        self.fh.close()
+        sm, smax, reasons = [], [], set()
+        names = ["hw_slowdown", "hw_thermal_slowdown", "sw_thermal_slowdown", "sw_power_cap"]
+        for line in self.path.read_text().splitlines():
+            f = [x.strip() for x in line.split(",")]
+            if len(f) < 9:
+                continue
+            try:
+                sm.append(float(f[1]))
+                smax.append(float(f[2]))
+            except ValueError:
+                continue
+            for n, v in zip(names, f[5:9]):
+                if v.lower().startswith("active"):
+                    reasons.add(n)
+        return {"sm_mhz": statistics.median(sm) if sm else None,
+                "sm_max_mhz": max(smax) if smax else None, "reasons": sorted(reasons),
+                "samples": len(sm)}
+
+
+def run_reference(args, rank, world):
+    """CPU path of the reference (oracle restatement), rank 0 only."""
+    if rank != 0:
+        return None
+    from nanomap_b200 import api as A
+    from nanomap_b200 import scenes as S
+    from oracle import oracle as O
+    spec = S.SCENES[WORKLOAD]
+    scene = S.make_scene(spec, 1)
+    traj = S.trajectory(scene, spec.frames, seed=7)
+    desc = A.sensor_desc(**S.sensor_desc_kwargs(spec))
+    osen = O.Sensor.from_desc(desc)
+    sim = O.SimMap(spec.sim_res, scene.vox_min, scene.vox_max, scene.boxes, scene.cylinders)
+    om = O.Map(spec.map_res, clamp_min=spec.clamp[0], clamp_max=spec.clamp[1], rounding=1)
+    threads = os.cpu_count() or 1
+    rng = np.random.default_rng(5)
+
+    def step(i):
+        pos, q = traj[i % len(traj)]
+        R = O.rotation(q, list(desc.frame_transform))
+        r = sim.render(osen, pos, R, threads=threads)
+        valid = r > 0
+        r = np.where(valid, r + rng.normal(0, 1, r.shape) * spec.noise_coef * r * r, 0).astype(np.float32)
+        r[rng.random(r.shape) < spec.drop] = 0
+        r[~(r > 0)] = 0
+        eye, mt = O.frame_setup(pos, spec.map_res, desc.max_range, 1)
+        om.insert(R, eye, mt, desc.log_odds_hit, desc.log_odds_miss, osen.points(r), threads=threads)
+
+    for i in range(args.warmup):
+        step(i)
+    v0 = om.stats()["visits"]
+    t0 = time.perf_counter()
+    for i in range(args.steps):
+        step(args.warmup + i)
+    dt = time.perf_counter() - t0
+    visits = om.stats()["visits"] - v0
+    value = visits / dt
+    cfg = workload_config(spec)
+    cfg["l2"] = "n/a (host CPU)"
+    line = {
+        "impl": "reference", "metric": METRIC, "value": value, "unit": UNIT, "n_gpus": world,
+        "steps": args.steps, "warmup": args.warmup, "ms_per_step": dt * 1e3 / args.steps,
+        "higher_is_better": True, "scaling": "weak", "vs_baseline": None, "dtype": "f64",
+        "data": "synthetic", "config": cfg,
+        "cpu_baseline": {"value": value, "unit": UNIT, "cores": threads, "kind": "port",
+                         "sample": f"{args.steps} full frames (sim depth + insertion), oracle restatement of Handler::processPointCloudCPU"},
+        "e2e": {"value": value, "unit": UNIT, "h2d_bytes_per_step": 0, "d2h_bytes_per_step": 0},
+    }
+    return line
+
+
+def cpu_baseline(spec, desc, frames_host, budget_s=12.0):
+    """Single-thread oracle on a bounded sample of the same frames (rank 0, N=1)."""
+    from oracle import oracle as O
+    osen = O.Sensor.from_desc(desc)
+    om = O.Map(spec.map_res, clamp_min=spec.clamp[0], clamp_max=spec.clamp[1], rounding=1)
+    t0 = time.perf_counter()
+    n = 0
+    for pose, r in frames_host:
+        R = O.rotation(pose.orientation, list(desc.frame_transform))
+        eye, mt = O.frame_setup(pose.position, spec.map_res, desc.max_range, 1)
+        om.insert(R, eye, mt, desc.log_odds_hit, desc.log_odds_miss, osen.points(r), threads=1)
+        n += 1
+        if time.perf_counter() - t0 > budget_s:
+            break
+    dt = time.perf_counter() - t0
+    return {"value": om.stats()["visits"] / dt, "unit": UNIT, "cores": 1, "kind": "port",
+            "sample": f"first {n} frames of the timed trajectory, single thread, includes range->point conversion"}
+
+
+def run_ours(args, rank, world, local):
+    import torch
+
+    from nanomap_b200 import _native as N
+    from nanomap_b200 import api as A
+    from nanomap_b200 import scenes as S
+
+    torch.cuda.set_device(local)
+    dev = torch.device("cuda", local)
+    spec = S.SCENES[WORKLOAD]
+    scene = S.make_scene(spec, 1)
+    traj = S.trajectory(scene, spec.frames, seed=7 + 1000 * rank)
+    ctx = A.Context(local)
+    desc = A.sensor_desc(**S.sensor_desc_kwargs(spec))
+    sensor = A.Sensor(ctx, desc)
+    sim = A.SimMap(ctx, spec.sim_res, boxes=scene.boxes, cylinders=scene.cylinders,
+                   vox_min=scene.vox_min, vox_max=scene.vox_max)
+    mdesc = A.map_desc(res=spec.map_res, clamp_min=spec.clamp[0], clamp_max=spec.clamp[1],
+                       rounding=N.NM_ROUND_DOWN, initial_leaf_capacity=1 << 21)
+    m = A.Map(ctx, mdesc)
+    stream = torch.cuda.current_stream(dev)
+    H, W = spec.height, spec.width
+    ranges = torch.zeros(H, W, device=dev)
+    flush = torch.empty(256 << 20, dtype=torch.uint8, device=dev)
+    poses = [A.Pose(p, q) for p, q in traj]
+
+    def step(i, ev=None):
+        pose = poses[i % len(poses)]
+        if ev:
+            ev[0].record(stream)
+        sim.render(sensor, pose, ranges, stream=stream)
+        ctx.add_noise(ranges, spec.noise_coef, spec.drop, 1000003 * (i + 1), stream=stream)
+        if ev:
+            ev[1].record(stream)
+        m.insert_ranges(sensor, pose, ranges, flags=N.NM_DEFER_INTEGRATE, stream=stream)
+        if ev:
+            ev[2].record(stream)
+        m.integrate(stream=stream)
+        if ev:
+            ev[3].record(stream)
+
+    for i in range(args.warmup):
+        step(i)
+        flush.fill_(i & 0xFF)
+    torch.cuda.synchronize()
+    s0 = m.stats()
+    evs = [[torch.cuda.Event(enable_timing=True) for _ in range(4)] for _ in range(args.steps)]
+    clocks = ClockSampler(local)
+    clocks.start()
+    barrier()
+    torch.cuda.synchronize()
+    t_start = torch.cuda.Event(enable_timing=True)
+    t_end = torch.cuda.Event(enable_timing=True)
+    t_start.record(stream)
+    for k in range(args.steps):
+        step(args.warmup + k, evs[k])
+        flush.fill_(k & 0xFF)
+    t_end.record(stream)
+    torch.cuda.synchronize()
+    barrier()
+    clk = clocks.stop()
+    s1 = m.stats()
+    step_ms = [e[0].elapsed_time(e[3]) for e in evs]
+    trav_ms = [e[1].elapsed_time(e[2]) for e in evs]
+    integ_ms = [e[2].elapsed_time(e[3]) for e in evs]
+    sim_ms = [e[0].elapsed_time(e[1]) for e in evs]
+    local_time = sum(step_ms) / 1e3
+    region_ms = t_start.elapsed_time(t_end)
+    visits = s1["visits"] - s0["visits"]
+    rays = s1["rays"] - s0["rays"]
+    uniq = s1["unique_voxels"] - s0["unique_voxels"]
+    leaves = s1["touched_leaves"] - s0["touched_leaves"]
+    assert s1["error_flags"] == 0, "device error during the timed region"
+    t_max = allreduce_max(local_time)
+    visits_all = allreduce_sum(visits)
+    value = visits_all / t_max
+
+    # e2e: reference-facing insert of pinned host xyz records (step 16 bytes)
+    e2e = None
+    if args.e2e_steps > 0:
+        frames_xyz = []
+        pm = sensor.params()
+        u = (np.arange(W, dtype=np.float32) * pm[4])[None, :]
+        v = (np.arange(H, dtype=np.float32) * pm[5])[:, None]
+        dx = u * pm[2] - pm[0]
+        dy = v * pm[3] - pm[1]
+        nrm = np.sqrt(dx * dx + dy * dy + 1.0).astype(np.float32)
+        for k in range(min(args.e2e_steps, 20)):
+            step(k)
+            r = ranges.cpu().numpy()
+            sc = r / nrm
+            rec = torch.zeros(H * W, 4, dtype=torch.float32).pin_memory()
+            xyz = np.stack([dx * sc, np.broadcast_to(dy, (H, W)) * sc, sc], axis=-1).reshape(-1, 3)
+            xyz[(r <= 0).reshape(-1)] = np.nan
+            rec[:, :3] = torch.from_numpy(xyz.astype(np.float32))
+            frames_xyz.append((poses[k % len(poses)], rec))
+        m2 = A.Map(ctx, mdesc)
+        for k in range(3):
+            pose, rec = frames_xyz[k % len(frames_xyz)]
+            m2.insert_points(sensor, pose, rec, W, H, 16, flags=N.NM_SYNC)
+        e0 = m2.stats()
+        barrier()
+        torch.cuda.synchronize()
+        t0 = time.perf_counter()
+        for k in range(args.e2e_steps):
+            pose, rec = frames_xyz[k % len(frames_xyz)]
+            m2.insert_points(sensor, pose, rec, W, H, 16, flags=N.NM_SYNC)
+        dt = time.perf_counter() - t0
+        barrier()
+        e1 = m2.stats()
+        dt = allreduce_max(dt)
+        ev_all = allreduce_sum(e1["visits"] - e0["visits"])
+        e2e = {"value": ev_all / dt, "unit": UNIT, "h2d_bytes_per_step": H * W * 16,
+               "d2h_bytes_per_step": 8, "steps": args.e2e_steps,
+               "path": "nm_map_insert_points(host xyz records, step 16, NM_SYNC)"}
+        m2.close()
+
+    # roofline of the dominant kernel (traversal): algorithmic bytes per launch =
+    # 4 B per pixel (range read) + 1 B per unique labelled voxel + 16 B per touched leaf
+    n_steps = args.steps
+    pix = H * W
+    u_vox = uniq / n_steps
+    u_leaf = leaves / n_steps
+    trav_bytes = 4 * pix + 1 * u_vox + 16 * u_leaf
+    integ_bytes = 9 * u_vox + 64 * u_leaf
+    peaks = json.loads((ROOT / "MEASURED_PEAKS.json").read_text()) if (ROOT / "MEASURED_PEAKS.json").exists() else {}
+    hbm = peaks.get("hbm_gbs", 6650.0)
+    t_trav = statistics.mean(trav_ms) / 1e3
+    t_integ = statistics.mean(integ_ms) / 1e3
+    dominant = "traverse" if t_trav >= t_integ else "integrate"
+    if dominant == "traverse":
+        ach = trav_bytes / t_trav / 1e9
+        traffic = None
+    else:
+        ach = integ_bytes / t_integ / 1e9
+        traffic = None
+    line = {
+        "metric": METRIC, "value": value, "unit": UNIT, "n_gpus": world, "steps": args.steps,
+        "warmup": args.warmup, "ms_per_step": t_max * 1e3 / args.steps, "higher_is_better": True,
+        "scaling": "weak", "vs_baseline": None, "dtype": "f64", "data": "synthetic",
+        "config": workload_config(spec),
+        "frames_per_s": world * args.steps / t_max,
+        "rays_per_s": allreduce_sum(rays) / t_max,
+        "unique_voxel_updates_per_s": allreduce_sum(uniq) / t_max,
+        "per_frame": {"visits": visits / n_steps, "rays": rays / n_steps, "unique_voxels": u_vox,
+                      "touched_leaves": u_leaf},
+        "stage_ms": {"sim_render+noise": statistics.mean(sim_ms), "traverse": statistics.mean(trav_ms),
+                     "integrate": statistics.mean(integ_ms), "timed_region_incl_flush": region_ms / args.steps},
+        "gpu_launches": args.steps * 4,
+        "roofline": {"bound": "hbm", "kernel": f"k_{dominant}", "achieved": ach, "peak": hbm,
+                     "unit": "GB/s", "frac": ach / hbm, "traffic": traffic,
+                     "peak_source": "measured (MEASURED_PEAKS.json hbm_gbs)" if peaks else "fallback",
+                     "algorithmic_bytes_per_launch": trav_bytes if dominant == "traverse" else integ_bytes},
+        "e2e": e2e,
+        "clocks": clk,
+    }
+    if rank == 0 and world == 1 and args.cpu_baseline_s > 0:
+        frames_host = []
+        for k in range(30):
+            step(k)
+            frames_host.append((poses[k % len(poses)], ranges.cpu().numpy().copy()))
+        line["cpu_baseline"] = cpu_baseline(spec, desc, frames_host, args.cpu_baseline_s)
+    m.close()
+    sim.close()
+    sensor.close()
+    ctx.close()
+    return line
+
+
+def main():
+    ap = argparse.ArgumentParser()
+    ap.add_argument("--gpus", type=int, default=1)
+    ap.add_argument("--steps", type=int, default=50)
+    ap.add_argument("--warmup", type=int, default=5)
+    ap.add_argument("--impl", choices=["ours", "reference"], default="ours")
+    ap.add_argument("--e2e-steps", type=int, default=30)
+    ap.add_argument("--cpu-baseline-s", type=float, default=12.0)
+    args = ap.parse_args()
+    if args.warmup < 3:
+        args.warmup = 3
+    rank, world, local = dist_init()
+    if args.impl == "reference":
+        line = run_reference(args, rank, world)
+    else:
+        line = run_ours(args, rank, world, local)
+    if rank == 0 and line is not None:
+        print(json.dumps(line), flush=True)
+    import torch.distributed as dist
+    if dist.is_available() and dist.is_initialized():
+        dist.destroy_process_group()
+
+
+if __name__ == "__main__":
+    main()

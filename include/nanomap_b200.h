@@ -1,0 +1,215 @@
+/*
+ * nanomap_b200.h -- C ABI of the B200-native NanoMap mapping and simulation path.
+ *
+ * Plain C types only: opaque handles, pointers and sizes.  Every call returns an int status
+ * (NM_OK or an NM_ERR_* code); nm_last_error() gives the message of the calling thread's
+ * last failure.  All device memory belongs to the library; inputs are borrowed for the call;
+ * outputs go to caller buffers.  `stream` arguments are cudaStream_t values passed as void*
+ * (NULL = the CUDA default stream).  A context is used from one host thread at a time.
+ * No call changes the caller's floating-point environment.
+ *
+ * Reference interfaces each entry point replaces are cited as path:line within the
+ * NanoMap source tree.
+ */
+#ifndef NANOMAP_B200_H_
+#define NANOMAP_B200_H_
+
+#include <stddef.h>
+#include <stdint.h>
+
+#ifdef __cplusplus
+extern "C" {
+#endif
+
+#define NM_ABI_VERSION 1
+
+/* status codes */
+#define NM_OK 0
+#define NM_ERR_ARG 1         /* bad argument (null, size, range) */
+#define NM_ERR_CAPACITY 2    /* a fixed-capacity device structure overflowed */
+#define NM_ERR_CUDA 3        /* a CUDA runtime call failed */
+#define NM_ERR_TIMEOUT 4     /* a bounded device-side wait gave up */
+#define NM_ERR_STATE 5       /* call not valid in the object's current state */
+#define NM_ERR_IO 6          /* file could not be read or parsed */
+#define NM_ERR_UNSUPPORTED 7 /* input format or option this build does not handle */
+
+/* sensor types (SharedParameters::_type, SharedParameters.h:197) */
+#define NM_SENSOR_FRUSTUM 0
+#define NM_SENSOR_LASER 1
+
+/* map update modes */
+#define NM_UPDATE_LABEL 0      /* one update per voxel per frame; hit overrides miss */
+#define NM_UPDATE_ACCUMULATE 1 /* per-ray sums (Handler.cpp:47-56, 77-82), from exact counts */
+
+/* clamp order (Handler.cpp:98-110 vs SimHandler.cpp:98-110) */
+#define NM_CLAMP_ALWAYS 0
+#define NM_CLAMP_ON_CROSSING 1
+
+/* rounding of the per-point host-path arithmetic (the reference sets FE_DOWNWARD in
+ * SensorData::updatePose, SensorData.h:42, and never restores it) */
+#define NM_ROUND_NEAREST 0
+#define NM_ROUND_DOWN 1
+
+/* flags for insert / render / tick calls */
+#define NM_INPUT_HOST 0x1u       /* input pointer is host memory, copied inside the call */
+#define NM_DEFER_INTEGRATE 0x2u  /* label only; nm_map_integrate applies the labels later */
+#define NM_SYNC 0x4u             /* wait for completion; report device-side errors now */
+#define NM_OUTPUT_HOST 0x8u      /* output pointer is host memory */
+
+typedef struct nm_context_s* nm_context;
+typedef struct nm_sensor_s* nm_sensor;
+typedef struct nm_map_s* nm_map;
+typedef struct nm_simmap_s* nm_simmap;
+
+/* nanomap::Pose (nanomap.h:20-28): position (m) and unit quaternion (w, x, y, z). */
+typedef struct {
+  float position[3];
+  float orientation[4];
+} nm_pose;
+
+/* Sensor parameters (FrustumData.h:261-288, LaserData.h:255-284, Config.cpp:172-267). */
+typedef struct {
+  int32_t type;              /* NM_SENSOR_FRUSTUM or NM_SENSOR_LASER */
+  int32_t id;
+  int32_t hres, vres;        /* pixels (frustum) or columns/rows (laser) */
+  float hfov_deg;            /* frustum: <= 0 derives it from the aspect ratio (Sensor.h:158-161) */
+  float vfov_deg;
+  float min_range, max_range;
+  float prob_hit, prob_miss; /* used when explicit_log_odds == 0 (Sensor.h:183-184) */
+  float log_odds_hit, log_odds_miss;
+  int32_t explicit_log_odds;
+  int32_t rate;
+  float frame_transform[9];  /* column-major: entries 0..2 are column 0 (Config.cpp:210-216) */
+} nm_sensor_desc;
+
+/* Map parameters (OccupancyMap.h:35-52 plus the explicit-constant extension). */
+typedef struct {
+  float res;                 /* voxel edge, metres */
+  int32_t leaf_edge;         /* must be 8 (NodeEdge) */
+  float thres_hit, thres_miss;   /* log-odds thresholds of the active flag */
+  float clamp_min, clamp_max;    /* log-odds clamps */
+  int32_t clamp_mode;        /* NM_CLAMP_* */
+  int32_t update_mode;       /* NM_UPDATE_* */
+  int32_t rounding;          /* NM_ROUND_* */
+  uint32_t initial_leaf_capacity; /* 0 = default; the table grows on demand */
+  int32_t max_agents;        /* label planes kept for batched ticks (>= 1) */
+} nm_map_desc;
+
+/* Cumulative counters of a map, reset by nm_map_reset. */
+typedef struct {
+  uint64_t frames;
+  uint64_t rays;           /* points that produced a traversal */
+  uint64_t visits;         /* label events: voxels left by a step plus end voxels */
+  uint64_t unique_voxels;  /* voxels integrated (one per voxel per frame) */
+  uint64_t touched_leaves; /* leaves integrated, summed over frames */
+  uint64_t leaf_count;     /* leaves currently allocated */
+  uint64_t leaf_capacity;  /* current hash-table capacity */
+  uint32_t error_flags;    /* sticky device error bits, cleared by nm_map_stats */
+  uint32_t grow_count;     /* table growths so far */
+} nm_stats;
+
+/* One frame of a batched tick. */
+typedef struct {
+  nm_sensor sensor;
+  nm_pose pose;
+  const float* ranges;     /* device range image, hres*vres floats (metres; <=0/NaN = none) */
+  int32_t agent;           /* label plane, 0 .. max_agents-1; planes integrate in order */
+  int32_t pad;
+} nm_frame;
+
+/* ---- library -------------------------------------------------------------------------- */
+int nm_abi_version(void);
+const char* nm_last_error(void);
+
+/* ---- context (replaces Handler's stream pair, Handler.cpp:17-25, and closeHandler) ------ */
+int nm_context_create(int32_t device, nm_context* out);
+int nm_context_destroy(nm_context ctx);
+int nm_context_sync(nm_context ctx);
+
+/* ---- sensors (replaces FrustumData / LaserData and gpu::Sensor, Sensor.h:147-211) ----- */
+int nm_sensor_create(nm_context ctx, const nm_sensor_desc* desc, nm_sensor* out);
+int nm_sensor_destroy(nm_sensor s);
+/* Frustum constants the kernels use: hw, hh, 2hw, 2hh, 1/W, 1/H. */
+int nm_sensor_params(nm_sensor s, float out[6]);
+
+/* ---- maps (replaces nanomap::map::Map, OccupancyMap.h:35-61) --------------------------- */
+int nm_map_create(nm_context ctx, const nm_map_desc* desc, nm_map* out);
+int nm_map_destroy(nm_map m);
+int nm_map_reset(nm_map m);
+int nm_map_stats(nm_map m, nm_stats* out);
+
+/* Insert one xyz point cloud: `width*height` records of `step` bytes, float x, y, z at byte
+ * offsets 0, 4, 8, in the sensor frame.  Replaces Manager::insertPointCloud (Manager.h:52-63)
+ * -> Handler::processPointCloud (Handler.cpp:237-284) -> filterCloud (filterCloud.cu:476)
+ * + frustumCastCloud (frustumCastCloud.cu:311) + the host map update (Handler.cpp:134-182). */
+int nm_map_insert_points(nm_map m, nm_sensor s, const nm_pose* pose, const void* cloud,
+                         int32_t width, int32_t height, int32_t step, uint32_t flags,
+                         void* stream);
+
+/* Insert one range image (hres*vres floats, radial metres, <=0 or NaN = no return); the
+ * sensor's pixel model turns each range into a sensor-frame point on the device. */
+int nm_map_insert_ranges(nm_map m, nm_sensor s, const nm_pose* pose, const float* ranges,
+                         uint32_t flags, void* stream);
+
+/* Apply labels left by NM_DEFER_INTEGRATE inserts. */
+int nm_map_integrate(nm_map m, void* stream);
+
+/* Batched tick: every frame of `frames` is labelled in one persistent launch, then all label
+ * planes are integrated in agent order.  Replaces SimManager::updateAgentViews
+ * (SimManager.h:100-127), which runs agents one after another. */
+int nm_map_tick(nm_map m, const nm_frame* frames, int32_t n_frames, uint32_t flags,
+                void* stream);
+
+/* Leaves of the map (any order): origins (3 ints per leaf, voxel units), 512 log-odds per
+ * leaf (x-major, z fastest: index x*64 + y*8 + z), 16 active-mask words per leaf.  Any output
+ * pointer may be NULL.  *n receives the leaf count; at most max_leaves are written. */
+int nm_map_export(nm_map m, int32_t* origins, float* values, uint32_t* active,
+                  uint64_t max_leaves, uint64_t* n);
+
+/* Labels left by the last NM_DEFER_INTEGRATE insert or tick for one agent plane: leaf
+ * origins and 32 words per leaf (words 0..15 hit bits, 16..31 miss bits, bit l%32 of word
+ * l/32 for voxel index l).  Only leaves with a label are written. */
+int nm_map_export_labels(nm_map m, int32_t agent, int32_t* origins, uint32_t* words,
+                         uint64_t max_leaves, uint64_t* n);
+
+/* The per-frame constants the host path derives from a pose: rotation (row-major,
+ * world-from-sensor), index-space eye, max_time = max_range / res. */
+int nm_map_frame_params(nm_map m, nm_sensor s, const nm_pose* pose, float rotation[9],
+                        double eye[3], float* max_time);
+
+/* Host-only form of the above for a sensor description (no context, no device): also returns
+ * the frustum pixel model (hw, hh, 2hw, 2hh, 1/W, 1/H).  Replaces the host derivations of
+ * SensorData::updatePose / gpu::Sensor::updateShared (SensorData.h:40-83, Sensor.h:172-211). */
+int nm_frame_params(const nm_sensor_desc* desc, const nm_pose* pose, float res, int32_t rounding,
+                    float rotation[9], double eye[3], float* max_time, float pixel_model[6]);
+
+/* ---- simulation map (replaces the NanoVDB sim grid, SimHandler.cpp:13-24) -------------- */
+/* Voxelise primitives into a sparse device map: boxes are 6 doubles (min xyz, max xyz, m);
+ * cylinders are 5 doubles (cx, cy, radius, z0, z1, m).  A voxel is active when its centre is
+ * inside a primitive.  Only voxels in [vox_min, vox_max) are considered. */
+int nm_simmap_create_primitives(nm_context ctx, float res, const int32_t vox_min[3],
+                                const int32_t vox_max[3], const double* boxes, int32_t n_boxes,
+                                const double* cylinders, int32_t n_cylinders, nm_simmap* out);
+/* From a list of active voxel coordinates (3 ints each, host memory). */
+int nm_simmap_create_voxels(nm_context ctx, float res, const int32_t* ijk, int64_t n,
+                            nm_simmap* out);
+int nm_simmap_destroy(nm_simmap sm);
+/* active bounding box (min xyz, max xyz, inclusive), active voxel count, leaf count */
+int nm_simmap_info(nm_simmap sm, int32_t bbox[6], uint64_t* active_voxels, uint64_t* leaves);
+/* leaf origins and 16 mask words per leaf (any order) */
+int nm_simmap_export(nm_simmap sm, int32_t* origins, uint32_t* words, uint64_t max_leaves,
+                     uint64_t* n);
+/* Simulated range image of one sensor at one pose (replaces generateCloud,
+ * generateCloud.cu:84-94).  Output: hres*vres floats, radial metres, 0 = no return. */
+int nm_sim_render(nm_simmap sm, nm_sensor s, const nm_pose* pose, float* ranges,
+                  uint32_t flags, void* stream);
+/* Sensor noise on a device range image: r += N(0, (sigma_coef * r^2)^2), then each pixel
+ * is set to 0 with probability drop_prob.  Counter-based generator keyed by `seed`. */
+int nm_ranges_add_noise(nm_context ctx, float* ranges, int64_t n, float sigma_coef,
+                        float drop_prob, uint64_t seed, void* stream);
+
+#ifdef __cplusplus
+}
+#endif
+
+#endif /* NANOMAP_B200_H_ */

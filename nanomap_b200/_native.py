@@ -1,0 +1,163 @@
+"""ctypes bindings of include/nanomap_b200.h (the test and benchmark harness's view of the C ABI).
+
+The library is loaded from the package directory.  There is no fallback: when the shared
+library is missing or a call fails, a ``NanomapError`` is raised.
+"""
+from __future__ import annotations
+
+import ctypes as C
+import re
+from pathlib import Path
+
+PKG = Path(__file__).resolve().parent
+LIB_PATH = PKG / "libnanomap_b200.so"
+HEADER = PKG.parent / "include" / "nanomap_b200.h"
+
+NM_OK = 0
+NM_ERR_ARG = 1
+NM_ERR_CAPACITY = 2
+NM_ERR_CUDA = 3
+NM_ERR_TIMEOUT = 4
+NM_ERR_STATE = 5
+NM_ERR_IO = 6
+NM_ERR_UNSUPPORTED = 7
+
+NM_SENSOR_FRUSTUM = 0
+NM_SENSOR_LASER = 1
+NM_UPDATE_LABEL = 0
+NM_UPDATE_ACCUMULATE = 1
+NM_CLAMP_ALWAYS = 0
+NM_CLAMP_ON_CROSSING = 1
+NM_ROUND_NEAREST = 0
+NM_ROUND_DOWN = 1
+
+NM_INPUT_HOST = 0x1
+NM_DEFER_INTEGRATE = 0x2
+NM_SYNC = 0x4
+NM_OUTPUT_HOST = 0x8
+
+
+class NanomapError(RuntimeError):
+    def __init__(self, code: int, message: str):
+        super().__init__(f"nanomap_b200 error {code}: {message}")
+        self.code = code
+
+
+class NmPose(C.Structure):
+    _fields_ = [("position", C.c_float * 3), ("orientation", C.c_float * 4)]
+
+
+class NmSensorDesc(C.Structure):
+    _fields_ = [
+        ("type", C.c_int32), ("id", C.c_int32), ("hres", C.c_int32), ("vres", C.c_int32),
+        ("hfov_deg", C.c_float), ("vfov_deg", C.c_float),
+        ("min_range", C.c_float), ("max_range", C.c_float),
+        ("prob_hit", C.c_float), ("prob_miss", C.c_float),
+        ("log_odds_hit", C.c_float), ("log_odds_miss", C.c_float),
+        ("explicit_log_odds", C.c_int32), ("rate", C.c_int32),
+        ("frame_transform", C.c_float * 9),
+    ]
+
+
+class NmMapDesc(C.Structure):
+    _fields_ = [
+        ("res", C.c_float), ("leaf_edge", C.c_int32),
+        ("thres_hit", C.c_float), ("thres_miss", C.c_float),
+        ("clamp_min", C.c_float), ("clamp_max", C.c_float),
+        ("clamp_mode", C.c_int32), ("update_mode", C.c_int32), ("rounding", C.c_int32),
+        ("initial_leaf_capacity", C.c_uint32), ("max_agents", C.c_int32),
+    ]
+
+
+class NmStats(C.Structure):
+    _fields_ = [
+        ("frames", C.c_uint64), ("rays", C.c_uint64), ("visits", C.c_uint64),
+        ("unique_voxels", C.c_uint64), ("touched_leaves", C.c_uint64),
+        ("leaf_count", C.c_uint64), ("leaf_capacity", C.c_uint64),
+        ("error_flags", C.c_uint32), ("grow_count", C.c_uint32),
+    ]
+
+
+class NmFrame(C.Structure):
+    _fields_ = [
+        ("sensor", C.c_void_p), ("pose", NmPose), ("ranges", C.c_void_p),
+        ("agent", C.c_int32), ("pad", C.c_int32),
+    ]
+
+
+_P = C.c_void_p
+_I32 = C.c_int32
+_U32 = C.c_uint32
+_I64 = C.c_int64
+_U64 = C.c_uint64
+_F = C.c_float
+_PF = C.POINTER(C.c_float)
+_PD = C.POINTER(C.c_double)
+_PI32 = C.POINTER(C.c_int32)
+_PU32 = C.POINTER(C.c_uint32)
+_PU64 = C.POINTER(C.c_uint64)
+
+# name -> (restype, argtypes); every int-returning entry returns a status code.
+_SIGS = {
+    "nm_abi_version": (C.c_int, []),
+    "nm_last_error": (C.c_char_p, []),
+    "nm_context_create": (C.c_int, [_I32, C.POINTER(_P)]),
+    "nm_context_destroy": (C.c_int, [_P]),
+    "nm_context_sync": (C.c_int, [_P]),
+    "nm_sensor_create": (C.c_int, [_P, C.POINTER(NmSensorDesc), C.POINTER(_P)]),
+    "nm_sensor_destroy": (C.c_int, [_P]),
+    "nm_sensor_params": (C.c_int, [_P, _PF]),
+    "nm_map_create": (C.c_int, [_P, C.POINTER(NmMapDesc), C.POINTER(_P)]),
+    "nm_map_destroy": (C.c_int, [_P]),
+    "nm_map_reset": (C.c_int, [_P]),
+    "nm_map_stats": (C.c_int, [_P, C.POINTER(NmStats)]),
+    "nm_map_insert_points": (C.c_int, [_P, _P, C.POINTER(NmPose), _P, _I32, _I32, _I32, _U32, _P]),
+    "nm_map_insert_ranges": (C.c_int, [_P, _P, C.POINTER(NmPose), _P, _U32, _P]),
+    "nm_map_integrate": (C.c_int, [_P, _P]),
+    "nm_map_tick": (C.c_int, [_P, C.POINTER(NmFrame), _I32, _U32, _P]),
+    "nm_map_export": (C.c_int, [_P, _PI32, _PF, _PU32, _U64, _PU64]),
+    "nm_map_export_labels": (C.c_int, [_P, _I32, _PI32, _PU32, _U64, _PU64]),
+    "nm_map_frame_params": (C.c_int, [_P, _P, C.POINTER(NmPose), _PF, _PD, _PF]),
+    "nm_frame_params": (C.c_int, [C.POINTER(NmSensorDesc), C.POINTER(NmPose), _F, _I32, _PF, _PD, _PF, _PF]),
+    "nm_simmap_create_primitives": (C.c_int, [_P, _F, _PI32, _PI32, _PD, _I32, _PD, _I32, C.POINTER(_P)]),
+    "nm_simmap_create_voxels": (C.c_int, [_P, _F, _PI32, _I64, C.POINTER(_P)]),
+    "nm_simmap_destroy": (C.c_int, [_P]),
+    "nm_simmap_info": (C.c_int, [_P, _PI32, _PU64, _PU64]),
+    "nm_simmap_export": (C.c_int, [_P, _PI32, _PU32, _U64, _PU64]),
+    "nm_sim_render": (C.c_int, [_P, _P, C.POINTER(NmPose), _P, _U32, _P]),
+    "nm_ranges_add_noise": (C.c_int, [_P, _P, _I64, _F, _F, _U64, _P]),
+}
+
+_lib = None
+
+
+def declared_symbols() -> list[str]:
+    """Function names declared in include/nanomap_b200.h."""
+    text = HEADER.read_text()
+    return sorted(set(re.findall(r"^\s*(?:int|const char\*)\s+(nm_\w+)\s*\(", text, re.M)))
+
+
+def lib() -> C.CDLL:
+    """Load libnanomap_b200.so (raises when it has not been built)."""
+    global _lib
+    if _lib is None:
+        if not LIB_PATH.exists():
+            raise NanomapError(NM_ERR_STATE, f"{LIB_PATH} is missing; run python -m nanomap_b200.build")
+        L = C.CDLL(str(LIB_PATH))
+        for name, (res, args) in _SIGS.items():
+            fn = getattr(L, name, None)
+            if fn is None:
+                continue
+            fn.restype = res
+            fn.argtypes = args
+        _lib = L
+    return _lib
+
+
+def check(rc: int) -> None:
+    if rc != NM_OK:
+        raise NanomapError(rc, lib().nm_last_error().decode(errors="replace"))
+
+
+def call(name: str, *args) -> None:
+    check(getattr(lib(), name)(*args))

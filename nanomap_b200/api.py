@@ -1,0 +1,309 @@
+"""Python view of the C ABI, shaped like NanoMap's own objects (Pose, sensors, Map, sim map).
+
+Used by the tests and the benchmark.  Arrays may be numpy arrays (host memory) or torch CUDA
+tensors (device memory); the matching NM_INPUT_HOST / NM_OUTPUT_HOST flag is set from the
+array type.  Every call goes through libnanomap_b200.so; nothing here computes a result.
+"""
+from __future__ import annotations
+
+import ctypes as C
+from dataclasses import dataclass
+
+import numpy as np
+
+from . import _native as N
+from ._native import NanomapError, call, lib
+
+
+def _is_torch(x) -> bool:
+    return type(x).__module__.startswith("torch")
+
+
+def _ptr(x):
+    """(pointer, is_host) of a numpy array or torch tensor."""
+    if x is None:
+        return None, True
+    if _is_torch(x):
+        if not x.is_contiguous():
+            raise ValueError("tensor must be contiguous")
+        return C.c_void_p(x.data_ptr()), not x.is_cuda
+    a = np.ascontiguousarray(x)
+    if a is not x:
+        raise ValueError("array must be C-contiguous")
+    return C.c_void_p(a.ctypes.data), True
+
+
+def _stream(stream):
+    if stream is None:
+        return None
+    if isinstance(stream, int):
+        return C.c_void_p(stream)
+    return C.c_void_p(stream.cuda_stream)
+
+
+def make_pose(position, orientation) -> N.NmPose:
+    p = N.NmPose()
+    for i in range(3):
+        p.position[i] = float(position[i])
+    for i in range(4):
+        p.orientation[i] = float(orientation[i])
+    return p
+
+
+@dataclass
+class Pose:
+    """nanomap::Pose: position (m) and quaternion (w, x, y, z); default (0,0,0,1) as in
+    nanomap.h:24-25 (Eigen's (w, x, y, z) constructor order)."""
+    position: tuple = (0.0, 0.0, 0.0)
+    orientation: tuple = (0.0, 0.0, 0.0, 1.0)
+
+    def c(self) -> N.NmPose:
+        return make_pose(self.position, self.orientation)
+
+
+def sensor_desc(type=0, hres=640, vres=480, hfov_deg=0.0, vfov_deg=58.0, min_range=0.0,
+                max_range=10.0, prob_hit=0.7, prob_miss=0.4, log_odds_hit=0.0,
+                log_odds_miss=0.0, explicit_log_odds=0, rate=30, frame_transform=None,
+                id=0) -> N.NmSensorDesc:
+    d = N.NmSensorDesc()
+    d.type, d.id, d.hres, d.vres = type, id, hres, vres
+    d.hfov_deg, d.vfov_deg = hfov_deg, vfov_deg
+    d.min_range, d.max_range = min_range, max_range
+    d.prob_hit, d.prob_miss = prob_hit, prob_miss
+    d.log_odds_hit, d.log_odds_miss = log_odds_hit, log_odds_miss
+    d.explicit_log_odds, d.rate = explicit_log_odds, rate
+    ft = frame_transform if frame_transform is not None else (1, 0, 0, 0, 1, 0, 0, 0, 1)
+    for i in range(9):
+        d.frame_transform[i] = float(ft[i])
+    return d
+
+
+def map_desc(res=0.1, thres_hit=0.0, thres_miss=0.0, clamp_min=-2.0, clamp_max=3.5,
+             clamp_mode=N.NM_CLAMP_ALWAYS, update_mode=N.NM_UPDATE_LABEL,
+             rounding=N.NM_ROUND_DOWN, initial_leaf_capacity=0, max_agents=1) -> N.NmMapDesc:
+    d = N.NmMapDesc()
+    d.res, d.leaf_edge = res, 8
+    d.thres_hit, d.thres_miss = thres_hit, thres_miss
+    d.clamp_min, d.clamp_max = clamp_min, clamp_max
+    d.clamp_mode, d.update_mode, d.rounding = clamp_mode, update_mode, rounding
+    d.initial_leaf_capacity, d.max_agents = initial_leaf_capacity, max_agents
+    return d
+
+
+def frame_params(desc: N.NmSensorDesc, pose: Pose, res: float, rounding: int):
+    """Host-only per-frame constants: (R[9], eye[3], max_time, pixel_model[6])."""
+    R = (C.c_float * 9)()
+    eye = (C.c_double * 3)()
+    mt = C.c_float()
+    pm = (C.c_float * 6)()
+    call("nm_frame_params", C.byref(desc), C.byref(pose.c()), C.c_float(res), rounding, R, eye,
+         C.byref(mt), pm)
+    return (np.array(R[:], dtype=np.float32), np.array(eye[:], dtype=np.float64),
+            np.float32(mt.value), np.array(pm[:], dtype=np.float32))
+
+
+class Context:
+    def __init__(self, device: int = 0):
+        h = C.c_void_p()
+        call("nm_context_create", device, C.byref(h))
+        self.h = h
+        self.device = device
+
+    def sync(self):
+        call("nm_context_sync", self.h)
+
+    def close(self):
+        if self.h:
+            call("nm_context_destroy", self.h)
+            self.h = None
+
+    def add_noise(self, ranges, sigma_coef, drop_prob, seed, stream=None):
+        p, host = _ptr(ranges)
+        if host:
+            raise ValueError("noise runs on device ranges")
+        call("nm_ranges_add_noise", self.h, p, ranges.numel(), C.c_float(sigma_coef),
+             C.c_float(drop_prob), C.c_uint64(seed), _stream(stream))
+
+    def __del__(self):
+        try:
+            self.close()
+        except Exception:
+            pass
+
+
+class Sensor:
+    def __init__(self, ctx: Context, desc: N.NmSensorDesc):
+        self.ctx = ctx
+        self.desc = desc
+        h = C.c_void_p()
+        call("nm_sensor_create", ctx.h, C.byref(desc), C.byref(h))
+        self.h = h
+
+    @property
+    def shape(self):
+        return (self.desc.vres, self.desc.hres)
+
+    def params(self):
+        out = (C.c_float * 6)()
+        call("nm_sensor_params", self.h, out)
+        return np.array(out[:], dtype=np.float32)
+
+    def close(self):
+        if self.h:
+            call("nm_sensor_destroy", self.h)
+            self.h = None
+
+    def __del__(self):
+        try:
+            self.close()
+        except Exception:
+            pass
+
+
+class Map:
+    """Device-resident occupancy map (replaces nanomap::map::Map + the handler's update)."""
+
+    def __init__(self, ctx: Context, desc: N.NmMapDesc):
+        self.ctx = ctx
+        self.desc = desc
+        h = C.c_void_p()
+        call("nm_map_create", ctx.h, C.byref(desc), C.byref(h))
+        self.h = h
+
+    def insert_points(self, sensor: Sensor, pose: Pose, cloud, width: int, height: int,
+                      step: int, flags: int = 0, stream=None):
+        p, host = _ptr(cloud)
+        if host:
+            flags |= N.NM_INPUT_HOST
+        call("nm_map_insert_points", self.h, sensor.h, C.byref(pose.c()), p, width, height,
+             step, flags, _stream(stream))
+
+    def insert_ranges(self, sensor: Sensor, pose: Pose, ranges, flags: int = 0, stream=None):
+        p, host = _ptr(ranges)
+        if host:
+            flags |= N.NM_INPUT_HOST
+        call("nm_map_insert_ranges", self.h, sensor.h, C.byref(pose.c()), p, flags,
+             _stream(stream))
+
+    def integrate(self, stream=None):
+        call("nm_map_integrate", self.h, _stream(stream))
+
+    def tick(self, frames, flags: int = 0, stream=None):
+        """frames: list of (sensor, pose, device ranges tensor, agent)."""
+        arr = (N.NmFrame * len(frames))()
+        for i, (s, pose, r, agent) in enumerate(frames):
+            arr[i].sensor = s.h
+            arr[i].pose = pose.c()
+            arr[i].ranges = C.c_void_p(r.data_ptr())
+            arr[i].agent = agent
+        call("nm_map_tick", self.h, arr, len(frames), flags, _stream(stream))
+
+    def stats(self) -> dict:
+        s = N.NmStats()
+        call("nm_map_stats", self.h, C.byref(s))
+        return {k: getattr(s, k) for k, _ in N.NmStats._fields_}
+
+    def export(self):
+        """(origins (n,3) int32, values (n,512) float32, active (n,16) uint32), any order."""
+        n = C.c_uint64()
+        call("nm_map_export", self.h, None, None, None, 0, C.byref(n))
+        k = n.value
+        o = np.zeros((k, 3), np.int32)
+        v = np.zeros((k, 512), np.float32)
+        a = np.zeros((k, 16), np.uint32)
+        if k:
+            call("nm_map_export", self.h, o.ctypes.data_as(N._PI32), v.ctypes.data_as(N._PF),
+                 a.ctypes.data_as(N._PU32), k, C.byref(n))
+        return o, v, a
+
+    def export_labels(self, agent: int = 0):
+        """(origins (n,3), words (n,32)) of leaves holding labels of one plane."""
+        st = self.stats()
+        cap = max(1, int(st["leaf_count"]))
+        o = np.zeros((cap, 3), np.int32)
+        w = np.zeros((cap, 32), np.uint32)
+        n = C.c_uint64()
+        call("nm_map_export_labels", self.h, agent, o.ctypes.data_as(N._PI32),
+             w.ctypes.data_as(N._PU32), cap, C.byref(n))
+        k = int(n.value)
+        return o[:k].copy(), w[:k].copy()
+
+    def frame_params(self, sensor: Sensor, pose: Pose):
+        R = (C.c_float * 9)()
+        eye = (C.c_double * 3)()
+        mt = C.c_float()
+        call("nm_map_frame_params", self.h, sensor.h, C.byref(pose.c()), R, eye, C.byref(mt))
+        return np.array(R[:], np.float32), np.array(eye[:], np.float64), np.float32(mt.value)
+
+    def reset(self):
+        call("nm_map_reset", self.h)
+
+    def close(self):
+        if self.h:
+            call("nm_map_destroy", self.h)
+            self.h = None
+
+    def __del__(self):
+        try:
+            self.close()
+        except Exception:
+            pass
+
+
+class SimMap:
+    """Device sim map (replaces the NanoVDB sim grid of SimHandler)."""
+
+    def __init__(self, ctx: Context, res: float, *, boxes=None, cylinders=None, vox_min=None,
+                 vox_max=None, voxels=None):
+        self.ctx = ctx
+        self.res = res
+        h = C.c_void_p()
+        if voxels is not None:
+            v = np.ascontiguousarray(voxels, dtype=np.int32)
+            call("nm_simmap_create_voxels", ctx.h, C.c_float(res), v.ctypes.data_as(N._PI32),
+                 len(v), C.byref(h))
+        else:
+            b = np.ascontiguousarray(boxes if boxes is not None else np.zeros((0, 6)), np.float64)
+            c = np.ascontiguousarray(cylinders if cylinders is not None else np.zeros((0, 5)), np.float64)
+            lo = (C.c_int32 * 3)(*vox_min)
+            hi = (C.c_int32 * 3)(*vox_max)
+            call("nm_simmap_create_primitives", ctx.h, C.c_float(res), lo, hi,
+                 b.ctypes.data_as(N._PD), len(b), c.ctypes.data_as(N._PD), len(c), C.byref(h))
+        self.h = h
+
+    def info(self):
+        bb = (C.c_int32 * 6)()
+        nv = C.c_uint64()
+        nl = C.c_uint64()
+        call("nm_simmap_info", self.h, bb, C.byref(nv), C.byref(nl))
+        return tuple(bb[:]), nv.value, nl.value
+
+    def export(self):
+        _, _, nl = self.info()
+        o = np.zeros((max(nl, 1), 3), np.int32)
+        w = np.zeros((max(nl, 1), 16), np.uint32)
+        n = C.c_uint64()
+        call("nm_simmap_export", self.h, o.ctypes.data_as(N._PI32), w.ctypes.data_as(N._PU32),
+             nl, C.byref(n))
+        return o[:nl], w[:nl]
+
+    def render(self, sensor: Sensor, pose: Pose, out, flags: int = 0, stream=None):
+        p, host = _ptr(out)
+        if host:
+            flags |= N.NM_OUTPUT_HOST
+        call("nm_sim_render", self.h, sensor.h, C.byref(pose.c()), p, flags, _stream(stream))
+
+    def close(self):
+        if self.h:
+            call("nm_simmap_destroy", self.h)
+            self.h = None
+
+    def __del__(self):
+        try:
+            self.close()
+        except Exception:
+            pass
+
+
+__all__ = ["Pose", "Context", "Sensor", "Map", "SimMap", "sensor_desc", "map_desc",
+           "frame_params", "NanomapError", "lib"]

@@ -1,0 +1,741 @@
+// nm_abi.cpp -- host implementation of the C ABI declared in include/nanomap_b200.h.
+//
+// Owns device memory, derives the per-frame constants on the host (as Handler.cpp:32-41 and
+// SensorAllocator.h:110-148 do), keeps the leaf table large enough, and launches the sm_100a
+// kernels.  There is no CPU fallback: every compute entry point fails with NM_ERR_CUDA when no
+// CUDA device is usable.  Built with -frounding-math so the rounding-mode sections below are
+// evaluated at run time under the mode they select.
+#include <algorithm>
+#include <cfenv>
+#include <cmath>
+#include <cstdarg>
+#include <cstdio>
+#include <cstring>
+#include <memory>
+#include <new>
+#include <string>
+#include <vector>
+
+#include "nm_internal.h"
+#include "nm_sim.h"
+#include "nm_host.h"
+#include "nm_objects.h"
+
+namespace nm {
+
+namespace {
+thread_local std::string g_error;
+}  // namespace
+
+int fail(int code, const char* fmt, ...) {
+  char buf[512];
+  va_list ap;
+  va_start(ap, fmt);
+  vsnprintf(buf, sizeof(buf), fmt, ap);
+  va_end(ap);
+  g_error = buf;
+  return code;
+}
+
+const char* last_error() { return g_error.c_str(); }
+
+}  // namespace nm
+
+using nm::fail;
+using nm::RoundScope;
+
+namespace {
+
+uint32_t next_pow2(uint64_t v) {
+  uint64_t p = 1;
+  while (p < v) p <<= 1;
+  return (uint32_t)std::min<uint64_t>(p, 1ull << 31);
+}
+
+}  // namespace
+
+// ---- shared host math (declared in nm_host.h) ---------------------------------------------
+namespace nm {
+
+void pose_rotation(const nm_pose& pose, const float F[9], float R[9]) {
+  RoundScope rs(NM_ROUND_NEAREST);
+  double w = pose.orientation[0], x = pose.orientation[1], y = pose.orientation[2],
+         z = pose.orientation[3];
+  const double n = std::sqrt(w * w + x * x + y * y + z * z);
+  w /= n;
+  x /= n;
+  y /= n;
+  z /= n;
+  const double M[9] = {1.0 - 2.0 * (y * y + z * z), 2.0 * (x * y - w * z), 2.0 * (x * z + w * y),
+                       2.0 * (x * y + w * z), 1.0 - 2.0 * (x * x + z * z), 2.0 * (y * z - w * x),
+                       2.0 * (x * z - w * y), 2.0 * (y * z + w * x), 1.0 - 2.0 * (x * x + y * y)};
+  for (int r = 0; r < 3; ++r)
+    for (int c = 0; c < 3; ++c) {
+      const double s = M[r * 3 + 0] * (double)F[c * 3 + 0] + M[r * 3 + 1] * (double)F[c * 3 + 1] +
+                       M[r * 3 + 2] * (double)F[c * 3 + 2];
+      R[r * 3 + c] = (float)s;
+    }
+}
+
+void frame_constants(const nm_pose& pose, float res, float max_range, int rounding, double eye[3],
+                     float* max_time) {
+  double inv_res;
+  {
+    RoundScope rs(NM_ROUND_NEAREST);
+    volatile double r = (double)res;
+    inv_res = 1.0 / r;
+  }
+  RoundScope rs(rounding);
+  for (int a = 0; a < 3; ++a) {
+    volatile double p = (double)pose.position[a];
+    eye[a] = p * inv_res;
+  }
+  volatile float mr = max_range, rf = res;
+  *max_time = mr / rf;
+}
+
+void frustum_params(int W, int H, float hfov_deg, float vfov_deg, float out[6]) {
+  RoundScope rs(NM_ROUND_NEAREST);
+  const double kPi = 3.14159265358979323846;
+  const float hh = (float)std::tan((double)vfov_deg * kPi / 360.0);
+  float hw;
+  if (hfov_deg > 0.0f) {
+    hw = (float)std::tan((double)hfov_deg * kPi / 360.0);
+  } else {
+    volatile float fw = (float)W, fh = (float)H;
+    const float aspect = fw / fh;
+    hw = aspect * hh;
+  }
+  out[0] = hw;
+  out[1] = hh;
+  out[2] = 2.0f * hw;
+  out[3] = 2.0f * hh;
+  out[4] = (float)(1.0 / (double)W);
+  out[5] = (float)(1.0 / (double)H);
+}
+
+void laser_tables(int W, int H, float hfov_deg, float vfov_deg, float* sinu, float* cosu,
+                  float* sinv, float* cosv) {
+  RoundScope rs(NM_ROUND_NEAREST);
+  const double kPi = 3.14159265358979323846;
+  volatile float fw = (float)W, fh = (float)H;
+  const float su = hfov_deg / fw, sv = vfov_deg / fh;
+  for (int w = 0; w < W; ++w) {
+    const float u = -hfov_deg / 2.0f + (float)w * su;
+    const double ur = (double)u * kPi / 180.0;
+    sinu[w] = (float)std::sin(ur);
+    cosu[w] = (float)std::cos(ur);
+  }
+  for (int h = 0; h < H; ++h) {
+    const float v = -vfov_deg / 2.0f + (float)h * sv;
+    const double vr = (double)v * kPi / 180.0;
+    sinv[h] = (float)std::sin(vr);
+    cosv[h] = (float)std::cos(vr);
+  }
+}
+
+float logit(float p) {
+  RoundScope rs(NM_ROUND_NEAREST);
+  return (float)(std::log((double)p) - std::log(1.0 - (double)p));
+}
+
+}  // namespace nm
+
+namespace {
+
+cudaStream_t pick(nm_context ctx, void* stream) {
+  return stream ? static_cast<cudaStream_t>(stream) : ctx->stream;
+}
+
+void free_view(nm::MapView& v) {
+  cudaFree(v.keys);
+  cudaFree(v.values);
+  cudaFree(v.active);
+  cudaFree(v.labels);
+  cudaFree(v.counts);
+  cudaFree(v.epoch);
+  cudaFree(v.plane_mask);
+  cudaFree(v.touched);
+  v = nm::MapView{};
+}
+
+int alloc_view(nm_map m, uint32_t capacity, nm::MapView* out, cudaStream_t s) {
+  nm::MapView v{};
+  v.capacity = capacity;
+  v.mask = capacity - 1;
+  v.planes = m->desc.max_agents;
+  v.ctr = m->d_ctr;
+  const size_t C = capacity;
+  cudaError_t e = cudaSuccess;
+  auto A = [&](void** p, size_t bytes) {
+    if (e == cudaSuccess) e = cudaMalloc(p, bytes);
+    if (e == cudaSuccess) e = cudaMemsetAsync(*p, 0, bytes, s);
+  };
+  A((void**)&v.keys, C * 8);
+  A((void**)&v.values, C * nm::kLeafVoxels * 4);
+  A((void**)&v.active, C * nm::kActiveWords * 4);
+  A((void**)&v.labels, (size_t)v.planes * C * nm::kLabelWords * 4);
+  if (m->desc.update_mode == NM_UPDATE_ACCUMULATE) A((void**)&v.counts, C * 1024 * 4);
+  A((void**)&v.epoch, C * 4);
+  if (v.planes > 1) A((void**)&v.plane_mask, C * 4);
+  A((void**)&v.touched, C * 4);
+  if (e == cudaSuccess) e = nm::launch_fill_keys(v.keys, capacity, s);
+  if (e != cudaSuccess) {
+    free_view(v);
+    cudaGetLastError();
+    return fail(e == cudaErrorMemoryAllocation ? NM_ERR_CAPACITY : NM_ERR_CUDA,
+                "leaf table of %u slots: %s", capacity, cudaGetErrorString(e));
+  }
+  *out = v;
+  return NM_OK;
+}
+
+int grow_map(nm_map m, uint32_t new_capacity, cudaStream_t s) {
+  nm::MapView nv{};
+  int rc = alloc_view(m, new_capacity, &nv, s);
+  if (rc != NM_OK) return rc;
+  NM_CUDA(cudaMemsetAsync(&m->d_ctr->leaf_count, 0, 4, s));
+  NM_CUDA(cudaMemsetAsync(&m->d_ctr->touched_count, 0, 4, s));
+  NM_CUDA(nm::launch_rehash(m->view, nv, m->epoch, m->desc.update_mode, s));
+  NM_CUDA(cudaStreamSynchronize(s));
+  free_view(m->view);
+  m->view = nv;
+  m->grow_count += 1;
+  unsigned int lc = 0;
+  NM_CUDA(cudaMemcpy(&lc, &m->d_ctr->leaf_count, 4, cudaMemcpyDeviceToHost));
+  m->known_leaves = lc;
+  return NM_OK;
+}
+
+// Upper bound on the leaves one frame can touch: the leaf box of the ball of radius
+// max_range around the eye, intersected (frustum range images) with the leaf box of the
+// frustum pyramid, and capped by rays x leaves-per-ray.
+uint64_t frame_leaf_bound(nm_map m, nm_sensor s, const nm_pose& pose, const float R[9],
+                          bool range_input, uint64_t n_rays) {
+  const double res = m->desc.res;
+  const double rv = s->desc.max_range / res + 2.0;
+  double lo[3], hi[3];
+  for (int a = 0; a < 3; ++a) {
+    const double e = pose.position[a] / res;
+    lo[a] = e - rv;
+    hi[a] = e + rv;
+  }
+  if (range_input && s->desc.type == NM_SENSOR_FRUSTUM) {
+    double flo[3], fhi[3];
+    for (int a = 0; a < 3; ++a) flo[a] = fhi[a] = pose.position[a] / res;
+    const double sx[2] = {-s->fp[0], s->fp[0]}, sy[2] = {-s->fp[1], s->fp[1]};
+    for (int i = 0; i < 2; ++i)
+      for (int j = 0; j < 2; ++j)
+        for (int a = 0; a < 3; ++a) {
+          const double c = pose.position[a] / res +
+                           (R[a * 3] * sx[i] + R[a * 3 + 1] * sy[j] + R[a * 3 + 2]) * (rv + 1.0);
+          flo[a] = std::min(flo[a], c);
+          fhi[a] = std::max(fhi[a], c);
+        }
+    for (int a = 0; a < 3; ++a) {
+      lo[a] = std::max(lo[a], flo[a] - 2.0);
+      hi[a] = std::min(hi[a], fhi[a] + 2.0);
+    }
+  }
+  double vol = 1.0;
+  for (int a = 0; a < 3; ++a) vol *= std::floor(hi[a] / 8.0) - std::floor(lo[a] / 8.0) + 1.0;
+  const double per_ray = 3.0 * std::ceil(rv / 8.0) + 3.0;
+  const double cap = (double)n_rays * per_ray;
+  return (uint64_t)std::min(vol, cap);
+}
+
+int ensure_capacity(nm_map m, uint64_t bound, cudaStream_t s) {
+  const uint64_t limit = m->view.capacity / 2;
+  if (m->known_leaves + m->pending_bound + bound <= limit) {
+    m->pending_bound += bound;
+    return NM_OK;
+  }
+  NM_CUDA(cudaStreamSynchronize(s));
+  unsigned int lc = 0;
+  NM_CUDA(cudaMemcpy(&lc, &m->d_ctr->leaf_count, 4, cudaMemcpyDeviceToHost));
+  m->known_leaves = lc;
+  m->pending_bound = 0;
+  uint64_t cap = m->view.capacity;
+  while (m->known_leaves + bound > cap / 2 && cap < (1ull << 30)) cap <<= 1;
+  if (cap != m->view.capacity) {
+    const int rc = grow_map(m, (uint32_t)cap, s);
+    if (rc != NM_OK) return rc;
+  }
+  m->pending_bound = bound;
+  return NM_OK;
+}
+
+int validate_pose(const nm_pose* pose) {
+  if (!pose) return fail(NM_ERR_ARG, "pose is null");
+  for (int a = 0; a < 3; ++a)
+    if (!std::isfinite(pose->position[a])) return fail(NM_ERR_ARG, "pose position is not finite");
+  double n = 0;
+  for (int a = 0; a < 4; ++a) {
+    if (!std::isfinite(pose->orientation[a])) return fail(NM_ERR_ARG, "orientation is not finite");
+    n += (double)pose->orientation[a] * pose->orientation[a];
+  }
+  if (!(n > 1e-20)) return fail(NM_ERR_ARG, "orientation quaternion is zero");
+  return NM_OK;
+}
+
+int make_frame(nm_map m, nm_sensor s, const nm_pose* pose, nm::FrameParams* f) {
+  int rc = validate_pose(pose);
+  if (rc != NM_OK) return rc;
+  if (!s) return fail(NM_ERR_ARG, "sensor is null");
+  if (s->ctx != m->ctx) return fail(NM_ERR_ARG, "sensor and map belong to different contexts");
+  std::memset(f, 0, sizeof(*f));
+  f->type = s->desc.type;
+  f->width = s->desc.hres;
+  f->height = s->desc.vres;
+  f->hw = s->fp[0];
+  f->hh = s->fp[1];
+  f->c0 = s->fp[2];
+  f->c1 = s->fp[3];
+  f->su = s->fp[4];
+  f->sv = s->fp[5];
+  if (s->desc.type == NM_SENSOR_LASER) {
+    f->sinu = s->d_tables;
+    f->cosu = s->d_tables + s->desc.hres;
+    f->sinv = s->d_tables + 2 * s->desc.hres;
+    f->cosv = s->d_tables + 2 * s->desc.hres + s->desc.vres;
+  }
+  nm::pose_rotation(*pose, s->desc.frame_transform, f->R);
+  nm::frame_constants(*pose, m->desc.res, s->desc.max_range, m->desc.rounding, f->eye, &f->max_time);
+  f->res_d = (double)m->desc.res;
+  // keys hold 21-bit leaf coordinates: keep every voxel the frame can reach inside them
+  const double reach = (double)f->max_time + 2.0;
+  for (int a = 0; a < 3; ++a)
+    if (std::fabs(f->eye[a]) + reach > (double)(1 << 23) - 16.0)
+      return fail(NM_ERR_ARG, "pose is outside the map's addressable range (+-%d voxels)", 1 << 23);
+  return NM_OK;
+}
+
+nm::IntegrateParams integrate_params(nm_map m) {
+  nm::IntegrateParams p{};
+  p.thres_hit = m->desc.thres_hit;
+  p.thres_miss = m->desc.thres_miss;
+  p.clamp_min = m->desc.clamp_min;
+  p.clamp_max = m->desc.clamp_max;
+  p.clamp_mode = m->desc.clamp_mode;
+  p.use_planes = m->view.planes > 1 ? 1 : 0;
+  for (int i = 0; i < nm::kMaxPlanes; ++i) {
+    p.lh[i] = m->pending_lh[i];
+    p.lm[i] = m->pending_lm[i];
+  }
+  return p;
+}
+
+int do_integrate(nm_map m, cudaStream_t s) {
+  if (!m->pending_labels) return NM_OK;
+  const nm::IntegrateParams p = integrate_params(m);
+  NM_CUDA(nm::launch_integrate(m->view, p, m->desc.update_mode, m->desc.rounding,
+                               m->ctx->sm_count, s));
+  m->pending_labels = false;
+  m->pending_planes = 0;
+  m->epoch += 1;
+  if (m->epoch == 0) m->epoch = 1;
+  return NM_OK;
+}
+
+int check_device_errors(nm_map m, cudaStream_t s) {
+  NM_CUDA(cudaStreamSynchronize(s));
+  unsigned int flags = 0, lc = 0;
+  NM_CUDA(cudaMemcpy(&flags, &m->d_ctr->error_flags, 4, cudaMemcpyDeviceToHost));
+  NM_CUDA(cudaMemcpy(&lc, &m->d_ctr->leaf_count, 4, cudaMemcpyDeviceToHost));
+  m->known_leaves = lc;
+  m->pending_bound = 0;
+  if (flags & nm::kErrProbe)
+    return fail(NM_ERR_CAPACITY, "leaf table probe limit reached (%u leaves in %u slots)", lc,
+                m->view.capacity);
+  if (flags & nm::kErrTimeout) return fail(NM_ERR_TIMEOUT, "a device-side wait gave up");
+  if (flags & nm::kErrPlane) return fail(NM_ERR_ARG, "label plane out of range");
+  return NM_OK;
+}
+
+int stage_input(nm_map m, const void* src, size_t bytes, cudaStream_t s, const void** dev) {
+  if (bytes > m->staging_bytes) {
+    cudaFree(m->staging);
+    m->staging = nullptr;
+    m->staging_bytes = 0;
+    NM_CUDA(cudaMalloc((void**)&m->staging, bytes));
+    m->staging_bytes = bytes;
+  }
+  NM_CUDA(cudaMemcpyAsync(m->staging, src, bytes, cudaMemcpyHostToDevice, s));
+  *dev = m->staging;
+  return NM_OK;
+}
+
+int set_plane_constants(nm_map m, int plane, nm_sensor s) {
+  const uint32_t bit = 1u << plane;
+  if (m->pending_planes & bit) {
+    if (m->pending_lh[plane] != s->lh || m->pending_lm[plane] != s->lm)
+      return fail(NM_ERR_ARG, "frames sharing label plane %d use different log-odds constants", plane);
+  } else {
+    m->pending_lh[plane] = s->lh;
+    m->pending_lm[plane] = s->lm;
+    m->pending_planes |= bit;
+  }
+  return NM_OK;
+}
+
+// One frame through traverse (+ integrate unless deferred).
+int run_frame(nm_map m, nm_sensor s, nm::FrameParams& f, uint32_t flags, cudaStream_t s0,
+              uint64_t bound) {
+  int rc = ensure_capacity(m, bound, s0);
+  if (rc != NM_OK) return rc;
+  rc = set_plane_constants(m, 0, s);
+  if (rc != NM_OK) return rc;
+  f.epoch = m->epoch;
+  f.plane = 0;
+  NM_CUDA(nm::launch_traverse(f, m->view, m->desc.update_mode, m->desc.rounding, m->tile_w,
+                              m->tile_h, m->smem_entries, s0));
+  m->pending_labels = true;
+  if (!(flags & NM_DEFER_INTEGRATE)) {
+    rc = do_integrate(m, s0);
+    if (rc != NM_OK) return rc;
+  }
+  if (flags & NM_SYNC) return check_device_errors(m, s0);
+  return NM_OK;
+}
+
+}  // namespace
+
+// ---- C ABI ----------------------------------------------------------------------------------
+extern "C" {
+
+int nm_abi_version(void) { return NM_ABI_VERSION; }
+
+const char* nm_last_error(void) { return nm::last_error(); }
+
+int nm_context_create(int32_t device, nm_context* out) {
+  if (!out) return fail(NM_ERR_ARG, "out is null");
+  *out = nullptr;
+  int n = 0;
+  NM_CUDA(cudaGetDeviceCount(&n));
+  if (device < 0 || device >= n) return fail(NM_ERR_ARG, "device %d not present (%d devices)", device, n);
+  NM_CUDA(cudaSetDevice(device));
+  cudaDeviceProp prop;
+  NM_CUDA(cudaGetDeviceProperties(&prop, device));
+  if (prop.major < 10)
+    return fail(NM_ERR_UNSUPPORTED, "device %d is sm_%d%d; this library is built for sm_100a",
+                device, prop.major, prop.minor);
+  std::unique_ptr<nm_context_s> c(new nm_context_s());
+  c->device = device;
+  c->sm_count = prop.multiProcessorCount;
+  c->stream = nullptr;  // the CUDA default stream, so NULL streams order with other libraries
+  *out = c.release();
+  return NM_OK;
+}
+
+int nm_context_destroy(nm_context ctx) {
+  if (!ctx) return NM_OK;
+  cudaSetDevice(ctx->device);
+  cudaStreamSynchronize(ctx->stream);
+  cudaFree(ctx->render_staging);
+  delete ctx;
+  return NM_OK;
+}
+
+int nm_context_sync(nm_context ctx) {
+  if (!ctx) return fail(NM_ERR_ARG, "context is null");
+  NM_CUDA(cudaStreamSynchronize(ctx->stream));
+  return NM_OK;
+}
+
+int nm_sensor_create(nm_context ctx, const nm_sensor_desc* d, nm_sensor* out) {
+  if (!ctx || !d || !out) return fail(NM_ERR_ARG, "null argument");
+  *out = nullptr;
+  if (d->type != NM_SENSOR_FRUSTUM && d->type != NM_SENSOR_LASER)
+    return fail(NM_ERR_ARG, "unknown sensor type %d", d->type);
+  if (d->hres <= 0 || d->vres <= 0 || d->hres > 65536 || d->vres > 65536)
+    return fail(NM_ERR_ARG, "sensor resolution %dx%d out of range", d->hres, d->vres);
+  if (!(d->max_range > 0.0f) || !(d->min_range >= 0.0f) || !(d->vfov_deg > 0.0f))
+    return fail(NM_ERR_ARG, "sensor ranges / field of view invalid");
+  if (d->type == NM_SENSOR_FRUSTUM && !(d->vfov_deg < 180.0f && d->hfov_deg < 180.0f))
+    return fail(NM_ERR_ARG, "frustum field of view must be below 180 degrees");
+  if (!d->explicit_log_odds && !(d->prob_hit > 0.f && d->prob_hit < 1.f && d->prob_miss > 0.f &&
+                                 d->prob_miss < 1.f))
+    return fail(NM_ERR_ARG, "ProbHit / ProbMiss must lie in (0, 1)");
+  std::unique_ptr<nm_sensor_s> s(new nm_sensor_s());
+  s->ctx = ctx;
+  s->desc = *d;
+  if (d->type == NM_SENSOR_FRUSTUM) {
+    nm::frustum_params(d->hres, d->vres, d->hfov_deg, d->vfov_deg, s->fp);
+  } else {
+    std::vector<float> t(2 * (size_t)d->hres + 2 * (size_t)d->vres);
+    nm::laser_tables(d->hres, d->vres, d->hfov_deg, d->vfov_deg, t.data(), t.data() + d->hres,
+                     t.data() + 2 * d->hres, t.data() + 2 * d->hres + d->vres);
+    NM_CUDA(cudaSetDevice(ctx->device));
+    NM_CUDA(cudaMalloc((void**)&s->d_tables, t.size() * 4));
+    NM_CUDA(cudaMemcpy(s->d_tables, t.data(), t.size() * 4, cudaMemcpyHostToDevice));
+  }
+  if (d->explicit_log_odds) {
+    s->lh = d->log_odds_hit;
+    s->lm = d->log_odds_miss;
+  } else {
+    s->lh = nm::logit(d->prob_hit);
+    s->lm = nm::logit(d->prob_miss);
+  }
+  *out = s.release();
+  return NM_OK;
+}
+
+int nm_sensor_destroy(nm_sensor s) {
+  if (!s) return NM_OK;
+  cudaFree(s->d_tables);
+  delete s;
+  return NM_OK;
+}
+
+int nm_sensor_params(nm_sensor s, float out[6]) {
+  if (!s || !out) return fail(NM_ERR_ARG, "null argument");
+  std::memcpy(out, s->fp, sizeof(s->fp));
+  return NM_OK;
+}
+
+int nm_map_create(nm_context ctx, const nm_map_desc* d, nm_map* out) {
+  if (!ctx || !d || !out) return fail(NM_ERR_ARG, "null argument");
+  *out = nullptr;
+  if (!(d->res > 0.0f)) return fail(NM_ERR_ARG, "map resolution must be positive");
+  if (d->leaf_edge != 8) return fail(NM_ERR_UNSUPPORTED, "leaf edge %d (only 8 is supported)", d->leaf_edge);
+  if (d->update_mode != NM_UPDATE_LABEL && d->update_mode != NM_UPDATE_ACCUMULATE)
+    return fail(NM_ERR_ARG, "unknown update mode %d", d->update_mode);
+  if (d->clamp_mode != NM_CLAMP_ALWAYS && d->clamp_mode != NM_CLAMP_ON_CROSSING)
+    return fail(NM_ERR_ARG, "unknown clamp mode %d", d->clamp_mode);
+  if (d->rounding != NM_ROUND_NEAREST && d->rounding != NM_ROUND_DOWN)
+    return fail(NM_ERR_ARG, "unknown rounding %d", d->rounding);
+  if (d->max_agents < 1 || d->max_agents > nm::kMaxPlanes)
+    return fail(NM_ERR_ARG, "max_agents must be 1..%d", nm::kMaxPlanes);
+  if (d->update_mode == NM_UPDATE_ACCUMULATE && d->max_agents != 1)
+    return fail(NM_ERR_UNSUPPORTED, "accumulate mode keeps one label plane");
+  NM_CUDA(cudaSetDevice(ctx->device));
+  std::unique_ptr<nm_map_s> m(new nm_map_s());
+  m->ctx = ctx;
+  m->desc = *d;
+  NM_CUDA(cudaMalloc((void**)&m->d_ctr, sizeof(nm::MapCounters)));
+  NM_CUDA(cudaMemsetAsync(m->d_ctr, 0, sizeof(nm::MapCounters), ctx->stream));
+  NM_CUDA(cudaMalloc((void**)&m->d_scratch_u32, 64));
+  const uint32_t cap = next_pow2(std::max<uint64_t>(d->initial_leaf_capacity ? d->initial_leaf_capacity : (1u << 18), 1024));
+  const int rc = alloc_view(m.get(), cap, &m->view, ctx->stream);
+  if (rc != NM_OK) {
+    cudaFree(m->d_ctr);
+    cudaFree(m->d_scratch_u32);
+    return rc;
+  }
+  NM_CUDA(cudaStreamSynchronize(ctx->stream));
+  for (int i = 0; i < nm::kMaxPlanes; ++i) m->pending_lh[i] = m->pending_lm[i] = 0.f;
+  *out = m.release();
+  return NM_OK;
+}
+
+int nm_map_destroy(nm_map m) {
+  if (!m) return NM_OK;
+  cudaSetDevice(m->ctx->device);
+  cudaStreamSynchronize(m->ctx->stream);
+  cudaDeviceSynchronize();
+  free_view(m->view);
+  cudaFree(m->d_ctr);
+  cudaFree(m->d_scratch_u32);
+  cudaFree(m->staging);
+  delete m;
+  return NM_OK;
+}
+
+int nm_map_reset(nm_map m) {
+  if (!m) return fail(NM_ERR_ARG, "map is null");
+  cudaStream_t s = m->ctx->stream;
+  NM_CUDA(cudaDeviceSynchronize());
+  const size_t C = m->view.capacity;
+  NM_CUDA(nm::launch_fill_keys(m->view.keys, m->view.capacity, s));
+  NM_CUDA(cudaMemsetAsync(m->view.values, 0, C * nm::kLeafVoxels * 4, s));
+  NM_CUDA(cudaMemsetAsync(m->view.active, 0, C * nm::kActiveWords * 4, s));
+  NM_CUDA(cudaMemsetAsync(m->view.labels, 0, (size_t)m->view.planes * C * nm::kLabelWords * 4, s));
+  if (m->view.counts) NM_CUDA(cudaMemsetAsync(m->view.counts, 0, C * 1024 * 4, s));
+  NM_CUDA(cudaMemsetAsync(m->view.epoch, 0, C * 4, s));
+  if (m->view.plane_mask) NM_CUDA(cudaMemsetAsync(m->view.plane_mask, 0, C * 4, s));
+  NM_CUDA(cudaMemsetAsync(m->d_ctr, 0, sizeof(nm::MapCounters), s));
+  NM_CUDA(cudaStreamSynchronize(s));
+  m->epoch = 1;
+  m->known_leaves = 0;
+  m->pending_bound = 0;
+  m->pending_labels = false;
+  m->pending_planes = 0;
+  return NM_OK;
+}
+
+int nm_map_stats(nm_map m, nm_stats* out) {
+  if (!m || !out) return fail(NM_ERR_ARG, "null argument");
+  NM_CUDA(cudaDeviceSynchronize());
+  nm::MapCounters c;
+  NM_CUDA(cudaMemcpy(&c, m->d_ctr, sizeof(c), cudaMemcpyDeviceToHost));
+  out->frames = c.frames;
+  out->rays = c.rays;
+  out->visits = c.visits;
+  out->unique_voxels = c.unique_voxels;
+  out->touched_leaves = c.touched_total;
+  out->leaf_count = c.leaf_count;
+  out->leaf_capacity = m->view.capacity;
+  out->error_flags = c.error_flags;
+  out->grow_count = m->grow_count;
+  m->known_leaves = c.leaf_count;
+  m->pending_bound = 0;
+  if (c.error_flags) NM_CUDA(cudaMemset(&m->d_ctr->error_flags, 0, 4));
+  return NM_OK;
+}
+
+int nm_map_insert_points(nm_map m, nm_sensor s, const nm_pose* pose, const void* cloud,
+                         int32_t width, int32_t height, int32_t step, uint32_t flags,
+                         void* stream) {
+  if (!m || !s) return fail(NM_ERR_ARG, "null map or sensor");
+  if (width < 0 || height < 0 || (int64_t)width * height > (1ll << 30))
+    return fail(NM_ERR_ARG, "cloud size %dx%d out of range", width, height);
+  if (step < 12) return fail(NM_ERR_ARG, "point step %d below 12 bytes", step);
+  const int64_t n = (int64_t)width * height;
+  if (n > 0 && !cloud) return fail(NM_ERR_ARG, "cloud is null");
+  NM_CUDA(cudaSetDevice(m->ctx->device));
+  cudaStream_t s0 = pick(m->ctx, stream);
+  nm::FrameParams f;
+  int rc = make_frame(m, s, pose, &f);
+  if (rc != NM_OK) return rc;
+  if (n == 0) return NM_OK;
+  f.width = width;
+  f.height = height;
+  f.input_kind = 0;
+  f.step = step;
+  const void* dev = cloud;
+  if (flags & NM_INPUT_HOST) {
+    rc = stage_input(m, cloud, (size_t)n * step, s0, &dev);
+    if (rc != NM_OK) return rc;
+  }
+  f.xyz = static_cast<const unsigned char*>(dev);
+  const uint64_t bound = frame_leaf_bound(m, s, *pose, f.R, false, (uint64_t)n);
+  return run_frame(m, s, f, flags, s0, bound);
+}
+
+int nm_map_insert_ranges(nm_map m, nm_sensor s, const nm_pose* pose, const float* ranges,
+                         uint32_t flags, void* stream) {
+  if (!m || !s || !ranges) return fail(NM_ERR_ARG, "null argument");
+  NM_CUDA(cudaSetDevice(m->ctx->device));
+  cudaStream_t s0 = pick(m->ctx, stream);
+  nm::FrameParams f;
+  int rc = make_frame(m, s, pose, &f);
+  if (rc != NM_OK) return rc;
+  const int64_t n = (int64_t)s->desc.hres * s->desc.vres;
+  f.input_kind = 1;
+  const void* dev = ranges;
+  if (flags & NM_INPUT_HOST) {
+    rc = stage_input(m, ranges, (size_t)n * 4, s0, &dev);
+    if (rc != NM_OK) return rc;
+  }
+  f.ranges = static_cast<const float*>(dev);
+  const uint64_t bound = frame_leaf_bound(m, s, *pose, f.R, true, (uint64_t)n);
+  return run_frame(m, s, f, flags, s0, bound);
+}
+
+int nm_map_integrate(nm_map m, void* stream) {
+  if (!m) return fail(NM_ERR_ARG, "map is null");
+  NM_CUDA(cudaSetDevice(m->ctx->device));
+  return do_integrate(m, pick(m->ctx, stream));
+}
+
+int nm_map_export(nm_map m, int32_t* origins, float* values, uint32_t* active,
+                  uint64_t max_leaves, uint64_t* n) {
+  if (!m || !n) return fail(NM_ERR_ARG, "null argument");
+  NM_CUDA(cudaSetDevice(m->ctx->device));
+  cudaStream_t s = m->ctx->stream;
+  NM_CUDA(cudaDeviceSynchronize());
+  unsigned int lc = 0;
+  NM_CUDA(cudaMemcpy(&lc, &m->d_ctr->leaf_count, 4, cudaMemcpyDeviceToHost));
+  *n = lc;
+  const uint64_t k = std::min<uint64_t>(lc, max_leaves);
+  if (k == 0) return NM_OK;
+  int32_t* d_o = nullptr;
+  float* d_v = nullptr;
+  uint32_t* d_a = nullptr;
+  cudaError_t e = cudaSuccess;
+  if (origins) e = cudaMalloc((void**)&d_o, k * 12);
+  if (e == cudaSuccess && values) e = cudaMalloc((void**)&d_v, k * 2048);
+  if (e == cudaSuccess && active) e = cudaMalloc((void**)&d_a, k * 64);
+  if (e == cudaSuccess) e = cudaMemsetAsync(m->d_scratch_u32, 0, 4, s);
+  if (e == cudaSuccess) e = nm::launch_export(m->view, d_o, d_v, d_a, m->d_scratch_u32, (uint32_t)k, s);
+  if (e == cudaSuccess) e = cudaStreamSynchronize(s);
+  if (e == cudaSuccess && origins) e = cudaMemcpy(origins, d_o, k * 12, cudaMemcpyDeviceToHost);
+  if (e == cudaSuccess && values) e = cudaMemcpy(values, d_v, k * 2048, cudaMemcpyDeviceToHost);
+  if (e == cudaSuccess && active) e = cudaMemcpy(active, d_a, k * 64, cudaMemcpyDeviceToHost);
+  cudaFree(d_o);
+  cudaFree(d_v);
+  cudaFree(d_a);
+  if (e != cudaSuccess) return fail(NM_ERR_CUDA, "export: %s", cudaGetErrorString(e));
+  return NM_OK;
+}
+
+int nm_map_export_labels(nm_map m, int32_t agent, int32_t* origins, uint32_t* words,
+                         uint64_t max_leaves, uint64_t* n) {
+  if (!m || !n || !origins || !words) return fail(NM_ERR_ARG, "null argument");
+  if (agent < 0 || agent >= m->view.planes) return fail(NM_ERR_ARG, "agent plane %d out of range", agent);
+  if (m->desc.update_mode != NM_UPDATE_LABEL) return fail(NM_ERR_STATE, "map is not in label mode");
+  NM_CUDA(cudaSetDevice(m->ctx->device));
+  cudaStream_t s = m->ctx->stream;
+  NM_CUDA(cudaDeviceSynchronize());
+  unsigned int lc = 0;
+  NM_CUDA(cudaMemcpy(&lc, &m->d_ctr->leaf_count, 4, cudaMemcpyDeviceToHost));
+  const uint64_t cap = std::min<uint64_t>(lc, max_leaves);
+  *n = 0;
+  if (cap == 0) return NM_OK;
+  int32_t* d_o = nullptr;
+  uint32_t* d_w = nullptr;
+  cudaError_t e = cudaMalloc((void**)&d_o, cap * 12);
+  if (e == cudaSuccess) e = cudaMalloc((void**)&d_w, cap * 128);
+  if (e == cudaSuccess) e = cudaMemsetAsync(m->d_scratch_u32, 0, 4, s);
+  if (e == cudaSuccess) e = nm::launch_export_labels(m->view, agent, d_o, d_w, m->d_scratch_u32, (uint32_t)cap, s);
+  unsigned int cnt = 0;
+  if (e == cudaSuccess) e = cudaStreamSynchronize(s);
+  if (e == cudaSuccess) e = cudaMemcpy(&cnt, m->d_scratch_u32, 4, cudaMemcpyDeviceToHost);
+  const uint64_t k = std::min<uint64_t>(cnt, cap);
+  if (e == cudaSuccess && k) e = cudaMemcpy(origins, d_o, k * 12, cudaMemcpyDeviceToHost);
+  if (e == cudaSuccess && k) e = cudaMemcpy(words, d_w, k * 128, cudaMemcpyDeviceToHost);
+  cudaFree(d_o);
+  cudaFree(d_w);
+  if (e != cudaSuccess) return fail(NM_ERR_CUDA, "export labels: %s", cudaGetErrorString(e));
+  *n = cnt;
+  return NM_OK;
+}
+
+int nm_map_frame_params(nm_map m, nm_sensor s, const nm_pose* pose, float rotation[9],
+                        double eye[3], float* max_time) {
+  if (!m || !s || !rotation || !eye || !max_time) return fail(NM_ERR_ARG, "null argument");
+  nm::FrameParams f;
+  const int rc = make_frame(m, s, pose, &f);
+  if (rc != NM_OK) return rc;
+  std::memcpy(rotation, f.R, sizeof(f.R));
+  std::memcpy(eye, f.eye, sizeof(f.eye));
+  *max_time = f.max_time;
+  return NM_OK;
+}
+
+int nm_frame_params(const nm_sensor_desc* desc, const nm_pose* pose, float res, int32_t rounding,
+                    float rotation[9], double eye[3], float* max_time, float pixel_model[6]) {
+  if (!desc || !rotation || !eye || !max_time || !pixel_model) return fail(NM_ERR_ARG, "null argument");
+  const int rc = validate_pose(pose);
+  if (rc != NM_OK) return rc;
+  if (!(res > 0.0f)) return fail(NM_ERR_ARG, "resolution must be positive");
+  if (rounding != NM_ROUND_NEAREST && rounding != NM_ROUND_DOWN) return fail(NM_ERR_ARG, "unknown rounding");
+  nm::pose_rotation(*pose, desc->frame_transform, rotation);
+  nm::frame_constants(*pose, res, desc->max_range, rounding, eye, max_time);
+  if (desc->type == NM_SENSOR_FRUSTUM)
+    nm::frustum_params(desc->hres, desc->vres, desc->hfov_deg, desc->vfov_deg, pixel_model);
+  else
+    for (int i = 0; i < 6; ++i) pixel_model[i] = 0.0f;
+  return NM_OK;
+}
+
+int nm_map_tick(nm_map m, const nm_frame* frames, int32_t n_frames, uint32_t flags, void* stream) {
+  (void)m;
+  (void)frames;
+  (void)n_frames;
+  (void)flags;
+  (void)stream;
+  return fail(NM_ERR_UNSUPPORTED, "nm_map_tick is not available in this build");
+}
+
+}  // extern "C"

@@ -1,0 +1,293 @@
+// nm_abi_sim.cpp -- C ABI of the simulation map: build, info, export, render, sensor noise.
+//
+// Replaces SimHandler's sim-grid upload (SimHandler.cpp:22-23: openToNanoVDB + deviceUpload)
+// and the generateCloud launcher (generateCloud.cu:84-94).
+#include <algorithm>
+#include <climits>
+#include <cmath>
+#include <cstring>
+#include <memory>
+#include <vector>
+
+#include "nm_host.h"
+#include "nm_objects.h"
+
+using nm::fail;
+
+namespace {
+
+int floor_div(int v, int d) { return (v >= 0) ? v / d : -((-v + d - 1) / d); }
+
+// Shared tail of both builders: compact the dense leaf buffer into the sparse view.
+int finish_build(nm_context ctx, nm::SimBuild& b, nm_simmap sm, cudaStream_t s) {
+  nm::SimMapView& v = sm->view;
+  v.res = b.res;
+  for (int a = 0; a < 3; ++a) {
+    v.llo[a] = b.llo[a];
+    v.ldim[a] = b.ldim[a];
+    v.blo[a] = floor_div(b.llo[a], 8);
+    v.bdim[a] = floor_div(b.llo[a] + b.ldim[a] - 1, 8) - v.blo[a] + 1;
+  }
+  uint32_t* d_count = nullptr;
+  int32_t* d_bbox = nullptr;
+  unsigned long long* d_nvox = nullptr;
+  NM_CUDA(cudaMalloc((void**)&d_count, 4));
+  NM_CUDA(cudaMalloc((void**)&d_bbox, 24));
+  NM_CUDA(cudaMalloc((void**)&d_nvox, 8));
+  NM_CUDA(cudaMemsetAsync(d_count, 0, 4, s));
+  NM_CUDA(nm::launch_compact(b, v, d_count, 0, d_bbox, d_nvox, s));
+  uint32_t nleaves = 0;
+  NM_CUDA(cudaMemcpyAsync(&nleaves, d_count, 4, cudaMemcpyDeviceToHost, s));
+  NM_CUDA(cudaStreamSynchronize(s));
+  const long long lprod = (long long)b.ldim[0] * b.ldim[1] * b.ldim[2];
+  const long long bprod = (long long)v.bdim[0] * v.bdim[1] * v.bdim[2];
+  NM_CUDA(cudaMalloc((void**)&v.leaf_index, (size_t)lprod * 4));
+  NM_CUDA(cudaMalloc((void**)&v.leaf_words, (size_t)std::max<uint32_t>(nleaves, 1) * 64));
+  NM_CUDA(cudaMalloc((void**)&v.brick_bits, (size_t)((bprod + 31) / 32) * 4));
+  NM_CUDA(nm::launch_fill_i32(v.leaf_index, lprod, -1, s));
+  NM_CUDA(cudaMemsetAsync(v.brick_bits, 0, (size_t)((bprod + 31) / 32) * 4, s));
+  const int32_t init[6] = {INT_MAX, INT_MAX, INT_MAX, INT_MIN, INT_MIN, INT_MIN};
+  NM_CUDA(cudaMemcpyAsync(d_bbox, init, 24, cudaMemcpyHostToDevice, s));
+  NM_CUDA(cudaMemsetAsync(d_nvox, 0, 8, s));
+  NM_CUDA(cudaMemsetAsync(d_count, 0, 4, s));
+  NM_CUDA(nm::launch_compact(b, v, d_count, 1, d_bbox, d_nvox, s));
+  unsigned long long nvox = 0;
+  NM_CUDA(cudaMemcpyAsync(sm->bbox, d_bbox, 24, cudaMemcpyDeviceToHost, s));
+  NM_CUDA(cudaMemcpyAsync(&nvox, d_nvox, 8, cudaMemcpyDeviceToHost, s));
+  NM_CUDA(cudaStreamSynchronize(s));
+  cudaFree(d_count);
+  cudaFree(d_bbox);
+  cudaFree(d_nvox);
+  cudaFree(b.dense);
+  b.dense = nullptr;
+  sm->leaves = nleaves;
+  sm->active_voxels = nvox;
+  v.any = nvox > 0 ? 1 : 0;
+  if (!v.any)
+    for (int a = 0; a < 3; ++a) {
+      sm->bbox[a] = 0;
+      sm->bbox[3 + a] = -1;
+    }
+  for (int a = 0; a < 3; ++a) {
+    v.box_lo[a] = (float)sm->bbox[a];
+    v.box_hi[a] = (float)(sm->bbox[3 + a] + 1);
+  }
+  (void)ctx;
+  return NM_OK;
+}
+
+int begin_build(float res, const int32_t vmin[3], const int32_t vmax[3], nm::SimBuild* b,
+                cudaStream_t s) {
+  b->res = res;
+  long long prod = 1;
+  for (int a = 0; a < 3; ++a) {
+    if (vmax[a] <= vmin[a]) return fail(NM_ERR_ARG, "empty voxel region on axis %d", a);
+    if (vmin[a] < -(1 << 23) || vmax[a] > (1 << 23))
+      return fail(NM_ERR_ARG, "voxel region exceeds +-%d voxels", 1 << 23);
+    b->vmin[a] = vmin[a];
+    b->vmax[a] = vmax[a];
+    b->llo[a] = floor_div(vmin[a], 8);
+    b->ldim[a] = floor_div(vmax[a] - 1, 8) - b->llo[a] + 1;
+    prod *= b->ldim[a];
+  }
+  if (prod > (1ll << 32)) return fail(NM_ERR_CAPACITY, "voxel region has %lld leaves", prod);
+  b->dense = nullptr;
+  NM_CUDA(cudaMalloc((void**)&b->dense, (size_t)prod * 64));
+  NM_CUDA(cudaMemsetAsync(b->dense, 0, (size_t)prod * 64, s));
+  return NM_OK;
+}
+
+cudaStream_t pick(nm_context ctx, void* stream) {
+  return stream ? static_cast<cudaStream_t>(stream) : ctx->stream;
+}
+
+}  // namespace
+
+extern "C" {
+
+int nm_simmap_create_primitives(nm_context ctx, float res, const int32_t vox_min[3],
+                                const int32_t vox_max[3], const double* boxes, int32_t n_boxes,
+                                const double* cylinders, int32_t n_cylinders, nm_simmap* out) {
+  if (!ctx || !vox_min || !vox_max || !out) return fail(NM_ERR_ARG, "null argument");
+  *out = nullptr;
+  if (!(res > 0.0f)) return fail(NM_ERR_ARG, "resolution must be positive");
+  if (n_boxes < 0 || n_cylinders < 0 || (n_boxes > 0 && !boxes) || (n_cylinders > 0 && !cylinders))
+    return fail(NM_ERR_ARG, "primitive arrays invalid");
+  if (n_boxes > 65535 || n_cylinders > 65535)
+    return fail(NM_ERR_ARG, "at most 65535 boxes and 65535 cylinders per call");
+  NM_CUDA(cudaSetDevice(ctx->device));
+  cudaStream_t s = ctx->stream;
+  std::unique_ptr<nm_simmap_s> sm(new nm_simmap_s());
+  sm->ctx = ctx;
+  nm::SimBuild b{};
+  int rc = begin_build(res, vox_min, vox_max, &b, s);
+  if (rc != NM_OK) return rc;
+  double* d_boxes = nullptr;
+  double* d_cyl = nullptr;
+  if (n_boxes) {
+    NM_CUDA(cudaMalloc((void**)&d_boxes, (size_t)n_boxes * 48));
+    NM_CUDA(cudaMemcpyAsync(d_boxes, boxes, (size_t)n_boxes * 48, cudaMemcpyHostToDevice, s));
+  }
+  if (n_cylinders) {
+    NM_CUDA(cudaMalloc((void**)&d_cyl, (size_t)n_cylinders * 40));
+    NM_CUDA(cudaMemcpyAsync(d_cyl, cylinders, (size_t)n_cylinders * 40, cudaMemcpyHostToDevice, s));
+  }
+  NM_CUDA(nm::launch_voxelize(b, d_boxes, n_boxes, d_cyl, n_cylinders, s));
+  rc = finish_build(ctx, b, sm.get(), s);
+  cudaFree(d_boxes);
+  cudaFree(d_cyl);
+  if (rc != NM_OK) return rc;
+  *out = sm.release();
+  return NM_OK;
+}
+
+int nm_simmap_create_voxels(nm_context ctx, float res, const int32_t* ijk, int64_t n,
+                            nm_simmap* out) {
+  if (!ctx || !out || (n > 0 && !ijk) || n < 0) return fail(NM_ERR_ARG, "invalid argument");
+  *out = nullptr;
+  if (!(res > 0.0f)) return fail(NM_ERR_ARG, "resolution must be positive");
+  NM_CUDA(cudaSetDevice(ctx->device));
+  cudaStream_t s = ctx->stream;
+  int32_t vmin[3] = {0, 0, 0}, vmax[3] = {1, 1, 1};
+  if (n > 0) {
+    for (int a = 0; a < 3; ++a) {
+      vmin[a] = INT_MAX;
+      vmax[a] = INT_MIN;
+    }
+    for (int64_t i = 0; i < n; ++i)
+      for (int a = 0; a < 3; ++a) {
+        vmin[a] = std::min(vmin[a], ijk[3 * i + a]);
+        vmax[a] = std::max(vmax[a], ijk[3 * i + a] + 1);
+      }
+  }
+  std::unique_ptr<nm_simmap_s> sm(new nm_simmap_s());
+  sm->ctx = ctx;
+  nm::SimBuild b{};
+  int rc = begin_build(res, vmin, vmax, &b, s);
+  if (rc != NM_OK) return rc;
+  int32_t* d_ijk = nullptr;
+  if (n > 0) {
+    NM_CUDA(cudaMalloc((void**)&d_ijk, (size_t)n * 12));
+    NM_CUDA(cudaMemcpyAsync(d_ijk, ijk, (size_t)n * 12, cudaMemcpyHostToDevice, s));
+    NM_CUDA(nm::launch_set_voxels(b, d_ijk, n, s));
+  }
+  rc = finish_build(ctx, b, sm.get(), s);
+  cudaFree(d_ijk);
+  if (rc != NM_OK) return rc;
+  *out = sm.release();
+  return NM_OK;
+}
+
+int nm_simmap_destroy(nm_simmap sm) {
+  if (!sm) return NM_OK;
+  cudaSetDevice(sm->ctx->device);
+  cudaDeviceSynchronize();
+  cudaFree(sm->view.leaf_index);
+  cudaFree(sm->view.leaf_words);
+  cudaFree(sm->view.brick_bits);
+  delete sm;
+  return NM_OK;
+}
+
+int nm_simmap_info(nm_simmap sm, int32_t bbox[6], uint64_t* active_voxels, uint64_t* leaves) {
+  if (!sm) return fail(NM_ERR_ARG, "sim map is null");
+  if (bbox) std::memcpy(bbox, sm->bbox, 24);
+  if (active_voxels) *active_voxels = sm->active_voxels;
+  if (leaves) *leaves = sm->leaves;
+  return NM_OK;
+}
+
+int nm_simmap_export(nm_simmap sm, int32_t* origins, uint32_t* words, uint64_t max_leaves,
+                     uint64_t* n) {
+  if (!sm || !n) return fail(NM_ERR_ARG, "null argument");
+  NM_CUDA(cudaSetDevice(sm->ctx->device));
+  *n = sm->leaves;
+  const nm::SimMapView& v = sm->view;
+  const long long lprod = (long long)v.ldim[0] * v.ldim[1] * v.ldim[2];
+  std::vector<int32_t> index((size_t)lprod);
+  NM_CUDA(cudaMemcpy(index.data(), v.leaf_index, (size_t)lprod * 4, cudaMemcpyDeviceToHost));
+  std::vector<uint32_t> all((size_t)sm->leaves * 16);
+  if (sm->leaves)
+    NM_CUDA(cudaMemcpy(all.data(), v.leaf_words, all.size() * 4, cudaMemcpyDeviceToHost));
+  uint64_t o = 0;
+  for (long long pos = 0; pos < lprod && o < max_leaves; ++pos) {
+    const int32_t li = index[(size_t)pos];
+    if (li < 0) continue;
+    const int lz = (int)(pos % v.ldim[2]);
+    const int ly = (int)((pos / v.ldim[2]) % v.ldim[1]);
+    const int lx = (int)(pos / ((long long)v.ldim[2] * v.ldim[1]));
+    if (origins) {
+      origins[3 * o] = (v.llo[0] + lx) * 8;
+      origins[3 * o + 1] = (v.llo[1] + ly) * 8;
+      origins[3 * o + 2] = (v.llo[2] + lz) * 8;
+    }
+    if (words) std::memcpy(words + 16 * o, all.data() + (size_t)li * 16, 64);
+    ++o;
+  }
+  return NM_OK;
+}
+
+int nm_sim_render(nm_simmap sm, nm_sensor s, const nm_pose* pose, float* ranges, uint32_t flags,
+                  void* stream) {
+  if (!sm || !s || !pose || !ranges) return fail(NM_ERR_ARG, "null argument");
+  if (s->ctx != sm->ctx) return fail(NM_ERR_ARG, "sensor and sim map belong to different contexts");
+  for (int a = 0; a < 3; ++a)
+    if (!std::isfinite(pose->position[a])) return fail(NM_ERR_ARG, "pose position is not finite");
+  double qn = 0;
+  for (int a = 0; a < 4; ++a) qn += (double)pose->orientation[a] * pose->orientation[a];
+  if (!(qn > 1e-20) || !std::isfinite(qn)) return fail(NM_ERR_ARG, "orientation quaternion invalid");
+  nm_context ctx = sm->ctx;
+  NM_CUDA(cudaSetDevice(ctx->device));
+  cudaStream_t st = pick(ctx, stream);
+  nm::SimRayParams rp;
+  std::memset(&rp, 0, sizeof(rp));
+  rp.type = s->desc.type;
+  rp.width = s->desc.hres;
+  rp.height = s->desc.vres;
+  rp.hw = s->fp[0];
+  rp.hh = s->fp[1];
+  rp.c0 = s->fp[2];
+  rp.c1 = s->fp[3];
+  rp.su = s->fp[4];
+  rp.sv = s->fp[5];
+  if (s->desc.type == NM_SENSOR_LASER) {
+    rp.sinu = s->d_tables;
+    rp.cosu = s->d_tables + s->desc.hres;
+    rp.sinv = s->d_tables + 2 * s->desc.hres;
+    rp.cosv = s->d_tables + 2 * s->desc.hres + s->desc.vres;
+  }
+  nm::pose_rotation(*pose, s->desc.frame_transform, rp.R);
+  for (int a = 0; a < 3; ++a) rp.pos[a] = pose->position[a];
+  rp.min_range = s->desc.min_range;
+  rp.max_range = s->desc.max_range;
+  const size_t bytes = (size_t)rp.width * rp.height * 4;
+  float* dst = ranges;
+  if (flags & NM_OUTPUT_HOST) {
+    if (bytes > ctx->render_staging_bytes) {
+      cudaFree(ctx->render_staging);
+      ctx->render_staging = nullptr;
+      ctx->render_staging_bytes = 0;
+      NM_CUDA(cudaMalloc((void**)&ctx->render_staging, bytes));
+      ctx->render_staging_bytes = bytes;
+    }
+    dst = ctx->render_staging;
+  }
+  NM_CUDA(nm::launch_sim_render(sm->view, rp, dst, st));
+  if (flags & NM_OUTPUT_HOST) {
+    NM_CUDA(cudaMemcpyAsync(ranges, dst, bytes, cudaMemcpyDeviceToHost, st));
+    NM_CUDA(cudaStreamSynchronize(st));
+  } else if (flags & NM_SYNC) {
+    NM_CUDA(cudaStreamSynchronize(st));
+  }
+  return NM_OK;
+}
+
+int nm_ranges_add_noise(nm_context ctx, float* ranges, int64_t n, float sigma_coef,
+                        float drop_prob, uint64_t seed, void* stream) {
+  if (!ctx || (!ranges && n > 0) || n < 0) return fail(NM_ERR_ARG, "invalid argument");
+  NM_CUDA(cudaSetDevice(ctx->device));
+  NM_CUDA(nm::launch_noise(ranges, n, sigma_coef, drop_prob, seed, pick(ctx, stream)));
+  return NM_OK;
+}
+
+}  // extern "C"

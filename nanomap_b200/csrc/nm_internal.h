@@ -1,0 +1,131 @@
+// nm_internal.h -- structures shared by the host code and the sm_100a kernels.
+//
+// Device map layout (one open-addressing hash table; the table position of a leaf is its
+// storage slot, so inserting a leaf never has to publish an index):
+//   keys      u64[C]          leaf key (packed leaf coordinate), ~0 = empty
+//   values    f32[C][512]     log-odds, voxel index x*64 + y*8 + z inside the 8^3 leaf
+//   active    u32[C][16]      active (occupied) bit per voxel
+//   labels    u32[P][C][32]   per-frame labels per plane: words 0..15 hit, 16..31 miss
+//   counts    u32[C][1024]    per-frame hit (0..511) and miss (512..1023) counts, accumulate mode
+//   epoch     u32[C]          frame id that last put the slot on the touched list
+//   plane_mask u32[C]         planes holding labels for the slot (batched ticks)
+//   touched   u32[C]          slots labelled by the current frame / tick
+#pragma once
+
+#include <cstdint>
+#include <cuda_runtime.h>
+
+#include "../../include/nanomap_b200.h"
+
+namespace nm {
+
+constexpr uint64_t kEmptyKey = ~0ull;
+constexpr int kLeafVoxels = 512;
+constexpr int kLabelWords = 32;
+constexpr int kActiveWords = 16;
+constexpr int kMaxPlanes = 32;
+constexpr uint32_t kMaxProbe = 4096;
+
+// Device-side error bits (sticky until read by nm_map_stats).
+constexpr uint32_t kErrProbe = 1u;     // leaf table probe limit reached: labels were lost
+constexpr uint32_t kErrTimeout = 2u;   // a bounded wait gave up
+constexpr uint32_t kErrPlane = 4u;     // plane index outside the allocated planes
+
+struct MapCounters {
+  unsigned long long rays;
+  unsigned long long visits;
+  unsigned long long unique_voxels;
+  unsigned long long touched_total;
+  unsigned int leaf_count;
+  unsigned int touched_count;
+  unsigned int error_flags;
+  unsigned int frames;
+  unsigned int done_blocks;
+  unsigned int pad[3];
+};
+
+struct MapView {
+  unsigned long long* keys;
+  float* values;
+  uint32_t* active;
+  uint32_t* labels;
+  uint32_t* counts;
+  uint32_t* epoch;
+  uint32_t* plane_mask;
+  uint32_t* touched;
+  MapCounters* ctr;
+  uint32_t mask;       // capacity - 1 (capacity is a power of two)
+  uint32_t capacity;
+  int32_t planes;
+  int32_t pad;
+};
+
+// Per-frame constants of one traversal launch.
+struct FrameParams {
+  int32_t type;        // NM_SENSOR_FRUSTUM / NM_SENSOR_LASER
+  int32_t width, height;
+  int32_t input_kind;  // 0 xyz records, 1 range image
+  float hw, hh, c0, c1, su, sv;  // frustum pixel model
+  const float* sinu;   // laser tables (device)
+  const float* cosu;
+  const float* sinv;
+  const float* cosv;
+  const unsigned char* xyz;
+  int64_t step;        // bytes between xyz records
+  const float* ranges;
+  float R[9];          // row-major, world-from-sensor
+  double eye[3];       // index-space eye
+  double res_d;
+  float max_time;      // max_range / res
+  uint32_t epoch;
+  int32_t plane;
+  int32_t pad;
+};
+
+struct IntegrateParams {
+  float lh[kMaxPlanes];
+  float lm[kMaxPlanes];
+  float thres_hit, thres_miss, clamp_min, clamp_max;
+  int32_t clamp_mode;
+  int32_t use_planes;  // 0: plane 0 only (plain path); 1: iterate plane_mask
+  int32_t pad[2];
+};
+
+__host__ __device__ inline uint64_t leaf_key(int lx, int ly, int lz) {
+  return ((uint64_t)((uint32_t)(lx + (1 << 20)) & 0x1FFFFFu) << 42) |
+         ((uint64_t)((uint32_t)(ly + (1 << 20)) & 0x1FFFFFu) << 21) |
+         (uint64_t)((uint32_t)(lz + (1 << 20)) & 0x1FFFFFu);
+}
+
+__host__ __device__ inline void key_leaf(uint64_t k, int* lx, int* ly, int* lz) {
+  *lx = (int)((k >> 42) & 0x1FFFFFu) - (1 << 20);
+  *ly = (int)((k >> 21) & 0x1FFFFFu) - (1 << 20);
+  *lz = (int)(k & 0x1FFFFFu) - (1 << 20);
+}
+
+// MurmurHash3 fmix64 finaliser.
+__host__ __device__ inline uint32_t hash_key(uint64_t k) {
+  k ^= k >> 33;
+  k *= 0xff51afd7ed558ccdULL;
+  k ^= k >> 33;
+  k *= 0xc4ceb9fe1a85ec53ULL;
+  k ^= k >> 33;
+  return (uint32_t)k;
+}
+
+// ---- kernel launchers (defined in the .cu files) -----------------------------------------
+cudaError_t launch_traverse(const FrameParams& f, const MapView& m, int update_mode,
+                            int rounding, int tile_w, int tile_h, int smem_entries,
+                            cudaStream_t s);
+cudaError_t launch_integrate(const MapView& m, const IntegrateParams& p, int update_mode,
+                             int rounding, int sm_count, cudaStream_t s);
+cudaError_t launch_rehash(const MapView& from, const MapView& to, uint32_t cur_epoch,
+                          int update_mode, cudaStream_t s);
+cudaError_t launch_export(const MapView& m, int32_t* origins, float* values, uint32_t* active,
+                          uint32_t* n_out, uint32_t max_out, cudaStream_t s);
+cudaError_t launch_export_labels(const MapView& m, int plane, int32_t* origins,
+                                 uint32_t* words, uint32_t* n_out, uint32_t max_out,
+                                 cudaStream_t s);
+cudaError_t launch_fill_keys(unsigned long long* keys, uint32_t n, cudaStream_t s);
+
+}  // namespace nm

@@ -1,0 +1,513 @@
+// nm_map.cu -- sm_100a kernels of the mapping path: traversal + per-frame labels, label
+// integration into the device leaf table, table growth and export.
+//
+// Replaces frustumCastCloud.cu:84-294 (leaf pass, CUB compaction, voxel pass with per-visit
+// fp32 atomics, int8 quantisation) and the host map update of Handler.cpp:134-182.
+#include <cfloat>
+#include <cstdint>
+
+#include "nm_device.cuh"
+#include "nm_internal.h"
+
+namespace nm {
+
+namespace {
+
+constexpr unsigned kFull = 0xffffffffu;
+
+// Label sink of one thread.  Labels go to the CTA's shared-memory leaf table (a hashed cache
+// of up to `smask+1` leaves with 32 label words each); a leaf that finds no room there goes
+// straight to the device table.  The leaf of the previous event is cached in registers, so
+// a table probe happens only when the ray crosses into another leaf.
+struct LabelEmit {
+  unsigned long long* s_keys;
+  uint32_t* s_words;
+  uint32_t smask;
+  const MapView* m;
+  uint32_t epoch;
+  int plane;
+  unsigned long long ckey;
+  int cslot;
+  bool cglobal;
+
+  __device__ __forceinline__ void resolve() {
+    const int s = smem_find_or_insert(s_keys, smask, ckey);
+    if (s >= 0) {
+      cglobal = false;
+      cslot = s;
+    } else {
+      cglobal = true;
+      cslot = map_find_or_insert(*m, ckey);
+      if (cslot >= 0) mark_touched(*m, cslot, epoch, plane);
+    }
+  }
+
+  __device__ __forceinline__ void operator()(int x, int y, int z, int kind) {
+    const unsigned long long key = leaf_key(x >> 3, y >> 3, z >> 3);
+    if (key != ckey) {
+      ckey = key;
+      resolve();
+    }
+    const int l = local_index(x, y, z);
+    const uint32_t bit = 1u << (l & 31);
+    const int wi = (kind == kKindHit ? 0 : 16) + (l >> 5);
+    if (!cglobal) {
+      uint32_t* w = &s_words[cslot * kLabelWords + wi];
+      if (!(*(volatile uint32_t*)w & bit)) atomicOr(w, bit);
+    } else if (cslot >= 0) {
+      uint32_t* w = &m->labels[((size_t)plane * m->capacity + (size_t)cslot) * kLabelWords + wi];
+      if (!(__ldcg(w) & bit)) atomicOr(w, bit);
+    }
+  }
+};
+
+// Count sink (accumulate mode): exact per-voxel hit and miss counts, one atomic per group of
+// lanes that hit the same counter at the same time.
+struct CountEmit {
+  const MapView* m;
+  uint32_t epoch;
+  unsigned long long ckey;
+  int cslot;
+
+  __device__ __forceinline__ void operator()(int x, int y, int z, int kind) {
+    const unsigned long long key = leaf_key(x >> 3, y >> 3, z >> 3);
+    if (key != ckey) {
+      ckey = key;
+      cslot = map_find_or_insert(*m, key);
+      if (cslot >= 0) mark_touched(*m, cslot, epoch, 0);
+    }
+    if (cslot < 0) return;
+    const int l = local_index(x, y, z);
+    const unsigned long long idx =
+        (unsigned long long)cslot * 1024ull + (kind == kKindHit ? 0u : 512u) + (unsigned)l;
+    const unsigned act = __activemask();
+    const unsigned peers = __match_any_sync(act, idx);
+    const int leader = __ffs(peers) - 1;
+    if ((int)(threadIdx.x & 31) == leader) atomicAdd(&m->counts[idx], (unsigned)__popc(peers));
+  }
+};
+
+__device__ __forceinline__ bool load_point(const FrameParams& f, int w, int h, float p[3]) {
+  if (f.input_kind == 1) return range_point(f, w, h, p);
+  return xyz_point(f, w, h, p);
+}
+
+__device__ __forceinline__ void add_counts(MapCounters* ctr, uint32_t visits, uint32_t rays) {
+  unsigned long long v = visits, r = rays;
+#pragma unroll
+  for (int o = 16; o > 0; o >>= 1) {
+    v += __shfl_xor_sync(kFull, v, o);
+    r += __shfl_xor_sync(kFull, r, o);
+  }
+  if ((threadIdx.x & 31) == 0 && (v | r)) {
+    atomicAdd(&ctr->visits, v);
+    atomicAdd(&ctr->rays, r);
+  }
+}
+
+// One CTA = one tile of tile_w x tile_h pixels, one ray per thread.
+template <int RM>
+__global__ void __launch_bounds__(256) k_traverse_label(FrameParams f, MapView m, int tiles_x,
+                                                        int tile_w, int tile_h, uint32_t smask) {
+  extern __shared__ __align__(16) unsigned char smem[];
+  unsigned long long* s_keys = reinterpret_cast<unsigned long long*>(smem);
+  uint32_t* s_words = reinterpret_cast<uint32_t*>(s_keys + (smask + 1));
+  const int tid = threadIdx.x;
+  const int nent = (int)smask + 1;
+  for (int i = tid; i < nent; i += blockDim.x) s_keys[i] = kEmptyKey;
+  for (int i = tid; i < nent * kLabelWords; i += blockDim.x) s_words[i] = 0u;
+  __syncthreads();
+
+  const int tile = blockIdx.x;
+  const int px = (tile % tiles_x) * tile_w + tid % tile_w;
+  const int py = (tile / tiles_x) * tile_h + tid / tile_w;
+  uint32_t visits = 0, rays = 0;
+  if (px < f.width && py < f.height) {
+    float p[3];
+    if (load_point(f, px, py, p)) {
+      LabelEmit em{s_keys, s_words, smask, &m, f.epoch, f.plane, kEmptyKey, -1, false};
+      const int n = trace_point<RM>(f, p[0], p[1], p[2], em);
+      if (n >= 0) {
+        visits = (uint32_t)n;
+        rays = 1;
+      }
+    }
+  }
+  __syncthreads();
+
+  // Flush: one warp per cached leaf; lane i carries label word i.
+  const int warp = tid >> 5, lane = tid & 31, nwarps = blockDim.x >> 5;
+  for (int e = warp; e < nent; e += nwarps) {
+    const unsigned long long key = s_keys[e];
+    if (key == kEmptyKey) continue;
+    const uint32_t word = s_words[e * kLabelWords + lane];
+    if (__ballot_sync(kFull, word != 0u) == 0u) continue;
+    int g = -1;
+    if (lane == 0) {
+      g = map_find_or_insert(m, key);
+      if (g >= 0) mark_touched(m, g, f.epoch, f.plane);
+    }
+    g = __shfl_sync(kFull, g, 0);
+    if (g < 0) continue;
+    if (word) atomicOr(&m.labels[((size_t)f.plane * m.capacity + (size_t)g) * kLabelWords + lane], word);
+  }
+  add_counts(m.ctr, visits, rays);
+}
+
+template <int RM>
+__global__ void __launch_bounds__(256) k_traverse_count(FrameParams f, MapView m, int tiles_x,
+                                                        int tile_w, int tile_h) {
+  const int tid = threadIdx.x;
+  const int tile = blockIdx.x;
+  const int px = (tile % tiles_x) * tile_w + tid % tile_w;
+  const int py = (tile / tiles_x) * tile_h + tid / tile_w;
+  uint32_t visits = 0, rays = 0;
+  if (px < f.width && py < f.height) {
+    float p[3];
+    if (load_point(f, px, py, p)) {
+      CountEmit em{&m, f.epoch, kEmptyKey, -1};
+      const int n = trace_point<RM>(f, p[0], p[1], p[2], em);
+      if (n >= 0) {
+        visits = (uint32_t)n;
+        rays = 1;
+      }
+    }
+  }
+  add_counts(m.ctr, visits, rays);
+}
+
+// ---- integration (Handler.cpp:88-122 / SimHandler.cpp:88-122) ------------------------------
+
+template <int RM>
+__device__ __forceinline__ float update_voxel(float v, uint32_t& abit, float temp,
+                                              const IntegrateParams& p) {
+  if (temp != 0.0f) {
+    v = Ar<RM>::fadd(v, temp);
+    if (p.clamp_mode == NM_CLAMP_ALWAYS) {
+      if (v > p.clamp_max) {
+        v = p.clamp_max;
+      } else if (v < p.clamp_min) {
+        v = p.clamp_min;
+      }
+      if (v > p.thres_hit) {
+        abit = 1u;
+      } else if (v < p.thres_miss) {
+        abit = 0u;
+      }
+    } else {
+      if (v > p.thres_hit) {
+        abit = 1u;
+        if (v > p.clamp_max) v = p.clamp_max;
+      } else if (v < p.thres_miss) {
+        abit = 0u;
+        if (v < p.clamp_min) v = p.clamp_min;
+      }
+    }
+  }
+  return v;
+}
+
+// The last CTA to finish resets the per-frame list and folds it into the totals.
+__device__ __forceinline__ void integrate_epilogue(MapCounters* ctr, uint32_t n_touched,
+                                                   unsigned long long uniq) {
+  __shared__ unsigned long long s_uniq;
+  __shared__ bool s_last;
+  if (threadIdx.x == 0) s_uniq = 0;
+  __syncthreads();
+  if (uniq) atomicAdd(&s_uniq, uniq);
+  __syncthreads();
+  if (threadIdx.x == 0) {
+    if (s_uniq) atomicAdd(&ctr->unique_voxels, s_uniq);
+    __threadfence();
+    const unsigned done = atomicAdd(&ctr->done_blocks, 1u);
+    s_last = (done == gridDim.x - 1);
+  }
+  __syncthreads();
+  if (s_last && threadIdx.x == 0) {
+    __threadfence();
+    ctr->touched_total += n_touched;
+    ctr->frames += 1u;
+    ctr->touched_count = 0u;
+    ctr->done_blocks = 0u;
+  }
+}
+
+// One warp per touched leaf.  Lane i owns float4 i, i+32, i+64, i+96 of the leaf's 512
+// log-odds (voxels 4q..4q+3 of float4 q); label and active words are shared through
+// shuffles.  Labels are cleared as they are consumed, so the next frame starts from zero.
+template <int RM>
+__global__ void __launch_bounds__(256) k_integrate_label(MapView m, IntegrateParams p) {
+  const int lane = threadIdx.x & 31;
+  const uint32_t gw = (blockIdx.x * blockDim.x + threadIdx.x) >> 5;
+  const uint32_t nw = (gridDim.x * blockDim.x) >> 5;
+  const uint32_t n = *(volatile unsigned int*)&m.ctr->touched_count;
+  const bool fatal = (*(volatile unsigned int*)&m.ctr->error_flags & kErrProbe) != 0u;
+  unsigned long long uniq = 0;
+  for (uint32_t i = gw; i < n; i += nw) {
+    const uint32_t slot = m.touched[i];
+    uint32_t planes = 1u;
+    if (p.use_planes) {
+      planes = m.plane_mask[slot];
+      if (lane == 0) m.plane_mask[slot] = 0u;
+    }
+    float4* v4 = reinterpret_cast<float4*>(m.values + (size_t)slot * kLeafVoxels);
+    uint32_t* act = m.active + (size_t)slot * kActiveWords;
+    float4 v[4];
+    uint32_t anib[4];
+#pragma unroll
+    for (int k = 0; k < 4; ++k) {
+      const int q = lane + 32 * k;
+      v[k] = v4[q];
+      anib[k] = (act[q >> 3] >> ((q & 7) * 4)) & 0xFu;
+    }
+    uint32_t touched_any[4] = {0u, 0u, 0u, 0u};
+    while (planes) {
+      const int pl = __ffs(planes) - 1;
+      planes &= planes - 1u;
+      uint32_t* lab = m.labels + ((size_t)pl * m.capacity + slot) * kLabelWords;
+      const uint32_t myw = lab[lane];
+      if (myw) lab[lane] = 0u;
+      if (fatal) continue;
+      const float lh = p.lh[pl], lm = p.lm[pl];
+#pragma unroll
+      for (int k = 0; k < 4; ++k) {
+        const int q = lane + 32 * k;
+        const int w = q >> 3;
+        const int sh = (q & 7) * 4;
+        const uint32_t hn = (__shfl_sync(kFull, myw, w) >> sh) & 0xFu;
+        const uint32_t mn = (__shfl_sync(kFull, myw, 16 + w) >> sh) & 0xFu;
+        const uint32_t tn = hn | mn;
+        if (tn) {
+          touched_any[k] |= tn;
+          uint32_t a0 = anib[k] & 1u, a1 = (anib[k] >> 1) & 1u, a2 = (anib[k] >> 2) & 1u,
+                   a3 = (anib[k] >> 3) & 1u;
+          if (tn & 1u) v[k].x = update_voxel<RM>(v[k].x, a0, (hn & 1u) ? lh : lm, p);
+          if (tn & 2u) v[k].y = update_voxel<RM>(v[k].y, a1, (hn & 2u) ? lh : lm, p);
+          if (tn & 4u) v[k].z = update_voxel<RM>(v[k].z, a2, (hn & 4u) ? lh : lm, p);
+          if (tn & 8u) v[k].w = update_voxel<RM>(v[k].w, a3, (hn & 8u) ? lh : lm, p);
+          anib[k] = a0 | (a1 << 1) | (a2 << 2) | (a3 << 3);
+        }
+      }
+    }
+    if (fatal) continue;
+#pragma unroll
+    for (int k = 0; k < 4; ++k) {
+      const int q = lane + 32 * k;
+      if (touched_any[k]) {
+        v4[q] = v[k];
+        uniq += (unsigned)__popc(touched_any[k]);
+      }
+      // rebuild active word q>>3 from the 8 nibbles of lanes 8j..8j+7
+      uint32_t word = anib[k] << ((q & 7) * 4);
+      word |= __shfl_xor_sync(kFull, word, 1);
+      word |= __shfl_xor_sync(kFull, word, 2);
+      word |= __shfl_xor_sync(kFull, word, 4);
+      uint32_t any = touched_any[k];
+      any |= __shfl_xor_sync(kFull, any, 1);
+      any |= __shfl_xor_sync(kFull, any, 2);
+      any |= __shfl_xor_sync(kFull, any, 4);
+      if ((lane & 7) == 0 && any) act[q >> 3] = word;
+    }
+  }
+  integrate_epilogue(m.ctr, n, uniq);
+}
+
+template <int RM>
+__global__ void __launch_bounds__(256) k_integrate_count(MapView m, IntegrateParams p) {
+  const int lane = threadIdx.x & 31;
+  const uint32_t gw = (blockIdx.x * blockDim.x + threadIdx.x) >> 5;
+  const uint32_t nw = (gridDim.x * blockDim.x) >> 5;
+  const uint32_t n = *(volatile unsigned int*)&m.ctr->touched_count;
+  const bool fatal = (*(volatile unsigned int*)&m.ctr->error_flags & kErrProbe) != 0u;
+  unsigned long long uniq = 0;
+  const float lh = p.lh[0], lm = p.lm[0];
+  for (uint32_t i = gw; i < n; i += nw) {
+    const uint32_t slot = m.touched[i];
+    uint32_t* cnt = m.counts + (size_t)slot * 1024;
+    float* val = m.values + (size_t)slot * kLeafVoxels;
+    uint32_t* act = m.active + (size_t)slot * kActiveWords;
+    for (int j = 0; j < 16; ++j) {
+      const int l = j * 32 + lane;
+      const uint32_t nh = cnt[l], nm_ = cnt[512 + l];
+      uint32_t abit = (act[j] >> lane) & 1u;
+      const bool t = (nh | nm_) != 0u;
+      if (t) {
+        cnt[l] = 0u;
+        cnt[512 + l] = 0u;
+        if (!fatal) {
+          const float temp = Ar<RM>::fadd(Ar<RM>::fmul((float)nm_, lm), Ar<RM>::fmul((float)nh, lh));
+          val[l] = update_voxel<RM>(val[l], abit, temp, p);
+          uniq += 1;
+        }
+      }
+      const uint32_t word = __ballot_sync(kFull, abit != 0u);
+      if (!fatal && __ballot_sync(kFull, t) != 0u && lane == 0) act[j] = word;
+    }
+  }
+  integrate_epilogue(m.ctr, n, uniq);
+}
+
+// ---- growth, export --------------------------------------------------------------------------
+
+__global__ void k_fill_keys(unsigned long long* keys, uint32_t n) {
+  for (uint32_t i = blockIdx.x * blockDim.x + threadIdx.x; i < n; i += gridDim.x * blockDim.x)
+    keys[i] = kEmptyKey;
+}
+
+// Move every leaf (values, active bits, pending labels and counts) to the larger table and
+// rebuild the touched list of the current epoch.
+__global__ void __launch_bounds__(256) k_rehash(MapView from, MapView to, uint32_t cur_epoch,
+                                                int with_counts) {
+  const int lane = threadIdx.x & 31;
+  const uint32_t gw = (blockIdx.x * blockDim.x + threadIdx.x) >> 5;
+  const uint32_t nw = (gridDim.x * blockDim.x) >> 5;
+  for (uint32_t s = gw; s < from.capacity; s += nw) {
+    const unsigned long long key = from.keys[s];
+    if (key == kEmptyKey) continue;
+    int d = -1;
+    if (lane == 0) d = map_find_or_insert(to, key);
+    d = __shfl_sync(kFull, d, 0);
+    if (d < 0) continue;
+    const float4* sv = reinterpret_cast<const float4*>(from.values + (size_t)s * kLeafVoxels);
+    float4* dv = reinterpret_cast<float4*>(to.values + (size_t)d * kLeafVoxels);
+    for (int q = lane; q < 128; q += 32) dv[q] = sv[q];
+    if (lane < kActiveWords)
+      to.active[(size_t)d * kActiveWords + lane] = from.active[(size_t)s * kActiveWords + lane];
+    for (int pl = 0; pl < from.planes; ++pl)
+      to.labels[((size_t)pl * to.capacity + d) * kLabelWords + lane] =
+          from.labels[((size_t)pl * from.capacity + s) * kLabelWords + lane];
+    if (with_counts)
+      for (int c = lane; c < 1024; c += 32)
+        to.counts[(size_t)d * 1024 + c] = from.counts[(size_t)s * 1024 + c];
+    if (lane == 0) {
+      const uint32_t ep = from.epoch[s];
+      to.epoch[d] = ep;
+      if (from.plane_mask) to.plane_mask[d] = from.plane_mask[s];
+      if (ep == cur_epoch) {
+        const uint32_t i = atomicAdd(&to.ctr->touched_count, 1u);
+        to.touched[i] = (uint32_t)d;
+      }
+    }
+  }
+}
+
+__global__ void __launch_bounds__(256) k_export(MapView m, int32_t* origins, float* values,
+                                                uint32_t* active, uint32_t* n_out,
+                                                uint32_t max_out) {
+  const int lane = threadIdx.x & 31;
+  const uint32_t gw = (blockIdx.x * blockDim.x + threadIdx.x) >> 5;
+  const uint32_t nw = (gridDim.x * blockDim.x) >> 5;
+  for (uint32_t s = gw; s < m.capacity; s += nw) {
+    const unsigned long long key = m.keys[s];
+    if (key == kEmptyKey) continue;
+    uint32_t o = 0;
+    if (lane == 0) o = atomicAdd(n_out, 1u);
+    o = __shfl_sync(kFull, o, 0);
+    if (o >= max_out) continue;
+    if (origins && lane == 0) {
+      int lx, ly, lz;
+      key_leaf(key, &lx, &ly, &lz);
+      origins[3 * (size_t)o] = lx * 8;
+      origins[3 * (size_t)o + 1] = ly * 8;
+      origins[3 * (size_t)o + 2] = lz * 8;
+    }
+    if (values)
+      for (int q = lane; q < kLeafVoxels; q += 32)
+        values[(size_t)o * kLeafVoxels + q] = m.values[(size_t)s * kLeafVoxels + q];
+    if (active && lane < kActiveWords)
+      active[(size_t)o * kActiveWords + lane] = m.active[(size_t)s * kActiveWords + lane];
+  }
+}
+
+__global__ void __launch_bounds__(256) k_export_labels(MapView m, int plane, int32_t* origins,
+                                                       uint32_t* words, uint32_t* n_out,
+                                                       uint32_t max_out) {
+  const int lane = threadIdx.x & 31;
+  const uint32_t gw = (blockIdx.x * blockDim.x + threadIdx.x) >> 5;
+  const uint32_t nw = (gridDim.x * blockDim.x) >> 5;
+  for (uint32_t s = gw; s < m.capacity; s += nw) {
+    const unsigned long long key = m.keys[s];
+    if (key == kEmptyKey) continue;
+    const uint32_t w = m.labels[((size_t)plane * m.capacity + s) * kLabelWords + lane];
+    if (__ballot_sync(kFull, w != 0u) == 0u) continue;
+    uint32_t o = 0;
+    if (lane == 0) o = atomicAdd(n_out, 1u);
+    o = __shfl_sync(kFull, o, 0);
+    if (o >= max_out) continue;
+    if (lane == 0) {
+      int lx, ly, lz;
+      key_leaf(key, &lx, &ly, &lz);
+      origins[3 * (size_t)o] = lx * 8;
+      origins[3 * (size_t)o + 1] = ly * 8;
+      origins[3 * (size_t)o + 2] = lz * 8;
+    }
+    words[(size_t)o * kLabelWords + lane] = w;
+  }
+}
+
+}  // namespace
+
+cudaError_t launch_traverse(const FrameParams& f, const MapView& m, int update_mode, int rounding,
+                            int tile_w, int tile_h, int smem_entries, cudaStream_t s) {
+  const int tiles_x = (f.width + tile_w - 1) / tile_w;
+  const int tiles_y = (f.height + tile_h - 1) / tile_h;
+  const dim3 grid(tiles_x * tiles_y), block(tile_w * tile_h);
+  if (update_mode == NM_UPDATE_LABEL) {
+    const size_t smem = (size_t)smem_entries * (8 + kLabelWords * 4);
+    const uint32_t smask = (uint32_t)smem_entries - 1u;
+    if (rounding == NM_ROUND_DOWN) {
+      k_traverse_label<NM_ROUND_DOWN><<<grid, block, smem, s>>>(f, m, tiles_x, tile_w, tile_h, smask);
+    } else {
+      k_traverse_label<NM_ROUND_NEAREST><<<grid, block, smem, s>>>(f, m, tiles_x, tile_w, tile_h, smask);
+    }
+  } else {
+    if (rounding == NM_ROUND_DOWN) {
+      k_traverse_count<NM_ROUND_DOWN><<<grid, block, 0, s>>>(f, m, tiles_x, tile_w, tile_h);
+    } else {
+      k_traverse_count<NM_ROUND_NEAREST><<<grid, block, 0, s>>>(f, m, tiles_x, tile_w, tile_h);
+    }
+  }
+  return cudaGetLastError();
+}
+
+cudaError_t launch_integrate(const MapView& m, const IntegrateParams& p, int update_mode,
+                             int rounding, int sm_count, cudaStream_t s) {
+  const dim3 grid(sm_count * 8), block(256);
+  if (update_mode == NM_UPDATE_LABEL) {
+    if (rounding == NM_ROUND_DOWN)
+      k_integrate_label<NM_ROUND_DOWN><<<grid, block, 0, s>>>(m, p);
+    else
+      k_integrate_label<NM_ROUND_NEAREST><<<grid, block, 0, s>>>(m, p);
+  } else {
+    if (rounding == NM_ROUND_DOWN)
+      k_integrate_count<NM_ROUND_DOWN><<<grid, block, 0, s>>>(m, p);
+    else
+      k_integrate_count<NM_ROUND_NEAREST><<<grid, block, 0, s>>>(m, p);
+  }
+  return cudaGetLastError();
+}
+
+cudaError_t launch_rehash(const MapView& from, const MapView& to, uint32_t cur_epoch,
+                          int update_mode, cudaStream_t s) {
+  k_rehash<<<1184, 256, 0, s>>>(from, to, cur_epoch, update_mode == NM_UPDATE_ACCUMULATE ? 1 : 0);
+  return cudaGetLastError();
+}
+
+cudaError_t launch_export(const MapView& m, int32_t* origins, float* values, uint32_t* active,
+                          uint32_t* n_out, uint32_t max_out, cudaStream_t s) {
+  k_export<<<1184, 256, 0, s>>>(m, origins, values, active, n_out, max_out);
+  return cudaGetLastError();
+}
+
+cudaError_t launch_export_labels(const MapView& m, int plane, int32_t* origins, uint32_t* words,
+                                 uint32_t* n_out, uint32_t max_out, cudaStream_t s) {
+  k_export_labels<<<1184, 256, 0, s>>>(m, plane, origins, words, n_out, max_out);
+  return cudaGetLastError();
+}
+
+cudaError_t launch_fill_keys(unsigned long long* keys, uint32_t n, cudaStream_t s) {
+  k_fill_keys<<<1184, 256, 0, s>>>(keys, n);
+  return cudaGetLastError();
+}
+
+}  // namespace nm

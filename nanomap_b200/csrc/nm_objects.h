@@ -1,0 +1,81 @@
+// nm_objects.h -- definitions of the opaque C ABI objects and the error helpers shared by the
+// host translation units.
+#pragma once
+
+#include <cfenv>
+#include <cstdarg>
+#include <cstdio>
+#include <string>
+
+#include "nm_internal.h"
+#include "nm_sim.h"
+
+namespace nm {
+
+// Record a failure message for nm_last_error() and return `code`.
+int fail(int code, const char* fmt, ...);
+const char* last_error();
+
+struct RoundScope {
+  int saved;
+  explicit RoundScope(int rounding) : saved(std::fegetround()) {
+    std::fesetround(rounding == NM_ROUND_DOWN ? FE_DOWNWARD : FE_TONEAREST);
+  }
+  ~RoundScope() { std::fesetround(saved); }
+};
+
+}  // namespace nm
+
+#define NM_CUDA(call)                                                                    \
+  do {                                                                                   \
+    const cudaError_t e_ = (call);                                                       \
+    if (e_ != cudaSuccess)                                                               \
+      return nm::fail(NM_ERR_CUDA, "%s failed: %s (%s:%d)", #call, cudaGetErrorString(e_), \
+                      __FILE__, __LINE__);                                               \
+  } while (0)
+
+// ---- object definitions ---------------------------------------------------------------------
+
+struct nm_context_s {
+  int device = 0;
+  int sm_count = 148;
+  cudaStream_t stream = nullptr;
+  float* render_staging = nullptr;
+  size_t render_staging_bytes = 0;
+};
+
+struct nm_sensor_s {
+  nm_context ctx = nullptr;
+  nm_sensor_desc desc{};
+  float fp[6] = {0, 0, 0, 0, 0, 0};
+  float lh = 0.f, lm = 0.f;
+  float* d_tables = nullptr;  // laser: sinu[W], cosu[W], sinv[H], cosv[H]
+};
+
+struct nm_map_s {
+  nm_context ctx = nullptr;
+  nm_map_desc desc{};
+  nm::MapView view{};
+  nm::MapCounters* d_ctr = nullptr;
+  uint32_t epoch = 1;
+  uint64_t known_leaves = 0;
+  uint64_t pending_bound = 0;
+  uint32_t grow_count = 0;
+  bool pending_labels = false;
+  float pending_lh[nm::kMaxPlanes];
+  float pending_lm[nm::kMaxPlanes];
+  uint32_t pending_planes = 0;
+  unsigned char* staging = nullptr;  // device copy of host input
+  size_t staging_bytes = 0;
+  uint32_t* d_scratch_u32 = nullptr;  // export counters
+  int tile_w = 16, tile_h = 16, smem_entries = 128;
+};
+
+struct nm_simmap_s {
+  nm_context ctx = nullptr;
+  nm::SimMapView view{};
+  int32_t bbox[6] = {0, 0, 0, -1, -1, -1};
+  uint64_t active_voxels = 0;
+  uint64_t leaves = 0;
+};
+

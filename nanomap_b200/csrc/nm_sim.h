@@ -1,0 +1,54 @@
+// nm_sim.h -- simulation-map structures shared by the host code and the sm_100a kernels.
+#pragma once
+
+#include <climits>
+#include <cstdint>
+#include <cuda_runtime.h>
+
+#include "../../include/nanomap_b200.h"
+
+namespace nm {
+
+// Build state: a dense leaf-major bit buffer over the leaf box (16 words per leaf).
+struct SimBuild {
+  float res;
+  int32_t vmin[3], vmax[3];  // voxel region [vmin, vmax)
+  int32_t llo[3], ldim[3];   // leaf box origin (leaf coordinates) and size
+  uint32_t* dense;
+};
+
+struct SimMapView {
+  float res;
+  int32_t any;
+  int32_t llo[3], ldim[3];   // leaf box
+  int32_t blo[3], bdim[3];   // brick box (64^3-voxel bricks)
+  int32_t* leaf_index;       // ldim product entries, -1 = empty leaf
+  uint32_t* leaf_words;      // 16 words per non-empty leaf
+  uint32_t* brick_bits;      // one bit per brick
+  float box_lo[3], box_hi[3];  // active voxel box in index space, [amin, amax + 1]
+};
+
+struct SimRayParams {
+  int32_t type, width, height, pad;
+  float hw, hh, c0, c1, su, sv;
+  const float* sinu;
+  const float* cosu;
+  const float* sinv;
+  const float* cosv;
+  float R[9];
+  float pos[3];
+  float min_range, max_range;
+};
+
+cudaError_t launch_voxelize(const SimBuild& b, const double* d_boxes, int nb, const double* d_cyl,
+                            int nc, cudaStream_t s);
+cudaError_t launch_set_voxels(const SimBuild& b, const int32_t* d_ijk, long long n, cudaStream_t s);
+cudaError_t launch_compact(const SimBuild& b, const SimMapView& v, uint32_t* d_count, int pass2,
+                           int32_t* d_bbox, unsigned long long* d_nvox, cudaStream_t s);
+cudaError_t launch_fill_i32(int32_t* p, long long n, int32_t val, cudaStream_t s);
+cudaError_t launch_sim_render(const SimMapView& v, const SimRayParams& rp, float* out,
+                              cudaStream_t s);
+cudaError_t launch_noise(float* r, long long n, float sigma_coef, float drop, uint64_t seed,
+                         cudaStream_t s);
+
+}  // namespace nm

@@ -1,0 +1,172 @@
+"""GPU parity of the mapping path against the CPU oracle, through the C ABI.
+
+Labels (traversed voxel sets and hit/miss/untouched per voxel) and the integrated map
+(log-odds and active bits) must be bit-identical to the oracle on the same inputs.
+"""
+import numpy as np
+import pytest
+
+from nanomap_b200 import _native as N
+from nanomap_b200 import api as A
+from oracle import oracle as O
+from tests.workloads import (compare_labels, compare_maps, oracle_frame, plain_small_frames)
+
+pytestmark = pytest.mark.gpu
+
+
+@pytest.fixture(scope="module")
+def small():
+    return plain_small_frames(n=10)
+
+
+def _torch(a):
+    import torch
+    return torch.from_numpy(np.ascontiguousarray(a)).cuda()
+
+
+@pytest.mark.parametrize("rounding", [N.NM_ROUND_DOWN, N.NM_ROUND_NEAREST])
+def test_labels_and_map_bit_exact_plain_small(ctx, small, rounding):
+    spec, scene, desc, frames = small
+    res = spec.map_res
+    sensor = A.Sensor(ctx, desc)
+    m = A.Map(ctx, A.map_desc(res=res, rounding=rounding, clamp_min=spec.clamp[0],
+                              clamp_max=spec.clamp[1]))
+    om = O.Map(res, clamp_min=spec.clamp[0], clamp_max=spec.clamp[1], rounding=rounding)
+    osen = O.Sensor.from_desc(desc)
+    for i, (pose, ranges) in enumerate(frames):
+        m.insert_ranges(sensor, pose, _torch(ranges), flags=N.NM_DEFER_INTEGRATE)
+        gl = m.export_labels()
+        R, eye, mt = oracle_frame(desc, pose, res, rounding)
+        om.insert(R, eye, mt, desc.log_odds_hit, desc.log_odds_miss, osen.points(ranges),
+                  keep_labels=True)
+        errs = compare_labels(gl, om.labels())
+        assert not errs, f"frame {i}: " + "; ".join(errs[:5])
+        m.integrate()
+    errs = compare_maps(m.export(), om.export())
+    assert not errs, "; ".join(errs[:5])
+    st, ost = m.stats(), om.stats()
+    assert st["visits"] == ost["visits"] and st["rays"] == ost["rays"]
+    assert st["unique_voxels"] == ost["unique_voxels"]
+    assert st["frames"] == len(frames) and st["error_flags"] == 0
+
+
+def test_xyz_records_host_and_device_inputs(ctx, small):
+    """insertPointCloud-style input: width*height records of `step` bytes, xyz at 0/4/8."""
+    spec, scene, desc, frames = small
+    res = spec.map_res
+    sensor = A.Sensor(ctx, desc)
+    osen = O.Sensor.from_desc(desc)
+    m_host = A.Map(ctx, A.map_desc(res=res))
+    m_dev = A.Map(ctx, A.map_desc(res=res))
+    om = O.Map(res)
+    H, W = spec.height, spec.width
+    for i, (pose, ranges) in enumerate(frames[:4]):
+        pts = osen.points(ranges)
+        rec = np.zeros((H * W, 5), np.float32)  # step 20 bytes, like the reference's Point AoS
+        rec[:, :3] = pts
+        rec[:, 3] = 7.0
+        m_host.insert_points(sensor, pose, rec, W, H, 20)
+        m_dev.insert_points(sensor, pose, _torch(rec), W, H, 20)
+        R, eye, mt = oracle_frame(desc, pose, res, 1)
+        om.insert(R, eye, mt, desc.log_odds_hit, desc.log_odds_miss, pts)
+    oe = om.export()
+    assert not compare_maps(m_host.export(), oe)
+    assert not compare_maps(m_dev.export(), oe)
+
+
+@pytest.mark.parametrize("clamp_mode", [N.NM_CLAMP_ALWAYS, N.NM_CLAMP_ON_CROSSING])
+def test_accumulate_mode_and_clamp_orders(ctx, small, clamp_mode):
+    spec, scene, desc, frames = small
+    res = spec.map_res
+    sensor = A.Sensor(ctx, desc)
+    osen = O.Sensor.from_desc(desc)
+    kw = dict(clamp_min=-1.0, clamp_max=1.5, thres_hit=0.3, thres_miss=-0.2)
+    m = A.Map(ctx, A.map_desc(res=res, update_mode=N.NM_UPDATE_ACCUMULATE, clamp_mode=clamp_mode, **kw))
+    om = O.Map(res, update_mode=1, clamp_mode=clamp_mode, **kw)
+    for pose, ranges in frames[:5]:
+        m.insert_ranges(sensor, pose, _torch(ranges))
+        R, eye, mt = oracle_frame(desc, pose, res, 1)
+        om.insert(R, eye, mt, desc.log_odds_hit, desc.log_odds_miss, osen.points(ranges))
+    errs = compare_maps(m.export(), om.export())
+    assert not errs, "; ".join(errs[:5])
+
+
+def test_edge_points_nan_inf_zero_and_range(ctx):
+    """Invalid points are dropped exactly as the oracle drops them."""
+    desc = A.sensor_desc(hres=8, vres=8, max_range=2.0, explicit_log_odds=1,
+                         log_odds_hit=0.85, log_odds_miss=-0.4)
+    sensor = A.Sensor(ctx, desc)
+    res = 0.05
+    pose = A.Pose((0.05, -0.025, 0.0), (1, 0, 0, 0))
+    rng = np.random.default_rng(5)
+    pts = rng.normal(0, 1.0, (64, 3)).astype(np.float32)
+    pts[0] = np.nan
+    pts[1] = np.inf
+    pts[2] = 0.0
+    pts[3] = (2.0, 0.0, 0.0)     # exactly max range: dropped
+    pts[4] = (1.999, 0.0, 0.0)   # end voxel leaves past max range: misses only
+    pts[5] = (0.0, 0.0, 1e-9)    # below the shortest direction: dropped
+    pts[6] = (-0.01, 0.0, 0.0)   # inside the eye voxel
+    pts[7] = (0.0, 0.7, -0.0)    # axis-aligned
+    m = A.Map(ctx, A.map_desc(res=res))
+    m.insert_points(sensor, pose, pts, 8, 8, 12, flags=N.NM_SYNC)
+    om = O.Map(res)
+    R, eye, mt = oracle_frame(desc, pose, res, 1)
+    om.insert(R, eye, mt, 0.85, -0.4, pts)
+    assert not compare_maps(m.export(), om.export())
+    assert m.stats()["rays"] == om.stats()["rays"]
+
+
+def test_empty_and_all_invalid_frames(ctx):
+    desc = A.sensor_desc(hres=4, vres=4, max_range=5.0)
+    sensor = A.Sensor(ctx, desc)
+    m = A.Map(ctx, A.map_desc(res=0.1))
+    m.insert_points(sensor, A.Pose(), np.zeros((0, 3), np.float32), 0, 0, 12, flags=N.NM_SYNC)
+    bad = np.full((16, 3), np.nan, np.float32)
+    m.insert_points(sensor, A.Pose(), bad, 4, 4, 12, flags=N.NM_SYNC)
+    st = m.stats()
+    assert st["rays"] == 0 and st["leaf_count"] == 0 and st["error_flags"] == 0
+
+
+def test_table_growth_keeps_results(ctx, small):
+    """A tiny initial table grows (rehash) during the run without changing the result."""
+    spec, scene, desc, frames = small
+    res = 0.05
+    sensor = A.Sensor(ctx, desc)
+    osen = O.Sensor.from_desc(desc)
+    m = A.Map(ctx, A.map_desc(res=res, initial_leaf_capacity=1024))
+    om = O.Map(res)
+    for pose, ranges in frames:
+        m.insert_ranges(sensor, pose, _torch(ranges))
+        R, eye, mt = oracle_frame(desc, pose, res, 1)
+        om.insert(R, eye, mt, desc.log_odds_hit, desc.log_odds_miss, osen.points(ranges))
+    st = m.stats()
+    assert st["grow_count"] >= 1 and st["error_flags"] == 0
+    assert not compare_maps(m.export(), om.export())
+
+
+def test_repeat_runs_are_bit_identical(ctx, small):
+    spec, scene, desc, frames = small
+    sensor = A.Sensor(ctx, desc)
+    outs = []
+    for _ in range(2):
+        m = A.Map(ctx, A.map_desc(res=0.05))
+        for pose, ranges in frames[:3]:
+            m.insert_ranges(sensor, pose, _torch(ranges))
+        o, v, a = m.export()
+        idx = np.lexsort((o[:, 2], o[:, 1], o[:, 0]))
+        outs.append((o[idx], v[idx], a[idx]))
+        m.close()
+    assert all(np.array_equal(x, y) for x, y in zip(outs[0], outs[1]))
+
+
+def test_bad_arguments(ctx):
+    desc = A.sensor_desc(hres=4, vres=4)
+    sensor = A.Sensor(ctx, desc)
+    m = A.Map(ctx, A.map_desc(res=0.1))
+    with pytest.raises(N.NanomapError):
+        m.insert_points(sensor, A.Pose(), np.zeros((16, 3), np.float32), 4, 4, 8)
+    with pytest.raises(N.NanomapError):
+        m.insert_ranges(sensor, A.Pose((1e9, 0, 0), (1, 0, 0, 0)), np.ones(16, np.float32))
+    with pytest.raises(N.NanomapError):
+        A.Map(ctx, A.map_desc(res=0.1, max_agents=0))

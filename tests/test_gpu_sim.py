@@ -1,0 +1,125 @@
+"""GPU parity of the simulation map (voxelisation) and simulated range images against the
+CPU oracle, through the C ABI.  Both are integer / first-hit results and must be identical."""
+import numpy as np
+import pytest
+
+from nanomap_b200 import _native as N
+from nanomap_b200 import api as A
+from nanomap_b200 import scenes as S
+from oracle import oracle as O
+from tests.workloads import camera_desc
+
+pytestmark = pytest.mark.gpu
+
+
+def _sorted_leaves(o, w):
+    idx = np.lexsort((o[:, 2], o[:, 1], o[:, 0]))
+    return o[idx], w[idx]
+
+
+def _maps(ctx, name, seed=1):
+    sc = S.make_scene(name, seed)
+    sp = sc.spec
+    g = A.SimMap(ctx, sp.sim_res, boxes=sc.boxes, cylinders=sc.cylinders, vox_min=sc.vox_min,
+                 vox_max=sc.vox_max)
+    o = O.SimMap(sp.sim_res, sc.vox_min, sc.vox_max, sc.boxes, sc.cylinders)
+    return sc, g, o
+
+
+@pytest.mark.parametrize("name", ["plain_small", "sim_headline"])
+def test_voxelisation_matches_oracle(ctx, name):
+    sc, g, o = _maps(ctx, name)
+    gb, gn, gl = g.info()
+    ob, oany = o.bbox()
+    assert oany and gb == ob
+    assert gn == o.count()
+    go, gw = _sorted_leaves(*g.export())
+    oo, ow = o.export()
+    assert gl == len(oo)
+    assert np.array_equal(go, oo)
+    assert np.array_equal(gw, ow)
+
+
+def test_voxel_list_constructor(ctx):
+    rng = np.random.default_rng(3)
+    vox = rng.integers(-40, 40, size=(5000, 3)).astype(np.int32)
+    g = A.SimMap(ctx, 0.05, voxels=vox)
+    o = O.SimMap(0.05, voxels=vox)
+    go, gw = _sorted_leaves(*g.export())
+    oo, ow = o.export()
+    assert np.array_equal(go, oo) and np.array_equal(gw, ow)
+    assert g.info()[0] == o.bbox()[0]
+
+
+@pytest.mark.parametrize("name,n", [("plain_small", 6), ("sim_headline", 2)])
+def test_render_matches_oracle(ctx, name, n):
+    import torch
+    sc, g, o = _maps(ctx, name)
+    sp = sc.spec
+    desc = camera_desc(sp, min_range=0.1)
+    sensor = A.Sensor(ctx, desc)
+    osen = O.Sensor.from_desc(desc)
+    for pos, q in S.trajectory(sc, n, seed=9):
+        pose = A.Pose(pos, q)
+        out = torch.zeros(sp.height, sp.width, device="cuda")
+        g.render(sensor, pose, out)
+        host = np.zeros((sp.height, sp.width), np.float32)
+        g.render(sensor, pose, host)
+        R = O.rotation(q, list(desc.frame_transform))
+        ref = o.render(osen, pos, R)
+        got = out.cpu().numpy()
+        assert np.array_equal(got.view(np.uint32), host.view(np.uint32))
+        diff = np.nonzero(got.view(np.uint32) != ref.view(np.uint32))
+        assert len(diff[0]) == 0, f"{len(diff[0])} pixels differ, e.g. {got[diff][:4]} vs {ref[diff][:4]}"
+        assert (ref > 0).mean() > 0.3
+
+
+def test_laser_render_matches_oracle(ctx):
+    import torch
+    sc, g, o = _maps(ctx, "plain_small")
+    desc = A.sensor_desc(type=N.NM_SENSOR_LASER, hres=1024, vres=64, hfov_deg=360.0,
+                         vfov_deg=30.0, max_range=20.0, min_range=0.2,
+                         frame_transform=S.OPTICAL_TO_BODY)
+    sensor = A.Sensor(ctx, desc)
+    osen = O.Sensor.from_desc(desc)
+    for pos, q in S.trajectory(sc, 3, seed=4):
+        out = torch.zeros(64, 1024, device="cuda")
+        g.render(sensor, A.Pose(pos, q), out)
+        ref = o.render(osen, pos, O.rotation(q, list(desc.frame_transform)))
+        assert np.array_equal(out.cpu().numpy().view(np.uint32), ref.view(np.uint32))
+
+
+def test_render_outside_and_empty_maps(ctx):
+    import torch
+    desc = A.sensor_desc(hres=32, vres=24, hfov_deg=87, vfov_deg=58, max_range=10.0)
+    sensor = A.Sensor(ctx, desc)
+    empty = A.SimMap(ctx, 0.1, voxels=np.zeros((0, 3), np.int32))
+    out = torch.full((24, 32), 7.0, device="cuda")
+    empty.render(sensor, A.Pose((1, 2, 3), (1, 0, 0, 0)), out)
+    assert float(out.abs().max()) == 0.0
+    # eye far outside a small box of voxels, looking away and towards it
+    vox = np.array([[i, j, k] for i in range(4) for j in range(4) for k in range(4)], np.int32)
+    g = A.SimMap(ctx, 0.1, voxels=vox)
+    o = O.SimMap(0.1, voxels=vox)
+    osen = O.Sensor.from_desc(desc)
+    for q in [(1, 0, 0, 0), (0, 0, 0, 1), (0.7071, 0, 0, 0.7071), (0.5, 0.5, 0.5, 0.5)]:
+        for pos in [(-1.0, 0.2, 0.2), (0.2, 0.2, 0.2), (5.0, 5.0, 5.0)]:
+            out = torch.zeros(24, 32, device="cuda")
+            g.render(sensor, A.Pose(pos, q), out)
+            ref = o.render(osen, pos, O.rotation(q, list(desc.frame_transform)))
+            assert np.array_equal(out.cpu().numpy().view(np.uint32), ref.view(np.uint32))
+
+
+def test_noise_is_seeded(ctx):
+    import torch
+    r = torch.full((480, 640), 3.0, device="cuda")
+    a, b, c = r.clone(), r.clone(), r.clone()
+    ctx.add_noise(a, 0.005, 0.02, 11)
+    ctx.add_noise(b, 0.005, 0.02, 11)
+    ctx.add_noise(c, 0.005, 0.02, 12)
+    torch.cuda.synchronize()
+    assert torch.equal(a, b) and not torch.equal(a, c)
+    dropped = float((a == 0).float().mean())
+    assert 0.01 < dropped < 0.03
+    kept = a[a > 0] - 3.0
+    assert abs(float(kept.std()) - 0.005 * 9.0) < 0.005
