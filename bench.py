@@ -234,7 +234,7 @@ def run_ours(args, rank, world, local):
     sim = A.SimMap(ctx, spec.sim_res, boxes=scene.boxes, cylinders=scene.cylinders,
                    vox_min=scene.vox_min, vox_max=scene.vox_max)
     mdesc = A.map_desc(res=spec.map_res, clamp_min=spec.clamp[0], clamp_max=spec.clamp[1],
-                       rounding=N.NM_ROUND_DOWN, initial_leaf_capacity=1 << 21)
+                       rounding=N.NM_ROUND_DOWN, initial_leaf_capacity=1 << args.capacity_log2)
     m = A.Map(ctx, mdesc)
     stream = torch.cuda.current_stream(dev)
     H, W = spec.height, spec.width
@@ -393,6 +393,8 @@ def main():
     ap.add_argument("--impl", choices=["ours", "reference"], default="ours")
     ap.add_argument("--e2e-steps", type=int, default=30)
     ap.add_argument("--cpu-baseline-s", type=float, default=12.0)
+    ap.add_argument("--capacity-log2", type=int, default=21,
+                    help="initial leaf-table capacity (log2 slots); smaller for profiling runs")
     args = ap.parse_args()
     if args.warmup < 3:
         args.warmup = 3

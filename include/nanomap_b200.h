@@ -60,6 +60,7 @@ typedef struct nm_context_s* nm_context;
 typedef struct nm_sensor_s* nm_sensor;
 typedef struct nm_map_s* nm_map;
 typedef struct nm_simmap_s* nm_simmap;
+typedef struct nm_tick_plan_s* nm_tick_plan;
 
 /* nanomap::Pose (nanomap.h:20-28): position (m) and unit quaternion (w, x, y, z). */
 typedef struct {
@@ -151,6 +152,12 @@ int nm_map_insert_points(nm_map m, nm_sensor s, const nm_pose* pose, const void*
 int nm_map_insert_ranges(nm_map m, nm_sensor s, const nm_pose* pose, const float* ranges,
                          uint32_t flags, void* stream);
 
+/* Launch shape of the traversal: tile of tile_w x tile_h pixels per work item (area 64, 128
+ * or a multiple of 256 up to 4096; a CTA has min(area, 256) threads) and shared-memory
+ * leaf-table entries per CTA (power of two, 16..512).  Results do not depend on it; the autotuner picks it.  No reference
+ * counterpart (the reference launches fixed 8x8 / 512-thread grids, filterCloud.cu:482). */
+int nm_map_set_launch(nm_map m, int32_t tile_w, int32_t tile_h, int32_t leaf_table_entries);
+
 /* Apply labels left by NM_DEFER_INTEGRATE inserts. */
 int nm_map_integrate(nm_map m, void* stream);
 
@@ -159,6 +166,26 @@ int nm_map_integrate(nm_map m, void* stream);
  * (SimManager.h:100-127), which runs agents one after another. */
 int nm_map_tick(nm_map m, const nm_frame* frames, int32_t n_frames, uint32_t flags,
                 void* stream);
+
+/* Tick plans: a batched tick over fixed slots (sensor, device range buffer, agent plane),
+ * replayed as a CUDA graph each tick: upload of the per-frame constants derived from the
+ * slots' poses, one launch rendering (and noising) every slot from `sim` when it is given,
+ * one persistent traversal over all slots, and one integration of all planes in agent order.
+ * At most 32 slots.  Always integrates (no NM_DEFER_INTEGRATE).  Replaces the per-agent loop
+ * of SimManager::updateAgentViews(map) (SimManager.h:114-127). */
+int nm_tick_plan_create(nm_map m, nm_simmap sim, const nm_frame* slots, int32_t n_slots,
+                        nm_tick_plan* out);
+int nm_tick_plan_destroy(nm_tick_plan p);
+int nm_tick_plan_set_pose(nm_tick_plan p, int32_t slot, const nm_pose* pose);
+/* Range noise of rendered slots: sigma = sigma_coef * r^2, drop probability; seeded per tick. */
+int nm_tick_plan_set_noise(nm_tick_plan p, float sigma_coef, float drop_prob, uint64_t seed);
+int nm_tick_plan_set_launch(nm_tick_plan p, int32_t tile_w, int32_t tile_h, int32_t entries);
+int nm_tick_plan_run(nm_tick_plan p, uint32_t flags, void* stream);
+/* Autotuner: times candidate traversal shapes (tile, leaf-table entries) on a scratch map with
+ * the plan's slots and poses, applies the fastest to the plan, and appends it to cache_path
+ * (reused on later calls with the same device and slot shapes).  best = tile_w, tile_h,
+ * entries. */
+int nm_tick_plan_autotune(nm_tick_plan p, const char* cache_path, int32_t best[3], float* best_us);
 
 /* Leaves of the map (any order): origins (3 ints per leaf, voxel units), 512 log-odds per
  * leaf (x-major, z fastest: index x*64 + y*8 + z), 16 active-mask words per leaf.  Any output

@@ -114,7 +114,15 @@ _SIGS = {
     "nm_map_insert_points": (C.c_int, [_P, _P, C.POINTER(NmPose), _P, _I32, _I32, _I32, _U32, _P]),
     "nm_map_insert_ranges": (C.c_int, [_P, _P, C.POINTER(NmPose), _P, _U32, _P]),
     "nm_map_integrate": (C.c_int, [_P, _P]),
+    "nm_map_set_launch": (C.c_int, [_P, _I32, _I32, _I32]),
     "nm_map_tick": (C.c_int, [_P, C.POINTER(NmFrame), _I32, _U32, _P]),
+    "nm_tick_plan_create": (C.c_int, [_P, _P, C.POINTER(NmFrame), _I32, C.POINTER(_P)]),
+    "nm_tick_plan_destroy": (C.c_int, [_P]),
+    "nm_tick_plan_set_pose": (C.c_int, [_P, _I32, C.POINTER(NmPose)]),
+    "nm_tick_plan_set_noise": (C.c_int, [_P, _F, _F, _U64]),
+    "nm_tick_plan_set_launch": (C.c_int, [_P, _I32, _I32, _I32]),
+    "nm_tick_plan_run": (C.c_int, [_P, _U32, _P]),
+    "nm_tick_plan_autotune": (C.c_int, [_P, C.c_char_p, _PI32, _PF]),
     "nm_map_export": (C.c_int, [_P, _PI32, _PF, _PU32, _U64, _PU64]),
     "nm_map_export_labels": (C.c_int, [_P, _I32, _PI32, _PU32, _U64, _PU64]),
     "nm_map_frame_params": (C.c_int, [_P, _P, C.POINTER(NmPose), _PF, _PD, _PF]),

@@ -185,6 +185,9 @@ class Map:
         call("nm_map_insert_ranges", self.h, sensor.h, C.byref(pose.c()), p, flags,
              _stream(stream))
 
+    def set_launch(self, tile_w: int, tile_h: int, leaf_table_entries: int):
+        call("nm_map_set_launch", self.h, tile_w, tile_h, leaf_table_entries)
+
     def integrate(self, stream=None):
         call("nm_map_integrate", self.h, _stream(stream))
 
@@ -241,6 +244,53 @@ class Map:
     def close(self):
         if self.h:
             call("nm_map_destroy", self.h)
+            self.h = None
+
+    def __del__(self):
+        try:
+            self.close()
+        except Exception:
+            pass
+
+
+class TickPlan:
+    """A batched tick over fixed slots, replayed as a CUDA graph (nm_tick_plan_*)."""
+
+    def __init__(self, m: "Map", slots, sim: "SimMap | None" = None):
+        """slots: list of (sensor, device range tensor, agent plane)."""
+        self.map = m
+        self.slots = slots
+        arr = (N.NmFrame * len(slots))()
+        for i, (s, r, agent) in enumerate(slots):
+            arr[i].sensor = s.h
+            arr[i].ranges = C.c_void_p(r.data_ptr())
+            arr[i].agent = agent
+            arr[i].pose.orientation[0] = 1.0
+        h = C.c_void_p()
+        call("nm_tick_plan_create", m.h, sim.h if sim is not None else None, arr, len(slots), C.byref(h))
+        self.h = h
+
+    def set_pose(self, slot: int, pose: Pose):
+        call("nm_tick_plan_set_pose", self.h, slot, C.byref(pose.c()))
+
+    def set_noise(self, sigma_coef: float, drop_prob: float, seed: int):
+        call("nm_tick_plan_set_noise", self.h, C.c_float(sigma_coef), C.c_float(drop_prob), C.c_uint64(seed))
+
+    def set_launch(self, tile_w: int, tile_h: int, entries: int):
+        call("nm_tick_plan_set_launch", self.h, tile_w, tile_h, entries)
+
+    def run(self, flags: int = 0, stream=None):
+        call("nm_tick_plan_run", self.h, flags, _stream(stream))
+
+    def autotune(self, cache_path: str | None = None):
+        best = (C.c_int32 * 3)()
+        us = C.c_float()
+        call("nm_tick_plan_autotune", self.h, cache_path.encode() if cache_path else None, best, C.byref(us))
+        return tuple(best[:]), us.value
+
+    def close(self):
+        if self.h:
+            call("nm_tick_plan_destroy", self.h)
             self.h = None
 
     def __del__(self):

@@ -141,7 +141,17 @@ float logit(float p) {
 
 }  // namespace nm
 
-namespace {
+namespace nm {
+
+int check_launch_shape(int tile_w, int tile_h, int entries) {
+  const int64_t n = (int64_t)tile_w * tile_h;
+  if (tile_w <= 0 || tile_h <= 0 || n % 64 != 0 || n > 4096 || (n < 256 && (n & (n - 1)) != 0))
+    return fail(NM_ERR_ARG, "tile %dx%d: area must be 64, 128, or a multiple of 256 up to 4096",
+                tile_w, tile_h);
+  if (entries < 16 || entries > 512 || (entries & (entries - 1)) != 0)
+    return fail(NM_ERR_ARG, "leaf table entries must be a power of two in 16..512");
+  return NM_OK;
+}
 
 cudaStream_t pick(nm_context ctx, void* stream) {
   return stream ? static_cast<cudaStream_t>(stream) : ctx->stream;
@@ -387,8 +397,23 @@ int run_frame(nm_map m, nm_sensor s, nm::FrameParams& f, uint32_t flags, cudaStr
   if (rc != NM_OK) return rc;
   f.epoch = m->epoch;
   f.plane = 0;
-  NM_CUDA(nm::launch_traverse(f, m->view, m->desc.update_mode, m->desc.rounding, m->tile_w,
-                              m->tile_h, m->smem_entries, s0));
+  if (m->desc.update_mode == NM_UPDATE_LABEL) {
+    nm::TickWork<1> w;
+    std::memset(&w, 0, sizeof(w));
+    w.n_frames = 1;
+    w.tile_w = m->tile_w;
+    w.tile_h = m->tile_h;
+    w.smask = (uint32_t)m->smem_entries - 1u;
+    w.tiles_x[0] = (f.width + w.tile_w - 1) / w.tile_w;
+    const int tiles_y = (f.height + w.tile_h - 1) / w.tile_h;
+    w.tile_start[0] = 0;
+    w.tile_start[1] = (uint32_t)(w.tiles_x[0] * tiles_y);
+    w.total_tiles = w.tile_start[1];
+    w.fr[0] = f;
+    if (w.total_tiles > 0) NM_CUDA(nm::launch_traverse_labels<1>(w, m->view, m->desc.rounding, s0));
+  } else {
+    NM_CUDA(nm::launch_traverse_counts(f, m->view, m->desc.rounding, s0));
+  }
   m->pending_labels = true;
   if (!(flags & NM_DEFER_INTEGRATE)) {
     rc = do_integrate(m, s0);
@@ -398,7 +423,9 @@ int run_frame(nm_map m, nm_sensor s, nm::FrameParams& f, uint32_t flags, cudaStr
   return NM_OK;
 }
 
-}  // namespace
+}  // namespace nm
+
+using namespace nm;
 
 // ---- C ABI ----------------------------------------------------------------------------------
 extern "C" {
@@ -632,6 +659,16 @@ int nm_map_insert_ranges(nm_map m, nm_sensor s, const nm_pose* pose, const float
   return run_frame(m, s, f, flags, s0, bound);
 }
 
+int nm_map_set_launch(nm_map m, int32_t tile_w, int32_t tile_h, int32_t leaf_table_entries) {
+  if (!m) return fail(NM_ERR_ARG, "map is null");
+  const int rc = nm::check_launch_shape(tile_w, tile_h, leaf_table_entries);
+  if (rc != NM_OK) return rc;
+  m->tile_w = tile_w;
+  m->tile_h = tile_h;
+  m->smem_entries = leaf_table_entries;
+  return NM_OK;
+}
+
 int nm_map_integrate(nm_map m, void* stream) {
   if (!m) return fail(NM_ERR_ARG, "map is null");
   NM_CUDA(cudaSetDevice(m->ctx->device));
@@ -730,12 +767,52 @@ int nm_frame_params(const nm_sensor_desc* desc, const nm_pose* pose, float res, 
 }
 
 int nm_map_tick(nm_map m, const nm_frame* frames, int32_t n_frames, uint32_t flags, void* stream) {
-  (void)m;
-  (void)frames;
-  (void)n_frames;
-  (void)flags;
-  (void)stream;
-  return fail(NM_ERR_UNSUPPORTED, "nm_map_tick is not available in this build");
+  if (!m || !frames) return fail(NM_ERR_ARG, "null argument");
+  if (n_frames < 1 || n_frames > nm::kMaxTickFrames)
+    return fail(NM_ERR_ARG, "a tick takes 1..%d frames (got %d)", nm::kMaxTickFrames, n_frames);
+  if (m->desc.update_mode != NM_UPDATE_LABEL)
+    return fail(NM_ERR_UNSUPPORTED, "batched ticks run in label mode");
+  NM_CUDA(cudaSetDevice(m->ctx->device));
+  cudaStream_t s0 = pick(m->ctx, stream);
+  std::unique_ptr<nm::TickWork<nm::kMaxTickFrames>> w(new nm::TickWork<nm::kMaxTickFrames>());
+  std::memset(w.get(), 0, sizeof(*w));
+  w->n_frames = n_frames;
+  w->tile_w = m->tile_w;
+  w->tile_h = m->tile_h;
+  w->smask = (uint32_t)m->smem_entries - 1u;
+  uint64_t bound = 0;
+  for (int i = 0; i < n_frames; ++i) {
+    const nm_frame& fr = frames[i];
+    if (!fr.sensor || !fr.ranges) return fail(NM_ERR_ARG, "frame %d: null sensor or ranges", i);
+    if (fr.agent < 0 || fr.agent >= m->view.planes)
+      return fail(NM_ERR_ARG, "frame %d: agent plane %d outside 0..%d", i, fr.agent, m->view.planes - 1);
+    int rc = make_frame(m, fr.sensor, &fr.pose, &w->fr[i]);
+    if (rc != NM_OK) return rc;
+    rc = set_plane_constants(m, fr.agent, fr.sensor);
+    if (rc != NM_OK) return rc;
+    nm::FrameParams& f = w->fr[i];
+    f.input_kind = 1;
+    f.ranges = fr.ranges;
+    f.plane = fr.agent;
+    w->tiles_x[i] = (f.width + w->tile_w - 1) / w->tile_w;
+    const int ty = (f.height + w->tile_h - 1) / w->tile_h;
+    w->tile_start[i + 1] = w->tile_start[i] + (uint32_t)(w->tiles_x[i] * ty);
+    bound += frame_leaf_bound(m, fr.sensor, fr.pose, f.R, true,
+                              (uint64_t)fr.sensor->desc.hres * fr.sensor->desc.vres);
+  }
+  w->total_tiles = w->tile_start[n_frames];
+  int rc = ensure_capacity(m, bound, s0);
+  if (rc != NM_OK) return rc;
+  for (int i = 0; i < n_frames; ++i) w->fr[i].epoch = m->epoch;
+  if (w->total_tiles > 0)
+    NM_CUDA(nm::launch_traverse_labels<nm::kMaxTickFrames>(*w, m->view, m->desc.rounding, s0));
+  m->pending_labels = true;
+  if (!(flags & NM_DEFER_INTEGRATE)) {
+    rc = do_integrate(m, s0);
+    if (rc != NM_OK) return rc;
+  }
+  if (flags & NM_SYNC) return check_device_errors(m, s0);
+  return NM_OK;
 }
 
 }  // extern "C"

@@ -103,6 +103,33 @@ cudaStream_t pick(nm_context ctx, void* stream) {
 
 }  // namespace
 
+namespace nm {
+
+void make_ray_params(nm_sensor s, const nm_pose& pose, SimRayParams* rp) {
+  std::memset(rp, 0, sizeof(*rp));
+  rp->type = s->desc.type;
+  rp->width = s->desc.hres;
+  rp->height = s->desc.vres;
+  rp->hw = s->fp[0];
+  rp->hh = s->fp[1];
+  rp->c0 = s->fp[2];
+  rp->c1 = s->fp[3];
+  rp->su = s->fp[4];
+  rp->sv = s->fp[5];
+  if (s->desc.type == NM_SENSOR_LASER) {
+    rp->sinu = s->d_tables;
+    rp->cosu = s->d_tables + s->desc.hres;
+    rp->sinv = s->d_tables + 2 * s->desc.hres;
+    rp->cosv = s->d_tables + 2 * s->desc.hres + s->desc.vres;
+  }
+  pose_rotation(pose, s->desc.frame_transform, rp->R);
+  for (int a = 0; a < 3; ++a) rp->pos[a] = pose.position[a];
+  rp->min_range = s->desc.min_range;
+  rp->max_range = s->desc.max_range;
+}
+
+}  // namespace nm
+
 extern "C" {
 
 int nm_simmap_create_primitives(nm_context ctx, float res, const int32_t vox_min[3],
@@ -240,26 +267,7 @@ int nm_sim_render(nm_simmap sm, nm_sensor s, const nm_pose* pose, float* ranges,
   NM_CUDA(cudaSetDevice(ctx->device));
   cudaStream_t st = pick(ctx, stream);
   nm::SimRayParams rp;
-  std::memset(&rp, 0, sizeof(rp));
-  rp.type = s->desc.type;
-  rp.width = s->desc.hres;
-  rp.height = s->desc.vres;
-  rp.hw = s->fp[0];
-  rp.hh = s->fp[1];
-  rp.c0 = s->fp[2];
-  rp.c1 = s->fp[3];
-  rp.su = s->fp[4];
-  rp.sv = s->fp[5];
-  if (s->desc.type == NM_SENSOR_LASER) {
-    rp.sinu = s->d_tables;
-    rp.cosu = s->d_tables + s->desc.hres;
-    rp.sinv = s->d_tables + 2 * s->desc.hres;
-    rp.cosv = s->d_tables + 2 * s->desc.hres + s->desc.vres;
-  }
-  nm::pose_rotation(*pose, s->desc.frame_transform, rp.R);
-  for (int a = 0; a < 3; ++a) rp.pos[a] = pose->position[a];
-  rp.min_range = s->desc.min_range;
-  rp.max_range = s->desc.max_range;
+  nm::make_ray_params(s, *pose, &rp);
   const size_t bytes = (size_t)rp.width * rp.height * 4;
   float* dst = ranges;
   if (flags & NM_OUTPUT_HOST) {

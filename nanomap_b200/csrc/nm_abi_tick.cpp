@@ -1,0 +1,377 @@
+// nm_abi_tick.cpp -- reusable batched ticks replayed as CUDA graphs, and their autotuner.
+//
+// A tick plan fixes the frame slots of a multi-agent tick (sensor, range buffer, label plane,
+// optionally a sim map that renders the ranges).  Each tick the host derives the per-frame
+// constants from the slots' poses (the work SimManager::updateAgentViews does agent by agent,
+// SimManager.h:100-127) into pinned memory; the replayed graph copies them to the device,
+// renders and noises every slot in one launch, labels every slot in one persistent launch,
+// and integrates all label planes in agent order.  No host synchronisation inside a tick.
+#include <algorithm>
+#include <chrono>
+#include <cmath>
+#include <cstdio>
+#include <cstring>
+#include <fstream>
+#include <memory>
+#include <sstream>
+#include <string>
+#include <vector>
+
+#include "nm_host.h"
+#include "nm_objects.h"
+
+using nm::fail;
+
+namespace {
+
+struct TickStage {
+  nm::TickWork<nm::kMaxTickFrames> work;
+  nm::RenderBatch render;
+};
+
+}  // namespace
+
+struct nm_tick_plan_s {
+  nm_map map = nullptr;
+  nm_simmap sim = nullptr;
+  int n = 0;
+  nm_frame slots[nm::kMaxTickFrames];
+  bool pose_set[nm::kMaxTickFrames];
+  int noise = 0;
+  float noise_coef = 0.f, drop = 0.f;
+  uint64_t seed = 0;
+  uint64_t tick = 0;
+  TickStage* h_stage[2] = {nullptr, nullptr};  // pinned
+  TickStage* d_stage = nullptr;
+  cudaStream_t cap_stream = nullptr;
+  cudaGraphExec_t exec[2] = {nullptr, nullptr};
+  cudaEvent_t done[2] = {nullptr, nullptr};
+  bool launched[2] = {false, false};
+  uint32_t captured_capacity = 0;
+  unsigned long long* captured_keys = nullptr;
+  int parity = 0;
+  int tile_w = 16, tile_h = 16, entries = 128;
+  nm::IntegrateParams integ{};
+};
+
+namespace {
+
+void drop_graphs(nm_tick_plan p) {
+  for (int i = 0; i < 2; ++i) {
+    if (p->exec[i]) cudaGraphExecDestroy(p->exec[i]);
+    p->exec[i] = nullptr;
+  }
+}
+
+// Fill the staging area of `k` with this tick's frames.
+int fill_stage(nm_tick_plan p, TickStage* st, uint64_t* bound) {
+  nm_map m = p->map;
+  auto& w = st->work;
+  std::memset(&w, 0, sizeof(w));
+  w.n_frames = p->n;
+  w.tile_w = p->tile_w;
+  w.tile_h = p->tile_h;
+  w.smask = (uint32_t)p->entries - 1u;
+  auto& rb = st->render;
+  std::memset(&rb, 0, sizeof(rb));
+  rb.n = p->n;
+  rb.noise = p->noise;
+  rb.noise_coef = p->noise_coef;
+  rb.drop = p->drop;
+  *bound = 0;
+  for (int i = 0; i < p->n; ++i) {
+    const nm_frame& fr = p->slots[i];
+    int rc = nm::make_frame(m, fr.sensor, &fr.pose, &w.fr[i]);
+    if (rc != NM_OK) return rc;
+    nm::FrameParams& f = w.fr[i];
+    f.input_kind = 1;
+    f.ranges = fr.ranges;
+    f.plane = fr.agent;
+    f.epoch = m->epoch;
+    w.tiles_x[i] = (f.width + w.tile_w - 1) / w.tile_w;
+    const int ty = (f.height + w.tile_h - 1) / w.tile_h;
+    w.tile_start[i + 1] = w.tile_start[i] + (uint32_t)(w.tiles_x[i] * ty);
+    *bound += nm::frame_leaf_bound(m, fr.sensor, fr.pose, f.R, true,
+                                   (uint64_t)fr.sensor->desc.hres * fr.sensor->desc.vres);
+    if (p->sim) {
+      nm::make_ray_params(fr.sensor, fr.pose, &rb.rp[i]);
+      rb.out[i] = const_cast<float*>(fr.ranges);
+      rb.tiles_x[i] = (fr.sensor->desc.hres + 15) / 16;
+      rb.tile_start[i + 1] = rb.tile_start[i] + (uint32_t)(rb.tiles_x[i] * ((fr.sensor->desc.vres + 15) / 16));
+      rb.noise_seed[i] = p->seed ^ (0x9E3779B97F4A7C15ull * (p->tick + 1)) ^ (0xBF58476D1CE4E5B9ull * (uint64_t)(i + 1));
+    }
+  }
+  w.total_tiles = w.tile_start[p->n];
+  return NM_OK;
+}
+
+int capture(nm_tick_plan p, int k) {
+  nm_map m = p->map;
+  TickStage* h = p->h_stage[k];
+  const uint32_t render_tiles = h->render.tile_start[p->n];
+  const uint32_t total_tiles = h->work.total_tiles;
+  // occupancy queries and attributes are settled before capture begins
+  NM_CUDA(nm::prepare_traverse_dev(p->tile_w, p->tile_h, (uint32_t)p->entries - 1u, m->desc.rounding));
+  NM_CUDA(cudaStreamBeginCapture(p->cap_stream, cudaStreamCaptureModeThreadLocal));
+  cudaError_t e = cudaMemcpyAsync(p->d_stage, h, sizeof(TickStage), cudaMemcpyHostToDevice, p->cap_stream);
+  if (e == cudaSuccess && p->sim)
+    e = nm::launch_render_batch(&p->d_stage->render, render_tiles, p->sim->view, p->cap_stream);
+  if (e == cudaSuccess && total_tiles > 0)
+    e = nm::launch_traverse_labels_dev(&p->d_stage->work, total_tiles, p->tile_w, p->tile_h,
+                                       (uint32_t)p->entries - 1u, m->view, m->desc.rounding,
+                                       p->cap_stream);
+  if (e == cudaSuccess)
+    e = nm::launch_integrate(m->view, p->integ, m->desc.update_mode, m->desc.rounding,
+                             m->ctx->sm_count, p->cap_stream);
+  cudaGraph_t g = nullptr;
+  const cudaError_t e2 = cudaStreamEndCapture(p->cap_stream, &g);
+  if (e != cudaSuccess || e2 != cudaSuccess) {
+    if (g) cudaGraphDestroy(g);
+    cudaGetLastError();
+    return fail(NM_ERR_CUDA, "tick capture failed: %s", cudaGetErrorString(e != cudaSuccess ? e : e2));
+  }
+  e = cudaGraphInstantiate(&p->exec[k], g, 0);
+  cudaGraphDestroy(g);
+  if (e != cudaSuccess) return fail(NM_ERR_CUDA, "tick instantiate: %s", cudaGetErrorString(e));
+  return NM_OK;
+}
+
+int run_plan(nm_tick_plan p, uint32_t flags, cudaStream_t s) {
+  nm_map m = p->map;
+  for (int i = 0; i < p->n; ++i)
+    if (!p->pose_set[i]) return fail(NM_ERR_STATE, "slot %d has no pose", i);
+  if (m->pending_labels) return fail(NM_ERR_STATE, "map has deferred labels; integrate first");
+  const int k = p->parity;
+  if (p->launched[k]) NM_CUDA(cudaEventSynchronize(p->done[k]));  // staging k free again
+  uint64_t bound = 0;
+  int rc = fill_stage(p, p->h_stage[k], &bound);
+  if (rc != NM_OK) return rc;
+  rc = nm::ensure_capacity(m, bound, s);
+  if (rc != NM_OK) return rc;
+  if (m->view.capacity != p->captured_capacity || m->view.keys != p->captured_keys) {
+    NM_CUDA(cudaStreamSynchronize(s));
+    drop_graphs(p);
+    p->captured_capacity = m->view.capacity;
+    p->captured_keys = m->view.keys;
+  }
+  for (int i = 0; i < p->n; ++i) p->h_stage[k]->work.fr[i].epoch = m->epoch;
+  if (!p->exec[k]) {
+    rc = capture(p, k);
+    if (rc != NM_OK) return rc;
+  }
+  NM_CUDA(cudaGraphLaunch(p->exec[k], s));
+  NM_CUDA(cudaEventRecord(p->done[k], s));
+  p->launched[k] = true;
+  p->parity ^= 1;
+  p->tick += 1;
+  m->epoch += 1;
+  if (m->epoch == 0) m->epoch = 1;
+  if (flags & NM_SYNC) return nm::check_device_errors(m, s);
+  return NM_OK;
+}
+
+}  // namespace
+
+extern "C" {
+
+int nm_tick_plan_create(nm_map m, nm_simmap sim, const nm_frame* slots, int32_t n,
+                        nm_tick_plan* out) {
+  if (!m || !slots || !out) return fail(NM_ERR_ARG, "null argument");
+  *out = nullptr;
+  if (n < 1 || n > nm::kMaxTickFrames) return fail(NM_ERR_ARG, "a plan takes 1..%d slots", nm::kMaxTickFrames);
+  if (m->desc.update_mode != NM_UPDATE_LABEL) return fail(NM_ERR_UNSUPPORTED, "tick plans run in label mode");
+  if (sim && sim->ctx != m->ctx) return fail(NM_ERR_ARG, "sim map and map belong to different contexts");
+  NM_CUDA(cudaSetDevice(m->ctx->device));
+  std::unique_ptr<nm_tick_plan_s> p(new nm_tick_plan_s());
+  p->map = m;
+  p->sim = sim;
+  p->n = n;
+  for (int i = 0; i < n; ++i) {
+    const nm_frame& fr = slots[i];
+    if (!fr.sensor || !fr.ranges) return fail(NM_ERR_ARG, "slot %d: null sensor or range buffer", i);
+    if (fr.sensor->ctx != m->ctx) return fail(NM_ERR_ARG, "slot %d: sensor of another context", i);
+    if (fr.agent < 0 || fr.agent >= m->view.planes)
+      return fail(NM_ERR_ARG, "slot %d: agent plane %d outside 0..%d", i, fr.agent, m->view.planes - 1);
+    for (int j = 0; j < i; ++j)
+      if (slots[j].agent == fr.agent &&
+          (slots[j].sensor->lh != fr.sensor->lh || slots[j].sensor->lm != fr.sensor->lm))
+        return fail(NM_ERR_ARG, "slots %d and %d share plane %d with different log-odds", j, i, fr.agent);
+    p->slots[i] = fr;
+    p->pose_set[i] = nm::validate_pose(&fr.pose) == NM_OK;
+  }
+  p->tile_w = m->tile_w;
+  p->tile_h = m->tile_h;
+  p->entries = m->smem_entries;
+  p->integ = nm::integrate_params(m);
+  for (int i = 0; i < n; ++i) {
+    p->integ.lh[slots[i].agent] = slots[i].sensor->lh;
+    p->integ.lm[slots[i].agent] = slots[i].sensor->lm;
+  }
+  for (int k = 0; k < 2; ++k) {
+    NM_CUDA(cudaMallocHost((void**)&p->h_stage[k], sizeof(TickStage)));
+    std::memset(p->h_stage[k], 0, sizeof(TickStage));
+    NM_CUDA(cudaEventCreateWithFlags(&p->done[k], cudaEventDisableTiming));
+  }
+  NM_CUDA(cudaMalloc((void**)&p->d_stage, sizeof(TickStage)));
+  NM_CUDA(cudaStreamCreateWithFlags(&p->cap_stream, cudaStreamNonBlocking));
+  *out = p.release();
+  return NM_OK;
+}
+
+int nm_tick_plan_destroy(nm_tick_plan p) {
+  if (!p) return NM_OK;
+  cudaSetDevice(p->map->ctx->device);
+  cudaDeviceSynchronize();
+  drop_graphs(p);
+  for (int k = 0; k < 2; ++k) {
+    cudaFreeHost(p->h_stage[k]);
+    if (p->done[k]) cudaEventDestroy(p->done[k]);
+  }
+  cudaFree(p->d_stage);
+  if (p->cap_stream) cudaStreamDestroy(p->cap_stream);
+  delete p;
+  return NM_OK;
+}
+
+int nm_tick_plan_set_pose(nm_tick_plan p, int32_t slot, const nm_pose* pose) {
+  if (!p) return fail(NM_ERR_ARG, "plan is null");
+  if (slot < 0 || slot >= p->n) return fail(NM_ERR_ARG, "slot %d outside 0..%d", slot, p->n - 1);
+  const int rc = nm::validate_pose(pose);
+  if (rc != NM_OK) return rc;
+  p->slots[slot].pose = *pose;
+  p->pose_set[slot] = true;
+  return NM_OK;
+}
+
+int nm_tick_plan_set_noise(nm_tick_plan p, float sigma_coef, float drop_prob, uint64_t seed) {
+  if (!p) return fail(NM_ERR_ARG, "plan is null");
+  if (!p->sim) return fail(NM_ERR_STATE, "noise applies to plans that render from a sim map");
+  p->noise = (sigma_coef != 0.f || drop_prob != 0.f) ? 1 : 0;
+  p->noise_coef = sigma_coef;
+  p->drop = drop_prob;
+  p->seed = seed;
+  drop_graphs(p);
+  return NM_OK;
+}
+
+int nm_tick_plan_set_launch(nm_tick_plan p, int32_t tile_w, int32_t tile_h, int32_t entries) {
+  if (!p) return fail(NM_ERR_ARG, "plan is null");
+  const int rc = nm::check_launch_shape(tile_w, tile_h, entries);
+  if (rc != NM_OK) return rc;
+  cudaDeviceSynchronize();
+  p->tile_w = tile_w;
+  p->tile_h = tile_h;
+  p->entries = entries;
+  drop_graphs(p);
+  p->launched[0] = p->launched[1] = false;
+  return NM_OK;
+}
+
+int nm_tick_plan_run(nm_tick_plan p, uint32_t flags, void* stream) {
+  if (!p) return fail(NM_ERR_ARG, "plan is null");
+  NM_CUDA(cudaSetDevice(p->map->ctx->device));
+  return run_plan(p, flags, nm::pick(p->map->ctx, stream));
+}
+
+// Times candidate launch shapes on a scratch map with the plan's slots and poses (the plan's
+// own map is not touched), keeps the fastest, and records it in `cache_path` (one line per
+// workload key: key tile_w tile_h entries microseconds).  A cached entry is reused without
+// timing.
+int nm_tick_plan_autotune(nm_tick_plan p, const char* cache_path, int32_t best[3],
+                          float* best_us) {
+  if (!p) return fail(NM_ERR_ARG, "plan is null");
+  nm_map m = p->map;
+  NM_CUDA(cudaSetDevice(m->ctx->device));
+  cudaDeviceProp prop;
+  NM_CUDA(cudaGetDeviceProperties(&prop, m->ctx->device));
+  std::ostringstream key;
+  key << prop.name << "|sm" << prop.multiProcessorCount << "|res" << m->desc.res << "|n" << p->n;
+  for (int i = 0; i < p->n; ++i)
+    key << "|" << p->slots[i].sensor->desc.type << "x" << p->slots[i].sensor->desc.hres << "x"
+        << p->slots[i].sensor->desc.vres << "x" << p->slots[i].sensor->desc.max_range;
+  std::string k = key.str();
+  for (char& c : k)
+    if (c == ' ') c = '_';
+  if (cache_path) {
+    std::ifstream in(cache_path);
+    std::string line;
+    while (std::getline(in, line)) {
+      std::istringstream ls(line);
+      std::string kk;
+      int tw, th, en;
+      float us;
+      if (ls >> kk >> tw >> th >> en >> us && kk == k) {
+        const int rc = nm_tick_plan_set_launch(p, tw, th, en);
+        if (rc != NM_OK) return rc;
+        if (best) {
+          best[0] = tw;
+          best[1] = th;
+          best[2] = en;
+        }
+        if (best_us) *best_us = us;
+        return NM_OK;
+      }
+    }
+  }
+  const int cands[][3] = {{16, 16, 128}, {16, 16, 256}, {16, 8, 128}, {32, 8, 128},
+                          {32, 16, 128}, {32, 16, 256}, {8, 8, 64},   {16, 16, 64}};
+  nm_map scratch = nullptr;
+  nm_map_desc d = m->desc;
+  d.initial_leaf_capacity = m->view.capacity;
+  int rc = nm_map_create(m->ctx, &d, &scratch);
+  if (rc != NM_OK) return rc;
+  nm_tick_plan tp = nullptr;
+  rc = nm_tick_plan_create(scratch, p->sim, p->slots, p->n, &tp);
+  if (rc != NM_OK) {
+    nm_map_destroy(scratch);
+    return rc;
+  }
+  tp->noise = p->noise;
+  tp->noise_coef = p->noise_coef;
+  tp->drop = p->drop;
+  tp->seed = p->seed;
+  cudaEvent_t e0, e1;
+  cudaEventCreate(&e0);
+  cudaEventCreate(&e1);
+  float best_t = 1e30f;
+  int bi = 0;
+  for (int c = 0; c < (int)(sizeof(cands) / sizeof(cands[0])); ++c) {
+    rc = nm_tick_plan_set_launch(tp, cands[c][0], cands[c][1], cands[c][2]);
+    if (rc != NM_OK) break;
+    for (int it = 0; it < 3 && rc == NM_OK; ++it) rc = run_plan(tp, 0, nullptr);
+    if (rc != NM_OK) break;
+    cudaDeviceSynchronize();
+    cudaEventRecord(e0, nullptr);
+    const int reps = 5;
+    for (int it = 0; it < reps && rc == NM_OK; ++it) rc = run_plan(tp, 0, nullptr);
+    cudaEventRecord(e1, nullptr);
+    cudaEventSynchronize(e1);
+    float ms = 0.f;
+    cudaEventElapsedTime(&ms, e0, e1);
+    const float us = ms * 1000.f / reps;
+    if (us < best_t) {
+      best_t = us;
+      bi = c;
+    }
+  }
+  cudaEventDestroy(e0);
+  cudaEventDestroy(e1);
+  nm_tick_plan_destroy(tp);
+  nm_map_destroy(scratch);
+  if (rc != NM_OK) return rc;
+  rc = nm_tick_plan_set_launch(p, cands[bi][0], cands[bi][1], cands[bi][2]);
+  if (rc != NM_OK) return rc;
+  if (cache_path) {
+    std::ofstream o(cache_path, std::ios::app);
+    o << k << " " << cands[bi][0] << " " << cands[bi][1] << " " << cands[bi][2] << " " << best_t << "\n";
+  }
+  if (best) {
+    best[0] = cands[bi][0];
+    best[1] = cands[bi][1];
+    best[2] = cands[bi][2];
+  }
+  if (best_us) *best_us = best_t;
+  return NM_OK;
+}
+
+}  // extern "C"

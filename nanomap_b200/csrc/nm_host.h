@@ -1,7 +1,7 @@
 // nm_host.h -- host-side math shared by the C ABI translation units.
 #pragma once
 
-#include "../../include/nanomap_b200.h"
+#include "nanomap_b200.h"
 
 namespace nm {
 

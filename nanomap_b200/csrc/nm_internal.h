@@ -15,7 +15,7 @@
 #include <cstdint>
 #include <cuda_runtime.h>
 
-#include "../../include/nanomap_b200.h"
+#include "nanomap_b200.h"
 
 namespace nm {
 
@@ -41,7 +41,8 @@ struct MapCounters {
   unsigned int error_flags;
   unsigned int frames;
   unsigned int done_blocks;
-  unsigned int pad[3];
+  unsigned int tile_queue;  // persistent traversal work counter (reset by its last reader)
+  unsigned int pad[2];
 };
 
 struct MapView {
@@ -82,6 +83,22 @@ struct FrameParams {
   int32_t pad;
 };
 
+constexpr int kMaxTickFrames = 32;
+
+// Work list of one traversal launch: frames and the prefix sum of their tile counts.
+// Passed by value as a __grid_constant__ kernel parameter (no host-to-device copy, so a
+// launch can be captured in a CUDA graph).
+template <int MaxF>
+struct TickWork {
+  int32_t n_frames;
+  int32_t tile_w, tile_h;
+  uint32_t smask;         // shared-memory leaf table entries - 1 (power of two)
+  uint32_t total_tiles;
+  uint32_t tile_start[MaxF + 1];
+  int32_t tiles_x[MaxF];
+  FrameParams fr[MaxF];
+};
+
 struct IntegrateParams {
   float lh[kMaxPlanes];
   float lm[kMaxPlanes];
@@ -114,9 +131,15 @@ __host__ __device__ inline uint32_t hash_key(uint64_t k) {
 }
 
 // ---- kernel launchers (defined in the .cu files) -----------------------------------------
-cudaError_t launch_traverse(const FrameParams& f, const MapView& m, int update_mode,
-                            int rounding, int tile_w, int tile_h, int smem_entries,
-                            cudaStream_t s);
+template <int MaxF>
+cudaError_t launch_traverse_labels(const TickWork<MaxF>& w, const MapView& m, int rounding,
+                                   cudaStream_t s);
+cudaError_t prepare_traverse_dev(int tile_w, int tile_h, uint32_t smask, int rounding);
+cudaError_t launch_traverse_labels_dev(const TickWork<kMaxTickFrames>* d_work, uint32_t total_tiles,
+                                       int tile_w, int tile_h, uint32_t smask, const MapView& m,
+                                       int rounding, cudaStream_t s);
+cudaError_t launch_traverse_counts(const FrameParams& f, const MapView& m, int rounding,
+                                   cudaStream_t s);
 cudaError_t launch_integrate(const MapView& m, const IntegrateParams& p, int update_mode,
                              int rounding, int sm_count, cudaStream_t s);
 cudaError_t launch_rehash(const MapView& from, const MapView& to, uint32_t cur_epoch,

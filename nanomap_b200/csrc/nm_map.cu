@@ -15,52 +15,6 @@ namespace {
 
 constexpr unsigned kFull = 0xffffffffu;
 
-// Label sink of one thread.  Labels go to the CTA's shared-memory leaf table (a hashed cache
-// of up to `smask+1` leaves with 32 label words each); a leaf that finds no room there goes
-// straight to the device table.  The leaf of the previous event is cached in registers, so
-// a table probe happens only when the ray crosses into another leaf.
-struct LabelEmit {
-  unsigned long long* s_keys;
-  uint32_t* s_words;
-  uint32_t smask;
-  const MapView* m;
-  uint32_t epoch;
-  int plane;
-  unsigned long long ckey;
-  int cslot;
-  bool cglobal;
-
-  __device__ __forceinline__ void resolve() {
-    const int s = smem_find_or_insert(s_keys, smask, ckey);
-    if (s >= 0) {
-      cglobal = false;
-      cslot = s;
-    } else {
-      cglobal = true;
-      cslot = map_find_or_insert(*m, ckey);
-      if (cslot >= 0) mark_touched(*m, cslot, epoch, plane);
-    }
-  }
-
-  __device__ __forceinline__ void operator()(int x, int y, int z, int kind) {
-    const unsigned long long key = leaf_key(x >> 3, y >> 3, z >> 3);
-    if (key != ckey) {
-      ckey = key;
-      resolve();
-    }
-    const int l = local_index(x, y, z);
-    const uint32_t bit = 1u << (l & 31);
-    const int wi = (kind == kKindHit ? 0 : 16) + (l >> 5);
-    if (!cglobal) {
-      uint32_t* w = &s_words[cslot * kLabelWords + wi];
-      if (!(*(volatile uint32_t*)w & bit)) atomicOr(w, bit);
-    } else if (cslot >= 0) {
-      uint32_t* w = &m->labels[((size_t)plane * m->capacity + (size_t)cslot) * kLabelWords + wi];
-      if (!(__ldcg(w) & bit)) atomicOr(w, bit);
-    }
-  }
-};
-
 // Count sink (accumulate mode): exact per-voxel hit and miss counts, one atomic per group of
 // lanes that hit the same counter at the same time.
 struct CountEmit {
@@ -103,55 +57,6 @@ __device__ __forceinline__ void add_counts(MapCounters* ctr, uint32_t visits, ui
     atomicAdd(&ctr->visits, v);
     atomicAdd(&ctr->rays, r);
   }
-}
-
-// One CTA = one tile of tile_w x tile_h pixels, one ray per thread.
-template <int RM>
-__global__ void __launch_bounds__(256) k_traverse_label(FrameParams f, MapView m, int tiles_x,
-                                                        int tile_w, int tile_h, uint32_t smask) {
-  extern __shared__ __align__(16) unsigned char smem[];
-  unsigned long long* s_keys = reinterpret_cast<unsigned long long*>(smem);
-  uint32_t* s_words = reinterpret_cast<uint32_t*>(s_keys + (smask + 1));
-  const int tid = threadIdx.x;
-  const int nent = (int)smask + 1;
-  for (int i = tid; i < nent; i += blockDim.x) s_keys[i] = kEmptyKey;
-  for (int i = tid; i < nent * kLabelWords; i += blockDim.x) s_words[i] = 0u;
-  __syncthreads();
-
-  const int tile = blockIdx.x;
-  const int px = (tile % tiles_x) * tile_w + tid % tile_w;
-  const int py = (tile / tiles_x) * tile_h + tid / tile_w;
-  uint32_t visits = 0, rays = 0;
-  if (px < f.width && py < f.height) {
-    float p[3];
-    if (load_point(f, px, py, p)) {
-      LabelEmit em{s_keys, s_words, smask, &m, f.epoch, f.plane, kEmptyKey, -1, false};
-      const int n = trace_point<RM>(f, p[0], p[1], p[2], em);
-      if (n >= 0) {
-        visits = (uint32_t)n;
-        rays = 1;
-      }
-    }
-  }
-  __syncthreads();
-
-  // Flush: one warp per cached leaf; lane i carries label word i.
-  const int warp = tid >> 5, lane = tid & 31, nwarps = blockDim.x >> 5;
-  for (int e = warp; e < nent; e += nwarps) {
-    const unsigned long long key = s_keys[e];
-    if (key == kEmptyKey) continue;
-    const uint32_t word = s_words[e * kLabelWords + lane];
-    if (__ballot_sync(kFull, word != 0u) == 0u) continue;
-    int g = -1;
-    if (lane == 0) {
-      g = map_find_or_insert(m, key);
-      if (g >= 0) mark_touched(m, g, f.epoch, f.plane);
-    }
-    g = __shfl_sync(kFull, g, 0);
-    if (g < 0) continue;
-    if (word) atomicOr(&m.labels[((size_t)f.plane * m.capacity + (size_t)g) * kLabelWords + lane], word);
-  }
-  add_counts(m.ctr, visits, rays);
 }
 
 template <int RM>
@@ -447,25 +352,16 @@ __global__ void __launch_bounds__(256) k_export_labels(MapView m, int plane, int
 
 }  // namespace
 
-cudaError_t launch_traverse(const FrameParams& f, const MapView& m, int update_mode, int rounding,
-                            int tile_w, int tile_h, int smem_entries, cudaStream_t s) {
+cudaError_t launch_traverse_counts(const FrameParams& f, const MapView& m, int rounding,
+                                   cudaStream_t s) {
+  const int tile_w = 16, tile_h = 16;
   const int tiles_x = (f.width + tile_w - 1) / tile_w;
   const int tiles_y = (f.height + tile_h - 1) / tile_h;
   const dim3 grid(tiles_x * tiles_y), block(tile_w * tile_h);
-  if (update_mode == NM_UPDATE_LABEL) {
-    const size_t smem = (size_t)smem_entries * (8 + kLabelWords * 4);
-    const uint32_t smask = (uint32_t)smem_entries - 1u;
-    if (rounding == NM_ROUND_DOWN) {
-      k_traverse_label<NM_ROUND_DOWN><<<grid, block, smem, s>>>(f, m, tiles_x, tile_w, tile_h, smask);
-    } else {
-      k_traverse_label<NM_ROUND_NEAREST><<<grid, block, smem, s>>>(f, m, tiles_x, tile_w, tile_h, smask);
-    }
+  if (rounding == NM_ROUND_DOWN) {
+    k_traverse_count<NM_ROUND_DOWN><<<grid, block, 0, s>>>(f, m, tiles_x, tile_w, tile_h);
   } else {
-    if (rounding == NM_ROUND_DOWN) {
-      k_traverse_count<NM_ROUND_DOWN><<<grid, block, 0, s>>>(f, m, tiles_x, tile_w, tile_h);
-    } else {
-      k_traverse_count<NM_ROUND_NEAREST><<<grid, block, 0, s>>>(f, m, tiles_x, tile_w, tile_h);
-    }
+    k_traverse_count<NM_ROUND_NEAREST><<<grid, block, 0, s>>>(f, m, tiles_x, tile_w, tile_h);
   }
   return cudaGetLastError();
 }

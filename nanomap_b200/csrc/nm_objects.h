@@ -79,3 +79,19 @@ struct nm_simmap_s {
   uint64_t leaves = 0;
 };
 
+
+// Host helpers shared by the C ABI translation units (defined in nm_abi.cpp / nm_abi_sim.cpp).
+namespace nm {
+cudaStream_t pick(nm_context ctx, void* stream);
+int make_frame(nm_map m, nm_sensor s, const nm_pose* pose, FrameParams* f);
+uint64_t frame_leaf_bound(nm_map m, nm_sensor s, const nm_pose& pose, const float R[9],
+                          bool range_input, uint64_t n_rays);
+int ensure_capacity(nm_map m, uint64_t bound, cudaStream_t s);
+int set_plane_constants(nm_map m, int plane, nm_sensor s);
+IntegrateParams integrate_params(nm_map m);
+int do_integrate(nm_map m, cudaStream_t s);
+int check_device_errors(nm_map m, cudaStream_t s);
+int validate_pose(const nm_pose* pose);
+void make_ray_params(nm_sensor s, const nm_pose& pose, SimRayParams* rp);
+int check_launch_shape(int tile_w, int tile_h, int entries);
+}  // namespace nm

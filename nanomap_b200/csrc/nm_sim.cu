@@ -217,11 +217,8 @@ __device__ __forceinline__ int sim_level(const SimMapView& v, int x, int y, int 
   return 0;
 }
 
-__global__ void __launch_bounds__(256) k_sim_render(SimMapView v, SimRayParams rp, float* out) {
-  const int w = blockIdx.x * 16 + (threadIdx.x & 15);
-  const int h = blockIdx.y * 16 + (threadIdx.x >> 4);
-  if (w >= rp.width || h >= rp.height) return;
-  float* o = out + (size_t)h * rp.width + w;
+// Range of pixel (w, h): the first active voxel entered along the pixel ray, or 0.
+__device__ __forceinline__ float sim_ray(const SimMapView& v, const SimRayParams& rp, int w, int h) {
   float result = 0.0f;
   if (v.any) {
     float d0, d1, d2;
@@ -322,7 +319,14 @@ __global__ void __launch_bounds__(256) k_sim_render(SimMapView v, SimRayParams r
       }
     }
   }
-  *o = result;
+  return result;
+}
+
+__global__ void __launch_bounds__(256) k_sim_render(SimMapView v, SimRayParams rp, float* out) {
+  const int w = blockIdx.x * 16 + (threadIdx.x & 15);
+  const int h = blockIdx.y * 16 + (threadIdx.x >> 4);
+  if (w >= rp.width || h >= rp.height) return;
+  out[(size_t)h * rp.width + w] = sim_ray(v, rp, w, h);
 }
 
 // splitmix64 (Steele, Lea, Flood 2014) as a counter-based generator.
@@ -333,22 +337,53 @@ __device__ __forceinline__ uint64_t mix64(uint64_t z) {
   return z ^ (z >> 31);
 }
 
+__device__ __forceinline__ float noisy(float x, uint64_t seed, long long i, float sigma_coef,
+                                       float drop) {
+  const uint64_t a = mix64(seed ^ mix64((uint64_t)i));
+  const uint64_t b = mix64(a);
+  const float u1 = ((float)(a >> 40) + 0.5f) * (1.0f / 16777216.0f);
+  const float u2 = (float)((a >> 16) & 0xFFFFFFu) * (1.0f / 16777216.0f);
+  const float u3 = (float)(b >> 40) * (1.0f / 16777216.0f);
+  if (x > 0.0f) {
+    const float g = sqrtf(-2.0f * logf(u1)) * cospif(2.0f * u2);
+    x = x + g * sigma_coef * x * x;
+    if (u3 < drop || !(x > 0.0f)) x = 0.0f;
+  }
+  return x;
+}
+
 __global__ void k_noise(float* r, long long n, float sigma_coef, float drop, uint64_t seed) {
   for (long long i = (long long)blockIdx.x * blockDim.x + threadIdx.x; i < n;
-       i += (long long)gridDim.x * blockDim.x) {
-    const uint64_t a = mix64(seed ^ mix64((uint64_t)i));
-    const uint64_t b = mix64(a);
-    const float u1 = ((float)(a >> 40) + 0.5f) * (1.0f / 16777216.0f);
-    const float u2 = (float)((a >> 16) & 0xFFFFFFu) * (1.0f / 16777216.0f);
-    const float u3 = (float)(b >> 40) * (1.0f / 16777216.0f);
-    float x = r[i];
-    if (x > 0.0f) {
-      const float g = sqrtf(-2.0f * logf(u1)) * cospif(2.0f * u2);
-      x = x + g * sigma_coef * x * x;
-      if (u3 < drop || !(x > 0.0f)) x = 0.0f;
-      r[i] = x;
-    }
+       i += (long long)gridDim.x * blockDim.x)
+    r[i] = noisy(r[i], seed, i, sigma_coef, drop);
+}
+
+// All slots of a tick plan in one launch: one CTA per 16x16 tile of some slot.
+__global__ void __launch_bounds__(256) k_sim_render_batch(const RenderBatch* b, SimMapView v) {
+  __shared__ SimRayParams s_rp;
+  __shared__ int s_slot;
+  const uint32_t tile = blockIdx.x;
+  if (threadIdx.x == 0) {
+    int sl = 0;
+    while (sl + 1 < b->n && b->tile_start[sl + 1] <= tile) ++sl;
+    s_slot = sl;
   }
+  __syncthreads();
+  const int sl = s_slot;
+  {
+    const uint32_t* src = reinterpret_cast<const uint32_t*>(&b->rp[sl]);
+    uint32_t* dst = reinterpret_cast<uint32_t*>(&s_rp);
+    for (int i = threadIdx.x; i < (int)(sizeof(SimRayParams) / 4); i += blockDim.x) dst[i] = src[i];
+  }
+  __syncthreads();
+  const uint32_t lt = tile - b->tile_start[sl];
+  const int tx = (int)(lt % (uint32_t)b->tiles_x[sl]), ty = (int)(lt / (uint32_t)b->tiles_x[sl]);
+  const int w = tx * 16 + (threadIdx.x & 15), h = ty * 16 + (threadIdx.x >> 4);
+  if (w >= s_rp.width || h >= s_rp.height) return;
+  float x = sim_ray(v, s_rp, w, h);
+  const long long i = (long long)h * s_rp.width + w;
+  if (b->noise) x = noisy(x, b->noise_seed[sl], i, b->noise_coef, b->drop);
+  b->out[sl][i] = x;
 }
 
 }  // namespace
@@ -379,6 +414,12 @@ cudaError_t launch_fill_i32(int32_t* p, long long n, int32_t val, cudaStream_t s
 cudaError_t launch_sim_render(const SimMapView& v, const SimRayParams& rp, float* out, cudaStream_t s) {
   const dim3 grid((rp.width + 15) / 16, (rp.height + 15) / 16);
   k_sim_render<<<grid, 256, 0, s>>>(v, rp, out);
+  return cudaGetLastError();
+}
+
+cudaError_t launch_render_batch(const RenderBatch* d_batch, uint32_t total_tiles,
+                                const SimMapView& v, cudaStream_t s) {
+  if (total_tiles > 0) k_sim_render_batch<<<total_tiles, 256, 0, s>>>(d_batch, v);
   return cudaGetLastError();
 }
 

@@ -5,7 +5,7 @@
 #include <cstdint>
 #include <cuda_runtime.h>
 
-#include "../../include/nanomap_b200.h"
+#include "nanomap_b200.h"
 
 namespace nm {
 
@@ -40,6 +40,22 @@ struct SimRayParams {
   float min_range, max_range;
 };
 
+constexpr int kMaxRenderSlots = 32;
+
+// Every slot of a tick plan rendered (and optionally noised) in one launch.
+struct RenderBatch {
+  int32_t n;
+  int32_t noise;
+  float noise_coef, drop;
+  uint32_t tile_start[kMaxRenderSlots + 1];  // 16x16 tiles per slot, prefix sums
+  int32_t tiles_x[kMaxRenderSlots];
+  float* out[kMaxRenderSlots];
+  uint64_t noise_seed[kMaxRenderSlots];
+  SimRayParams rp[kMaxRenderSlots];
+};
+
+cudaError_t launch_render_batch(const RenderBatch* d_batch, uint32_t total_tiles,
+                                const SimMapView& v, cudaStream_t s);
 cudaError_t launch_voxelize(const SimBuild& b, const double* d_boxes, int nb, const double* d_cyl,
                             int nc, cudaStream_t s);
 cudaError_t launch_set_voxels(const SimBuild& b, const int32_t* d_ijk, long long n, cudaStream_t s);

@@ -50,12 +50,13 @@ def leaf_dict(origins, *arrays):
     return {tuple(int(v) for v in o): tuple(a[i] for a in arrays) for i, o in enumerate(origins)}
 
 
-def compare_maps(gpu_export, oracle_export):
-    """Return a list of mismatch descriptions between a GPU export and an oracle export."""
+def compare_maps(gpu_export, other_export):
+    """Mismatch descriptions between a GPU export and another export (an oracle export with
+    512 active bytes per leaf, or a second GPU export with 16 active words per leaf)."""
     go, gv, ga = gpu_export
-    oo, ov, oa = oracle_export
+    oo, ov, oa = other_export
     G = leaf_dict(go, gv, ga)
-    Od = leaf_dict(oo, ov, active_bits_from_bytes(oa))
+    Od = leaf_dict(oo, ov, oa if oa.shape[1:] == (16,) else active_bits_from_bytes(oa))
     errs = []
     zero_v = np.zeros(512, np.float32)
     zero_a = np.zeros(16, np.uint32)
