@@ -210,6 +210,24 @@ int nm_map_frame_params(nm_map m, nm_sensor s, const nm_pose* pose, float rotati
 int nm_frame_params(const nm_sensor_desc* desc, const nm_pose* pose, float res, int32_t rounding,
                     float rotation[9], double eye[3], float* max_time, float pixel_model[6]);
 
+/* Labels of one range image without any device allocation (no counterpart in the reference;
+ * an addition for callers that cannot allocate device memory while they run, such as
+ * real-time loops that forbid allocation after start-up, or hosts whose memory pool owns the
+ * device).  Same traversal and labels as nm_map_insert_ranges + NM_DEFER_INTEGRATE on a map
+ * of resolution `res` and rounding `rounding`, but the working memory is a fixed static
+ * device array of about 9 MiB that every GPU loading the library holds until exit.  Inputs
+ * and outputs are device memory owned by the caller: `ranges` (hres*vres floats),
+ * `origins` (3 ints per leaf), `words` (32 label words per leaf, as nm_map_export_labels),
+ * `status` (2 uints: labelled leaf count, error bits).  Limits: at most 8388608 pixels per
+ * frame (larger frames are rejected with NM_ERR_ARG) and at most 32768 labelled leaves per
+ * call (more is reported as NM_ERR_CAPACITY under NM_SYNC, else in status[1]).  The first
+ * call on a device looks up the array's device address; make that first call before any
+ * stream capture.  Every call shares the array and first clears it; calls that overlap on
+ * the GPU race on it. */
+int nm_label_frame_static(nm_sensor s, const nm_pose* pose, const float* ranges, float res,
+                          int32_t rounding, int32_t* origins, uint32_t* words,
+                          uint32_t max_leaves, uint32_t* status, uint32_t flags, void* stream);
+
 /* ---- simulation map (replaces the NanoVDB sim grid, SimHandler.cpp:13-24) -------------- */
 /* Voxelise primitives into a sparse device map: boxes are 6 doubles (min xyz, max xyz, m);
  * cylinders are 5 doubles (cx, cy, radius, z0, z1, m).  A voxel is active when its centre is

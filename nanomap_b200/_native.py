@@ -127,6 +127,7 @@ _SIGS = {
     "nm_map_export_labels": (C.c_int, [_P, _I32, _PI32, _PU32, _U64, _PU64]),
     "nm_map_frame_params": (C.c_int, [_P, _P, C.POINTER(NmPose), _PF, _PD, _PF]),
     "nm_frame_params": (C.c_int, [C.POINTER(NmSensorDesc), C.POINTER(NmPose), _F, _I32, _PF, _PD, _PF, _PF]),
+    "nm_label_frame_static": (C.c_int, [_P, C.POINTER(NmPose), _P, _F, _I32, _P, _P, _U32, _P, _U32, _P]),
     "nm_simmap_create_primitives": (C.c_int, [_P, _F, _PI32, _PI32, _PD, _I32, _PD, _I32, C.POINTER(_P)]),
     "nm_simmap_create_voxels": (C.c_int, [_P, _F, _PI32, _I64, C.POINTER(_P)]),
     "nm_simmap_destroy": (C.c_int, [_P]),
