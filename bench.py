@@ -346,12 +346,14 @@ def run_ours(args, rank, world, local):
     t_trav = statistics.mean(trav_ms) / 1e3
     t_integ = statistics.mean(integ_ms) / 1e3
     dominant = "traverse" if t_trav >= t_integ else "integrate"
+    traffic = None
+    tf = ROOT / "profiles" / "roofline_traffic.json"
+    if tf.exists():
+        traffic = json.loads(tf.read_text()).get("k_" + dominant, {}).get("dram_bytes_per_launch")
     if dominant == "traverse":
         ach = trav_bytes / t_trav / 1e9
-        traffic = None
     else:
         ach = integ_bytes / t_integ / 1e9
-        traffic = None
     line = {
         "metric": METRIC, "value": value, "unit": UNIT, "n_gpus": world, "steps": args.steps,
         "warmup": args.warmup, "ms_per_step": t_max * 1e3 / args.steps, "higher_is_better": True,
@@ -368,10 +370,13 @@ def run_ours(args, rank, world, local):
         "roofline": {"bound": "hbm", "kernel": f"k_{dominant}", "achieved": ach, "peak": hbm,
                      "unit": "GB/s", "frac": ach / hbm, "traffic": traffic,
                      "peak_source": "measured (MEASURED_PEAKS.json hbm_gbs)" if peaks else "fallback",
+                     "traffic_source": "ncu dram bytes of one headline frame (profiles/k_traverse_sim_headline.md)",
                      "algorithmic_bytes_per_launch": trav_bytes if dominant == "traverse" else integ_bytes},
         "e2e": e2e,
         "clocks": clk,
     }
+    if args.batched_ticks > args.warmup:
+        line["batched"] = run_batched(args, rank, world, local, args.batched_ticks)
     if rank == 0 and world == 1 and args.cpu_baseline_s > 0:
         frames_host = []
         for k in range(30):
@@ -385,6 +390,139 @@ def run_ours(args, rank, world, local):
     return line
 
 
+def batched_agents(spec_small):
+    """Sensor mix of the batched tick: (hres, vres, range m, type) per agent."""
+    mix = [(320, 240, 5.0, 0)] * 6 + [(640, 480, 10.0, 0)] * 6 + [(1280, 720, 8.0, 0)] * 3 + [(1024, 64, 20.0, 1)]
+    return mix
+
+
+def run_batched(args, rank, world, local, ticks):
+    """16-agent tick (config-1 world at 0.05 m): one graph-replayed, autotuned tick per step,
+    against the same agents run one frame per launch (render + insert per agent)."""
+    import torch
+
+    from nanomap_b200 import _native as N
+    from nanomap_b200 import api as A
+    from nanomap_b200 import scenes as S
+
+    dev = torch.device("cuda", local)
+    spec = S.SCENES["plain_small"]
+    scene = S.make_scene(spec, 1)
+    res = 0.05
+    ctx = A.Context(local)
+    sim = A.SimMap(ctx, res, boxes=scene.boxes, cylinders=scene.cylinders, vox_min=(0, 0, 0),
+                   vox_max=tuple(int(math.ceil(x / res)) for x in spec.size))
+    sensors, bufs, trajs = [], [], []
+    for a, (w, h, rng_m, typ) in enumerate(batched_agents(spec)):
+        if typ == 1:
+            d = A.sensor_desc(type=1, hres=w, vres=h, hfov_deg=360.0, vfov_deg=30.0, max_range=rng_m,
+                              explicit_log_odds=1, log_odds_hit=0.85, log_odds_miss=-0.4,
+                              frame_transform=S.OPTICAL_TO_BODY)
+        else:
+            d = A.sensor_desc(type=0, hres=w, vres=h, hfov_deg=87.0, vfov_deg=58.0, max_range=rng_m,
+                              explicit_log_odds=1, log_odds_hit=0.85, log_odds_miss=-0.4,
+                              frame_transform=S.OPTICAL_TO_BODY)
+        sensors.append(A.Sensor(ctx, d))
+        bufs.append(torch.zeros(h, w, device=dev))
+        trajs.append([A.Pose(p, q) for p, q in S.trajectory(scene, ticks, seed=101 + 37 * a + 7919 * rank)])
+    n = len(sensors)
+    rays_per_tick = sum(s.desc.hres * s.desc.vres for s in sensors)
+    cap = 1 << 21
+    stream = torch.cuda.current_stream(dev)
+    flush = torch.empty(256 << 20, dtype=torch.uint8, device=dev)
+
+    # batched: one tick plan (graph), autotuned on a scratch map
+    mb = A.Map(ctx, A.map_desc(res=res, clamp_min=-2.0, clamp_max=3.5, max_agents=n,
+                               rounding=N.NM_ROUND_DOWN, initial_leaf_capacity=cap))
+    plan = A.TickPlan(mb, [(sensors[a], bufs[a], a) for a in range(n)], sim=sim)
+    for a in range(n):
+        plan.set_pose(a, trajs[a][0])
+    best, best_us = plan.autotune(None)
+    for t in range(args.warmup):
+        for a in range(n):
+            plan.set_pose(a, trajs[a][t])
+        plan.run(stream=stream)
+    torch.cuda.synchronize()
+    b0 = mb.stats()
+    evs = []
+    for t in range(ticks - args.warmup):
+        e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+        flush.fill_(t & 255)
+        for a in range(n):
+            plan.set_pose(a, trajs[a][args.warmup + t])
+        e0.record(stream)
+        plan.run(stream=stream)
+        e1.record(stream)
+        evs.append((e0, e1))
+    torch.cuda.synchronize()
+    b1 = mb.stats()
+    tb = sum(e0.elapsed_time(e1) for e0, e1 in evs) / 1e3
+    nb = len(evs)
+    vb = b1["visits"] - b0["visits"]
+
+    # plain: the same frames, one render + one insert launch pair per agent frame
+    mp = A.Map(ctx, A.map_desc(res=res, clamp_min=-2.0, clamp_max=3.5, rounding=N.NM_ROUND_DOWN,
+                               initial_leaf_capacity=cap))
+    for t in range(args.warmup):
+        for a in range(n):
+            sim.render(sensors[a], trajs[a][t], bufs[a], stream=stream)
+            mp.insert_ranges(sensors[a], trajs[a][t], bufs[a], stream=stream)
+    torch.cuda.synchronize()
+    p0 = mp.stats()
+    evp = []
+    for t in range(ticks - args.warmup):
+        e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+        flush.fill_(t & 255)
+        e0.record(stream)
+        for a in range(n):
+            sim.render(sensors[a], trajs[a][args.warmup + t], bufs[a], stream=stream)
+            mp.insert_ranges(sensors[a], trajs[a][args.warmup + t], bufs[a], stream=stream)
+        e1.record(stream)
+        evp.append((e0, e1))
+    torch.cuda.synchronize()
+    p1 = mp.stats()
+    tp = sum(e0.elapsed_time(e1) for e0, e1 in evp) / 1e3
+    vp = p1["visits"] - p0["visits"]
+
+    # plain with a host round trip per frame (the reference's per-frame synchronous pipeline)
+    mq = A.Map(ctx, A.map_desc(res=res, clamp_min=-2.0, clamp_max=3.5, rounding=N.NM_ROUND_DOWN,
+                               initial_leaf_capacity=cap))
+    q0 = mq.stats()
+    nq = min(5, ticks - args.warmup)
+    torch.cuda.synchronize()
+    t0 = time.perf_counter()
+    for t in range(nq):
+        for a in range(n):
+            sim.render(sensors[a], trajs[a][args.warmup + t], bufs[a], stream=stream)
+            mq.insert_ranges(sensors[a], trajs[a][args.warmup + t], bufs[a], flags=N.NM_SYNC, stream=stream)
+    tq = time.perf_counter() - t0
+    q1 = mq.stats()
+    vq = q1["visits"] - q0["visits"]
+    out = {
+        "workload": ("16 agents / tick in the 20x20x5 m world mapped at 0.05 m: 6x320x240@5 m, "
+                     "6x640x480@10 m, 3x1280x720@8 m (87x58 deg), 1x1024x64 spinning@20 m; sim render "
+                     "+ labels + integration per tick; L2 flushed between ticks"),
+        "rays_per_tick": rays_per_tick,
+        "ticks": nb,
+        "batched_voxel_updates_per_s": vb / tb,
+        "batched_ms_per_tick": tb * 1e3 / nb,
+        "plain_voxel_updates_per_s": vp / tp,
+        "plain_ms_per_tick": tp * 1e3 / nb,
+        "plain_synchronous_voxel_updates_per_s": vq / tq,
+        "speedup_vs_plain": (vb / tb) / (vp / tp),
+        "speedup_vs_plain_synchronous": (vb / tb) / (vq / tq),
+        "autotuned_launch": {"tile": [best[0], best[1]], "leaf_table_entries": best[2], "tick_us": best_us},
+        "maps_equal_visits": vb == vp,
+        "table_growths": {"batched": b1["grow_count"], "plain": p1["grow_count"],
+                          "plain_synchronous": q1["grow_count"]},
+        "gpu_launches_per_tick": 4,
+    }
+    plan.close()
+    for mm in (mb, mp, mq):
+        mm.close()
+    return out
+
+
 def main():
     ap = argparse.ArgumentParser()
     ap.add_argument("--gpus", type=int, default=1)
@@ -393,6 +531,8 @@ def main():
     ap.add_argument("--impl", choices=["ours", "reference"], default="ours")
     ap.add_argument("--e2e-steps", type=int, default=30)
     ap.add_argument("--cpu-baseline-s", type=float, default=12.0)
+    ap.add_argument("--batched-ticks", type=int, default=40,
+                    help="ticks of the 16-agent batched comparison (0 = skip)")
     ap.add_argument("--capacity-log2", type=int, default=21,
                     help="initial leaf-table capacity (log2 slots); smaller for profiling runs")
     args = ap.parse_args()

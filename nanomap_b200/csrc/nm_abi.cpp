@@ -217,41 +217,71 @@ int grow_map(nm_map m, uint32_t new_capacity, cudaStream_t s) {
   return NM_OK;
 }
 
-// Upper bound on the leaves one frame can touch: the leaf box of the ball of radius
-// max_range around the eye, intersected (frustum range images) with the leaf box of the
-// frustum pyramid, and capped by rays x leaves-per-ray.
-uint64_t frame_leaf_bound(nm_map m, nm_sensor s, const nm_pose& pose, const float R[9],
-                          bool range_input, uint64_t n_rays) {
+// Box (index-space voxels) holding every voxel one frame can touch: the eye and the far ends
+// of the sensor's pixel directions at max range -- the frustum pyramid for frustum range
+// images, a sampled azimuth/elevation band (padded) for laser range images, the range ball
+// for xyz records (whose points may lie anywhere within range).
+void frame_box(nm_map m, nm_sensor s, const nm_pose& pose, const float R[9], bool range_input,
+               double lo[3], double hi[3]) {
   const double res = m->desc.res;
   const double rv = s->desc.max_range / res + 2.0;
-  double lo[3], hi[3];
+  double e[3];
   for (int a = 0; a < 3; ++a) {
-    const double e = pose.position[a] / res;
-    lo[a] = e - rv;
-    hi[a] = e + rv;
+    e[a] = pose.position[a] / res;
+    lo[a] = e[a] - rv;
+    hi[a] = e[a] + rv;
   }
-  if (range_input && s->desc.type == NM_SENSOR_FRUSTUM) {
-    double flo[3], fhi[3];
-    for (int a = 0; a < 3; ++a) flo[a] = fhi[a] = pose.position[a] / res;
+  if (!range_input) return;
+  double flo[3] = {e[0], e[1], e[2]}, fhi[3] = {e[0], e[1], e[2]};
+  auto add = [&](double dx, double dy, double dz, double len) {
+    for (int a = 0; a < 3; ++a) {
+      const double c = e[a] + (R[a * 3] * dx + R[a * 3 + 1] * dy + R[a * 3 + 2] * dz) * len;
+      flo[a] = std::min(flo[a], c);
+      fhi[a] = std::max(fhi[a], c);
+    }
+  };
+  double pad = 2.0;
+  if (s->desc.type == NM_SENSOR_FRUSTUM) {
     const double sx[2] = {-s->fp[0], s->fp[0]}, sy[2] = {-s->fp[1], s->fp[1]};
     for (int i = 0; i < 2; ++i)
-      for (int j = 0; j < 2; ++j)
-        for (int a = 0; a < 3; ++a) {
-          const double c = pose.position[a] / res +
-                           (R[a * 3] * sx[i] + R[a * 3 + 1] * sy[j] + R[a * 3 + 2]) * (rv + 1.0);
-          flo[a] = std::min(flo[a], c);
-          fhi[a] = std::max(fhi[a], c);
-        }
-    for (int a = 0; a < 3; ++a) {
-      lo[a] = std::max(lo[a], flo[a] - 2.0);
-      hi[a] = std::min(hi[a], fhi[a] + 2.0);
+      for (int j = 0; j < 2; ++j) add(sx[i], sy[j], 1.0, rv + 1.0);
+  } else {
+    const double kPi = 3.14159265358979323846;
+    const double hf = s->desc.hfov_deg * kPi / 180.0, vf = s->desc.vfov_deg * kPi / 180.0;
+    const int nu = 96, nv = 9;
+    for (int i = 0; i <= nu; ++i) {
+      const double u = -hf / 2 + hf * i / nu;
+      for (int j = 0; j <= nv; ++j) {
+        const double v = -vf / 2 + vf * j / nv;
+        add(std::sin(u) * std::cos(v), std::sin(v), std::cos(u) * std::cos(v), rv);
+      }
     }
+    pad = 2.0 + 0.01 * rv;  // sampling step (< 2 degrees) under-reaches by less than 1 %
   }
+  for (int a = 0; a < 3; ++a) {
+    lo[a] = std::max(lo[a], flo[a] - pad);
+    hi[a] = std::min(hi[a], fhi[a] + pad);
+  }
+}
+
+double box_leaves(const double lo[3], const double hi[3]) {
   double vol = 1.0;
   for (int a = 0; a < 3; ++a) vol *= std::floor(hi[a] / 8.0) - std::floor(lo[a] / 8.0) + 1.0;
-  const double per_ray = 3.0 * std::ceil(rv / 8.0) + 3.0;
-  const double cap = (double)n_rays * per_ray;
-  return (uint64_t)std::min(vol, cap);
+  return vol;
+}
+
+double ray_leaf_cap(nm_map m, nm_sensor s, uint64_t n_rays) {
+  const double rv = s->desc.max_range / m->desc.res + 2.0;
+  return (double)n_rays * (3.0 * std::ceil(rv / 8.0) + 3.0);
+}
+
+// Upper bound on the leaves one frame can touch: the leaf count of frame_box, capped by
+// rays x leaves-per-ray.
+uint64_t frame_leaf_bound(nm_map m, nm_sensor s, const nm_pose& pose, const float R[9],
+                          bool range_input, uint64_t n_rays) {
+  double lo[3], hi[3];
+  frame_box(m, s, pose, R, range_input, lo, hi);
+  return (uint64_t)std::min(box_leaves(lo, hi), ray_leaf_cap(m, s, n_rays));
 }
 
 int ensure_capacity(nm_map m, uint64_t bound, cudaStream_t s) {
@@ -781,6 +811,7 @@ int nm_map_tick(nm_map m, const nm_frame* frames, int32_t n_frames, uint32_t fla
   w->tile_h = m->tile_h;
   w->smask = (uint32_t)m->smem_entries - 1u;
   uint64_t bound = 0;
+  double ulo[3] = {0, 0, 0}, uhi[3] = {0, 0, 0}, cap = 0.0;
   for (int i = 0; i < n_frames; ++i) {
     const nm_frame& fr = frames[i];
     if (!fr.sensor || !fr.ranges) return fail(NM_ERR_ARG, "frame %d: null sensor or ranges", i);
@@ -797,9 +828,15 @@ int nm_map_tick(nm_map m, const nm_frame* frames, int32_t n_frames, uint32_t fla
     w->tiles_x[i] = (f.width + w->tile_w - 1) / w->tile_w;
     const int ty = (f.height + w->tile_h - 1) / w->tile_h;
     w->tile_start[i + 1] = w->tile_start[i] + (uint32_t)(w->tiles_x[i] * ty);
-    bound += frame_leaf_bound(m, fr.sensor, fr.pose, f.R, true,
-                              (uint64_t)fr.sensor->desc.hres * fr.sensor->desc.vres);
+    double lo[3], hi[3];
+    frame_box(m, fr.sensor, fr.pose, f.R, true, lo, hi);
+    for (int a = 0; a < 3; ++a) {
+      ulo[a] = i == 0 ? lo[a] : std::min(ulo[a], lo[a]);
+      uhi[a] = i == 0 ? hi[a] : std::max(uhi[a], hi[a]);
+    }
+    cap += ray_leaf_cap(m, fr.sensor, (uint64_t)fr.sensor->desc.hres * fr.sensor->desc.vres);
   }
+  bound = (uint64_t)std::min(box_leaves(ulo, uhi), cap);
   w->total_tiles = w->tile_start[n_frames];
   int rc = ensure_capacity(m, bound, s0);
   if (rc != NM_OK) return rc;

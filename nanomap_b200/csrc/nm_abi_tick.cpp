@@ -79,6 +79,7 @@ int fill_stage(nm_tick_plan p, TickStage* st, uint64_t* bound) {
   rb.noise_coef = p->noise_coef;
   rb.drop = p->drop;
   *bound = 0;
+  double ulo[3] = {0, 0, 0}, uhi[3] = {0, 0, 0}, cap = 0.0;
   for (int i = 0; i < p->n; ++i) {
     const nm_frame& fr = p->slots[i];
     int rc = nm::make_frame(m, fr.sensor, &fr.pose, &w.fr[i]);
@@ -91,8 +92,13 @@ int fill_stage(nm_tick_plan p, TickStage* st, uint64_t* bound) {
     w.tiles_x[i] = (f.width + w.tile_w - 1) / w.tile_w;
     const int ty = (f.height + w.tile_h - 1) / w.tile_h;
     w.tile_start[i + 1] = w.tile_start[i] + (uint32_t)(w.tiles_x[i] * ty);
-    *bound += nm::frame_leaf_bound(m, fr.sensor, fr.pose, f.R, true,
-                                   (uint64_t)fr.sensor->desc.hres * fr.sensor->desc.vres);
+    double lo[3], hi[3];
+    nm::frame_box(m, fr.sensor, fr.pose, f.R, true, lo, hi);
+    for (int a = 0; a < 3; ++a) {
+      ulo[a] = i == 0 ? lo[a] : std::min(ulo[a], lo[a]);
+      uhi[a] = i == 0 ? hi[a] : std::max(uhi[a], hi[a]);
+    }
+    cap += nm::ray_leaf_cap(m, fr.sensor, (uint64_t)fr.sensor->desc.hres * fr.sensor->desc.vres);
     if (p->sim) {
       nm::make_ray_params(fr.sensor, fr.pose, &rb.rp[i]);
       rb.out[i] = const_cast<float*>(fr.ranges);
@@ -102,6 +108,7 @@ int fill_stage(nm_tick_plan p, TickStage* st, uint64_t* bound) {
     }
   }
   w.total_tiles = w.tile_start[p->n];
+  *bound = (uint64_t)std::min(nm::box_leaves(ulo, uhi), cap);
   return NM_OK;
 }
 

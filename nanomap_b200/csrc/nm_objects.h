@@ -86,6 +86,10 @@ cudaStream_t pick(nm_context ctx, void* stream);
 int make_frame(nm_map m, nm_sensor s, const nm_pose* pose, FrameParams* f);
 uint64_t frame_leaf_bound(nm_map m, nm_sensor s, const nm_pose& pose, const float R[9],
                           bool range_input, uint64_t n_rays);
+void frame_box(nm_map m, nm_sensor s, const nm_pose& pose, const float R[9], bool range_input,
+               double lo[3], double hi[3]);
+double box_leaves(const double lo[3], const double hi[3]);
+double ray_leaf_cap(nm_map m, nm_sensor s, uint64_t n_rays);
 int ensure_capacity(nm_map m, uint64_t bound, cudaStream_t s);
 int set_plane_constants(nm_map m, int plane, nm_sensor s);
 IntegrateParams integrate_params(nm_map m);
