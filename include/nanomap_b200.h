@@ -61,6 +61,7 @@ typedef struct nm_sensor_s* nm_sensor;
 typedef struct nm_map_s* nm_map;
 typedef struct nm_simmap_s* nm_simmap;
 typedef struct nm_tick_plan_s* nm_tick_plan;
+typedef struct nm_config_s* nm_config;
 
 /* nanomap::Pose (nanomap.h:20-28): position (m) and unit quaternion (w, x, y, z). */
 typedef struct {
@@ -118,14 +119,51 @@ typedef struct {
   int32_t pad;
 } nm_frame;
 
+/* Main config values (Config.cpp:60-113 plus the optional extension keys). */
+typedef struct {
+  float mapping_res, grid_res;
+  float prob_hit_thres, prob_miss_thres;
+  float frustum_allocation_factor;
+  float clamp_min, clamp_max;
+  int32_t leaf_edge, filter_type, update_type, precision_type, publish_sensor, process_type;
+  int32_t update_mode, clamp_mode, rounding;
+  int32_t n_sensors, n_agents;
+  char sim_grid[512];
+} nm_config_info;
+
+/* One agent config (Agent.h:49-135). */
+typedef struct {
+  int32_t spawn_random;
+  float position[3];
+  int32_t num_obs;
+  float len_obs, collision_dist;
+  int32_t n_sensors;
+} nm_agent_info;
+
 /* ---- library -------------------------------------------------------------------------- */
 int nm_abi_version(void);
 const char* nm_last_error(void);
+
+/* ---- configuration files (replaces nanomap::config::Config, Config.cpp:18-267) ---------- */
+/* Parses a main config and the sensor / agent configs it names (paths as given, else
+ * relative to the main config's directory).  Host only; no device needed. */
+int nm_config_load(const char* path, nm_config* out);
+int nm_config_destroy(nm_config c);
+int nm_config_get_info(nm_config c, nm_config_info* out);
+int nm_config_sensor(nm_config c, int32_t i, nm_sensor_desc* desc, char* name, int32_t name_cap);
+int nm_config_agent(nm_config c, int32_t i, nm_agent_info* out);
+int nm_config_agent_sensor(nm_config c, int32_t agent, int32_t j, char* name, int32_t name_cap,
+                           nm_pose* origin);
+/* Map parameters a config implies (thresholds logit(ProbHitThres/ProbMissThres), clamps). */
+int nm_config_map_desc(nm_config c, nm_map_desc* out);
 
 /* ---- context (replaces Handler's stream pair, Handler.cpp:17-25, and closeHandler) ------ */
 int nm_context_create(int32_t device, nm_context* out);
 int nm_context_destroy(nm_context ctx);
 int nm_context_sync(nm_context ctx);
+/* Device buffers for callers without their own CUDA allocator (e.g. range images). */
+int nm_alloc_device(nm_context ctx, size_t bytes, void** out);
+int nm_free_device(void* p);
 
 /* ---- sensors (replaces FrustumData / LaserData and gpu::Sensor, Sensor.h:147-211) ----- */
 int nm_sensor_create(nm_context ctx, const nm_sensor_desc* desc, nm_sensor* out);
@@ -238,6 +276,11 @@ int nm_simmap_create_primitives(nm_context ctx, float res, const int32_t vox_min
 /* From a list of active voxel coordinates (3 ints each, host memory). */
 int nm_simmap_create_voxels(nm_context ctx, float res, const int32_t* ijk, int64_t n,
                             nm_simmap* out);
+/* From a voxel-list file: 8-byte magic "NMSIMv1", float res (m), int64 count, then count
+ * triplets of int32 voxel coordinates (little endian).  Replaces SimManager::loadSimGrid /
+ * loadGridFromFile (SimManager.h:171-213); OpenVDB .vdb files are refused with
+ * NM_ERR_UNSUPPORTED (no OpenVDB reader in this build). */
+int nm_simmap_load(nm_context ctx, const char* path, nm_simmap* out);
 int nm_simmap_destroy(nm_simmap sm);
 /* active bounding box (min xyz, max xyz, inclusive), active voxel count, leaf count */
 int nm_simmap_info(nm_simmap sm, int32_t bbox[6], uint64_t* active_voxels, uint64_t* leaves);

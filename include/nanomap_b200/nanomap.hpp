@@ -1,0 +1,420 @@
+// nanomap.hpp -- C++ facade with NanoMap's class names and signatures over the C ABI.
+//
+// Header only; link libnanomap_b200.so.  Mirrors the reference's public API for the mapping
+// and simulation path:
+//   nanomap::Pose                               nanomap.h:20-28
+//   nanomap::config::Config(std::string)        Config.h:42-91, Config.cpp:18-59
+//   nanomap::map::Map(gridRes, probThresHit, probThresMiss)   OccupancyMap.h:35-61
+//   nanomap::agent::Agent (updatePose, sensorPose, map)       Agent.h:49-210
+//   nanomap::manager::Manager::insertPointCloud               Manager.h:46-72
+//   nanomap::manager::SimManager::updateAgentViews([map])     SimManager.h:68-168
+// Eigen is not required: Vector3f / Quaternionf below keep Eigen's construction order
+// (Quaternionf(w, x, y, z)) and accessors.  Failures of the library raise nanomap::Error
+// (the reference reports nothing); an unknown sensor name in insertPointCloud is a no-op, as
+// in the reference's name scan (Manager.h:55-57).
+#pragma once
+
+#include <chrono>
+#include <cmath>
+#include <cstdint>
+#include <cstring>
+#include <iostream>
+#include <memory>
+#include <stdexcept>
+#include <string>
+#include <vector>
+
+#include "../nanomap_b200.h"
+
+namespace nanomap {
+
+class Error : public std::runtime_error {
+ public:
+  Error(int code, const std::string& what) : std::runtime_error(what), code_(code) {}
+  int code() const { return code_; }
+
+ private:
+  int code_;
+};
+
+namespace detail {
+inline void check(int rc) {
+  if (rc != NM_OK) throw Error(rc, std::string("nanomap_b200: ") + nm_last_error());
+}
+inline int& device_index() {
+  static int dev = 0;
+  return dev;
+}
+// One library context per process (created on first use, on device_index()).
+inline nm_context context() {
+  static std::shared_ptr<nm_context_s> ctx;
+  if (!ctx) {
+    nm_context c = nullptr;
+    check(nm_context_create(device_index(), &c));
+    ctx.reset(c, [](nm_context p) { nm_context_destroy(p); });
+  }
+  return ctx.get();
+}
+inline float logit(double p) { return (float)(std::log(p) - std::log(1.0 - p)); }
+}  // namespace detail
+
+// Device used by every object created afterwards (default 0).
+inline void setDevice(int device) { detail::device_index() = device; }
+
+struct Vector3f {
+  float v[3];
+  Vector3f() : v{0.f, 0.f, 0.f} {}
+  Vector3f(float x, float y, float z) : v{x, y, z} {}
+  float& operator()(int i) { return v[i]; }
+  float operator()(int i) const { return v[i]; }
+  float x() const { return v[0]; }
+  float y() const { return v[1]; }
+  float z() const { return v[2]; }
+  Vector3f operator+(const Vector3f& o) const { return {v[0] + o.v[0], v[1] + o.v[1], v[2] + o.v[2]}; }
+};
+
+struct Quaternionf {
+  float w_, x_, y_, z_;
+  Quaternionf() : w_(1.f), x_(0.f), y_(0.f), z_(0.f) {}
+  Quaternionf(float w, float x, float y, float z) : w_(w), x_(x), y_(y), z_(z) {}
+  float w() const { return w_; }
+  float x() const { return x_; }
+  float y() const { return y_; }
+  float z() const { return z_; }
+  Quaternionf normalized() const {
+    const float n = std::sqrt(w_ * w_ + x_ * x_ + y_ * y_ + z_ * z_);
+    return {w_ / n, x_ / n, y_ / n, z_ / n};
+  }
+  // Hamilton product, Eigen's operator* order (this applied after o).
+  Quaternionf operator*(const Quaternionf& o) const {
+    return {w_ * o.w_ - x_ * o.x_ - y_ * o.y_ - z_ * o.z_, w_ * o.x_ + x_ * o.w_ + y_ * o.z_ - z_ * o.y_,
+            w_ * o.y_ - x_ * o.z_ + y_ * o.w_ + z_ * o.x_, w_ * o.z_ + x_ * o.y_ - y_ * o.x_ + z_ * o.w_};
+  }
+};
+
+// nanomap.h:20-28: default orientation Quaternionf(0, 0, 0, 1), i.e. w = 0, z = 1.
+struct Pose {
+  Vector3f position;
+  Quaternionf orientation;
+  Pose() : position(0.f, 0.f, 0.f), orientation(0.f, 0.f, 0.f, 1.f) {}
+  nm_pose c() const {
+    nm_pose p;
+    for (int i = 0; i < 3; ++i) p.position[i] = position(i);
+    p.orientation[0] = orientation.w();
+    p.orientation[1] = orientation.x();
+    p.orientation[2] = orientation.y();
+    p.orientation[3] = orientation.z();
+    return p;
+  }
+};
+
+namespace sensor {
+// Parsed sensor description (the parts of FrustumData / LaserData the path uses).
+class SensorData {
+ public:
+  SensorData(std::string name, const nm_sensor_desc& d) : name_(std::move(name)), desc_(d) {}
+  std::string sensorName() const { return name_; }
+  std::string getName() const { return name_; }
+  int getId() const { return desc_.id; }
+  int type() const { return desc_.type; }
+  int hRes() const { return desc_.hres; }
+  int vRes() const { return desc_.vres; }
+  const nm_sensor_desc& desc() const { return desc_; }
+  // The library-side sensor (created on first use).
+  nm_sensor handle() {
+    if (!handle_) {
+      nm_sensor s = nullptr;
+      detail::check(nm_sensor_create(detail::context(), &desc_, &s));
+      handle_.reset(s, [](nm_sensor p) { nm_sensor_destroy(p); });
+    }
+    return handle_.get();
+  }
+
+ private:
+  std::string name_;
+  nm_sensor_desc desc_;
+  std::shared_ptr<nm_sensor_s> handle_;
+};
+}  // namespace sensor
+
+namespace config {
+class Config {
+ public:
+  explicit Config(std::string configFile) : file_(std::move(configFile)) {
+    nm_config c = nullptr;
+    detail::check(nm_config_load(file_.c_str(), &c));
+    cfg_.reset(c, [](nm_config p) { nm_config_destroy(p); });
+    detail::check(nm_config_get_info(c, &info_));
+    for (int i = 0; i < info_.n_sensors; ++i) {
+      nm_sensor_desc d;
+      char name[256];
+      detail::check(nm_config_sensor(c, i, &d, name, sizeof(name)));
+      sensors_.push_back(std::make_shared<sensor::SensorData>(name, d));
+    }
+  }
+  std::vector<std::shared_ptr<sensor::SensorData>>& sensorData() { return sensors_; }
+  std::shared_ptr<sensor::SensorData> sensorData(int index, bool searchById = false) {
+    if (searchById) {
+      for (auto& s : sensors_)
+        if (s->getId() == index) return s;
+      return nullptr;
+    }
+    return (index >= 0 && index < (int)sensors_.size()) ? sensors_[index] : nullptr;
+  }
+  std::shared_ptr<sensor::SensorData> sensorData(const std::string& name) {
+    for (auto& s : sensors_)
+      if (s->getName() == name) return s;
+    return nullptr;
+  }
+  float& mappingRes() { return info_.mapping_res; }
+  float& gridRes() { return info_.grid_res; }
+  int& leafEdge() { return info_.leaf_edge; }
+  int& filterType() { return info_.filter_type; }
+  int& updateType() { return info_.update_type; }
+  int& processType() { return info_.process_type; }
+  int& precisionType() { return info_.precision_type; }
+  int& publishSensor() { return info_.publish_sensor; }
+  float& probHitThres() { return info_.prob_hit_thres; }
+  float& probMissThres() { return info_.prob_miss_thres; }
+  float& frustumAllocationFactor() { return info_.frustum_allocation_factor; }
+  std::string& config() { return file_; }
+  std::string simGrid() const { return info_.sim_grid; }
+  int agentCount() const { return info_.n_agents; }
+  nm_config handle() const { return cfg_.get(); }
+  nm_map_desc mapDesc() const {
+    nm_map_desc d;
+    detail::check(nm_config_map_desc(cfg_.get(), &d));
+    return d;
+  }
+
+ private:
+  std::string file_;
+  std::shared_ptr<nm_config_s> cfg_;
+  nm_config_info info_{};
+  std::vector<std::shared_ptr<sensor::SensorData>> sensors_;
+};
+}  // namespace config
+
+namespace map {
+// OccupancyMap.h:35-52: thresholds logit(probThres*), clamps logit(0.12) / logit(0.97).  The
+// map lives on the device; exportLeaves() copies it out.
+class Map {
+ public:
+  Map() : Map(0.1f, 0.5f, 0.5f) {}
+  Map(float gridRes, float probThresHit, float probThresMiss, float mappingRes = 0,
+      float plannerRes = 0, int nodeEdge = 0) {
+    (void)mappingRes;
+    (void)plannerRes;
+    (void)nodeEdge;
+    std::memset(&desc_, 0, sizeof(desc_));
+    desc_.res = gridRes;
+    desc_.leaf_edge = 8;
+    desc_.thres_hit = detail::logit(probThresHit);
+    desc_.thres_miss = detail::logit(probThresMiss);
+    desc_.clamp_min = detail::logit(0.12);
+    desc_.clamp_max = detail::logit(0.97);
+    desc_.clamp_mode = NM_CLAMP_ALWAYS;
+    desc_.update_mode = NM_UPDATE_LABEL;
+    desc_.rounding = NM_ROUND_DOWN;
+    desc_.max_agents = 1;
+  }
+  explicit Map(const nm_map_desc& d) : desc_(d) {}
+  float occupiedClampingThreshold() const { return desc_.clamp_max; }
+  float emptyClampingThreshold() const { return desc_.clamp_min; }
+  float logOddsHitThreshold() const { return desc_.thres_hit; }
+  float logOddsMissThreshold() const { return desc_.thres_miss; }
+  float gridRes() const { return desc_.res; }
+  nm_map_desc& desc() { return desc_; }
+  nm_map handle() {
+    if (!handle_) {
+      nm_map m = nullptr;
+      detail::check(nm_map_create(detail::context(), &desc_, &m));
+      handle_.reset(m, [](nm_map p) { nm_map_destroy(p); });
+    }
+    return handle_.get();
+  }
+  // Leaves: origins (3 per leaf), log-odds (512 per leaf), active words (16 per leaf).
+  void exportLeaves(std::vector<int32_t>& origins, std::vector<float>& values,
+                    std::vector<uint32_t>& active) {
+    uint64_t n = 0;
+    detail::check(nm_map_export(handle(), nullptr, nullptr, nullptr, 0, &n));
+    origins.resize(n * 3);
+    values.resize(n * 512);
+    active.resize(n * 16);
+    if (n) detail::check(nm_map_export(handle(), origins.data(), values.data(), active.data(), n, &n));
+  }
+  nm_stats stats() {
+    nm_stats s;
+    detail::check(nm_map_stats(handle(), &s));
+    return s;
+  }
+
+ private:
+  nm_map_desc desc_;
+  std::shared_ptr<nm_map_s> handle_;
+};
+}  // namespace map
+
+namespace agent {
+class Agent {
+ public:
+  // Agent `index` of the config (Agent.h:49-135): fixed spawn position, the reference's fixed
+  // body rotation (columns (0,-1,0), (1,0,0), (0,0,1)), sensors with mount poses.
+  Agent(config::Config& cfg, int index, std::shared_ptr<map::Map> map = nullptr) {
+    nm_agent_info a;
+    detail::check(nm_config_agent(cfg.handle(), index, &a));
+    if (a.spawn_random)
+      throw Error(NM_ERR_UNSUPPORTED, "nanomap_b200: random agent spawns need the OpenVDB sim grid");
+    pose_.position = Vector3f(a.position[0], a.position[1], a.position[2]);
+    pose_.orientation = Quaternionf(std::sqrt(0.5f), 0.f, 0.f, -std::sqrt(0.5f));
+    for (int j = 0; j < a.n_sensors; ++j) {
+      char name[256];
+      nm_pose o;
+      detail::check(nm_config_agent_sensor(cfg.handle(), index, j, name, sizeof(name), &o));
+      Pose p;
+      p.position = Vector3f(o.position[0], o.position[1], o.position[2]);
+      p.orientation = Quaternionf(o.orientation[0], o.orientation[1], o.orientation[2], o.orientation[3]);
+      names_.push_back(name);
+      origins_.push_back(p);
+    }
+    poses_ = origins_;
+    map_ = map ? map : std::make_shared<map::Map>(cfg.mapDesc());
+    updatePose(pose_);
+  }
+  // Agent.h:136-145: sensor position = agent position (the mount offset is not applied),
+  // sensor orientation = agent orientation * mount orientation.
+  void updatePose(Pose pose) {
+    pose_ = pose;
+    for (size_t i = 0; i < origins_.size(); ++i) {
+      poses_[i].position = pose_.position;
+      poses_[i].orientation = pose_.orientation * origins_[i].orientation;
+    }
+  }
+  Pose pose() const { return pose_; }
+  Pose sensorPose(int index) const { return poses_[index]; }
+  std::vector<Pose> sensorPoses() const { return poses_; }
+  std::vector<Pose> sensorOrigins() const { return origins_; }
+  std::vector<std::string> sensorNames() const { return names_; }
+  std::shared_ptr<map::Map> map() { return map_; }
+  bool spawnRandom() const { return false; }
+
+ private:
+  Pose pose_;
+  std::vector<std::string> names_;
+  std::vector<Pose> origins_, poses_;
+  std::shared_ptr<map::Map> map_;
+};
+}  // namespace agent
+
+namespace manager {
+
+using Map = nanomap::map::Map;
+
+class Manager {
+ public:
+  explicit Manager(std::shared_ptr<config::Config> config) : config_(std::move(config)) {}
+
+  void insertPointCloud(std::string sensorName, int pcl_width, int pcl_height, int pcl_step,
+                        unsigned char* cloud, const nanomap::Pose& pose, std::shared_ptr<Map> map) {
+    for (auto& s : config_->sensorData()) {
+      if (s->sensorName() != sensorName) continue;
+      const auto t0 = std::chrono::high_resolution_clock::now();
+      const nm_pose p = pose.c();
+      detail::check(nm_map_insert_points(map->handle(), s->handle(), &p, cloud, pcl_width, pcl_height,
+                                         pcl_step, NM_INPUT_HOST | NM_SYNC, nullptr));
+      const auto t1 = std::chrono::high_resolution_clock::now();
+      gpu_ms_ += std::chrono::duration<double, std::milli>(t1 - t0).count();
+    }
+  }
+  void printUpdateTime(int count) {
+    std::cout << "gpu update time per loop:" << gpu_ms_ / count << std::endl;
+    std::cout << "map update time per loop:" << 0.0 << std::endl;
+  }
+  void closeHandler() {}
+  std::shared_ptr<config::Config> config() { return config_; }
+
+ private:
+  std::shared_ptr<config::Config> config_;
+  double gpu_ms_ = 0.0;
+};
+
+class SimManager {
+ public:
+  // Loads the sim grid named by the config's SimGrid: key (NMSIMv1 voxel list) and the agents.
+  explicit SimManager(std::shared_ptr<config::Config> config) : config_(std::move(config)) {
+    nm_simmap sm = nullptr;
+    detail::check(nm_simmap_load(detail::context(), config_->simGrid().c_str(), &sm));
+    sim_.reset(sm, [](nm_simmap p) { nm_simmap_destroy(p); });
+    load_agents();
+  }
+  // With a sim map built by the caller (nm_simmap_create_primitives / _voxels).
+  SimManager(std::shared_ptr<config::Config> config, nm_simmap sim) : config_(std::move(config)) {
+    sim_.reset(sim, [](nm_simmap) {});
+    load_agents();
+  }
+
+  void updateAgentPoses(std::vector<Pose> poses) {
+    for (size_t i = 0; i < poses.size() && i < agents_.size(); ++i) agents_[i]->updatePose(poses[i]);
+  }
+  std::vector<Pose> agentPoses() {
+    std::vector<Pose> out;
+    for (auto& a : agents_) out.push_back(a->pose());
+    return out;
+  }
+  // Every agent's sensors render from the sim map and map into the agent's own map.
+  void updateAgentViews() {
+    for (auto& a : agents_) view(*a, a->map());
+  }
+  // Every agent maps into one shared map (SimManager.h:114-127).
+  void updateAgentViews(std::shared_ptr<Map> map_ptr) {
+    for (auto& a : agents_) view(*a, map_ptr);
+  }
+  std::shared_ptr<Map> getMap(int index) { return agents_[index]->map(); }
+  std::shared_ptr<agent::Agent> agent(int index) { return agents_[index]; }
+  nm_simmap simMap() { return sim_.get(); }
+  void closeHandler() {}
+
+ private:
+  void load_agents() {
+    for (int i = 0; i < config_->agentCount(); ++i)
+      agents_.push_back(std::make_shared<agent::Agent>(*config_, i));
+  }
+  // Device range buffer shared by the agents' sensors: each render writes it and the insert
+  // that follows on the same stream reads it.
+  float* buffer(size_t floats) {
+    if (floats > buf_floats_) {
+      float* p = nullptr;
+      if (buf_) nm_free_device(buf_);
+      buf_ = nullptr;
+      detail::check(nm_alloc_device(detail::context(), floats * sizeof(float), (void**)&p));
+      buf_ = p;
+      buf_floats_ = floats;
+    }
+    return buf_;
+  }
+  void view(agent::Agent& a, std::shared_ptr<Map> map) {
+    const auto names = a.sensorNames();
+    for (size_t j = 0; j < names.size(); ++j) {
+      auto s = config_->sensorData(names[j]);
+      if (!s) continue;
+      float* r = buffer((size_t)s->hRes() * s->vRes());
+      const nm_pose p = a.sensorPose((int)j).c();
+      detail::check(nm_sim_render(sim_.get(), s->handle(), &p, r, 0, nullptr));
+      detail::check(nm_map_insert_ranges(map->handle(), s->handle(), &p, r, 0, nullptr));
+    }
+  }
+
+  std::shared_ptr<config::Config> config_;
+  std::shared_ptr<nm_simmap_s> sim_;
+  std::vector<std::shared_ptr<agent::Agent>> agents_;
+  float* buf_ = nullptr;
+  size_t buf_floats_ = 0;
+
+ public:
+  ~SimManager() {
+    if (buf_) nm_free_device(buf_);
+  }
+};
+
+}  // namespace manager
+}  // namespace nanomap

@@ -78,6 +78,27 @@ class NmStats(C.Structure):
     ]
 
 
+class NmConfigInfo(C.Structure):
+    _fields_ = [
+        ("mapping_res", C.c_float), ("grid_res", C.c_float),
+        ("prob_hit_thres", C.c_float), ("prob_miss_thres", C.c_float),
+        ("frustum_allocation_factor", C.c_float),
+        ("clamp_min", C.c_float), ("clamp_max", C.c_float),
+        ("leaf_edge", C.c_int32), ("filter_type", C.c_int32), ("update_type", C.c_int32),
+        ("precision_type", C.c_int32), ("publish_sensor", C.c_int32), ("process_type", C.c_int32),
+        ("update_mode", C.c_int32), ("clamp_mode", C.c_int32), ("rounding", C.c_int32),
+        ("n_sensors", C.c_int32), ("n_agents", C.c_int32),
+        ("sim_grid", C.c_char * 512),
+    ]
+
+
+class NmAgentInfo(C.Structure):
+    _fields_ = [
+        ("spawn_random", C.c_int32), ("position", C.c_float * 3), ("num_obs", C.c_int32),
+        ("len_obs", C.c_float), ("collision_dist", C.c_float), ("n_sensors", C.c_int32),
+    ]
+
+
 class NmFrame(C.Structure):
     _fields_ = [
         ("sensor", C.c_void_p), ("pose", NmPose), ("ranges", C.c_void_p),
@@ -104,6 +125,16 @@ _SIGS = {
     "nm_context_create": (C.c_int, [_I32, C.POINTER(_P)]),
     "nm_context_destroy": (C.c_int, [_P]),
     "nm_context_sync": (C.c_int, [_P]),
+    "nm_alloc_device": (C.c_int, [_P, C.c_size_t, C.POINTER(_P)]),
+    "nm_free_device": (C.c_int, [_P]),
+    "nm_config_load": (C.c_int, [C.c_char_p, C.POINTER(_P)]),
+    "nm_config_destroy": (C.c_int, [_P]),
+    "nm_config_get_info": (C.c_int, [_P, _P]),
+    "nm_config_sensor": (C.c_int, [_P, _I32, C.POINTER(NmSensorDesc), C.c_char_p, _I32]),
+    "nm_config_agent": (C.c_int, [_P, _I32, _P]),
+    "nm_config_agent_sensor": (C.c_int, [_P, _I32, _I32, C.c_char_p, _I32, C.POINTER(NmPose)]),
+    "nm_config_map_desc": (C.c_int, [_P, C.POINTER(NmMapDesc)]),
+    "nm_simmap_load": (C.c_int, [_P, C.c_char_p, C.POINTER(_P)]),
     "nm_sensor_create": (C.c_int, [_P, C.POINTER(NmSensorDesc), C.POINTER(_P)]),
     "nm_sensor_destroy": (C.c_int, [_P]),
     "nm_sensor_params": (C.c_int, [_P, _PF]),

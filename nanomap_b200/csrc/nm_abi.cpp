@@ -499,6 +499,19 @@ int nm_context_sync(nm_context ctx) {
   return NM_OK;
 }
 
+int nm_alloc_device(nm_context ctx, size_t bytes, void** out) {
+  if (!ctx || !out) return fail(NM_ERR_ARG, "null argument");
+  *out = nullptr;
+  NM_CUDA(cudaSetDevice(ctx->device));
+  NM_CUDA(cudaMalloc(out, bytes ? bytes : 1));
+  return NM_OK;
+}
+
+int nm_free_device(void* p) {
+  NM_CUDA(cudaFree(p));
+  return NM_OK;
+}
+
 int nm_sensor_create(nm_context ctx, const nm_sensor_desc* d, nm_sensor* out) {
   if (!ctx || !d || !out) return fail(NM_ERR_ARG, "null argument");
   *out = nullptr;

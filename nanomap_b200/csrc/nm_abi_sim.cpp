@@ -4,6 +4,7 @@
 // and the generateCloud launcher (generateCloud.cu:84-94).
 #include <algorithm>
 #include <climits>
+#include <cstdio>
 #include <cmath>
 #include <cstring>
 #include <memory>
@@ -203,6 +204,32 @@ int nm_simmap_create_voxels(nm_context ctx, float res, const int32_t* ijk, int64
   if (rc != NM_OK) return rc;
   *out = sm.release();
   return NM_OK;
+}
+
+int nm_simmap_load(nm_context ctx, const char* path, nm_simmap* out) {
+  if (!ctx || !path || !out) return fail(NM_ERR_ARG, "null argument");
+  *out = nullptr;
+  const size_t len = std::strlen(path);
+  if (len >= 4 && std::strcmp(path + len - 4, ".vdb") == 0)
+    return fail(NM_ERR_UNSUPPORTED,
+                "%s: OpenVDB .vdb grids cannot be read by this build; convert the active voxels to "
+                "an NMSIMv1 voxel list", path);
+  FILE* f = std::fopen(path, "rb");
+  if (!f) return fail(NM_ERR_IO, "cannot open sim grid '%s'", path);
+  char magic[8];
+  float res = 0.f;
+  int64_t n = 0;
+  bool ok = std::fread(magic, 1, 8, f) == 8 && std::memcmp(magic, "NMSIMv1", 8) == 0 &&
+            std::fread(&res, 4, 1, f) == 1 && std::fread(&n, 8, 1, f) == 1 && n >= 0 &&
+            n < (1ll << 34);
+  std::vector<int32_t> ijk;
+  if (ok) {
+    ijk.resize((size_t)n * 3);
+    ok = n == 0 || std::fread(ijk.data(), 12, (size_t)n, f) == (size_t)n;
+  }
+  std::fclose(f);
+  if (!ok) return fail(NM_ERR_IO, "%s: not an NMSIMv1 voxel list", path);
+  return nm_simmap_create_voxels(ctx, res, ijk.data(), n, out);
 }
 
 int nm_simmap_destroy(nm_simmap sm) {

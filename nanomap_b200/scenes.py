@@ -181,8 +181,24 @@ def trajectory(scene: Scene, n: int | None = None, seed: int = 7, step: float = 
     return out
 
 
-def pose_of(entry) -> tuple:
-    return entry
+def voxels_from_leaves(origins, words) -> np.ndarray:
+    """Active voxel coordinates (n, 3) int32 from leaf origins and 16-word bit masks."""
+    origins = np.asarray(origins, np.int64)
+    bits = np.unpackbits(np.ascontiguousarray(words, dtype="<u4").view(np.uint8), bitorder="little")
+    bits = bits.reshape(len(origins), 512)
+    leaf, l = np.nonzero(bits)
+    local = np.stack([l >> 6, (l >> 3) & 7, l & 7], axis=1)
+    return (origins[leaf] + local).astype(np.int32)
+
+
+def write_nmsim(path, res: float, voxels) -> None:
+    """Write an NMSIMv1 voxel list (the sim-grid file format nm_simmap_load reads)."""
+    v = np.ascontiguousarray(voxels, dtype="<i4").reshape(-1, 3)
+    with open(path, "wb") as f:
+        f.write(b"NMSIMv1\0")
+        f.write(np.float32(res).tobytes())
+        f.write(np.int64(len(v)).tobytes())
+        f.write(v.tobytes())
 
 
 def sensor_desc_kwargs(spec: SceneSpec) -> dict:
