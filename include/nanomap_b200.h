@@ -55,6 +55,13 @@ extern "C" {
 #define NM_DEFER_INTEGRATE 0x2u  /* label only; nm_map_integrate applies the labels later */
 #define NM_SYNC 0x4u             /* wait for completion; report device-side errors now */
 #define NM_OUTPUT_HOST 0x8u      /* output pointer is host memory */
+/* Voxel filter of an insert (SensorBucket filter type 1, filterCloud.cu:463-553): the points
+ * are binned by the voxel holding their end point and one ray is traced per occupied voxel,
+ * to the mean position of its points (voxelFilter + rayFromFilter, filterCloud.cu:84-133,
+ * 279-318) or, with NM_FILTER_CENTRE, to the voxel centre (the integer-buffer variants
+ * rayFromFilterSimple / rayFromFilterSimpleQuad, filterCloud.cu:360-434). */
+#define NM_FILTER_MEAN 0x10u
+#define NM_FILTER_CENTRE 0x20u
 
 typedef struct nm_context_s* nm_context;
 typedef struct nm_sensor_s* nm_sensor;
@@ -189,6 +196,17 @@ int nm_map_insert_points(nm_map m, nm_sensor s, const nm_pose* pose, const void*
  * sensor's pixel model turns each range into a sensor-frame point on the device. */
 int nm_map_insert_ranges(nm_map m, nm_sensor s, const nm_pose* pose, const float* ranges,
                          uint32_t flags, void* stream);
+
+/* The voxel filter alone: the rays an NM_FILTER_MEAN (or NM_FILTER_CENTRE) insert of this
+ * input would trace, as `points` (3 floats per voxel: the ray's end point as a world-frame
+ * offset from the sensor position, metres) and `counts` (input points per voxel), in voxel
+ * order (x, then y, then z of the end voxel).  step > 0: `input` is an xyz cloud as in
+ * nm_map_insert_points; step == 0: `input` is a range image of the sensor (width and height
+ * ignored).  NM_INPUT_HOST marks host input; outputs are host memory; the call waits.
+ * *n receives the voxel count; at most max_points are written. */
+int nm_map_filter_points(nm_map m, nm_sensor s, const nm_pose* pose, const void* input,
+                         int32_t width, int32_t height, int32_t step, uint32_t flags,
+                         float* points, uint32_t* counts, uint64_t max_points, uint64_t* n);
 
 /* Launch shape of the traversal: tile of tile_w x tile_h pixels per work item (area 64, 128
  * or a multiple of 256 up to 4096; a CTA has min(area, 256) threads) and shared-memory

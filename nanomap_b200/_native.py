@@ -35,6 +35,8 @@ NM_INPUT_HOST = 0x1
 NM_DEFER_INTEGRATE = 0x2
 NM_SYNC = 0x4
 NM_OUTPUT_HOST = 0x8
+NM_FILTER_MEAN = 0x10
+NM_FILTER_CENTRE = 0x20
 
 
 class NanomapError(RuntimeError):
@@ -143,6 +145,8 @@ _SIGS = {
     "nm_map_reset": (C.c_int, [_P]),
     "nm_map_stats": (C.c_int, [_P, C.POINTER(NmStats)]),
     "nm_map_insert_points": (C.c_int, [_P, _P, C.POINTER(NmPose), _P, _I32, _I32, _I32, _U32, _P]),
+    "nm_map_filter_points": (C.c_int, [_P, _P, C.POINTER(NmPose), _P, _I32, _I32, _I32, _U32,
+                                       _PF, _PU32, _U64, _PU64]),
     "nm_map_insert_ranges": (C.c_int, [_P, _P, C.POINTER(NmPose), _P, _U32, _P]),
     "nm_map_integrate": (C.c_int, [_P, _P]),
     "nm_map_set_launch": (C.c_int, [_P, _I32, _I32, _I32]),

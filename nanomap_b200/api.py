@@ -185,6 +185,24 @@ class Map:
         call("nm_map_insert_ranges", self.h, sensor.h, C.byref(pose.c()), p, flags,
              _stream(stream))
 
+    def filter_points(self, sensor: Sensor, pose: Pose, data, width: int = 0, height: int = 0,
+                      step: int = 0, centre: bool = False):
+        """Voxel filter alone: (points (n,3) float32 world offsets from the sensor position,
+        counts (n,) uint32) in voxel order.  step == 0: `data` is a range image of `sensor`."""
+        p, host = _ptr(data)
+        flags = N.NM_INPUT_HOST if host else 0
+        if centre:
+            flags |= N.NM_FILTER_CENTRE
+        n = C.c_uint64()
+        args = (self.h, sensor.h, C.byref(pose.c()), p, width, height, step)
+        call("nm_map_filter_points", *args, flags, None, None, 0, C.byref(n))
+        k = n.value
+        pts = np.zeros((k, 3), np.float32)
+        cnt = np.zeros(k, np.uint32)
+        call("nm_map_filter_points", *args, flags, pts.ctypes.data_as(N._PF),
+             cnt.ctypes.data_as(N._PU32), k, C.byref(n))
+        return pts, cnt
+
     def set_launch(self, tile_w: int, tile_h: int, leaf_table_entries: int):
         call("nm_map_set_launch", self.h, tile_w, tile_h, leaf_table_entries)
 

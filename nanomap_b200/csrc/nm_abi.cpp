@@ -418,6 +418,28 @@ int set_plane_constants(nm_map m, int plane, nm_sensor s) {
   return NM_OK;
 }
 
+// Voxel filter of one frame: runs the filter on `f`'s input and rewrites `f` into the frame
+// of the filtered points (input kind 2: one record per occupied voxel, counted on the device,
+// already rotated into the world frame).  A tile of the traversal covers consecutive
+// records, i.e. neighbouring voxels.
+int apply_filter(nm_map m, nm::FrameParams& f, uint32_t flags, cudaStream_t s0) {
+  const int64_t n = (int64_t)f.width * f.height;
+  const int kb = nm::filter_key_bits(f.max_time);
+  if (kb == 0) return fail(NM_ERR_UNSUPPORTED, "voxel filter: range of %g voxels is too long", (double)f.max_time);
+  NM_CUDA(nm::filter_reserve(&m->filter, n));
+  NM_CUDA(nm::run_voxel_filter(f, m->desc.rounding, (flags & NM_FILTER_CENTRE) ? 1 : 0, kb,
+                               m->filter, s0));
+  f.input_kind = 2;
+  f.xyz = reinterpret_cast<const unsigned char*>(m->filter.out_pts);
+  f.step = 12;
+  f.ranges = nullptr;
+  f.n_points = m->filter.n_out;
+  f.width = m->tile_w;
+  f.height = (int32_t)((n + f.width - 1) / f.width);
+  for (int i = 0; i < 9; ++i) f.R[i] = (i % 4 == 0) ? 1.0f : 0.0f;
+  return NM_OK;
+}
+
 // One frame through traverse (+ integrate unless deferred).
 int run_frame(nm_map m, nm_sensor s, nm::FrameParams& f, uint32_t flags, cudaStream_t s0,
               uint64_t bound) {
@@ -607,6 +629,7 @@ int nm_map_destroy(nm_map m) {
   cudaFree(m->d_ctr);
   cudaFree(m->d_scratch_u32);
   cudaFree(m->staging);
+  nm::filter_release(&m->filter);
   delete m;
   return NM_OK;
 }
@@ -679,6 +702,10 @@ int nm_map_insert_points(nm_map m, nm_sensor s, const nm_pose* pose, const void*
   }
   f.xyz = static_cast<const unsigned char*>(dev);
   const uint64_t bound = frame_leaf_bound(m, s, *pose, f.R, false, (uint64_t)n);
+  if (flags & (NM_FILTER_MEAN | NM_FILTER_CENTRE)) {
+    rc = apply_filter(m, f, flags, s0);
+    if (rc != NM_OK) return rc;
+  }
   return run_frame(m, s, f, flags, s0, bound);
 }
 
@@ -699,7 +726,56 @@ int nm_map_insert_ranges(nm_map m, nm_sensor s, const nm_pose* pose, const float
   }
   f.ranges = static_cast<const float*>(dev);
   const uint64_t bound = frame_leaf_bound(m, s, *pose, f.R, true, (uint64_t)n);
+  if (flags & (NM_FILTER_MEAN | NM_FILTER_CENTRE)) {
+    rc = apply_filter(m, f, flags, s0);
+    if (rc != NM_OK) return rc;
+  }
   return run_frame(m, s, f, flags, s0, bound);
+}
+
+int nm_map_filter_points(nm_map m, nm_sensor s, const nm_pose* pose, const void* input,
+                         int32_t width, int32_t height, int32_t step, uint32_t flags,
+                         float* points, uint32_t* counts, uint64_t max_points, uint64_t* n) {
+  if (!m || !s || !n) return fail(NM_ERR_ARG, "null argument");
+  *n = 0;
+  if (step < 0 || (step > 0 && step < 12)) return fail(NM_ERR_ARG, "point step %d (0 = range image, else >= 12)", step);
+  if (step > 0 && (width < 0 || height < 0 || (int64_t)width * height > (1ll << 30)))
+    return fail(NM_ERR_ARG, "cloud size %dx%d out of range", width, height);
+  NM_CUDA(cudaSetDevice(m->ctx->device));
+  cudaStream_t s0 = m->ctx->stream;
+  nm::FrameParams f;
+  int rc = make_frame(m, s, pose, &f);
+  if (rc != NM_OK) return rc;
+  if (step > 0) {
+    f.width = width;
+    f.height = height;
+    f.input_kind = 0;
+    f.step = step;
+  } else {
+    f.input_kind = 1;
+  }
+  const int64_t np = (int64_t)f.width * f.height;
+  if (np > 0 && !input) return fail(NM_ERR_ARG, "input is null");
+  if (np == 0) return NM_OK;
+  const void* dev = input;
+  if (flags & NM_INPUT_HOST) {
+    rc = stage_input(m, input, (size_t)np * (step > 0 ? (size_t)step : 4u), s0, &dev);
+    if (rc != NM_OK) return rc;
+  }
+  if (step > 0)
+    f.xyz = static_cast<const unsigned char*>(dev);
+  else
+    f.ranges = static_cast<const float*>(dev);
+  rc = apply_filter(m, f, flags | NM_FILTER_MEAN, s0);
+  if (rc != NM_OK) return rc;
+  NM_CUDA(cudaStreamSynchronize(s0));
+  uint32_t cnt = 0;
+  NM_CUDA(cudaMemcpy(&cnt, m->filter.n_out, 4, cudaMemcpyDeviceToHost));
+  *n = cnt;
+  const uint64_t k = std::min<uint64_t>(cnt, max_points);
+  if (k && points) NM_CUDA(cudaMemcpy(points, m->filter.out_pts, k * 12, cudaMemcpyDeviceToHost));
+  if (k && counts) NM_CUDA(cudaMemcpy(counts, m->filter.counts, k * 4, cudaMemcpyDeviceToHost));
+  return NM_OK;
 }
 
 int nm_map_set_launch(nm_map m, int32_t tile_w, int32_t tile_h, int32_t leaf_table_entries) {

@@ -65,7 +65,7 @@ struct MapView {
 struct FrameParams {
   int32_t type;        // NM_SENSOR_FRUSTUM / NM_SENSOR_LASER
   int32_t width, height;
-  int32_t input_kind;  // 0 xyz records, 1 range image
+  int32_t input_kind;  // 0 xyz records, 1 range image, 2 xyz records counted on the device
   float hw, hh, c0, c1, su, sv;  // frustum pixel model
   const float* sinu;   // laser tables (device)
   const float* cosu;
@@ -74,6 +74,7 @@ struct FrameParams {
   const unsigned char* xyz;
   int64_t step;        // bytes between xyz records
   const float* ranges;
+  const uint32_t* n_points;  // input_kind 2: records [0, *n_points) are valid
   float R[9];          // row-major, world-from-sensor
   double eye[3];       // index-space eye
   double res_d;
@@ -130,6 +131,25 @@ __host__ __device__ inline uint32_t hash_key(uint64_t k) {
   return (uint32_t)k;
 }
 
+// Working buffers of the voxel filter, sized for `capacity` input points.
+struct FilterBuffers {
+  unsigned long long* keys_in;
+  unsigned long long* keys_out;
+  unsigned long long* group_key;
+  uint32_t* idx_in;
+  uint32_t* idx_out;
+  uint32_t* heads;
+  uint32_t* seg;
+  uint32_t* counts;
+  uint32_t* n_out;     // device count of filtered points
+  long long* frac;     // 3 fixed-point fractions per input point
+  long long* sums;     // 3 fixed-point sums per voxel
+  float* out_pts;      // 3 floats per voxel: world-frame offset from the eye (m)
+  void* temp;
+  size_t temp_bytes;
+  int64_t capacity;
+};
+
 // ---- kernel launchers (defined in the .cu files) -----------------------------------------
 template <int MaxF>
 cudaError_t launch_traverse_labels(const TickWork<MaxF>& w, const MapView& m, int rounding,
@@ -150,5 +170,10 @@ cudaError_t launch_export_labels(const MapView& m, int plane, int32_t* origins,
                                  uint32_t* words, uint32_t* n_out, uint32_t max_out,
                                  cudaStream_t s);
 cudaError_t launch_fill_keys(unsigned long long* keys, uint32_t n, cudaStream_t s);
+cudaError_t filter_reserve(FilterBuffers* b, int64_t n);
+void filter_release(FilterBuffers* b);
+int filter_key_bits(float max_time);  // bits per axis of a filter key; 0 if out of range
+cudaError_t run_voxel_filter(const FrameParams& f, int rounding, int centre, int key_bits,
+                             const FilterBuffers& b, cudaStream_t s);
 
 }  // namespace nm

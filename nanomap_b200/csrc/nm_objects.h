@@ -69,6 +69,7 @@ struct nm_map_s {
   size_t staging_bytes = 0;
   uint32_t* d_scratch_u32 = nullptr;  // export counters
   int tile_w = 16, tile_h = 16, smem_entries = 128;
+  nm::FilterBuffers filter{};  // voxel-filter buffers, grown on first filtered insert
 };
 
 struct nm_simmap_s {

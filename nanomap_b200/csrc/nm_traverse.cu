@@ -116,6 +116,7 @@ __device__ __forceinline__ bool setup_ray(const FrameParams& f, const float p[3]
 
 __device__ __forceinline__ bool pixel_point(const FrameParams& f, int w, int h, float p[3]) {
   if (f.input_kind == 1) return range_point(f, w, h, p);
+  if (f.input_kind == 2 && (uint32_t)(h * f.width + w) >= __ldg(f.n_points)) return false;
   return xyz_point(f, w, h, p);
 }
 

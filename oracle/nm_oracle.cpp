@@ -44,6 +44,7 @@
 #include <cmath>
 #include <cstdint>
 #include <cstring>
+#include <map>
 #include <mutex>
 #include <thread>
 #include <unordered_map>
@@ -626,6 +627,78 @@ int orc_map_insert(void* mp, const float R[9], const double eye[3], double res_d
   m->visits += visits;
   m->rays += rays;
   return 0;
+}
+
+// Voxel filter (filterCloud.cu:84-133 and 279-318, FilterType 1) restated in the absolute
+// index frame: every point that the insertion would trace is binned by the voxel holding its
+// end point, q = eye + (R p) / res; each occupied voxel emits one point at the mean in-voxel
+// position of its points (centre != 0: at the voxel centre, the integer-buffer variants
+// rayFromFilterSimple / rayFromFilterSimpleQuad, filterCloud.cu:360-434).  The reference keys
+// by q but accumulates fractions without the voxel-origin offset (filterCloud.cu:119 vs :126);
+// here both use q.  Fractions are summed in 32-bit fixed point (exact and order-free; the sum
+// of 2^30 fractions stays below 2^62).  Output: world-frame offsets from the eye (metres) and
+// counts, sorted by voxel key (x, then y, then z relative to the eye voxel).
+int64_t orc_voxel_filter(const float R[9], const double eye[3], double res_d, float max_time,
+                         int rounding, int centre, const float* xyz, int64_t n, int64_t stride,
+                         float* out_pts, uint32_t* out_counts, int64_t cap) {
+  struct Acc {
+    int64_t s[3];
+    uint32_t n;
+  };
+  std::map<uint64_t, Acc> bins;
+  const double kFix = 4294967296.0;  // 2^32
+  double inv_res;
+  {
+    RoundGuard g(0);
+    inv_res = 1.0 / res_d;
+  }
+  const int ev[3] = {(int)std::floor(eye[0]), (int)std::floor(eye[1]), (int)std::floor(eye[2])};
+  for (int64_t i = 0; i < n; ++i) {
+    const float* p = xyz + i * stride;
+    float d[3];
+    bool valid;
+    {
+      RoundGuard g(rounding);
+      d[0] = (R[0] * p[0] + R[1] * p[1]) + R[2] * p[2];
+      d[1] = (R[3] * p[0] + R[4] * p[1]) + R[5] * p[2];
+      d[2] = (R[6] * p[0] + R[7] * p[1]) + R[8] * p[2];
+      const double dx = d[0], dy = d[1], dz = d[2];
+      const double len = std::sqrt((dx * dx + dy * dy) + dz * dz);
+      const double ray_len = len / res_d;
+      valid = (ray_len < (double)max_time) && (len > kMinLen);
+    }
+    if (!valid) continue;
+    RoundGuard g(0);
+    int64_t F[3];
+    uint64_t key = 0;
+    for (int a = 0; a < 3; ++a) {
+      const double q = eye[a] + (double)d[a] * inv_res;
+      const double v = std::floor(q);
+      const double f = q - v;
+      F[a] = (int64_t)(f * kFix);
+      const int dv = (int)v - ev[a];
+      key = (key << 21) | (uint64_t)((uint32_t)(dv + (1 << 20)) & 0x1FFFFFu);
+    }
+    Acc& A = bins[key];
+    for (int a = 0; a < 3; ++a) A.s[a] += F[a];
+    A.n += 1;
+  }
+  RoundGuard g(0);
+  int64_t k = 0;
+  for (auto& kv : bins) {
+    if (k < cap && out_pts && out_counts) {
+      for (int a = 0; a < 3; ++a) {
+        const int dv = (int)((kv.first >> (42 - 21 * a)) & 0x1FFFFFu) - (1 << 20);
+        const double v = (double)(ev[a] + dv);
+        const double mean =
+            centre ? 0.5 : ((double)kv.second.s[a] / (double)kv.second.n) * (1.0 / kFix);
+        out_pts[3 * k + a] = (float)(((v + mean) - eye[a]) * res_d);
+      }
+      out_counts[k] = kv.second.n;
+    }
+    ++k;
+  }
+  return (int64_t)bins.size();
 }
 
 // Labels of the last frame inserted with keep_labels (label mode), sorted by leaf key.

@@ -86,6 +86,9 @@ def lib() -> C.CDLL:
         L.orc_simmap_count.argtypes = [C.c_void_p]
         L.orc_simmap_count.restype = C.c_int64
         L.orc_sim_render.argtypes = [C.c_void_p, C.POINTER(OrcSensor), _PF, _PF, _PF, C.c_int]
+        L.orc_voxel_filter.argtypes = [_PF, _PD, C.c_double, C.c_float, C.c_int, C.c_int, _PF, C.c_int64,
+                                        C.c_int64, _PF, _PU32, C.c_int64]
+        L.orc_voxel_filter.restype = C.c_int64
         L.orc_render_boxes.argtypes = [C.POINTER(OrcSensor), _PD, _PD, _PD, C.c_int, _PF]
         _lib = L
     return _lib
@@ -280,6 +283,20 @@ def render_boxes(sensor: Sensor, pos, R64, boxes) -> np.ndarray:
     b = _d(boxes)
     lib().orc_render_boxes(C.byref(sensor.s), dp(p), dp(R), dp(b), len(b), fp(out))
     return out
+
+
+def voxel_filter(R, eye, res, max_time, rounding, points, centre=False):
+    """Filtered points (world offsets from the eye, metres) and counts, sorted by voxel key."""
+    pts = _f(points).reshape(-1, 3)
+    R = _f(R)
+    eye = _d(eye)
+    args = (fp(R), dp(eye), C.c_double(float(np.float32(res))), C.c_float(max_time), rounding,
+            1 if centre else 0, fp(pts), len(pts), 3)
+    n = lib().orc_voxel_filter(*args, None, None, 0)
+    out = np.zeros((n, 3), np.float32)
+    cnt = np.zeros(n, np.uint32)
+    lib().orc_voxel_filter(*args, fp(out), cnt.ctypes.data_as(_PU32), n)
+    return out, cnt
 
 
 def sort_leaves(origins, *arrays):
