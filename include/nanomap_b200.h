@@ -284,6 +284,60 @@ int nm_label_frame_static(nm_sensor s, const nm_pose* pose, const float* ranges,
                           int32_t rounding, int32_t* origins, uint32_t* words,
                           uint32_t max_leaves, uint32_t* status, uint32_t flags, void* stream);
 
+/* ---- soft expected-depth rendering, its adjoint, scan-to-map pose refinement ------------
+ * No reference counterpart: an addition beside the unchanged mapping path, reading the
+ * device map in place.  Per pixel ray (the sensor's pixel model, double precision): voxel DDA
+ * from the voxel holding the sensor over [0, max_range / res].  Occupancy
+ * o = sigmoid(scale * log-odds + bias) (log-odds 0 where the map has no leaf) is the
+ * probability that the ray ends within one voxel length of a voxel: a segment of length D_k in
+ * voxel k ends it with probability 1 - (1 - o_k)^D_k (density softplus(scale * L + bias)); the
+ * voxel holding the sensor is empty.  The expected depth, with the remaining probability at
+ * max range, is res times the integral of the transmittance, accumulated in FP32 (metres).  It
+ * is continuous in the pose. */
+
+/* Sensor pose with double precision: position (m) and world-from-sensor rotation (row-major,
+ * the sensor's frame transform included). */
+typedef struct {
+  double position[3];
+  double rotation[9];
+} nm_ray_pose;
+
+/* rotation = rot(q / |q|) * frame_transform, evaluated in double and not rounded to float. */
+int nm_ray_pose_from_pose(nm_sensor s, const nm_pose* pose, nm_ray_pose* out);
+
+/* The map's log-odds in slot layout (capacity * 512 floats, device to device); *n_floats
+ * receives the size.  `values` arguments below take this layout (NULL = the map's own). */
+int nm_map_values_copy(nm_map m, float* dst, uint64_t max_floats, uint64_t* n_floats,
+                       void* stream);
+/* Leaf origin (voxel units, 3 ints) of every slot, INT32_MIN for empty slots (host output). */
+int nm_map_slot_origins(nm_map m, int32_t* origins, uint64_t max_slots, uint64_t* n_slots);
+
+/* Expected depth of every pixel (hres*vres floats, device).  `values` holds n_floats floats
+ * (at least the map's capacity * 512; NULL = the map's own log-odds). */
+int nm_depth_render(nm_map m, nm_sensor s, const nm_ray_pose* pose, const float* values,
+                    uint64_t n_floats, float scale, float bias, float* depth, void* stream);
+
+/* Adjoint: for upstream gradients grad_depth (hres*vres floats, device), adds
+ * sum_pixels grad_depth * dD/dlog-odds into grad_values (slot layout, device, n_floats
+ * floats like `values`; may be NULL)
+ * and writes sum_pixels grad_depth * dD/dxi to grad_pose (host; may be NULL) for the
+ * world-frame pose increment xi = (rho, phi): position + rho, rotation exp([phi]x) R.
+ * The traversal is replayed, not stored (memory independent of ray length). */
+int nm_depth_backward(nm_map m, nm_sensor s, const nm_ray_pose* pose, const float* values,
+                      uint64_t n_floats, float scale, float bias, const float* grad_depth,
+                      float* grad_values, double grad_pose[6], void* stream);
+
+/* Scan-to-map pose refinement: `steps` Adam steps (learning rates lr_position in metres,
+ * lr_rotation in radians, decayed to zero over the steps by a cosine schedule) on the mean
+ * L1 distance between the expected depth and `target`, each residual truncated at
+ * max_residual metres when that is positive (0 = plain L1)
+ * (hres*vres floats, device; <= 0 or NaN = no return), each step re-linearised at the
+ * current pose.  `pose` is updated in place; losses (host, steps + 1 floats, may be NULL)
+ * receives the loss before each step and after the last. */
+int nm_pose_refine(nm_map m, nm_sensor s, nm_ray_pose* pose, const float* target, float scale,
+                   float bias, float max_residual, int32_t steps, float lr_position,
+                   float lr_rotation, float* losses);
+
 /* ---- simulation map (replaces the NanoVDB sim grid, SimHandler.cpp:13-24) -------------- */
 /* Voxelise primitives into a sparse device map: boxes are 6 doubles (min xyz, max xyz, m);
  * cylinders are 5 doubles (cx, cy, radius, z0, z1, m).  A voxel is active when its centre is

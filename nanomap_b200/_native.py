@@ -101,6 +101,10 @@ class NmAgentInfo(C.Structure):
     ]
 
 
+class NmRayPose(C.Structure):
+    _fields_ = [("position", C.c_double * 3), ("rotation", C.c_double * 9)]
+
+
 class NmFrame(C.Structure):
     _fields_ = [
         ("sensor", C.c_void_p), ("pose", NmPose), ("ranges", C.c_void_p),
@@ -145,6 +149,14 @@ _SIGS = {
     "nm_map_reset": (C.c_int, [_P]),
     "nm_map_stats": (C.c_int, [_P, C.POINTER(NmStats)]),
     "nm_map_insert_points": (C.c_int, [_P, _P, C.POINTER(NmPose), _P, _I32, _I32, _I32, _U32, _P]),
+    "nm_ray_pose_from_pose": (C.c_int, [_P, C.POINTER(NmPose), C.POINTER(NmRayPose)]),
+    "nm_map_values_copy": (C.c_int, [_P, _P, _U64, _PU64, _P]),
+    "nm_map_slot_origins": (C.c_int, [_P, _PI32, _U64, _PU64]),
+    "nm_depth_render": (C.c_int, [_P, _P, C.POINTER(NmRayPose), _P, _U64, _F, _F, _P, _P]),
+    "nm_depth_backward": (C.c_int, [_P, _P, C.POINTER(NmRayPose), _P, _U64, _F, _F, _P, _P, _PD,
+                                    _P]),
+    "nm_pose_refine": (C.c_int, [_P, _P, C.POINTER(NmRayPose), _P, _F, _F, _F, _I32, _F, _F,
+                                 _PF]),
     "nm_map_filter_points": (C.c_int, [_P, _P, C.POINTER(NmPose), _P, _I32, _I32, _I32, _U32,
                                        _PF, _PU32, _U64, _PU64]),
     "nm_map_insert_ranges": (C.c_int, [_P, _P, C.POINTER(NmPose), _P, _U32, _P]),

@@ -41,6 +41,17 @@ def _stream(stream):
     return C.c_void_p(stream.cuda_stream)
 
 
+def _ray_pose(position, rotation) -> N.NmRayPose:
+    rp = N.NmRayPose()
+    pos = np.asarray(position, np.float64).reshape(3)
+    rot = np.asarray(rotation, np.float64).reshape(9)
+    for i in range(3):
+        rp.position[i] = float(pos[i])
+    for i in range(9):
+        rp.rotation[i] = float(rot[i])
+    return rp
+
+
 def make_pose(position, orientation) -> N.NmPose:
     p = N.NmPose()
     for i in range(3):
@@ -202,6 +213,74 @@ class Map:
         call("nm_map_filter_points", *args, flags, pts.ctypes.data_as(N._PF),
              cnt.ctypes.data_as(N._PU32), k, C.byref(n))
         return pts, cnt
+
+    # ---- expected-depth rendering (device map read in place) ----------------------------
+    @staticmethod
+    def ray_pose(sensor: Sensor, pose: Pose):
+        """(position (3,), rotation (3, 3)) float64 of the sensor, frame transform included."""
+        rp = N.NmRayPose()
+        call("nm_ray_pose_from_pose", sensor.h, C.byref(pose.c()), C.byref(rp))
+        return np.array(rp.position[:]), np.array(rp.rotation[:]).reshape(3, 3)
+
+    def values_copy(self):
+        """The map's log-odds in slot layout as a (capacity, 512) float32 CUDA tensor."""
+        import torch
+        n = C.c_uint64()
+        call("nm_map_values_copy", self.h, None, 0, C.byref(n), None)
+        out = torch.empty(n.value, dtype=torch.float32, device="cuda")
+        call("nm_map_values_copy", self.h, C.c_void_p(out.data_ptr()), n.value, C.byref(n),
+             _stream(torch.cuda.current_stream()))
+        return out.view(-1, 512)
+
+    def slot_origins(self):
+        """(capacity, 3) int32 leaf origin of every slot (INT32_MIN for empty slots)."""
+        n = C.c_uint64()
+        call("nm_map_slot_origins", self.h, None, 0, C.byref(n))
+        out = np.zeros((n.value, 3), np.int32)
+        call("nm_map_slot_origins", self.h, out.ctypes.data_as(N._PI32), n.value, C.byref(n))
+        return out
+
+    def depth_render(self, sensor: Sensor, position, rotation, values=None, scale=1.0,
+                     bias=0.0):
+        """Expected depth (vres, hres) float32 CUDA tensor at a float64 sensor pose."""
+        import torch
+        rp = _ray_pose(position, rotation)
+        out = torch.empty((sensor.desc.vres, sensor.desc.hres), dtype=torch.float32, device="cuda")
+        vp = C.c_void_p(values.data_ptr()) if values is not None else None
+        nv = values.numel() if values is not None else 0
+        call("nm_depth_render", self.h, sensor.h, C.byref(rp), vp, nv, scale, bias,
+             C.c_void_p(out.data_ptr()), _stream(torch.cuda.current_stream()))
+        return out
+
+    def depth_backward(self, sensor: Sensor, position, rotation, grad_depth, values=None,
+                       grad_values=None, scale=1.0, bias=0.0):
+        """Adds sum grad_depth * dD/dlog-odds into grad_values (slot layout) and returns
+        sum grad_depth * dD/dxi (6,) float64 for xi = (rho, phi)."""
+        import torch
+        rp = _ray_pose(position, rotation)
+        g = np.zeros(6)
+        gd = grad_depth.contiguous()
+        vp = C.c_void_p(values.data_ptr()) if values is not None else None
+        gv = C.c_void_p(grad_values.data_ptr()) if grad_values is not None else None
+        sizes = [t.numel() for t in (values, grad_values) if t is not None]
+        nv = min(sizes) if sizes else 0
+        call("nm_depth_backward", self.h, sensor.h, C.byref(rp), vp, nv, scale, bias,
+             C.c_void_p(gd.data_ptr()), gv, g.ctypes.data_as(N._PD),
+             _stream(torch.cuda.current_stream()))
+        return g
+
+    def pose_refine(self, sensor: Sensor, position, rotation, target, steps=50,
+                    lr_position=0.005, lr_rotation=0.002, scale=1.0, bias=0.0,
+                    max_residual=0.0):
+        """Native Adam refinement; returns (position, rotation, losses (steps + 1,))."""
+        import torch
+        torch.cuda.current_stream().synchronize()
+        rp = _ray_pose(position, rotation)
+        losses = np.zeros(steps + 1, np.float32)
+        t = target.contiguous()
+        call("nm_pose_refine", self.h, sensor.h, C.byref(rp), C.c_void_p(t.data_ptr()), scale,
+             bias, max_residual, steps, lr_position, lr_rotation, losses.ctypes.data_as(N._PF))
+        return np.array(rp.position[:]), np.array(rp.rotation[:]).reshape(3, 3), losses
 
     def set_launch(self, tile_w: int, tile_h: int, leaf_table_entries: int):
         call("nm_map_set_launch", self.h, tile_w, tile_h, leaf_table_entries)

@@ -630,6 +630,7 @@ int nm_map_destroy(nm_map m) {
   cudaFree(m->d_scratch_u32);
   cudaFree(m->staging);
   nm::filter_release(&m->filter);
+  cudaFree(m->depth_scratch);
   delete m;
   return NM_OK;
 }

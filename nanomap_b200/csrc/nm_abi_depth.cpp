@@ -1,0 +1,253 @@
+// nm_abi_depth.cpp -- C ABI of the soft expected-depth renderer, its adjoint, and scan-to-map
+// pose refinement.  No reference counterpart: these run beside the unchanged mapping path and
+// read the device map in place.
+#include <algorithm>
+#include <climits>
+#include <cmath>
+#include <cstring>
+#include <vector>
+
+#include "nm_host.h"
+#include "nm_objects.h"
+
+using nm::fail;
+
+namespace {
+
+bool finite_all(const double* v, int n) {
+  for (int i = 0; i < n; ++i)
+    if (!std::isfinite(v[i])) return false;
+  return true;
+}
+
+int make_depth_params(nm_map m, nm_sensor s, const nm_ray_pose* rp, float scale, float bias,
+                      nm::DepthParams* p) {
+  if (!m || !s || !rp) return fail(NM_ERR_ARG, "null argument");
+  if (s->ctx != m->ctx) return fail(NM_ERR_ARG, "sensor and map belong to different contexts");
+  if (!finite_all(rp->position, 3) || !finite_all(rp->rotation, 9))
+    return fail(NM_ERR_ARG, "ray pose is not finite");
+  if (!std::isfinite(scale) || !std::isfinite(bias)) return fail(NM_ERR_ARG, "scale/bias not finite");
+  std::memset(p, 0, sizeof(*p));
+  p->type = s->desc.type;
+  p->width = s->desc.hres;
+  p->height = s->desc.vres;
+  p->hw = s->fp[0];
+  p->hh = s->fp[1];
+  p->c0 = s->fp[2];
+  p->c1 = s->fp[3];
+  p->su = s->fp[4];
+  p->sv = s->fp[5];
+  if (s->desc.type == NM_SENSOR_LASER) {
+    p->sinu = s->d_tables;
+    p->cosu = s->d_tables + s->desc.hres;
+    p->sinv = s->d_tables + 2 * s->desc.hres;
+    p->cosv = s->d_tables + 2 * s->desc.hres + s->desc.vres;
+  }
+  nm::RoundScope rs(NM_ROUND_NEAREST);
+  p->res = (double)m->desc.res;
+  for (int i = 0; i < 9; ++i) p->R[i] = rp->rotation[i];
+  for (int a = 0; a < 3; ++a) p->eye[a] = rp->position[a] / p->res;
+  p->t_max = (double)s->desc.max_range / p->res;
+  p->scale = scale;
+  p->bias = bias;
+  for (int a = 0; a < 3; ++a)
+    if (std::fabs(p->eye[a]) + p->t_max + 2.0 > (double)(1 << 23) - 16.0)
+      return fail(NM_ERR_ARG, "pose is outside the map's addressable range (+-%d voxels)", 1 << 23);
+  return NM_OK;
+}
+
+// Caller arrays in slot layout must cover every slot the kernels can address.
+int check_values_len(nm_map m, const float* values, const float* grad_values, uint64_t n) {
+  if (!values && !grad_values) return NM_OK;
+  const uint64_t need = (uint64_t)m->view.capacity * nm::kLeafVoxels;
+  if (n < need)
+    return fail(NM_ERR_ARG, "log-odds arrays hold %llu floats, the map's %u slots need %llu",
+                (unsigned long long)n, m->view.capacity, (unsigned long long)need);
+  return NM_OK;
+}
+
+int reserve_scratch(nm_map m, size_t n) {
+  if (n <= m->depth_scratch_n) return NM_OK;
+  cudaFree(m->depth_scratch);
+  m->depth_scratch = nullptr;
+  m->depth_scratch_n = 0;
+  NM_CUDA(cudaMalloc((void**)&m->depth_scratch, n * sizeof(double)));
+  m->depth_scratch_n = n;
+  return NM_OK;
+}
+
+// exp([phi]x) R (Rodrigues), row-major, in place.
+void rotate_left(const double phi[3], double R[9]) {
+  const double th = std::sqrt(phi[0] * phi[0] + phi[1] * phi[1] + phi[2] * phi[2]);
+  double K[9] = {0, -phi[2], phi[1], phi[2], 0, -phi[0], -phi[1], phi[0], 0};
+  double E[9] = {1, 0, 0, 0, 1, 0, 0, 0, 1};
+  if (th > 0.0) {
+    const double a = std::sin(th) / th, b = (1.0 - std::cos(th)) / (th * th);
+    double K2[9];
+    for (int r = 0; r < 3; ++r)
+      for (int c = 0; c < 3; ++c)
+        K2[3 * r + c] = K[3 * r] * K[c] + K[3 * r + 1] * K[3 + c] + K[3 * r + 2] * K[6 + c];
+    for (int i = 0; i < 9; ++i) E[i] += a * K[i] + b * K2[i];
+  }
+  double out[9];
+  for (int r = 0; r < 3; ++r)
+    for (int c = 0; c < 3; ++c)
+      out[3 * r + c] = E[3 * r] * R[c] + E[3 * r + 1] * R[3 + c] + E[3 * r + 2] * R[6 + c];
+  std::memcpy(R, out, sizeof(out));
+}
+
+}  // namespace
+
+extern "C" {
+
+int nm_ray_pose_from_pose(nm_sensor s, const nm_pose* pose, nm_ray_pose* out) {
+  if (!s || !out) return fail(NM_ERR_ARG, "null argument");
+  const int rc = nm::validate_pose(pose);
+  if (rc != NM_OK) return rc;
+  nm::RoundScope rs(NM_ROUND_NEAREST);
+  double w = pose->orientation[0], x = pose->orientation[1], y = pose->orientation[2],
+         z = pose->orientation[3];
+  const double n = std::sqrt(w * w + x * x + y * y + z * z);
+  w /= n;
+  x /= n;
+  y /= n;
+  z /= n;
+  const double M[9] = {1.0 - 2.0 * (y * y + z * z), 2.0 * (x * y - w * z), 2.0 * (x * z + w * y),
+                       2.0 * (x * y + w * z), 1.0 - 2.0 * (x * x + z * z), 2.0 * (y * z - w * x),
+                       2.0 * (x * z - w * y), 2.0 * (y * z + w * x), 1.0 - 2.0 * (x * x + y * y)};
+  const float* F = s->desc.frame_transform;  // column-major
+  for (int r = 0; r < 3; ++r)
+    for (int c = 0; c < 3; ++c)
+      out->rotation[3 * r + c] = M[3 * r] * (double)F[3 * c] + M[3 * r + 1] * (double)F[3 * c + 1] +
+                                 M[3 * r + 2] * (double)F[3 * c + 2];
+  for (int a = 0; a < 3; ++a) out->position[a] = (double)pose->position[a];
+  return NM_OK;
+}
+
+int nm_map_values_copy(nm_map m, float* dst, uint64_t max_floats, uint64_t* n_floats,
+                       void* stream) {
+  if (!m || !n_floats) return fail(NM_ERR_ARG, "null argument");
+  const uint64_t n = (uint64_t)m->view.capacity * nm::kLeafVoxels;
+  *n_floats = n;
+  if (!dst) return NM_OK;
+  if (max_floats < n) return fail(NM_ERR_ARG, "destination holds %llu floats, map needs %llu",
+                                  (unsigned long long)max_floats, (unsigned long long)n);
+  NM_CUDA(cudaSetDevice(m->ctx->device));
+  NM_CUDA(cudaMemcpyAsync(dst, m->view.values, n * sizeof(float), cudaMemcpyDeviceToDevice,
+                          nm::pick(m->ctx, stream)));
+  return NM_OK;
+}
+
+int nm_map_slot_origins(nm_map m, int32_t* origins, uint64_t max_slots, uint64_t* n_slots) {
+  if (!m || !n_slots) return fail(NM_ERR_ARG, "null argument");
+  const uint32_t C = m->view.capacity;
+  *n_slots = C;
+  if (!origins) return NM_OK;
+  NM_CUDA(cudaSetDevice(m->ctx->device));
+  NM_CUDA(cudaDeviceSynchronize());
+  std::vector<unsigned long long> keys(C);
+  NM_CUDA(cudaMemcpy(keys.data(), m->view.keys, (size_t)C * 8, cudaMemcpyDeviceToHost));
+  const uint64_t k = std::min<uint64_t>(C, max_slots);
+  for (uint64_t i = 0; i < k; ++i) {
+    if (keys[i] == nm::kEmptyKey) {
+      origins[3 * i] = origins[3 * i + 1] = origins[3 * i + 2] = INT32_MIN;
+    } else {
+      int lx, ly, lz;
+      nm::key_leaf(keys[i], &lx, &ly, &lz);
+      origins[3 * i] = lx * 8;
+      origins[3 * i + 1] = ly * 8;
+      origins[3 * i + 2] = lz * 8;
+    }
+  }
+  return NM_OK;
+}
+
+int nm_depth_render(nm_map m, nm_sensor s, const nm_ray_pose* pose, const float* values,
+                    uint64_t n_floats, float scale, float bias, float* depth, void* stream) {
+  nm::DepthParams p;
+  int rc = make_depth_params(m, s, pose, scale, bias, &p);
+  if (rc != NM_OK) return rc;
+  if (!depth) return fail(NM_ERR_ARG, "depth is null");
+  rc = check_values_len(m, values, nullptr, n_floats);
+  if (rc != NM_OK) return rc;
+  NM_CUDA(cudaSetDevice(m->ctx->device));
+  NM_CUDA(nm::launch_depth_forward(p, m->view, values ? values : m->view.values, depth,
+                                   nm::pick(m->ctx, stream)));
+  return NM_OK;
+}
+
+int nm_depth_backward(nm_map m, nm_sensor s, const nm_ray_pose* pose, const float* values,
+                      uint64_t n_floats, float scale, float bias, const float* grad_depth,
+                      float* grad_values, double grad_pose[6], void* stream) {
+  nm::DepthParams p;
+  int rc = make_depth_params(m, s, pose, scale, bias, &p);
+  if (rc != NM_OK) return rc;
+  if (!grad_depth) return fail(NM_ERR_ARG, "grad_depth is null");
+  rc = check_values_len(m, values, grad_values, n_floats);
+  if (rc != NM_OK) return rc;
+  NM_CUDA(cudaSetDevice(m->ctx->device));
+  const int nb = nm::depth_partial_blocks(p);
+  rc = reserve_scratch(m, (size_t)nb * 6 + 8);
+  if (rc != NM_OK) return rc;
+  cudaStream_t s0 = nm::pick(m->ctx, stream);
+  double* out6 = m->depth_scratch + (size_t)nb * 6;
+  NM_CUDA(nm::launch_depth_backward(p, m->view, values ? values : m->view.values, grad_depth,
+                                    grad_values, m->depth_scratch, out6, s0));
+  if (grad_pose) {
+    NM_CUDA(cudaMemcpyAsync(grad_pose, out6, 6 * sizeof(double), cudaMemcpyDeviceToHost, s0));
+    NM_CUDA(cudaStreamSynchronize(s0));
+  }
+  return NM_OK;
+}
+
+int nm_pose_refine(nm_map m, nm_sensor s, nm_ray_pose* pose, const float* target, float scale,
+                   float bias, float max_residual, int32_t steps, float lr_position,
+                   float lr_rotation, float* losses) {
+  if (!pose || !target) return fail(NM_ERR_ARG, "null argument");
+  if (!(max_residual >= 0.0f)) return fail(NM_ERR_ARG, "max_residual must be >= 0");
+  if (steps < 0) return fail(NM_ERR_ARG, "steps must be >= 0");
+  if (!(lr_position >= 0.0f) || !(lr_rotation >= 0.0f)) return fail(NM_ERR_ARG, "bad learning rate");
+  nm::DepthParams p;
+  int rc = make_depth_params(m, s, pose, scale, bias, &p);
+  if (rc != NM_OK) return rc;
+  NM_CUDA(cudaSetDevice(m->ctx->device));
+  const int nb = nm::depth_partial_blocks(p);
+  rc = reserve_scratch(m, (size_t)nb * 8 + 8);
+  if (rc != NM_OK) return rc;
+  cudaStream_t s0 = m->ctx->stream;
+  double* out8 = m->depth_scratch + (size_t)nb * 8;
+  // Adam on the left world-frame increment (rho, phi), re-linearised at every step, with the
+  // learning rates decayed to zero over the steps (cosine schedule).
+  const double b1 = 0.9, b2 = 0.999, eps = 1e-8;
+  double mom[6] = {0, 0, 0, 0, 0, 0}, var[6] = {0, 0, 0, 0, 0, 0};
+  nm_ray_pose cur = *pose;
+  for (int it = 0; it <= steps; ++it) {
+    rc = make_depth_params(m, s, &cur, scale, bias, &p);
+    if (rc != NM_OK) return rc;
+    NM_CUDA(nm::launch_depth_refine(p, m->view, m->view.values, target, max_residual,
+                                    m->depth_scratch, out8, s0));
+    double h[8];
+    NM_CUDA(cudaMemcpyAsync(h, out8, sizeof(h), cudaMemcpyDeviceToHost, s0));
+    NM_CUDA(cudaStreamSynchronize(s0));
+    if (h[1] < 1.0) return fail(NM_ERR_ARG, "target has no valid pixels");
+    if (losses) losses[it] = (float)(h[0] / h[1]);
+    if (it == steps) break;
+    const double t = (double)(it + 1);
+    const double decay = 0.5 * (1.0 + std::cos(3.14159265358979323846 * it / steps));
+    double step[6];
+    for (int i = 0; i < 6; ++i) {
+      const double g = h[2 + i] / h[1];
+      mom[i] = b1 * mom[i] + (1.0 - b1) * g;
+      var[i] = b2 * var[i] + (1.0 - b2) * g * g;
+      const double mh = mom[i] / (1.0 - std::pow(b1, t));
+      const double vh = var[i] / (1.0 - std::pow(b2, t));
+      step[i] = -decay * (i < 3 ? lr_position : lr_rotation) * mh / (std::sqrt(vh) + eps);
+    }
+    for (int a = 0; a < 3; ++a) cur.position[a] += step[a];
+    rotate_left(step + 3, cur.rotation);
+  }
+  *pose = cur;
+  return NM_OK;
+}
+
+}  // extern "C"

@@ -1,0 +1,347 @@
+// nm_depth.cu -- soft expected-depth renderer over the device map, its adjoint, and the
+// per-step kernel of scan-to-map pose refinement (sm_100a).  No reference counterpart.
+//
+// Per pixel ray (sensor pixel model, double): voxel DDA from the voxel holding the eye.  Every
+// voxel after it, entered at t_in < t_max and left at t_out (clamped to t_max), carries the
+// density sigma = softplus(scale L + bias) (L the map's log-odds, 0 for voxels of absent
+// leaves), so that sigmoid(scale L + bias) is the probability of the ray ending within one
+// voxel length of it; the start voxel holds the sensor and is empty.  The expected depth
+// (remaining probability placed at t_max) is the integral of the transmittance:
+//   D = res (t_1 + sum_k T_k (1 - exp(-sigma_k D_k)) / sigma_k),  T_{k+1} = T_k exp(-sigma_k D_k)
+// with D_k = t_out - t_in, accumulated in FP32.  D is continuous in the pose.
+// The adjoint replays the traversal twice instead of storing it: the first replay rebuilds D;
+// the second walks front to back with the running prefix P of the transmittance integral, so
+// the tail S = D/res - t_1 - P needs no per-ray storage:
+//   dD/dsigma_k = res (T_k D_k^2 g(sigma_k D_k) - D_k S_k),  g(u) = (u e^-u - 1 + e^-u) / u^2
+//   crossing c from voxel A into B: dD/dc = res (sigma_B - sigma_A) * (tail after c),
+//     c = (b - e_a) / d_a  ->  dc/de_a = -1/d_a,  dc/dd_a = -c/d_a
+// and for a left world-frame pose perturbation (rho, phi): dD/drho = dD_idx/de,
+// dD/dphi = res (d x dD_idx/dd).  The DDA runs in double with explicit round-to-nearest
+// operations (no contraction), so its voxel sequence equals the FP64 CPU definition's.
+#include <math_constants.h>
+
+#include <cstdint>
+
+#include "nm_device.cuh"
+#include "nm_internal.h"
+
+namespace nm {
+
+namespace {
+
+constexpr int kDepthTile = 16;  // 16 x 16 pixels per CTA
+
+struct LeafCache {
+  unsigned long long key;
+  int slot;
+};
+
+__device__ __forceinline__ void pixel_dir(const DepthParams& p, int w, int h, double d[3]) {
+  double x, y, z;
+  if (p.type == NM_SENSOR_FRUSTUM) {
+    const double u = __dmul_rn((double)w, (double)p.su);
+    const double v = __dmul_rn((double)h, (double)p.sv);
+    x = __dadd_rn(__dmul_rn(u, (double)p.c0), -(double)p.hw);
+    y = __dadd_rn(__dmul_rn(v, (double)p.c1), -(double)p.hh);
+    z = 1.0;
+  } else {
+    x = __dmul_rn((double)__ldg(&p.sinu[w]), (double)__ldg(&p.cosv[h]));
+    y = (double)__ldg(&p.sinv[h]);
+    z = __dmul_rn((double)__ldg(&p.cosu[w]), (double)__ldg(&p.cosv[h]));
+  }
+  const double n = __dsqrt_rn(__dadd_rn(__dadd_rn(__dmul_rn(x, x), __dmul_rn(y, y)), __dmul_rn(z, z)));
+  x = __ddiv_rn(x, n);
+  y = __ddiv_rn(y, n);
+  z = __ddiv_rn(z, n);
+#pragma unroll
+  for (int i = 0; i < 3; ++i)
+    d[i] = __dadd_rn(__dadd_rn(__dmul_rn(p.R[3 * i], x), __dmul_rn(p.R[3 * i + 1], y)),
+                     __dmul_rn(p.R[3 * i + 2], z));
+}
+
+__device__ __forceinline__ float softplus(float x) {
+  return x > 0.0f ? x + log1pf(expf(-x)) : log1pf(expf(x));
+}
+
+// (1 - exp(-sigma D)) / sigma: the segment's transmittance integral per unit entry transmittance.
+__device__ __forceinline__ float seg_integral(float sigma, float D) {
+  return sigma > 0.0f ? -expm1f(-sigma * D) / sigma : D;
+}
+
+// g(u) = (u e^-u - 1 + e^-u) / u^2, -1/2 at u = 0.
+__device__ __forceinline__ float seg_g(float u) {
+  if (u < 1e-2f) return -0.5f + u * (1.0f / 3.0f) - u * u * 0.125f;
+  return (u * expf(-u) + expm1f(-u)) / (u * u);
+}
+
+// Visits every voxel of the ray after the start voxel: f(v, t_in, a_in, t_out, a_out), the
+// voxel entered at t_in < t_max across axis a_in and left at t_out = min(next crossing,
+// t_max) across a_out (-1 when clamped to t_max).
+template <class F>
+__device__ __forceinline__ void walk(const double e[3], const double d[3], double t_max, F&& f) {
+  int v[3], s[3];
+  double tn[3];
+#pragma unroll
+  for (int a = 0; a < 3; ++a) {
+    v[a] = (int)floor(e[a]);
+    s[a] = d[a] > 0.0 ? 1 : (d[a] < 0.0 ? -1 : 0);
+    tn[a] = s[a] ? __ddiv_rn(__dadd_rn((double)(v[a] + (s[a] > 0 ? 1 : 0)), -e[a]), d[a]) : CUDART_INF;
+  }
+  int a_in = 2;
+  if (tn[1] < tn[a_in]) a_in = 1;
+  if (tn[0] < tn[a_in]) a_in = 0;
+  double t_in = tn[a_in];
+  const long long cap = 3ll * (long long)t_max + 16;
+  for (long long it = 0; it < cap && t_in < t_max; ++it) {
+    v[a_in] += s[a_in];
+    tn[a_in] = __ddiv_rn(__dadd_rn((double)(v[a_in] + (s[a_in] > 0 ? 1 : 0)), -e[a_in]), d[a_in]);
+    int a_out = 2;
+    if (tn[1] < tn[a_out]) a_out = 1;
+    if (tn[0] < tn[a_out]) a_out = 0;
+    const double t_out = tn[a_out];
+    if (t_out < t_max)
+      f(v, t_in, a_in, t_out, a_out);
+    else
+      f(v, t_in, a_in, t_max, -1);
+    a_in = a_out;
+    t_in = t_out;
+  }
+}
+
+__device__ __forceinline__ float voxel_logodds(const MapView& m, const float* vals, LeafCache& c,
+                                               const int v[3], int* slot, int* l) {
+  const unsigned long long key = leaf_key(v[0] >> 3, v[1] >> 3, v[2] >> 3);
+  if (key != c.key) {
+    c.key = key;
+    c.slot = map_find(m, key);
+  }
+  *slot = c.slot;
+  *l = local_index(v[0], v[1], v[2]);
+  return c.slot >= 0 ? __ldg(&vals[(size_t)c.slot * kLeafVoxels + *l]) : 0.0f;
+}
+
+// Expected depth in index units (integral of the transmittance over [0, t_max]), FP32.
+__device__ __forceinline__ float expected_index_depth(const DepthParams& p, const MapView& m,
+                                                      const float* vals, const double d[3],
+                                                      float* t1_out) {
+  LeafCache c{kEmptyKey, -1};
+  float T = 1.0f, acc = 0.0f;
+  double t1 = p.t_max;
+  bool first = true;
+  walk(p.eye, d, p.t_max, [&](const int v[3], double t_in, int, double t_out, int) {
+    int slot, l;
+    const float L = voxel_logodds(m, vals, c, v, &slot, &l);
+    const float sg = softplus(p.scale * L + p.bias);
+    const float Dk = (float)(t_out - t_in);
+    if (first) {
+      t1 = t_in;
+      first = false;
+    }
+    acc += T * seg_integral(sg, Dk);
+    T *= expf(-sg * Dk);
+  });
+  *t1_out = (float)t1;
+  return (float)t1 + acc;
+}
+
+// Gradient replay of one ray: adds gd-weighted log-odds gradients into grad_vals (when given)
+// and returns the ray's pose gradient (6: rho, phi) times gd.
+__device__ __forceinline__ void replay_gradients(const DepthParams& p, const MapView& m,
+                                                 const float* vals, const double d[3], float D,
+                                                 float t1, float gd, float* grad_vals,
+                                                 float g6[6]) {
+  LeafCache c{kEmptyKey, -1};
+  float T = 1.0f, P = 0.0f, sg_prev = 0.0f;
+  float ge[3] = {0.f, 0.f, 0.f}, gdir[3] = {0.f, 0.f, 0.f};
+  const float inv_d[3] = {(float)(1.0 / d[0]), (float)(1.0 / d[1]), (float)(1.0 / d[2])};
+  const float gv = gd * (float)p.res * p.scale;
+  const float tail0 = D - t1;
+  walk(p.eye, d, p.t_max, [&](const int v[3], double t_in, int a_in, double t_out, int) {
+    int slot, l;
+    const float L = voxel_logodds(m, vals, c, v, &slot, &l);
+    const float x = p.scale * L + p.bias;
+    const float sg = softplus(x);
+    const float Dk = (float)(t_out - t_in);
+    // entry crossing: the density steps from sg_prev to sg
+    const float gc = (sg - sg_prev) * (tail0 - P) * (a_in == 0 ? inv_d[0] : (a_in == 1 ? inv_d[1] : inv_d[2]));
+    const float ti = (float)t_in;
+    if (a_in == 0) {
+      ge[0] -= gc;
+      gdir[0] -= gc * ti;
+    } else if (a_in == 1) {
+      ge[1] -= gc;
+      gdir[1] -= gc * ti;
+    } else {
+      ge[2] -= gc;
+      gdir[2] -= gc * ti;
+    }
+    const float Pn = P + T * seg_integral(sg, Dk);
+    if (grad_vals && slot >= 0) {
+      const float sig = 1.0f / (1.0f + expf(-x));
+      const float dsig = T * Dk * Dk * seg_g(sg * Dk) - Dk * (tail0 - Pn);
+      atomicAdd(&grad_vals[(size_t)slot * kLeafVoxels + l], gv * sig * dsig);
+    }
+    P = Pn;
+    T *= expf(-sg * Dk);
+    sg_prev = sg;
+  });
+  const float r = gd * (float)p.res;
+  const float dx = (float)d[0], dy = (float)d[1], dz = (float)d[2];
+  g6[0] = gd * ge[0];
+  g6[1] = gd * ge[1];
+  g6[2] = gd * ge[2];
+  g6[3] = r * (dy * gdir[2] - dz * gdir[1]);
+  g6[4] = r * (dz * gdir[0] - dx * gdir[2]);
+  g6[5] = r * (dx * gdir[1] - dy * gdir[0]);
+}
+
+// Sum of N doubles over the CTA (blockDim.x * blockDim.y threads, a multiple of 32); thread 0
+// writes the CTA's partials to out[blockIdx * N ...].
+template <int N>
+__device__ __forceinline__ void block_partials(double (&x)[N], double* out) {
+  __shared__ double s[32][N];
+  const int tid = threadIdx.y * blockDim.x + threadIdx.x;
+  const int nw = (blockDim.x * blockDim.y) >> 5;
+#pragma unroll
+  for (int i = 0; i < N; ++i)
+    for (int o = 16; o > 0; o >>= 1) x[i] += __shfl_down_sync(0xffffffffu, x[i], o);
+  if ((tid & 31) == 0)
+#pragma unroll
+    for (int i = 0; i < N; ++i) s[tid >> 5][i] = x[i];
+  __syncthreads();
+  if (tid == 0) {
+    const size_t b = (size_t)blockIdx.y * gridDim.x + blockIdx.x;
+    for (int i = 0; i < N; ++i) {
+      double acc = 0.0;
+      for (int w = 0; w < nw; ++w) acc += s[w][i];
+      out[b * N + i] = acc;
+    }
+  }
+}
+
+__global__ void __launch_bounds__(kDepthTile * kDepthTile) k_depth_forward(DepthParams p, MapView m,
+                                                                           const float* vals,
+                                                                           float* depth) {
+  const int w = blockIdx.x * kDepthTile + threadIdx.x;
+  const int h = blockIdx.y * kDepthTile + threadIdx.y;
+  if (w >= p.width || h >= p.height) return;
+  double d[3];
+  pixel_dir(p, w, h, d);
+  float t1;
+  depth[(size_t)h * p.width + w] = expected_index_depth(p, m, vals, d, &t1) * (float)p.res;
+}
+
+__global__ void __launch_bounds__(kDepthTile * kDepthTile) k_depth_backward(
+    DepthParams p, MapView m, const float* vals, const float* grad_depth, float* grad_vals,
+    double* partials) {
+  const int w = blockIdx.x * kDepthTile + threadIdx.x;
+  const int h = blockIdx.y * kDepthTile + threadIdx.y;
+  double acc[6] = {0, 0, 0, 0, 0, 0};
+  if (w < p.width && h < p.height) {
+    const float gd = grad_depth[(size_t)h * p.width + w];
+    if (gd != 0.0f) {
+      double d[3];
+      pixel_dir(p, w, h, d);
+      float t1;
+      const float D = expected_index_depth(p, m, vals, d, &t1);
+      float g6[6];
+      replay_gradients(p, m, vals, d, D, t1, gd, grad_vals, g6);
+#pragma unroll
+      for (int i = 0; i < 6; ++i) acc[i] = (double)g6[i];
+    }
+  }
+  block_partials<6>(acc, partials);
+}
+
+// One refinement step: L1 loss against `target` (metres; <= 0 or NaN = no return), truncated
+// at max_residual when it is positive (residuals beyond it add max_residual and no gradient),
+// its pose gradient, and the number of pixels that took part.  Partials: loss, count, 6
+// gradients.
+__global__ void __launch_bounds__(kDepthTile * kDepthTile) k_depth_refine(
+    DepthParams p, MapView m, const float* vals, const float* target, float max_residual,
+    double* partials) {
+  const int w = blockIdx.x * kDepthTile + threadIdx.x;
+  const int h = blockIdx.y * kDepthTile + threadIdx.y;
+  double acc[8] = {0, 0, 0, 0, 0, 0, 0, 0};
+  if (w < p.width && h < p.height) {
+    const float r = target[(size_t)h * p.width + w];
+    if (r > 0.0f && r < CUDART_INF_F) {
+      double d[3];
+      pixel_dir(p, w, h, d);
+      float t1;
+      const float D = expected_index_depth(p, m, vals, d, &t1);
+      const float res = D * (float)p.res - r;
+      const bool clipped = max_residual > 0.0f && fabsf(res) > max_residual;
+      acc[0] = clipped ? (double)max_residual : fabs((double)res);
+      acc[1] = 1.0;
+      const float gd = clipped ? 0.0f : (res > 0.0f ? 1.0f : (res < 0.0f ? -1.0f : 0.0f));
+      if (gd != 0.0f) {
+        float g6[6];
+        replay_gradients(p, m, vals, d, D, t1, gd, nullptr, g6);
+#pragma unroll
+        for (int i = 0; i < 6; ++i) acc[2 + i] = (double)g6[i];
+      }
+    }
+  }
+  block_partials<8>(acc, partials);
+}
+
+// Column sums of an (n, N) array of partials in a fixed order (deterministic).
+__global__ void k_sum_partials(const double* partials, int n, int N, double* out) {
+  __shared__ double s[256];
+  for (int c = 0; c < N; ++c) {
+    double acc = 0.0;
+    for (int i = threadIdx.x; i < n; i += blockDim.x) acc += partials[(size_t)i * N + c];
+    s[threadIdx.x] = acc;
+    __syncthreads();
+    for (int k = blockDim.x / 2; k > 0; k >>= 1) {
+      if ((int)threadIdx.x < k) s[threadIdx.x] += s[threadIdx.x + k];
+      __syncthreads();
+    }
+    if (threadIdx.x == 0) out[c] = s[0];
+    __syncthreads();
+  }
+}
+
+dim3 depth_grid(const DepthParams& p) {
+  return dim3((p.width + kDepthTile - 1) / kDepthTile, (p.height + kDepthTile - 1) / kDepthTile);
+}
+
+}  // namespace
+
+int depth_partial_blocks(const DepthParams& p) {
+  const dim3 g = depth_grid(p);
+  return (int)(g.x * g.y);
+}
+
+cudaError_t launch_depth_forward(const DepthParams& p, const MapView& m, const float* vals,
+                                 float* depth, cudaStream_t s) {
+  k_depth_forward<<<depth_grid(p), dim3(kDepthTile, kDepthTile), 0, s>>>(p, m, vals, depth);
+  return cudaGetLastError();
+}
+
+cudaError_t launch_depth_backward(const DepthParams& p, const MapView& m, const float* vals,
+                                  const float* grad_depth, float* grad_vals, double* partials,
+                                  double* out6, cudaStream_t s) {
+  const dim3 g = depth_grid(p);
+  k_depth_backward<<<g, dim3(kDepthTile, kDepthTile), 0, s>>>(p, m, vals, grad_depth, grad_vals,
+                                                              partials);
+  cudaError_t e = cudaGetLastError();
+  if (e != cudaSuccess) return e;
+  k_sum_partials<<<1, 256, 0, s>>>(partials, (int)(g.x * g.y), 6, out6);
+  return cudaGetLastError();
+}
+
+cudaError_t launch_depth_refine(const DepthParams& p, const MapView& m, const float* vals,
+                                const float* target, float max_residual, double* partials,
+                                double* out8, cudaStream_t s) {
+  const dim3 g = depth_grid(p);
+  k_depth_refine<<<g, dim3(kDepthTile, kDepthTile), 0, s>>>(p, m, vals, target, max_residual,
+                                                            partials);
+  cudaError_t e = cudaGetLastError();
+  if (e != cudaSuccess) return e;
+  k_sum_partials<<<1, 256, 0, s>>>(partials, (int)(g.x * g.y), 8, out8);
+  return cudaGetLastError();
+}
+
+}  // namespace nm

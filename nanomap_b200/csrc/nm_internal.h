@@ -150,6 +150,21 @@ struct FilterBuffers {
   int64_t capacity;
 };
 
+// Constants of one expected-depth launch (double ray geometry, FP32 accumulation).
+struct DepthParams {
+  int32_t type, width, height, pad;
+  float hw, hh, c0, c1, su, sv;  // frustum pixel model
+  const float* sinu;             // laser tables (device)
+  const float* cosu;
+  const float* sinv;
+  const float* cosv;
+  double R[9];    // world-from-sensor, row-major
+  double eye[3];  // position / res
+  double t_max;   // max_range / res
+  double res;
+  float scale, bias;  // occupancy = sigmoid(scale * log-odds + bias)
+};
+
 // ---- kernel launchers (defined in the .cu files) -----------------------------------------
 template <int MaxF>
 cudaError_t launch_traverse_labels(const TickWork<MaxF>& w, const MapView& m, int rounding,
@@ -170,6 +185,15 @@ cudaError_t launch_export_labels(const MapView& m, int plane, int32_t* origins,
                                  uint32_t* words, uint32_t* n_out, uint32_t max_out,
                                  cudaStream_t s);
 cudaError_t launch_fill_keys(unsigned long long* keys, uint32_t n, cudaStream_t s);
+int depth_partial_blocks(const DepthParams& p);
+cudaError_t launch_depth_forward(const DepthParams& p, const MapView& m, const float* vals,
+                                 float* depth, cudaStream_t s);
+cudaError_t launch_depth_backward(const DepthParams& p, const MapView& m, const float* vals,
+                                  const float* grad_depth, float* grad_vals, double* partials,
+                                  double* out6, cudaStream_t s);
+cudaError_t launch_depth_refine(const DepthParams& p, const MapView& m, const float* vals,
+                                const float* target, float max_residual, double* partials,
+                                double* out8, cudaStream_t s);
 cudaError_t filter_reserve(FilterBuffers* b, int64_t n);
 void filter_release(FilterBuffers* b);
 int filter_key_bits(float max_time);  // bits per axis of a filter key; 0 if out of range

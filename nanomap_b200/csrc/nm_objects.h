@@ -70,6 +70,8 @@ struct nm_map_s {
   uint32_t* d_scratch_u32 = nullptr;  // export counters
   int tile_w = 16, tile_h = 16, smem_entries = 128;
   nm::FilterBuffers filter{};  // voxel-filter buffers, grown on first filtered insert
+  double* depth_scratch = nullptr;  // expected-depth partial sums (grown on demand)
+  size_t depth_scratch_n = 0;
 };
 
 struct nm_simmap_s {

@@ -50,6 +50,8 @@
 #include <unordered_map>
 #include <vector>
 
+#include "orc_types.h"
+
 namespace {
 
 constexpr int kHit = 1;
@@ -314,17 +316,6 @@ struct SimMap {
 }  // namespace
 
 extern "C" {
-
-typedef struct {
-  int32_t type;  // 0 frustum, 1 laser
-  int32_t width, height, pad;
-  float hw, hh, c0, c1, scale_u, scale_v;
-  float min_range, max_range;
-  const float* sinu;
-  const float* cosu;
-  const float* sinv;
-  const float* cosv;
-} orc_sensor;
 
 typedef struct {
   float res;

@@ -90,6 +90,9 @@ def lib() -> C.CDLL:
                                         C.c_int64, _PF, _PU32, C.c_int64]
         L.orc_voxel_filter.restype = C.c_int64
         L.orc_render_boxes.argtypes = [C.POINTER(OrcSensor), _PD, _PD, _PD, C.c_int, _PF]
+        L.orc_depth.argtypes = [C.POINTER(OrcSensor), _PD, _PD, C.c_double, _PI32, _PF, C.c_int64,
+                                C.c_double, C.c_double, _PI32, C.c_int64, _PD, _PD,
+                                C.POINTER(C.c_uint64), _PD, _PD]
         _lib = L
     return _lib
 
@@ -297,6 +300,35 @@ def voxel_filter(R, eye, res, max_time, rounding, points, centre=False):
     cnt = np.zeros(n, np.uint32)
     lib().orc_voxel_filter(*args, fp(out), cnt.ctypes.data_as(_PU32), n)
     return out, cnt
+
+
+def depth(sensor: Sensor, pos, R, res, origins, values, scale=1.0, bias=0.0, pixels=None,
+          grad_depth=None, want_grad=True):
+    """FP64 expected depth of the listed pixels (all when None) over a map given as leaf
+    origins (n, 3) and values (n, 512).  Returns (depth (m), dpose (n_pix, 6): d/drho, d/dphi,
+    sequence hashes, grad_values (n, 512) of sum grad_depth * depth or None)."""
+    s = sensor.s
+    if pixels is None:
+        pixels = np.arange(s.width * s.height, dtype=np.int32)
+    pixels = np.ascontiguousarray(pixels, np.int32)
+    origins = np.ascontiguousarray(origins, np.int32).reshape(-1, 3)
+    values = _f(values).reshape(-1, 512)
+    n = len(pixels)
+    out = np.zeros(n)
+    dpose = np.zeros((n, 6)) if want_grad else None
+    hashes = np.zeros(n, np.uint64)
+    gv = None
+    gd = None
+    if grad_depth is not None:
+        gd = _d(grad_depth).reshape(-1)
+        gv = np.zeros((len(origins), 512))
+    lib().orc_depth(C.byref(s), dp(_d(pos)), dp(_d(R).reshape(-1)), C.c_double(res),
+                    origins.ctypes.data_as(_PI32), fp(values), len(origins), C.c_double(scale),
+                    C.c_double(bias), pixels.ctypes.data_as(_PI32), n, dp(out),
+                    dp(dpose) if dpose is not None else None,
+                    hashes.ctypes.data_as(C.POINTER(C.c_uint64)),
+                    dp(gd) if gd is not None else None, dp(gv) if gv is not None else None)
+    return out, dpose, hashes, gv
 
 
 def sort_leaves(origins, *arrays):

@@ -5,6 +5,7 @@ import numpy as np
 
 from nanomap_b200 import scenes as S
 from nanomap_b200.api import Pose, sensor_desc
+from nanomap_b200.diff import so3_exp
 from oracle import oracle as O
 
 
@@ -87,3 +88,32 @@ def compare_labels(gpu_labels, oracle_labels):
         if len(errs) > 20:
             break
     return errs
+
+
+def central_differences(render, pos, R, h, n):
+    """FP64 central differences of render(pos, R) -> (values (n,), hashes) for the six pose
+    components at step h, and the mask of (pixel, component) pairs whose voxel sequence is the
+    same at both perturbed poses."""
+    _, base_hash = render(pos, R)
+    fd = np.zeros((n, 6))
+    ok = np.ones((n, 6), bool)
+    for i in range(6):
+        for sgn in (1.0, -1.0):
+            p2, R2 = pos.copy(), R
+            if i < 3:
+                p2[i] += sgn * h
+            else:
+                phi = np.zeros(3)
+                phi[i - 3] = sgn * h
+                R2 = so3_exp(phi) @ R
+            D2, h2 = render(p2, R2)
+            ok[:, i] &= h2 == base_hash
+            fd[:, i] += sgn * D2 / (2 * h)
+    return fd, ok
+
+
+def richardson(render, pos, R, h, n):
+    """Central differences at h and h/2 combined to cancel the h^2 error term."""
+    f1, ok1 = central_differences(render, pos, R, h, n)
+    f2, ok2 = central_differences(render, pos, R, h / 2, n)
+    return (4.0 * f2 - f1) / 3.0, ok1 & ok2
