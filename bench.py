@@ -375,6 +375,10 @@ def run_ours(args, rank, world, local):
         "e2e": e2e,
         "clocks": clk,
     }
+    if args.extras:
+        line["voxel_filter"] = run_filter_section(ctx, sensor, sim, mdesc, spec, poses, ranges,
+                                                  stream, args.warmup)
+        line["expected_depth"] = run_depth_section(ctx, m, sensor, sim, spec, poses, stream, hbm)
     if args.batched_ticks > args.warmup:
         line["batched"] = run_batched(args, rank, world, local, args.batched_ticks)
     if rank == 0 and world == 1 and args.cpu_baseline_s > 0:
@@ -388,6 +392,125 @@ def run_ours(args, rank, world, local):
     sensor.close()
     ctx.close()
     return line
+
+
+def run_filter_section(ctx, sensor, sim, mdesc, spec, poses, ranges, stream, warmup, frames=20):
+    """Voxel-filtered insert (filter type 1) against the plain insert on the same headline
+    frames: per-frame device time of insert + integrate, rays traced, voxel updates."""
+    import torch
+
+    from nanomap_b200 import _native as N
+    from nanomap_b200 import api as A
+    out = {}
+    H, W = spec.height, spec.width
+    imgs = []
+    for k in range(frames + warmup):
+        sim.render(sensor, poses[k % len(poses)], ranges, stream=stream)
+        ctx.add_noise(ranges, spec.noise_coef, spec.drop, 7919 * (k + 1), stream=stream)
+        imgs.append(ranges.clone())
+    for name, flags in (("plain", 0), ("filtered_mean", N.NM_FILTER_MEAN)):
+        mm = A.Map(ctx, mdesc)
+        for k in range(warmup):
+            mm.insert_ranges(sensor, poses[k % len(poses)], imgs[k], flags=flags, stream=stream)
+        torch.cuda.synchronize()
+        s0 = mm.stats()
+        evs = []
+        for k in range(warmup, warmup + frames):
+            e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+            e0.record(stream)
+            mm.insert_ranges(sensor, poses[k % len(poses)], imgs[k], flags=flags, stream=stream)
+            e1.record(stream)
+            evs.append((e0, e1))
+        torch.cuda.synchronize()
+        s1 = mm.stats()
+        ms = statistics.mean(e0.elapsed_time(e1) for e0, e1 in evs)
+        out[name] = {"ms_per_frame": ms, "rays_per_frame": (s1["rays"] - s0["rays"]) / frames,
+                     "visits_per_frame": (s1["visits"] - s0["visits"]) / frames,
+                     "input_points_per_s": H * W / (ms / 1e3),
+                     "voxel_updates_per_s": (s1["visits"] - s0["visits"]) / frames / (ms / 1e3)}
+        mm.close()
+    out["workload"] = (f"{frames} headline frames ({W}x{H} range images at {spec.map_res} m): "
+                       "insert + integrate per frame, with and without the voxel filter")
+    return out
+
+
+def run_depth_section(ctx, m, sensor, sim, spec, poses, stream, hbm, reps=10):
+    """Expected-depth forward and adjoint over the headline map after the timed run (640x480,
+    10 m, 0.05 m voxels), and scan-to-map refinement from a perturbed pose (50 Adam steps)."""
+    import torch
+
+    from nanomap_b200 import api as A
+    from nanomap_b200.diff import so3_exp
+    H, W = spec.height, spec.width
+    gt = poses[len(poses) // 2]
+    gpos, gR = A.Map.ray_pose(sensor, gt)
+    rng = np.random.default_rng(11)
+    pos = gpos + rng.uniform(-0.05, 0.05, 3)
+    R = so3_exp(np.radians(rng.uniform(-2.0, 2.0, 3))) @ gR
+    scale, bias = 4.0, 0.0
+    vals = m.values_copy()
+    gvals = torch.zeros_like(vals)
+    gd = torch.ones(H, W, device=vals.device)
+    for _ in range(3):
+        m.depth_render(sensor, pos, R, values=vals, scale=scale, bias=bias)
+        m.depth_backward(sensor, pos, R, gd, values=vals, grad_values=gvals, scale=scale, bias=bias)
+    torch.cuda.synchronize()
+    v0 = m.stats()["depth_visits"]
+    e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+    e0.record(stream)
+    for _ in range(reps):
+        m.depth_render(sensor, pos, R, values=vals, scale=scale, bias=bias)
+    e1.record(stream)
+    torch.cuda.synchronize()
+    fwd_ms = e0.elapsed_time(e1) / reps
+    v1 = m.stats()["depth_visits"]
+    t0 = time.perf_counter()
+    for _ in range(reps):
+        m.depth_backward(sensor, pos, R, gd, values=vals, grad_values=gvals, scale=scale, bias=bias)
+    torch.cuda.synchronize()
+    bwd_ms = (time.perf_counter() - t0) * 1e3 / reps
+    v2 = m.stats()["depth_visits"]
+    fv = (v1 - v0) / reps
+    bv = (v2 - v1) / reps
+    # gathered bytes: one 4-byte log-odds per voxel visit, 4 B per pixel written (forward);
+    # the adjoint replays twice and scatters one 4-byte gradient per visit of the second replay
+    fwd_bytes = 4 * fv + 4 * H * W
+    bwd_bytes = 4 * bv + 4 * (bv / 2) + 4 * H * W
+    out = {
+        "forward_ms": fwd_ms, "backward_ms_incl_host_sync": bwd_ms,
+        "rays_per_s_forward": H * W / (fwd_ms / 1e3),
+        "voxel_visits_per_frame": fv,
+        "roofline_forward": {"bound": "hbm", "achieved": fwd_bytes / (fwd_ms / 1e3) / 1e9, "peak": hbm,
+                             "unit": "GB/s", "frac": fwd_bytes / (fwd_ms / 1e3) / 1e9 / hbm,
+                             "bytes": "4 B log-odds per voxel visit + 4 B depth per pixel"},
+        "roofline_backward": {"bound": "hbm", "achieved": bwd_bytes / (bwd_ms / 1e3) / 1e9, "peak": hbm,
+                              "unit": "GB/s", "frac": bwd_bytes / (bwd_ms / 1e3) / 1e9 / hbm},
+        "occupancy": f"sigmoid({scale} * log-odds + {bias}) per voxel length",
+    }
+    # refinement: map-consistent scan (expected depth at the ground truth where the simulated
+    # sensor returns) and the simulated depth itself
+    sim_depth = torch.zeros(H, W, device=vals.device)
+    sim.render(sensor, gt, sim_depth, stream=stream)
+    scan = m.depth_render(sensor, gpos, gR, scale=scale, bias=bias)
+    scan = torch.where(sim_depth > 0, scan, torch.zeros_like(scan))
+
+    def errors(p, Rm):
+        ang = math.degrees(math.acos(max(-1.0, min(1.0, (np.trace(Rm @ gR.T) - 1) / 2))))
+        return float(np.linalg.norm(p - gpos)), ang
+
+    t_start, a_start = errors(pos, R)
+    ref = {"start_error_m": t_start, "start_error_deg": a_start, "steps": 50}
+    for name, tgt in (("map_consistent_scan", scan), ("sim_depth", sim_depth)):
+        torch.cuda.synchronize()
+        t0 = time.perf_counter()
+        p1, R1, losses = m.pose_refine(sensor, pos, R, tgt, steps=50, lr_position=0.01,
+                                       lr_rotation=0.004, scale=scale, bias=bias, max_residual=0.3)
+        dt = time.perf_counter() - t0
+        te, ae = errors(p1, R1)
+        ref[name] = {"final_error_m": te, "final_error_deg": ae, "loss_first": float(losses[0]),
+                     "loss_last": float(losses[-1]), "ms_per_step": dt * 1e3 / 50}
+    out["refine"] = ref
+    return out
 
 
 def batched_agents(spec_small):
@@ -533,6 +656,8 @@ def main():
     ap.add_argument("--cpu-baseline-s", type=float, default=12.0)
     ap.add_argument("--batched-ticks", type=int, default=40,
                     help="ticks of the 16-agent batched comparison (0 = skip)")
+    ap.add_argument("--extras", type=int, default=1,
+                    help="1 = also measure the voxel-filtered insert, expected depth and refinement")
     ap.add_argument("--capacity-log2", type=int, default=21,
                     help="initial leaf-table capacity (log2 slots); smaller for profiling runs")
     args = ap.parse_args()

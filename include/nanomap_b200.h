@@ -115,6 +115,7 @@ typedef struct {
   uint64_t leaf_capacity;  /* current hash-table capacity */
   uint32_t error_flags;    /* sticky device error bits, cleared by nm_map_stats */
   uint32_t grow_count;     /* table growths so far */
+  uint64_t depth_visits;   /* voxels visited by expected-depth renders, adjoints, refinement */
 } nm_stats;
 
 /* One frame of a batched tick. */

@@ -475,6 +475,40 @@ int run_frame(nm_map m, nm_sensor s, nm::FrameParams& f, uint32_t flags, cudaStr
   return NM_OK;
 }
 
+void release(nm_context c) {
+  if (!c || c->refs.fetch_sub(1, std::memory_order_acq_rel) != 1) return;
+  cudaSetDevice(c->device);
+  cudaStreamSynchronize(c->stream);
+  cudaFree(c->render_staging);
+  delete c;
+}
+
+void release(nm_sensor s) {
+  if (!s || s->refs.fetch_sub(1, std::memory_order_acq_rel) != 1) return;
+  nm_context c = s->ctx;
+  cudaSetDevice(c->device);
+  cudaDeviceSynchronize();
+  cudaFree(s->d_tables);
+  delete s;
+  release(c);
+}
+
+void release(nm_map m) {
+  if (!m || m->refs.fetch_sub(1, std::memory_order_acq_rel) != 1) return;
+  nm_context c = m->ctx;
+  cudaSetDevice(c->device);
+  cudaStreamSynchronize(c->stream);
+  cudaDeviceSynchronize();
+  free_view(m->view);
+  cudaFree(m->d_ctr);
+  cudaFree(m->d_scratch_u32);
+  cudaFree(m->staging);
+  filter_release(&m->filter);
+  cudaFree(m->depth_scratch);
+  delete m;
+  release(c);
+}
+
 }  // namespace nm
 
 using namespace nm;
@@ -507,11 +541,7 @@ int nm_context_create(int32_t device, nm_context* out) {
 }
 
 int nm_context_destroy(nm_context ctx) {
-  if (!ctx) return NM_OK;
-  cudaSetDevice(ctx->device);
-  cudaStreamSynchronize(ctx->stream);
-  cudaFree(ctx->render_staging);
-  delete ctx;
+  nm::release(ctx);
   return NM_OK;
 }
 
@@ -568,14 +598,13 @@ int nm_sensor_create(nm_context ctx, const nm_sensor_desc* d, nm_sensor* out) {
     s->lh = nm::logit(d->prob_hit);
     s->lm = nm::logit(d->prob_miss);
   }
+  nm::retain(ctx);
   *out = s.release();
   return NM_OK;
 }
 
 int nm_sensor_destroy(nm_sensor s) {
-  if (!s) return NM_OK;
-  cudaFree(s->d_tables);
-  delete s;
+  nm::release(s);
   return NM_OK;
 }
 
@@ -616,22 +645,13 @@ int nm_map_create(nm_context ctx, const nm_map_desc* d, nm_map* out) {
   }
   NM_CUDA(cudaStreamSynchronize(ctx->stream));
   for (int i = 0; i < nm::kMaxPlanes; ++i) m->pending_lh[i] = m->pending_lm[i] = 0.f;
+  nm::retain(ctx);
   *out = m.release();
   return NM_OK;
 }
 
 int nm_map_destroy(nm_map m) {
-  if (!m) return NM_OK;
-  cudaSetDevice(m->ctx->device);
-  cudaStreamSynchronize(m->ctx->stream);
-  cudaDeviceSynchronize();
-  free_view(m->view);
-  cudaFree(m->d_ctr);
-  cudaFree(m->d_scratch_u32);
-  cudaFree(m->staging);
-  nm::filter_release(&m->filter);
-  cudaFree(m->depth_scratch);
-  delete m;
+  nm::release(m);
   return NM_OK;
 }
 
@@ -671,6 +691,7 @@ int nm_map_stats(nm_map m, nm_stats* out) {
   out->leaf_capacity = m->view.capacity;
   out->error_flags = c.error_flags;
   out->grow_count = m->grow_count;
+  out->depth_visits = c.depth_visits;
   m->known_leaves = c.leaf_count;
   m->pending_bound = 0;
   if (c.error_flags) NM_CUDA(cudaMemset(&m->d_ctr->error_flags, 0, 4));

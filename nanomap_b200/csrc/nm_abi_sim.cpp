@@ -131,6 +131,20 @@ void make_ray_params(nm_sensor s, const nm_pose& pose, SimRayParams* rp) {
 
 }  // namespace nm
 
+namespace nm {
+void release(nm_simmap sm) {
+  if (!sm || sm->refs.fetch_sub(1, std::memory_order_acq_rel) != 1) return;
+  nm_context c = sm->ctx;
+  cudaSetDevice(c->device);
+  cudaDeviceSynchronize();
+  cudaFree(sm->view.leaf_index);
+  cudaFree(sm->view.leaf_words);
+  cudaFree(sm->view.brick_bits);
+  delete sm;
+  release(c);
+}
+}  // namespace nm
+
 extern "C" {
 
 int nm_simmap_create_primitives(nm_context ctx, float res, const int32_t vox_min[3],
@@ -165,6 +179,7 @@ int nm_simmap_create_primitives(nm_context ctx, float res, const int32_t vox_min
   cudaFree(d_boxes);
   cudaFree(d_cyl);
   if (rc != NM_OK) return rc;
+  nm::retain(ctx);
   *out = sm.release();
   return NM_OK;
 }
@@ -202,6 +217,7 @@ int nm_simmap_create_voxels(nm_context ctx, float res, const int32_t* ijk, int64
   rc = finish_build(ctx, b, sm.get(), s);
   cudaFree(d_ijk);
   if (rc != NM_OK) return rc;
+  nm::retain(ctx);
   *out = sm.release();
   return NM_OK;
 }
@@ -232,14 +248,9 @@ int nm_simmap_load(nm_context ctx, const char* path, nm_simmap* out) {
   return nm_simmap_create_voxels(ctx, res, ijk.data(), n, out);
 }
 
+
 int nm_simmap_destroy(nm_simmap sm) {
-  if (!sm) return NM_OK;
-  cudaSetDevice(sm->ctx->device);
-  cudaDeviceSynchronize();
-  cudaFree(sm->view.leaf_index);
-  cudaFree(sm->view.leaf_words);
-  cudaFree(sm->view.brick_bits);
-  delete sm;
+  nm::release(sm);
   return NM_OK;
 }
 

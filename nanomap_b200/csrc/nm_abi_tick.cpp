@@ -221,6 +221,9 @@ int nm_tick_plan_create(nm_map m, nm_simmap sim, const nm_frame* slots, int32_t 
   }
   NM_CUDA(cudaMalloc((void**)&p->d_stage, sizeof(TickStage)));
   NM_CUDA(cudaStreamCreateWithFlags(&p->cap_stream, cudaStreamNonBlocking));
+  nm::retain(m);
+  nm::retain(sim);
+  for (int i = 0; i < n; ++i) nm::retain(p->slots[i].sensor);
   *out = p.release();
   return NM_OK;
 }
@@ -236,6 +239,9 @@ int nm_tick_plan_destroy(nm_tick_plan p) {
   }
   cudaFree(p->d_stage);
   if (p->cap_stream) cudaStreamDestroy(p->cap_stream);
+  for (int i = 0; i < p->n; ++i) nm::release(p->slots[i].sensor);
+  nm::release(p->sim);
+  nm::release(p->map);
   delete p;
   return NM_OK;
 }

@@ -123,12 +123,14 @@ __device__ __forceinline__ float voxel_logodds(const MapView& m, const float* va
 // Expected depth in index units (integral of the transmittance over [0, t_max]), FP32.
 __device__ __forceinline__ float expected_index_depth(const DepthParams& p, const MapView& m,
                                                       const float* vals, const double d[3],
-                                                      float* t1_out) {
+                                                      float* t1_out, uint32_t* visits) {
   LeafCache c{kEmptyKey, -1};
   float T = 1.0f, acc = 0.0f;
   double t1 = p.t_max;
   bool first = true;
+  uint32_t n = 0;
   walk(p.eye, d, p.t_max, [&](const int v[3], double t_in, int, double t_out, int) {
+    ++n;
     int slot, l;
     const float L = voxel_logodds(m, vals, c, v, &slot, &l);
     const float sg = softplus(p.scale * L + p.bias);
@@ -141,6 +143,7 @@ __device__ __forceinline__ float expected_index_depth(const DepthParams& p, cons
     T *= expf(-sg * Dk);
   });
   *t1_out = (float)t1;
+  *visits += n;
   return (float)t1 + acc;
 }
 
@@ -149,8 +152,9 @@ __device__ __forceinline__ float expected_index_depth(const DepthParams& p, cons
 __device__ __forceinline__ void replay_gradients(const DepthParams& p, const MapView& m,
                                                  const float* vals, const double d[3], float D,
                                                  float t1, float gd, float* grad_vals,
-                                                 float g6[6]) {
+                                                 float g6[6], uint32_t* visits) {
   LeafCache c{kEmptyKey, -1};
+  uint32_t n = 0;
   float T = 1.0f, P = 0.0f, sg_prev = 0.0f;
   float ge[3] = {0.f, 0.f, 0.f}, gdir[3] = {0.f, 0.f, 0.f};
   const float inv_d[3] = {(float)(1.0 / d[0]), (float)(1.0 / d[1]), (float)(1.0 / d[2])};
@@ -159,6 +163,7 @@ __device__ __forceinline__ void replay_gradients(const DepthParams& p, const Map
   walk(p.eye, d, p.t_max, [&](const int v[3], double t_in, int a_in, double t_out, int) {
     int slot, l;
     const float L = voxel_logodds(m, vals, c, v, &slot, &l);
+    ++n;
     const float x = p.scale * L + p.bias;
     const float sg = softplus(x);
     const float Dk = (float)(t_out - t_in);
@@ -185,6 +190,7 @@ __device__ __forceinline__ void replay_gradients(const DepthParams& p, const Map
     T *= expf(-sg * Dk);
     sg_prev = sg;
   });
+  *visits += n;
   const float r = gd * (float)p.res;
   const float dx = (float)d[0], dy = (float)d[1], dz = (float)d[2];
   g6[0] = gd * ge[0];
@@ -193,6 +199,14 @@ __device__ __forceinline__ void replay_gradients(const DepthParams& p, const Map
   g6[3] = r * (dy * gdir[2] - dz * gdir[1]);
   g6[4] = r * (dz * gdir[0] - dx * gdir[2]);
   g6[5] = r * (dx * gdir[1] - dy * gdir[0]);
+}
+
+// Adds the active lanes' visit counts to the map's counter (one atomic per warp).
+__device__ __forceinline__ void add_depth_visits(const MapView& m, uint32_t n) {
+  const unsigned act = __activemask();
+  const uint32_t sum = __reduce_add_sync(act, n);
+  if (((threadIdx.y * blockDim.x + threadIdx.x) & 31) == (unsigned)(__ffs(act) - 1))
+    atomicAdd(&m.ctr->depth_visits, (unsigned long long)sum);
 }
 
 // Sum of N doubles over the CTA (blockDim.x * blockDim.y threads, a multiple of 32); thread 0
@@ -228,7 +242,9 @@ __global__ void __launch_bounds__(kDepthTile * kDepthTile) k_depth_forward(Depth
   double d[3];
   pixel_dir(p, w, h, d);
   float t1;
-  depth[(size_t)h * p.width + w] = expected_index_depth(p, m, vals, d, &t1) * (float)p.res;
+  uint32_t n = 0;
+  depth[(size_t)h * p.width + w] = expected_index_depth(p, m, vals, d, &t1, &n) * (float)p.res;
+  add_depth_visits(m, n);
 }
 
 __global__ void __launch_bounds__(kDepthTile * kDepthTile) k_depth_backward(
@@ -237,19 +253,21 @@ __global__ void __launch_bounds__(kDepthTile * kDepthTile) k_depth_backward(
   const int w = blockIdx.x * kDepthTile + threadIdx.x;
   const int h = blockIdx.y * kDepthTile + threadIdx.y;
   double acc[6] = {0, 0, 0, 0, 0, 0};
+  uint32_t n = 0;
   if (w < p.width && h < p.height) {
     const float gd = grad_depth[(size_t)h * p.width + w];
     if (gd != 0.0f) {
       double d[3];
       pixel_dir(p, w, h, d);
       float t1;
-      const float D = expected_index_depth(p, m, vals, d, &t1);
+      const float D = expected_index_depth(p, m, vals, d, &t1, &n);
       float g6[6];
-      replay_gradients(p, m, vals, d, D, t1, gd, grad_vals, g6);
+      replay_gradients(p, m, vals, d, D, t1, gd, grad_vals, g6, &n);
 #pragma unroll
       for (int i = 0; i < 6; ++i) acc[i] = (double)g6[i];
     }
   }
+  add_depth_visits(m, n);
   block_partials<6>(acc, partials);
 }
 
@@ -263,13 +281,14 @@ __global__ void __launch_bounds__(kDepthTile * kDepthTile) k_depth_refine(
   const int w = blockIdx.x * kDepthTile + threadIdx.x;
   const int h = blockIdx.y * kDepthTile + threadIdx.y;
   double acc[8] = {0, 0, 0, 0, 0, 0, 0, 0};
+  uint32_t n = 0;
   if (w < p.width && h < p.height) {
     const float r = target[(size_t)h * p.width + w];
     if (r > 0.0f && r < CUDART_INF_F) {
       double d[3];
       pixel_dir(p, w, h, d);
       float t1;
-      const float D = expected_index_depth(p, m, vals, d, &t1);
+      const float D = expected_index_depth(p, m, vals, d, &t1, &n);
       const float res = D * (float)p.res - r;
       const bool clipped = max_residual > 0.0f && fabsf(res) > max_residual;
       acc[0] = clipped ? (double)max_residual : fabs((double)res);
@@ -277,12 +296,13 @@ __global__ void __launch_bounds__(kDepthTile * kDepthTile) k_depth_refine(
       const float gd = clipped ? 0.0f : (res > 0.0f ? 1.0f : (res < 0.0f ? -1.0f : 0.0f));
       if (gd != 0.0f) {
         float g6[6];
-        replay_gradients(p, m, vals, d, D, t1, gd, nullptr, g6);
+        replay_gradients(p, m, vals, d, D, t1, gd, nullptr, g6, &n);
 #pragma unroll
         for (int i = 0; i < 6; ++i) acc[2 + i] = (double)g6[i];
       }
     }
   }
+  add_depth_visits(m, n);
   block_partials<8>(acc, partials);
 }
 

@@ -42,7 +42,7 @@ struct MapCounters {
   unsigned int frames;
   unsigned int done_blocks;
   unsigned int tile_queue;  // persistent traversal work counter (reset by its last reader)
-  unsigned int pad[2];
+  unsigned long long depth_visits;  // voxels visited by the expected-depth kernels
 };
 
 struct MapView {

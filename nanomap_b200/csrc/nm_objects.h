@@ -2,6 +2,7 @@
 // host translation units.
 #pragma once
 
+#include <atomic>
 #include <cfenv>
 #include <cstdarg>
 #include <cstdio>
@@ -35,8 +36,14 @@ struct RoundScope {
   } while (0)
 
 // ---- object definitions ---------------------------------------------------------------------
+//
+// Objects are reference counted: a handle holds one reference, and every object that uses
+// another holds one on it (sensors, maps and sim maps on their context; tick plans on their
+// map, sim map and slot sensors).  nm_*_destroy drops the handle's reference, so handles may be
+// destroyed in any order; the memory goes when the last user does.
 
 struct nm_context_s {
+  std::atomic<int> refs{1};
   int device = 0;
   int sm_count = 148;
   cudaStream_t stream = nullptr;
@@ -45,6 +52,7 @@ struct nm_context_s {
 };
 
 struct nm_sensor_s {
+  std::atomic<int> refs{1};
   nm_context ctx = nullptr;
   nm_sensor_desc desc{};
   float fp[6] = {0, 0, 0, 0, 0, 0};
@@ -53,6 +61,7 @@ struct nm_sensor_s {
 };
 
 struct nm_map_s {
+  std::atomic<int> refs{1};
   nm_context ctx = nullptr;
   nm_map_desc desc{};
   nm::MapView view{};
@@ -75,6 +84,7 @@ struct nm_map_s {
 };
 
 struct nm_simmap_s {
+  std::atomic<int> refs{1};
   nm_context ctx = nullptr;
   nm::SimMapView view{};
   int32_t bbox[6] = {0, 0, 0, -1, -1, -1};
@@ -85,6 +95,17 @@ struct nm_simmap_s {
 
 // Host helpers shared by the C ABI translation units (defined in nm_abi.cpp / nm_abi_sim.cpp).
 namespace nm {
+template <class T>
+T retain(T obj) {
+  if (obj) obj->refs.fetch_add(1, std::memory_order_relaxed);
+  return obj;
+}
+// Drop one reference; the last one frees the object (and drops the references it holds).
+void release(nm_context c);
+void release(nm_sensor s);
+void release(nm_map m);
+void release(nm_simmap sm);
+
 cudaStream_t pick(nm_context ctx, void* stream);
 int make_frame(nm_map m, nm_sensor s, const nm_pose* pose, FrameParams* f);
 uint64_t frame_leaf_bound(nm_map m, nm_sensor s, const nm_pose& pose, const float R[9],

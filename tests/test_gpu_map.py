@@ -170,3 +170,24 @@ def test_bad_arguments(ctx):
         m.insert_ranges(sensor, A.Pose((1e9, 0, 0), (1, 0, 0, 0)), np.ones(16, np.float32))
     with pytest.raises(N.NanomapError):
         A.Map(ctx, A.map_desc(res=0.1, max_agents=0))
+
+
+def test_handles_destroyed_in_any_order(small):
+    """Objects keep their context alive: destroying the context handle first leaves the map,
+    sensor and sim map usable, and the last one to go frees it."""
+    import torch
+    spec, scene, desc, frames = small
+    c2 = A.Context(0)
+    sensor = A.Sensor(c2, desc)
+    m = A.Map(c2, A.map_desc(res=spec.map_res))
+    sim = A.SimMap(c2, spec.sim_res, boxes=scene.boxes, cylinders=scene.cylinders,
+                   vox_min=scene.vox_min, vox_max=scene.vox_max)
+    c2.close()
+    pose, _ = frames[0]
+    r = torch.zeros((desc.vres, desc.hres), device="cuda")
+    sim.render(sensor, pose, r)
+    m.insert_ranges(sensor, pose, r, flags=N.NM_SYNC)
+    assert m.stats()["leaf_count"] > 0
+    sensor.close()
+    sim.close()
+    m.close()
