@@ -418,23 +418,31 @@ int set_plane_constants(nm_map m, int plane, nm_sensor s) {
   return NM_OK;
 }
 
+constexpr int kFilteredTile = 16;        // traversal tile edge of filtered frames
+constexpr uint32_t kFilteredEntries = 512;  // leaf-table entries per tile of filtered frames
+
 // Voxel filter of one frame: runs the filter on `f`'s input and rewrites `f` into the frame
-// of the filtered points (input kind 2: one record per occupied voxel, counted on the device,
-// already rotated into the world frame).  A tile of the traversal covers consecutive
-// records, i.e. neighbouring voxels.
+// of the filtered points (input kind 2: one record per occupied voxel, already rotated into
+// the world frame, packed in the input order of the voxels' first points, counted on the
+// device).  A traversal tile covers consecutive records: neighbouring rays.
 int apply_filter(nm_map m, nm::FrameParams& f, uint32_t flags, cudaStream_t s0) {
   const int64_t n = (int64_t)f.width * f.height;
   const int kb = nm::filter_key_bits(f.max_time);
   if (kb == 0) return fail(NM_ERR_UNSUPPORTED, "voxel filter: range of %g voxels is too long", (double)f.max_time);
-  NM_CUDA(nm::filter_reserve(&m->filter, n));
+  NM_CUDA(nm::filter_reserve(&m->filter, n, s0));
+  m->filter.tag += 1u;
+  if (m->filter.tag == 0u) {  // wrapped: no stale record may carry the new tag
+    m->filter.tag = 1u;
+    NM_CUDA(cudaMemsetAsync(m->filter.idx_tags, 0, (size_t)m->filter.capacity * 4, s0));
+  }
   NM_CUDA(nm::run_voxel_filter(f, m->desc.rounding, (flags & NM_FILTER_CENTRE) ? 1 : 0, kb,
                                m->filter, s0));
   f.input_kind = 2;
-  f.xyz = reinterpret_cast<const unsigned char*>(m->filter.out_pts);
+  f.xyz = reinterpret_cast<const unsigned char*>(m->filter.dense_pts);
   f.step = 12;
   f.ranges = nullptr;
-  f.n_points = m->filter.n_out;
-  f.width = m->tile_w;
+  f.n_valid = m->filter.n_dense;
+  f.width = kFilteredTile;
   f.height = (int32_t)((n + f.width - 1) / f.width);
   for (int i = 0; i < 9; ++i) f.R[i] = (i % 4 == 0) ? 1.0f : 0.0f;
   return NM_OK;
@@ -456,6 +464,12 @@ int run_frame(nm_map m, nm_sensor s, nm::FrameParams& f, uint32_t flags, cudaStr
     w.tile_w = m->tile_w;
     w.tile_h = m->tile_h;
     w.smask = (uint32_t)m->smem_entries - 1u;
+    if (f.input_kind == 2) {
+      // filtered rays: one per voxel, packed by image patch, so a tile's rays fan out over
+      // more leaves than a tile of neighbouring pixels does: a larger leaf table
+      w.tile_w = w.tile_h = kFilteredTile;
+      w.smask = kFilteredEntries - 1u;
+    }
     w.tiles_x[0] = (f.width + w.tile_w - 1) / w.tile_w;
     const int tiles_y = (f.height + w.tile_h - 1) / w.tile_h;
     w.tile_start[0] = 0;
@@ -792,11 +806,24 @@ int nm_map_filter_points(nm_map m, nm_sensor s, const nm_pose* pose, const void*
   if (rc != NM_OK) return rc;
   NM_CUDA(cudaStreamSynchronize(s0));
   uint32_t cnt = 0;
-  NM_CUDA(cudaMemcpy(&cnt, m->filter.n_out, 4, cudaMemcpyDeviceToHost));
+  NM_CUDA(cudaMemcpy(&cnt, m->filter.n_used, 4, cudaMemcpyDeviceToHost));
   *n = cnt;
+  if (!cnt || (!points && !counts) || !max_points) return NM_OK;
+  // the device emits voxels in first-use order; the caller gets them in voxel order
+  std::vector<unsigned long long> keys(cnt);
+  std::vector<float> pts(3 * (size_t)cnt);
+  std::vector<uint32_t> cn(cnt);
+  NM_CUDA(cudaMemcpy(keys.data(), m->filter.out_keys, (size_t)cnt * 8, cudaMemcpyDeviceToHost));
+  NM_CUDA(cudaMemcpy(pts.data(), m->filter.out_pts, (size_t)cnt * 12, cudaMemcpyDeviceToHost));
+  NM_CUDA(cudaMemcpy(cn.data(), m->filter.out_counts, (size_t)cnt * 4, cudaMemcpyDeviceToHost));
+  std::vector<uint32_t> order(cnt);
+  for (uint32_t i = 0; i < cnt; ++i) order[i] = i;
+  std::sort(order.begin(), order.end(), [&](uint32_t a, uint32_t b) { return keys[a] < keys[b]; });
   const uint64_t k = std::min<uint64_t>(cnt, max_points);
-  if (k && points) NM_CUDA(cudaMemcpy(points, m->filter.out_pts, k * 12, cudaMemcpyDeviceToHost));
-  if (k && counts) NM_CUDA(cudaMemcpy(counts, m->filter.counts, k * 4, cudaMemcpyDeviceToHost));
+  for (uint64_t i = 0; i < k; ++i) {
+    if (points) std::memcpy(points + 3 * i, &pts[3 * (size_t)order[i]], 12);
+    if (counts) counts[i] = cn[order[i]];
+  }
   return NM_OK;
 }
 

@@ -74,7 +74,7 @@ struct FrameParams {
   const unsigned char* xyz;
   int64_t step;        // bytes between xyz records
   const float* ranges;
-  const uint32_t* n_points;  // input_kind 2: records [0, *n_points) are valid
+  const uint32_t* n_valid;  // input_kind 2: records [0, *n_valid) are valid
   float R[9];          // row-major, world-from-sensor
   double eye[3];       // index-space eye
   double res_d;
@@ -131,23 +131,29 @@ __host__ __device__ inline uint32_t hash_key(uint64_t k) {
   return (uint32_t)k;
 }
 
-// Working buffers of the voxel filter, sized for `capacity` input points.
+// Working buffers of the voxel filter, sized for `capacity` input points: a hash table of
+// end-point voxels (at least 2 * capacity slots, kept empty between frames), the list of
+// slots a frame used, and the filtered points: compact in first-use order (for export), at
+// the input index of each voxel's first point, and packed densely in input order (for the
+// traversal: full tiles of neighbouring rays).
 struct FilterBuffers {
-  unsigned long long* keys_in;
-  unsigned long long* keys_out;
-  unsigned long long* group_key;
-  uint32_t* idx_in;
-  uint32_t* idx_out;
-  uint32_t* heads;
-  uint32_t* seg;
-  uint32_t* counts;
-  uint32_t* n_out;     // device count of filtered points
-  long long* frac;     // 3 fixed-point fractions per input point
-  long long* sums;     // 3 fixed-point sums per voxel
-  float* out_pts;      // 3 floats per voxel: world-frame offset from the eye (m)
-  void* temp;
-  size_t temp_bytes;
+  unsigned long long* table_keys;  // voxel key per slot, ~0 = empty
+  unsigned long long* table_sums;  // 3 fixed-point fraction sums per slot
+  uint32_t* table_counts;          // points per slot
+  uint32_t* table_first;           // lowest input index per slot, ~0 = none
+  uint32_t* used;                  // slots used by the current frame, in first-use order
+  uint32_t* n_used;                // device count of used slots = filtered points
+  float* out_pts;                  // compact: 3 floats per filtered point, world offset (m)
+  unsigned long long* out_keys;    // compact: voxel key per filtered point
+  uint32_t* out_counts;            // compact: input points per filtered point
+  float* idx_pts;                  // by input index: 3 floats at the voxel's first point
+  uint32_t* idx_tags;              // by input index: tag of the frame that wrote idx_pts
+  float* dense_pts;                // tagged idx_pts packed in input order
+  uint32_t* block_counts;          // compaction: tagged indices per block, then their prefix
+  uint32_t* n_dense;               // device count of dense points
   int64_t capacity;
+  uint32_t table_mask;
+  uint32_t tag;                    // tag of the current frame (never 0)
 };
 
 // Constants of one expected-depth launch (double ray geometry, FP32 accumulation).
@@ -194,7 +200,7 @@ cudaError_t launch_depth_backward(const DepthParams& p, const MapView& m, const 
 cudaError_t launch_depth_refine(const DepthParams& p, const MapView& m, const float* vals,
                                 const float* target, float max_residual, double* partials,
                                 double* out8, cudaStream_t s);
-cudaError_t filter_reserve(FilterBuffers* b, int64_t n);
+cudaError_t filter_reserve(FilterBuffers* b, int64_t n, cudaStream_t s);
 void filter_release(FilterBuffers* b);
 int filter_key_bits(float max_time);  // bits per axis of a filter key; 0 if out of range
 cudaError_t run_voxel_filter(const FrameParams& f, int rounding, int centre, int key_bits,

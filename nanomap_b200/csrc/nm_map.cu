@@ -43,7 +43,7 @@ struct CountEmit {
 
 __device__ __forceinline__ bool load_point(const FrameParams& f, int w, int h, float p[3]) {
   if (f.input_kind == 1) return range_point(f, w, h, p);
-  if (f.input_kind == 2 && (uint32_t)(h * f.width + w) >= __ldg(f.n_points)) return false;
+  if (f.input_kind == 2 && (uint32_t)(h * f.width + w) >= __ldg(f.n_valid)) return false;
   return xyz_point(f, w, h, p);
 }
 

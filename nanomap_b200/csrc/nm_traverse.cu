@@ -116,7 +116,7 @@ __device__ __forceinline__ bool setup_ray(const FrameParams& f, const float p[3]
 
 __device__ __forceinline__ bool pixel_point(const FrameParams& f, int w, int h, float p[3]) {
   if (f.input_kind == 1) return range_point(f, w, h, p);
-  if (f.input_kind == 2 && (uint32_t)(h * f.width + w) >= __ldg(f.n_points)) return false;
+  if (f.input_kind == 2 && (uint32_t)(h * f.width + w) >= __ldg(f.n_valid)) return false;
   return xyz_point(f, w, h, p);
 }
 
@@ -146,8 +146,6 @@ __device__ __forceinline__ void traverse_body(const TickWork<MaxF>& work, const 
       s_next = 0u;
       if (t == work.total_tiles + gridDim.x - 1) m.ctr->tile_queue = 0u;  // last reader resets
     }
-    for (int i = tid; i < nent; i += blockDim.x) s_keys[i] = kEmptyKey;
-    for (int i = tid; i < nent * kLabelWords; i += blockDim.x) s_words[i] = 0u;
     __syncthreads();
     const uint32_t tile = s_tile;
     if (tile >= work.total_tiles) break;
@@ -163,6 +161,14 @@ __device__ __forceinline__ void traverse_body(const TickWork<MaxF>& work, const 
     const int tx = (int)(lt % (uint32_t)work.tiles_x[fi]);
     const int ty = (int)(lt / (uint32_t)work.tiles_x[fi]);
     const int x0 = tx * work.tile_w, y0 = ty * work.tile_h;
+    // packed records (input kind 2) fill the first tiles only: later tiles have no work
+    if (f.input_kind == 2 && (uint32_t)(y0 * f.width + x0) >= __ldg(f.n_valid)) {
+      __syncthreads();
+      continue;
+    }
+    for (int i = tid; i < nent; i += blockDim.x) s_keys[i] = kEmptyKey;
+    for (int i = tid; i < nent * kLabelWords; i += blockDim.x) s_words[i] = 0u;
+    __syncthreads();
 
     Ray r;
     bool active = false;
