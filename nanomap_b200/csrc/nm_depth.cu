@@ -76,29 +76,56 @@ __device__ __forceinline__ float seg_g(float u) {
 
 // Visits every voxel of the ray after the start voxel: f(v, t_in, a_in, t_out, a_out), the
 // voxel entered at t_in < t_max across axis a_in and left at t_out = min(next crossing,
-// t_max) across a_out (-1 when clamped to t_max).
+// t_max) across a_out (-1 when clamped to t_max).  Crossings are (boundary - e) * (1 / d),
+// the reciprocal taken once per ray; per-axis state is kept in scalars (no local memory).
 template <class F>
 __device__ __forceinline__ void walk(const double e[3], const double d[3], double t_max, F&& f) {
-  int v[3], s[3];
-  double tn[3];
-#pragma unroll
-  for (int a = 0; a < 3; ++a) {
-    v[a] = (int)floor(e[a]);
-    s[a] = d[a] > 0.0 ? 1 : (d[a] < 0.0 ? -1 : 0);
-    tn[a] = s[a] ? __ddiv_rn(__dadd_rn((double)(v[a] + (s[a] > 0 ? 1 : 0)), -e[a]), d[a]) : CUDART_INF;
-  }
+  int vx = (int)floor(e[0]), vy = (int)floor(e[1]), vz = (int)floor(e[2]);
+  const int sx = d[0] > 0.0 ? 1 : (d[0] < 0.0 ? -1 : 0);
+  const int sy = d[1] > 0.0 ? 1 : (d[1] < 0.0 ? -1 : 0);
+  const int sz = d[2] > 0.0 ? 1 : (d[2] < 0.0 ? -1 : 0);
+  const double rx = sx ? __drcp_rn(d[0]) : 0.0;
+  const double ry = sy ? __drcp_rn(d[1]) : 0.0;
+  const double rz = sz ? __drcp_rn(d[2]) : 0.0;
+  auto cross = [](int v, int s, double e, double r) {
+    return __dmul_rn(__dadd_rn((double)(v + (s > 0 ? 1 : 0)), -e), r);
+  };
+  double tx = sx ? cross(vx, sx, e[0], rx) : CUDART_INF;
+  double ty = sy ? cross(vy, sy, e[1], ry) : CUDART_INF;
+  double tz = sz ? cross(vz, sz, e[2], rz) : CUDART_INF;
   int a_in = 2;
-  if (tn[1] < tn[a_in]) a_in = 1;
-  if (tn[0] < tn[a_in]) a_in = 0;
-  double t_in = tn[a_in];
+  double t_in = tz;
+  if (ty < t_in) {
+    a_in = 1;
+    t_in = ty;
+  }
+  if (tx < t_in) {
+    a_in = 0;
+    t_in = tx;
+  }
   const long long cap = 3ll * (long long)t_max + 16;
   for (long long it = 0; it < cap && t_in < t_max; ++it) {
-    v[a_in] += s[a_in];
-    tn[a_in] = __ddiv_rn(__dadd_rn((double)(v[a_in] + (s[a_in] > 0 ? 1 : 0)), -e[a_in]), d[a_in]);
+    if (a_in == 0) {
+      vx += sx;
+      tx = cross(vx, sx, e[0], rx);
+    } else if (a_in == 1) {
+      vy += sy;
+      ty = cross(vy, sy, e[1], ry);
+    } else {
+      vz += sz;
+      tz = cross(vz, sz, e[2], rz);
+    }
     int a_out = 2;
-    if (tn[1] < tn[a_out]) a_out = 1;
-    if (tn[0] < tn[a_out]) a_out = 0;
-    const double t_out = tn[a_out];
+    double t_out = tz;
+    if (ty < t_out) {
+      a_out = 1;
+      t_out = ty;
+    }
+    if (tx < t_out) {
+      a_out = 0;
+      t_out = tx;
+    }
+    const int v[3] = {vx, vy, vz};
     if (t_out < t_max)
       f(v, t_in, a_in, t_out, a_out);
     else

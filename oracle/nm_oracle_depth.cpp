@@ -11,7 +11,8 @@
  * space eye e = position / res; t_max = max_range / res.
  *
  * Traversal: voxel DDA (Amanatides & Woo, 1987) from the voxel holding e; next crossing per
- * axis tn_a = (boundary_a - e_a) / d_a, recomputed from the boundary after every step; the
+ * axis tn_a = (boundary_a - e_a) * r_a with r_a = 1 / d_a (once per ray), recomputed from the
+ * boundary after every step; the
  * axis with the smallest tn steps, ties to the higher axis.  Voxel k is entered at t_in (axis
  * a_in) when t_in < t_max and left at t_out = min(next crossing, t_max) (axis a_out, none when
  * clamped).  The start voxel holds the sensor and takes no part.
@@ -96,11 +97,12 @@ double seg_g(double u) {
 template <class F>
 void walk(const double e[3], const double d[3], double t_max, F&& f) {
   int v[3], s[3];
-  double tn[3];
+  double tn[3], r[3];
   for (int a = 0; a < 3; ++a) {
     v[a] = (int)std::floor(e[a]);
     s[a] = d[a] > 0.0 ? 1 : (d[a] < 0.0 ? -1 : 0);
-    tn[a] = s[a] ? ((double)(v[a] + (s[a] > 0 ? 1 : 0)) - e[a]) / d[a] : INFINITY;
+    r[a] = s[a] ? 1.0 / d[a] : 0.0;
+    tn[a] = s[a] ? ((double)(v[a] + (s[a] > 0 ? 1 : 0)) - e[a]) * r[a] : INFINITY;
   }
   auto next_axis = [&]() {
     int a = 2;
@@ -113,7 +115,7 @@ void walk(const double e[3], const double d[3], double t_max, F&& f) {
   const long cap = 3L * (long)t_max + 16;
   for (long it = 0; it < cap && t_in < t_max; ++it) {
     v[a_in] += s[a_in];
-    tn[a_in] = ((double)(v[a_in] + (s[a_in] > 0 ? 1 : 0)) - e[a_in]) / d[a_in];
+    tn[a_in] = ((double)(v[a_in] + (s[a_in] > 0 ? 1 : 0)) - e[a_in]) * r[a_in];
     const int a_out = next_axis();
     const double t_out = tn[a_out];
     if (t_out < t_max) {
