@@ -381,6 +381,8 @@ def run_ours(args, rank, world, local):
         line["expected_depth"] = run_depth_section(ctx, m, sensor, sim, spec, poses, stream, hbm)
     if args.batched_ticks > args.warmup:
         line["batched"] = run_batched(args, rank, world, local, args.batched_ticks)
+    if args.large:
+        line["large"] = run_large_section(local)
     if rank == 0 and world == 1 and args.cpu_baseline_s > 0:
         frames_host = []
         for k in range(30):
@@ -510,6 +512,77 @@ def run_depth_section(ctx, m, sensor, sim, spec, poses, stream, hbm, reps=10):
         ref[name] = {"final_error_m": te, "final_error_deg": ae, "loss_first": float(losses[0]),
                      "loss_last": float(losses[-1]), "ms_per_step": dt * 1e3 / 50}
     out["refine"] = ref
+    return out
+
+
+def run_large_section(local, frames=12, warmup=3):
+    """Config 5 at size (80 x 80 x 20 m, 10000 boxes + 2000 cylinders, 0.02 m voxels, one
+    1280x720 camera at 15 m): per frame sim render + noise + insert + integrate, and the
+    expected-depth forward and adjoint of one frame over the resulting map."""
+    import torch
+
+    from nanomap_b200 import _native as N
+    from nanomap_b200 import api as A
+    from nanomap_b200 import scenes as S
+    spec = S.SCENES["large_fine"]
+    scene = S.make_scene(spec, 1)
+    traj = S.trajectory(scene, frames + warmup, seed=7)
+    ctx = A.Context(local)
+    sensor = A.Sensor(ctx, A.sensor_desc(**S.sensor_desc_kwargs(spec)))
+    torch.cuda.synchronize()
+    t0 = time.perf_counter()
+    sim = A.SimMap(ctx, spec.sim_res, boxes=scene.boxes, cylinders=scene.cylinders,
+                   vox_min=scene.vox_min, vox_max=scene.vox_max)
+    torch.cuda.synchronize()
+    build_s = time.perf_counter() - t0
+    m = A.Map(ctx, A.map_desc(res=spec.map_res, clamp_min=spec.clamp[0], clamp_max=spec.clamp[1],
+                              rounding=N.NM_ROUND_DOWN, initial_leaf_capacity=1 << 22))
+    stream = torch.cuda.current_stream()
+    r = torch.zeros(spec.height, spec.width, device="cuda")
+    poses = [A.Pose(p, q) for p, q in traj]
+
+    def step(k):
+        sim.render(sensor, poses[k], r, stream=stream)
+        ctx.add_noise(r, spec.noise_coef, spec.drop, 7 * (k + 1), stream=stream)
+        m.insert_ranges(sensor, poses[k], r, stream=stream)
+
+    for k in range(warmup):
+        step(k)
+    torch.cuda.synchronize()
+    s0 = m.stats()
+    e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+    e0.record(stream)
+    for k in range(warmup, warmup + frames):
+        step(k)
+    e1.record(stream)
+    torch.cuda.synchronize()
+    s1 = m.stats()
+    ms = e0.elapsed_time(e1) / frames
+    visits = (s1["visits"] - s0["visits"]) / frames
+    pos, R = A.Map.ray_pose(sensor, poses[warmup])
+    gd = torch.ones(spec.height, spec.width, device="cuda")
+    m.depth_render(sensor, pos, R, scale=4.0)
+    torch.cuda.synchronize()
+    f0, f1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+    f0.record(stream)
+    m.depth_render(sensor, pos, R, scale=4.0)
+    f1.record(stream)
+    torch.cuda.synchronize()
+    t0 = time.perf_counter()
+    m.depth_backward(sensor, pos, R, gd, scale=4.0)
+    bwd_ms = (time.perf_counter() - t0) * 1e3
+    out = {
+        "workload": ("80x80x20 m, 10000 boxes + 2000 cylinders, 0.02 m voxels, 1280x720 87x58 deg "
+                     "camera at 15 m; per frame sim render + noise + insert + integrate"),
+        "frames": frames, "ms_per_frame": ms, "voxel_updates_per_s": visits / (ms / 1e3),
+        "visits_per_frame": visits, "rays_per_frame": (s1["rays"] - s0["rays"]) / frames,
+        "sim_build_s": build_s, "leaf_count": s1["leaf_count"], "table_growths": s1["grow_count"],
+        "expected_depth_forward_ms": f0.elapsed_time(f1), "expected_depth_adjoint_ms_incl_host_sync": bwd_ms,
+    }
+    m.close()
+    sim.close()
+    sensor.close()
+    ctx.close()
     return out
 
 
@@ -656,6 +729,8 @@ def main():
     ap.add_argument("--cpu-baseline-s", type=float, default=12.0)
     ap.add_argument("--batched-ticks", type=int, default=40,
                     help="ticks of the 16-agent batched comparison (0 = skip)")
+    ap.add_argument("--large", type=int, default=1,
+                    help="1 = also measure the large fine-resolution workload (0.02 m, 1280x720 at 15 m)")
     ap.add_argument("--extras", type=int, default=1,
                     help="1 = also measure the voxel-filtered insert, expected depth and refinement")
     ap.add_argument("--capacity-log2", type=int, default=21,
