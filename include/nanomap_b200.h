@@ -364,6 +364,21 @@ int nm_simmap_export(nm_simmap sm, int32_t* origins, uint32_t* words, uint64_t m
  * generateCloud.cu:84-94).  Output: hres*vres floats, radial metres, 0 = no return. */
 int nm_sim_render(nm_simmap sm, nm_sensor s, const nm_pose* pose, float* ranges,
                   uint32_t flags, void* stream);
+
+/* Ray casts against the sim map for agent observation and collision rays
+ * (SimManager::getAgentSimCollision, SimManager.h:141-168): n rays from `origins` (metres,
+ * 3 floats each) along `directions` (3 floats each, any length, normalised here); distances
+ * (metres) to the first active voxel entered within max_range, 0 when none (the voxel holding
+ * the origin is not tested).  NM_INPUT_HOST / NM_OUTPUT_HOST mark host arrays.  The reference
+ * intersects leaf-node spans (openvdb::tools::VolumeRayIntersector); this cast is exact to
+ * the voxel. */
+int nm_sim_cast_rays(nm_simmap sm, const float* origins, const float* directions, int64_t n,
+                     float max_range, float* distances, uint32_t flags, void* stream);
+
+/* The n unit observation directions of an agent (host output, 3 floats each): the spiral
+ * sphere of Agent::generateObservationSphere (Agent.h:147-192), n >= 2. */
+int nm_observation_sphere(int32_t n, float* directions);
+
 /* Sensor noise on a device range image: r += N(0, (sigma_coef * r^2)^2), then each pixel
  * is set to 0 with probability drop_prob.  Counter-based generator keyed by `seed`. */
 int nm_ranges_add_noise(nm_context ctx, float* ranges, int64_t n, float sigma_coef,

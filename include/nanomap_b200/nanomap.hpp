@@ -267,6 +267,15 @@ class Agent {
       throw Error(NM_ERR_UNSUPPORTED, "nanomap_b200: random agent spawns need the OpenVDB sim grid");
     pose_.position = Vector3f(a.position[0], a.position[1], a.position[2]);
     pose_.orientation = Quaternionf(std::sqrt(0.5f), 0.f, 0.f, -std::sqrt(0.5f));
+    num_obs_ = a.num_obs;
+    len_obs_ = a.len_obs;
+    collision_dist_ = a.collision_dist;
+    if (num_obs_ >= 2) {
+      std::vector<float> d(3 * (size_t)num_obs_);
+      detail::check(nm_observation_sphere(num_obs_, d.data()));
+      for (int i = 0; i < num_obs_; ++i)
+        obs_rays_.push_back(Vector3f(d[3 * i], d[3 * i + 1], d[3 * i + 2]));
+    }
     for (int j = 0; j < a.n_sensors; ++j) {
       char name[256];
       nm_pose o;
@@ -297,8 +306,16 @@ class Agent {
   std::vector<std::string> sensorNames() const { return names_; }
   std::shared_ptr<map::Map> map() { return map_; }
   bool spawnRandom() const { return false; }
+  // Observation sphere (Agent.h:147-192): unit ray directions, collision distance (m) and
+  // observation length (m) from the agent file's Observations: line.
+  const std::vector<Vector3f>& observationRays() const { return obs_rays_; }
+  float collisionDist() const { return collision_dist_; }
+  float observationLength() const { return len_obs_; }
 
  private:
+  int num_obs_ = 0;
+  float len_obs_ = 0.f, collision_dist_ = 0.f;
+  std::vector<Vector3f> obs_rays_;
   Pose pose_;
   std::vector<std::string> names_;
   std::vector<Pose> origins_, poses_;
@@ -370,6 +387,27 @@ class SimManager {
     for (auto& a : agents_) view(*a, map_ptr);
   }
   std::shared_ptr<Map> getMap(int index) { return agents_[index]->map(); }
+  // SimManager.h:141-168: true when agent `index` can move by positionDelta, i.e. none of its
+  // observation rays, cast from the new position, meets an active sim voxel closer than the
+  // agent's collision distance (exact to the voxel; the reference tests leaf-node spans).
+  bool getAgentSimCollision(int index, Vector3f positionDelta) {
+    const agent::Agent& a = *agents_[index];
+    const auto& rays = a.observationRays();
+    if (rays.empty()) return true;
+    const Vector3f eye = a.pose().position + positionDelta;
+    std::vector<float> o(3 * rays.size()), d(3 * rays.size()), dist(rays.size());
+    for (size_t i = 0; i < rays.size(); ++i)
+      for (int k = 0; k < 3; ++k) {
+        o[3 * i + k] = eye(k);
+        d[3 * i + k] = rays[i](k);
+      }
+    detail::check(nm_sim_cast_rays(sim_.get(), o.data(), d.data(), (int64_t)rays.size(),
+                                   a.collisionDist(), dist.data(),
+                                   NM_INPUT_HOST | NM_OUTPUT_HOST, nullptr));
+    for (float x : dist)
+      if (x > 0.f && x < a.collisionDist()) return false;
+    return true;
+  }
   std::shared_ptr<agent::Agent> agent(int index) { return agents_[index]; }
   nm_simmap simMap() { return sim_.get(); }
   void closeHandler() {}

@@ -52,6 +52,13 @@ def _ray_pose(position, rotation) -> N.NmRayPose:
     return rp
 
 
+def observation_sphere(n: int) -> np.ndarray:
+    """The n unit observation directions of an agent (Agent.h:147-192), (n, 3) float32."""
+    out = np.zeros((n, 3), np.float32)
+    call("nm_observation_sphere", n, out.ctypes.data_as(N._PF))
+    return out
+
+
 def make_pose(position, orientation) -> N.NmPose:
     p = N.NmPose()
     for i in range(3):
@@ -439,6 +446,24 @@ class SimMap:
         if host:
             flags |= N.NM_OUTPUT_HOST
         call("nm_sim_render", self.h, sensor.h, C.byref(pose.c()), p, flags, _stream(stream))
+
+    def cast_rays(self, origins, directions, max_range: float, stream=None):
+        """Distances (metres) to the first active voxel along each ray within max_range, 0 when
+        none.  numpy inputs give a numpy result; CUDA tensors give a CUDA tensor."""
+        if _is_torch(origins):
+            import torch
+            o = origins.contiguous().float()
+            d = directions.contiguous().float()
+            out = torch.empty(o.numel() // 3, dtype=torch.float32, device=o.device)
+            call("nm_sim_cast_rays", self.h, C.c_void_p(o.data_ptr()), C.c_void_p(d.data_ptr()),
+                 out.numel(), max_range, C.c_void_p(out.data_ptr()), 0, _stream(stream))
+            return out
+        o = np.ascontiguousarray(origins, np.float32).reshape(-1, 3)
+        d = np.ascontiguousarray(directions, np.float32).reshape(-1, 3)
+        out = np.zeros(len(o), np.float32)
+        call("nm_sim_cast_rays", self.h, o.ctypes.data, d.ctypes.data, len(o), max_range,
+             out.ctypes.data, N.NM_INPUT_HOST | N.NM_OUTPUT_HOST, _stream(stream))
+        return out
 
     def close(self):
         if self.h:

@@ -140,6 +140,7 @@ void release(nm_simmap sm) {
   cudaFree(sm->view.leaf_index);
   cudaFree(sm->view.leaf_words);
   cudaFree(sm->view.brick_bits);
+  cudaFree(sm->cast_staging);
   delete sm;
   release(c);
 }
@@ -324,6 +325,67 @@ int nm_sim_render(nm_simmap sm, nm_sensor s, const nm_pose* pose, float* ranges,
     NM_CUDA(cudaStreamSynchronize(st));
   } else if (flags & NM_SYNC) {
     NM_CUDA(cudaStreamSynchronize(st));
+  }
+  return NM_OK;
+}
+
+int nm_sim_cast_rays(nm_simmap sm, const float* origins, const float* directions, int64_t n,
+                     float max_range, float* distances, uint32_t flags, void* stream) {
+  if (!sm || n < 0 || (n > 0 && (!origins || !directions || !distances)))
+    return fail(NM_ERR_ARG, "invalid argument");
+  if (!(max_range >= 0.0f) || !std::isfinite(max_range)) return fail(NM_ERR_ARG, "max_range invalid");
+  if (n == 0) return NM_OK;
+  nm_context ctx = sm->ctx;
+  NM_CUDA(cudaSetDevice(ctx->device));
+  cudaStream_t st = pick(ctx, stream);
+  const float* d_o = origins;
+  const float* d_d = directions;
+  float* d_out = distances;
+  const bool host_in = (flags & NM_INPUT_HOST) != 0, host_out = (flags & NM_OUTPUT_HOST) != 0;
+  if (host_in || host_out) {
+    const size_t bytes = (size_t)n * 7 * sizeof(float);
+    if (bytes > sm->cast_staging_bytes) {
+      cudaFree(sm->cast_staging);
+      sm->cast_staging = nullptr;
+      sm->cast_staging_bytes = 0;
+      NM_CUDA(cudaMalloc((void**)&sm->cast_staging, bytes));
+      sm->cast_staging_bytes = bytes;
+    }
+    if (host_in) {
+      NM_CUDA(cudaMemcpyAsync(sm->cast_staging, origins, (size_t)n * 12, cudaMemcpyHostToDevice, st));
+      NM_CUDA(cudaMemcpyAsync(sm->cast_staging + 3 * n, directions, (size_t)n * 12,
+                              cudaMemcpyHostToDevice, st));
+      d_o = sm->cast_staging;
+      d_d = sm->cast_staging + 3 * n;
+    }
+    if (host_out) d_out = sm->cast_staging + 6 * n;
+  }
+  NM_CUDA(nm::launch_sim_cast(sm->view, d_o, d_d, n, max_range, d_out, st));
+  if (host_out) {
+    NM_CUDA(cudaMemcpyAsync(distances, d_out, (size_t)n * 4, cudaMemcpyDeviceToHost, st));
+    NM_CUDA(cudaStreamSynchronize(st));
+  } else if (flags & NM_SYNC) {
+    NM_CUDA(cudaStreamSynchronize(st));
+  }
+  return NM_OK;
+}
+
+int nm_observation_sphere(int32_t n, float* directions) {
+  if (n < 2 || !directions) return fail(NM_ERR_ARG, "an observation sphere needs n >= 2 rays");
+  nm::RoundScope rs(NM_ROUND_NEAREST);
+  // Spiral over the sphere (Agent.h:147-179): n points with latitude parameter s running
+  // over (-1, 1), longitude s * (0.1 + 1.2 n), evaluated in float like the reference.
+  const float x = (float)(0.1 + 1.2 * n);
+  const float start = (float)(-1.0 + 1.0 / (n - 1.0));
+  const float inc = (float)((2.0 - 2.0 / (n - 1.0)) / (n - 1.0));
+  for (int i = 0; i < n; ++i) {
+    const float sv = start + (float)i * inc;
+    const float lon = sv * x;
+    const float lat = (float)((3.14159265358979323846 / 2.0) * std::copysign(1.0, (double)sv) *
+                              (1.0 - std::sqrt(1.0 - std::fabs((double)sv))));
+    float p[3] = {std::cos(lon) * std::cos(lat), std::sin(lon) * std::cos(lat), std::sin(lat)};
+    const float nn = std::sqrt(p[0] * p[0] + p[1] * p[1] + p[2] * p[2]);
+    for (int a = 0; a < 3; ++a) directions[3 * i + a] = p[a] / nn;
   }
   return NM_OK;
 }

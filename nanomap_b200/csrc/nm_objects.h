@@ -90,6 +90,8 @@ struct nm_simmap_s {
   int32_t bbox[6] = {0, 0, 0, -1, -1, -1};
   uint64_t active_voxels = 0;
   uint64_t leaves = 0;
+  float* cast_staging = nullptr;  // host-side ray casts: origins, directions, distances
+  size_t cast_staging_bytes = 0;
 };
 
 

@@ -16,6 +16,7 @@
 // higher axis than the exit axis.
 #include <cfloat>
 #include <cmath>
+#include <algorithm>
 #include <cstdint>
 
 #include "nm_sim.h"
@@ -217,109 +218,116 @@ __device__ __forceinline__ int sim_level(const SimMapView& v, int x, int y, int 
   return 0;
 }
 
-// Range of pixel (w, h): the first active voxel entered along the pixel ray, or 0.
-__device__ __forceinline__ float sim_ray(const SimMapView& v, const SimRayParams& rp, int w, int h) {
+// Distance (metres) to the first active voxel entered along the ray from `eye` (index space)
+// in the unit direction `dir`, at a ray time within [tmin, tmax] (voxel units), or 0.  The
+// voxel holding the eye is not tested.
+__device__ __forceinline__ float sim_cast(const SimMapView& v, const float eye[3], float dir[3],
+                                          float tmin, float tmax) {
   float result = 0.0f;
-  if (v.any) {
-    float d0, d1, d2;
-    if (rp.type == NM_SENSOR_FRUSTUM) {
-      const float u = __fmul_rn((float)w, rp.su);
-      const float vv = __fmul_rn((float)h, rp.sv);
-      d0 = __fadd_rn(__fmul_rn(u, rp.c0), -rp.hw);
-      d1 = __fadd_rn(__fmul_rn(vv, rp.c1), -rp.hh);
-      d2 = 1.0f;
+  float inv[3];
+  int st[3];
+  float t_in = 0.0f, t_out = INFINITY;
+  bool miss = false;
+#pragma unroll
+  for (int a = 0; a < 3; ++a) {
+    if (fabsf(dir[a]) < 1e-30f) dir[a] = 0.0f;
+    if (dir[a] == 0.0f) {
+      st[a] = 0;
+      inv[a] = 0.0f;
+      if (eye[a] < v.box_lo[a] || eye[a] > v.box_hi[a]) miss = true;
     } else {
-      const float cv = __ldg(&rp.cosv[h]);
-      d0 = __fmul_rn(__ldg(&rp.sinu[w]), cv);
-      d1 = __ldg(&rp.sinv[h]);
-      d2 = __fmul_rn(__ldg(&rp.cosu[w]), cv);
-    }
-    const float* R = rp.R;
-    const float m0 = __fadd_rn(__fadd_rn(__fmul_rn(R[0], d0), __fmul_rn(R[1], d1)), __fmul_rn(R[2], d2));
-    const float m1 = __fadd_rn(__fadd_rn(__fmul_rn(R[3], d0), __fmul_rn(R[4], d1)), __fmul_rn(R[5], d2));
-    const float m2 = __fadd_rn(__fadd_rn(__fmul_rn(R[6], d0), __fmul_rn(R[7], d1)), __fmul_rn(R[8], d2));
-    const float norm = __fsqrt_rn(__fadd_rn(__fadd_rn(__fmul_rn(m0, m0), __fmul_rn(m1, m1)), __fmul_rn(m2, m2)));
-    float dir[3] = {__fdiv_rn(m0, norm), __fdiv_rn(m1, norm), __fdiv_rn(m2, norm)};
-    const float eye[3] = {__fdiv_rn(rp.pos[0], v.res), __fdiv_rn(rp.pos[1], v.res),
-                          __fdiv_rn(rp.pos[2], v.res)};
-    float tmin, tmax;
-    if (rp.type == NM_SENSOR_FRUSTUM) {
-      tmin = __fmul_rn(__fdiv_rn(rp.min_range, v.res), norm);
-      tmax = __fmul_rn(__fdiv_rn(rp.max_range, v.res), norm);
-    } else {
-      tmin = __fdiv_rn(rp.min_range, v.res);
-      tmax = __fdiv_rn(rp.max_range, v.res);
-    }
-    float inv[3];
-    int st[3];
-    float t_in = 0.0f, t_out = INFINITY;
-    bool miss = false;
-#pragma unroll
-    for (int a = 0; a < 3; ++a) {
-      if (fabsf(dir[a]) < 1e-30f) dir[a] = 0.0f;
-      if (dir[a] == 0.0f) {
-        st[a] = 0;
-        inv[a] = 0.0f;
-        if (eye[a] < v.box_lo[a] || eye[a] > v.box_hi[a]) miss = true;
-      } else {
-        inv[a] = __frcp_rn(dir[a]);
-        st[a] = dir[a] > 0.0f ? 1 : -1;
-        float ta = plane_time_f(v.box_lo[a], eye[a], inv[a]);
-        float tb = plane_time_f(v.box_hi[a], eye[a], inv[a]);
-        if (ta > tb) {
-          const float x = ta;
-          ta = tb;
-          tb = x;
-        }
-        if (ta > t_in) t_in = ta;
-        if (tb < t_out) t_out = tb;
+      inv[a] = __frcp_rn(dir[a]);
+      st[a] = dir[a] > 0.0f ? 1 : -1;
+      float ta = plane_time_f(v.box_lo[a], eye[a], inv[a]);
+      float tb = plane_time_f(v.box_hi[a], eye[a], inv[a]);
+      if (ta > tb) {
+        const float x = ta;
+        ta = tb;
+        tb = x;
       }
+      if (ta > t_in) t_in = ta;
+      if (tb < t_out) t_out = tb;
     }
-    if (!miss && !(t_in > t_out)) {
-      int k[3];
+  }
+  if (!miss && !(t_in > t_out)) {
+    int k[3];
 #pragma unroll
-      for (int a = 0; a < 3; ++a) k[a] = (int)floorf(__fadd_rn(eye[a], __fmul_rn(dir[a], t_in)));
-      float t = t_in;
-      bool first = true;
-      for (int iter = 0; iter < (1 << 22); ++iter) {
-        int leaf = -1;
-        const int lvl = sim_level(v, k[0], k[1], k[2], &leaf);
-        if (lvl == 0 && !first) {
-          const int l = ((k[0] & 7) << 6) | ((k[1] & 7) << 3) | (k[2] & 7);
-          if ((__ldg(&v.leaf_words[(size_t)leaf * 16 + (l >> 5)]) >> (l & 31)) & 1u) {
-            if (t >= tmin && t <= tmax) result = __fmul_rn(t, v.res);
-            break;
-          }
+    for (int a = 0; a < 3; ++a) k[a] = (int)floorf(__fadd_rn(eye[a], __fmul_rn(dir[a], t_in)));
+    float t = t_in;
+    bool first = true;
+    for (int iter = 0; iter < (1 << 22); ++iter) {
+      int leaf = -1;
+      const int lvl = sim_level(v, k[0], k[1], k[2], &leaf);
+      if (lvl == 0 && !first) {
+        const int l = ((k[0] & 7) << 6) | ((k[1] & 7) << 3) | (k[2] & 7);
+        if ((__ldg(&v.leaf_words[(size_t)leaf * 16 + (l >> 5)]) >> (l & 31)) & 1u) {
+          if (t >= tmin && t <= tmax) result = __fmul_rn(t, v.res);
+          break;
         }
-        first = false;
-        const int S = lvl == 2 ? 64 : (lvl == 1 ? 8 : 1);
-        int far[3];
-        float T[3];
-#pragma unroll
-        for (int a = 0; a < 3; ++a) {
-          if (st[a] == 0) {
-            far[a] = k[a];
-            T[a] = INFINITY;
-          } else {
-            far[a] = st[a] > 0 ? (k[a] | (S - 1)) : (k[a] & ~(S - 1));
-            T[a] = plane_time(st[a] > 0 ? far[a] + 1 : far[a], eye[a], inv[a]);
-          }
-        }
-        const int ax = (T[0] < T[1]) ? ((T[0] < T[2]) ? 0 : 2) : ((T[1] < T[2]) ? 1 : 2);
-        const float Tx = T[ax];
-        if (!(Tx <= t_out)) break;
-        if (S > 1) {
-#pragma unroll
-          for (int a = 0; a < 3; ++a)
-            if (a != ax && st[a] != 0)
-              k[a] = advance_axis(k[a], far[a], st[a], eye[a], dir[a], inv[a], Tx, a > ax);
-        }
-        k[ax] = far[ax] + st[ax];
-        t = Tx;
       }
+      first = false;
+      const int S = lvl == 2 ? 64 : (lvl == 1 ? 8 : 1);
+      int far[3];
+      float T[3];
+#pragma unroll
+      for (int a = 0; a < 3; ++a) {
+        if (st[a] == 0) {
+          far[a] = k[a];
+          T[a] = INFINITY;
+        } else {
+          far[a] = st[a] > 0 ? (k[a] | (S - 1)) : (k[a] & ~(S - 1));
+          T[a] = plane_time(st[a] > 0 ? far[a] + 1 : far[a], eye[a], inv[a]);
+        }
+      }
+      const int ax = (T[0] < T[1]) ? ((T[0] < T[2]) ? 0 : 2) : ((T[1] < T[2]) ? 1 : 2);
+      const float Tx = T[ax];
+      if (!(Tx <= t_out)) break;
+      if (S > 1) {
+#pragma unroll
+        for (int a = 0; a < 3; ++a)
+          if (a != ax && st[a] != 0)
+            k[a] = advance_axis(k[a], far[a], st[a], eye[a], dir[a], inv[a], Tx, a > ax);
+      }
+      k[ax] = far[ax] + st[ax];
+      t = Tx;
     }
   }
   return result;
+}
+
+// Range of pixel (w, h): the first active voxel entered along the pixel ray, or 0.
+__device__ __forceinline__ float sim_ray(const SimMapView& v, const SimRayParams& rp, int w, int h) {
+  if (!v.any) return 0.0f;
+  float d0, d1, d2;
+  if (rp.type == NM_SENSOR_FRUSTUM) {
+    const float u = __fmul_rn((float)w, rp.su);
+    const float vv = __fmul_rn((float)h, rp.sv);
+    d0 = __fadd_rn(__fmul_rn(u, rp.c0), -rp.hw);
+    d1 = __fadd_rn(__fmul_rn(vv, rp.c1), -rp.hh);
+    d2 = 1.0f;
+  } else {
+    const float cv = __ldg(&rp.cosv[h]);
+    d0 = __fmul_rn(__ldg(&rp.sinu[w]), cv);
+    d1 = __ldg(&rp.sinv[h]);
+    d2 = __fmul_rn(__ldg(&rp.cosu[w]), cv);
+  }
+  const float* R = rp.R;
+  const float m0 = __fadd_rn(__fadd_rn(__fmul_rn(R[0], d0), __fmul_rn(R[1], d1)), __fmul_rn(R[2], d2));
+  const float m1 = __fadd_rn(__fadd_rn(__fmul_rn(R[3], d0), __fmul_rn(R[4], d1)), __fmul_rn(R[5], d2));
+  const float m2 = __fadd_rn(__fadd_rn(__fmul_rn(R[6], d0), __fmul_rn(R[7], d1)), __fmul_rn(R[8], d2));
+  const float norm = __fsqrt_rn(__fadd_rn(__fadd_rn(__fmul_rn(m0, m0), __fmul_rn(m1, m1)), __fmul_rn(m2, m2)));
+  float dir[3] = {__fdiv_rn(m0, norm), __fdiv_rn(m1, norm), __fdiv_rn(m2, norm)};
+  const float eye[3] = {__fdiv_rn(rp.pos[0], v.res), __fdiv_rn(rp.pos[1], v.res),
+                        __fdiv_rn(rp.pos[2], v.res)};
+  float tmin, tmax;
+  if (rp.type == NM_SENSOR_FRUSTUM) {
+    tmin = __fmul_rn(__fdiv_rn(rp.min_range, v.res), norm);
+    tmax = __fmul_rn(__fdiv_rn(rp.max_range, v.res), norm);
+  } else {
+    tmin = __fdiv_rn(rp.min_range, v.res);
+    tmax = __fdiv_rn(rp.max_range, v.res);
+  }
+  return sim_cast(v, eye, dir, tmin, tmax);
 }
 
 __global__ void __launch_bounds__(256) k_sim_render(SimMapView v, SimRayParams rp, float* out) {
@@ -327,6 +335,29 @@ __global__ void __launch_bounds__(256) k_sim_render(SimMapView v, SimRayParams r
   const int h = blockIdx.y * 16 + (threadIdx.x >> 4);
   if (w >= rp.width || h >= rp.height) return;
   out[(size_t)h * rp.width + w] = sim_ray(v, rp, w, h);
+}
+
+// Arbitrary rays (agent observation / collision rays): origins in metres, directions of any
+// length (normalised here), first active voxel within max_range metres, else 0.
+__global__ void __launch_bounds__(256) k_sim_cast(SimMapView v, const float* origins,
+                                                  const float* dirs, long long n, float max_range,
+                                                  float* out) {
+  for (long long i = (long long)blockIdx.x * blockDim.x + threadIdx.x; i < n;
+       i += (long long)gridDim.x * blockDim.x) {
+    float r = 0.0f;
+    if (v.any) {
+      const float m0 = __ldg(&dirs[3 * i]), m1 = __ldg(&dirs[3 * i + 1]), m2 = __ldg(&dirs[3 * i + 2]);
+      const float norm = __fsqrt_rn(__fadd_rn(__fadd_rn(__fmul_rn(m0, m0), __fmul_rn(m1, m1)), __fmul_rn(m2, m2)));
+      if (norm > 0.0f && norm < INFINITY) {
+        float dir[3] = {__fdiv_rn(m0, norm), __fdiv_rn(m1, norm), __fdiv_rn(m2, norm)};
+        const float eye[3] = {__fdiv_rn(__ldg(&origins[3 * i]), v.res),
+                              __fdiv_rn(__ldg(&origins[3 * i + 1]), v.res),
+                              __fdiv_rn(__ldg(&origins[3 * i + 2]), v.res)};
+        r = sim_cast(v, eye, dir, 0.0f, __fdiv_rn(max_range, v.res));
+      }
+    }
+    out[i] = r;
+  }
 }
 
 // splitmix64 (Steele, Lea, Flood 2014) as a counter-based generator.
@@ -414,6 +445,14 @@ cudaError_t launch_fill_i32(int32_t* p, long long n, int32_t val, cudaStream_t s
 cudaError_t launch_sim_render(const SimMapView& v, const SimRayParams& rp, float* out, cudaStream_t s) {
   const dim3 grid((rp.width + 15) / 16, (rp.height + 15) / 16);
   k_sim_render<<<grid, 256, 0, s>>>(v, rp, out);
+  return cudaGetLastError();
+}
+
+cudaError_t launch_sim_cast(const SimMapView& v, const float* origins, const float* dirs,
+                            long long n, float max_range, float* out, cudaStream_t s) {
+  if (n <= 0) return cudaSuccess;
+  const long long blocks = std::min<long long>((n + 255) / 256, 148 * 16);
+  k_sim_cast<<<(unsigned)blocks, 256, 0, s>>>(v, origins, dirs, n, max_range, out);
   return cudaGetLastError();
 }
 

@@ -66,5 +66,7 @@ cudaError_t launch_sim_render(const SimMapView& v, const SimRayParams& rp, float
                               cudaStream_t s);
 cudaError_t launch_noise(float* r, long long n, float sigma_coef, float drop, uint64_t seed,
                          cudaStream_t s);
+cudaError_t launch_sim_cast(const SimMapView& v, const float* origins, const float* dirs,
+                            long long n, float max_range, float* out, cudaStream_t s);
 
 }  // namespace nm

@@ -858,14 +858,56 @@ void orc_sim_render(void* sp, const orc_sensor* sen, const float pos[3], const f
   for (auto& x : th) x.join();
 }
 
+// First active voxel entered along the ray from `eye` (index space) in the unit direction
+// `dir`, at a ray time within [tmin, tmax]: its distance in metres, or 0.  The voxel holding
+// the eye is not tested (generateCloud.cu:28-39).  Round-to-nearest float.
+static float sim_cast(const SimMap* s, const float eye[3], float dir[3], float tmin, float tmax) {
+  const float res = s->res;
+  const float lo[3] = {(float)s->amin[0], (float)s->amin[1], (float)s->amin[2]};
+  const float hi[3] = {(float)(s->amax[0] + 1), (float)(s->amax[1] + 1), (float)(s->amax[2] + 1)};
+  float inv[3];
+  int stp[3];
+  float t_in = 0.0f, t_out = INFINITY;
+  bool miss = false;
+  for (int a = 0; a < 3; ++a) {
+    if (std::fabs(dir[a]) < 1e-30f) dir[a] = 0.0f;
+    if (dir[a] == 0.0f) {
+      stp[a] = 0;
+      inv[a] = 0.0f;
+      if (eye[a] < lo[a] || eye[a] > hi[a]) miss = true;
+    } else {
+      inv[a] = 1.0f / dir[a];
+      stp[a] = dir[a] > 0.0f ? 1 : -1;
+      float ta = (lo[a] - eye[a]) * inv[a];
+      float tb = (hi[a] - eye[a]) * inv[a];
+      if (ta > tb) std::swap(ta, tb);
+      if (ta > t_in) t_in = ta;
+      if (tb < t_out) t_out = tb;
+    }
+  }
+  if (miss || t_in > t_out) return 0.0f;
+  int k[3];
+  for (int a = 0; a < 3; ++a) k[a] = (int)std::floor(eye[a] + dir[a] * t_in);
+  for (;;) {
+    float tn[3];
+    for (int a = 0; a < 3; ++a)
+      tn[a] = (stp[a] == 0) ? INFINITY
+                            : ((float)(k[a] + (stp[a] > 0 ? 1 : 0)) - eye[a]) * inv[a];
+    const int a = argmin_hi_f(tn);
+    const float t = tn[a];
+    if (!(t <= t_out)) break;
+    k[a] += stp[a];
+    if (s->active(k)) return (t >= tmin && t <= tmax) ? t * res : 0.0f;
+  }
+  return 0.0f;
+}
+
 static void sim_render_rows(const SimMap* s, const orc_sensor* sen, const float pos[3],
                             const float R[9], float* out, int h0, int h1) {
   RoundGuard g(0);
   const int W = sen->width;
   const float res = s->res;
   const float eye[3] = {pos[0] / res, pos[1] / res, pos[2] / res};
-  const float lo[3] = {(float)s->amin[0], (float)s->amin[1], (float)s->amin[2]};
-  const float hi[3] = {(float)(s->amax[0] + 1), (float)(s->amax[1] + 1), (float)(s->amax[2] + 1)};
   for (int h = h0; h < h1; ++h)
     for (int w = 0; w < W; ++w) {
       float* o = out + (size_t)h * W + w;
@@ -886,44 +928,27 @@ static void sim_render_rows(const SimMap* s, const orc_sensor* sen, const float 
         tmin = sen->min_range / res;
         tmax = sen->max_range / res;
       }
-      float inv[3];
-      int stp[3];
-      float t_in = 0.0f, t_out = INFINITY;
-      bool miss = false;
-      for (int a = 0; a < 3; ++a) {
-        if (std::fabs(dir[a]) < 1e-30f) dir[a] = 0.0f;
-        if (dir[a] == 0.0f) {
-          stp[a] = 0;
-          inv[a] = 0.0f;
-          if (eye[a] < lo[a] || eye[a] > hi[a]) miss = true;
-        } else {
-          inv[a] = 1.0f / dir[a];
-          stp[a] = dir[a] > 0.0f ? 1 : -1;
-          float ta = (lo[a] - eye[a]) * inv[a];
-          float tb = (hi[a] - eye[a]) * inv[a];
-          if (ta > tb) std::swap(ta, tb);
-          if (ta > t_in) t_in = ta;
-          if (tb < t_out) t_out = tb;
-        }
-      }
-      if (miss || t_in > t_out) continue;
-      int k[3];
-      for (int a = 0; a < 3; ++a) k[a] = (int)std::floor(eye[a] + dir[a] * t_in);
-      for (;;) {
-        float tn[3];
-        for (int a = 0; a < 3; ++a)
-          tn[a] = (stp[a] == 0) ? INFINITY
-                                : ((float)(k[a] + (stp[a] > 0 ? 1 : 0)) - eye[a]) * inv[a];
-        const int a = argmin_hi_f(tn);
-        const float t = tn[a];
-        if (!(t <= t_out)) break;
-        k[a] += stp[a];
-        if (s->active(k)) {
-          if (t >= tmin && t <= tmax) *o = t * res;
-          break;
-        }
-      }
+      *o = sim_cast(s, eye, dir, tmin, tmax);
     }
+}
+
+// Arbitrary rays (agent observation / collision rays): origins in metres, directions of any
+// length, distances to the first active voxel within max_range metres, else 0.
+void orc_sim_cast(void* sp, const float* origins, const float* dirs, int64_t n, float max_range,
+                  float* out) {
+  const SimMap* s = static_cast<const SimMap*>(sp);
+  RoundGuard g(0);
+  const float res = s->res;
+  for (int64_t i = 0; i < n; ++i) {
+    out[i] = 0.0f;
+    if (!s->any) continue;
+    const float m0 = dirs[3 * i], m1 = dirs[3 * i + 1], m2 = dirs[3 * i + 2];
+    const float norm = std::sqrt((m0 * m0 + m1 * m1) + m2 * m2);
+    if (!(norm > 0.0f && norm < INFINITY)) continue;
+    float dir[3] = {m0 / norm, m1 / norm, m2 / norm};
+    const float eye[3] = {origins[3 * i] / res, origins[3 * i + 1] / res, origins[3 * i + 2] / res};
+    out[i] = sim_cast(s, eye, dir, 0.0f, max_range / res);
+  }
 }
 
 // Analytic range image of axis-aligned boxes (world metres), FP64 slab intersections, rounded

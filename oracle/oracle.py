@@ -90,6 +90,7 @@ def lib() -> C.CDLL:
                                         C.c_int64, _PF, _PU32, C.c_int64]
         L.orc_voxel_filter.restype = C.c_int64
         L.orc_render_boxes.argtypes = [C.POINTER(OrcSensor), _PD, _PD, _PD, C.c_int, _PF]
+        L.orc_sim_cast.argtypes = [C.c_void_p, _PF, _PF, C.c_int64, C.c_float, _PF]
         L.orc_depth.argtypes = [C.POINTER(OrcSensor), _PD, _PD, C.c_double, _PI32, _PF, C.c_int64,
                                 C.c_double, C.c_double, _PI32, C.c_int64, _PD, _PD,
                                 C.POINTER(C.c_uint64), _PD, _PD]
@@ -264,6 +265,13 @@ class SimMap:
         if n:
             lib().orc_simmap_export(self.h, o.ctypes.data_as(_PI32), w.ctypes.data_as(_PU32), n)
         return o, w
+
+    def cast(self, origins, directions, max_range) -> np.ndarray:
+        o = _f(origins).reshape(-1, 3)
+        d = _f(directions).reshape(-1, 3)
+        out = np.zeros(len(o), np.float32)
+        lib().orc_sim_cast(self.h, fp(o), fp(d), len(o), C.c_float(max_range), fp(out))
+        return out
 
     def render(self, sensor: Sensor, pos, R, threads: int = 1) -> np.ndarray:
         out = np.zeros((sensor.s.height, sensor.s.width), np.float32)

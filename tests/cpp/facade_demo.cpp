@@ -1,10 +1,13 @@
 // facade_demo.cpp -- test program: drives the C++ facade the way a NanoMap user does.
 //
 // usage: facade_demo <config> <frames.bin> <manager_map.bin> <sim_map.bin> <sim_poses.bin>
+//                    [<collisions.bin>]
 //   frames.bin: int32 n, width, height, step; n poses (7 floats: x y z qw qx qy qz);
 //               n clouds of width*height records of `step` bytes (xyz at 0/4/8).
 // Writes the maps' leaves (uint64 n, then origins, log-odds, active words) and the sensor
-// poses the sim manager used (int32 count, then per view: int32 sensor index, 7 floats).
+// poses the sim manager used (int32 count, then per view: int32 sensor index, 7 floats), and
+// getAgentSimCollision for agent 0 over a 5x5x3 grid of position deltas (int32 count, then
+// per delta: 3 floats and an int32 0/1).
 #include <cstdint>
 #include <cstdio>
 #include <vector>
@@ -26,7 +29,7 @@ static void dump(nanomap::map::Map& m, const char* path) {
 }
 
 int main(int argc, char** argv) {
-  if (argc != 6) return 2;
+  if (argc != 6 && argc != 7) return 2;
   try {
     auto cfg = std::make_shared<nanomap::config::Config>(argv[1]);
     FILE* f = std::fopen(argv[2], "rb");
@@ -83,6 +86,20 @@ int main(int argc, char** argv) {
       std::fwrite(p.orientation, 4, 4, g);
     }
     std::fclose(g);
+    if (argc == 7) {
+      FILE* c = std::fopen(argv[6], "wb");
+      const int32_t nd = 5 * 5 * 3;
+      std::fwrite(&nd, 4, 1, c);
+      for (int i = 0; i < 5; ++i)
+        for (int j = 0; j < 5; ++j)
+          for (int k = 0; k < 3; ++k) {
+            const nanomap::Vector3f d(-2.0f + 1.0f * i, -2.0f + 1.0f * j, -0.5f + 0.5f * k);
+            const int32_t free_ = sim.getAgentSimCollision(0, d) ? 1 : 0;
+            std::fwrite(d.v, 4, 3, c);
+            std::fwrite(&free_, 4, 1, c);
+          }
+      std::fclose(c);
+    }
   } catch (const nanomap::Error& e) {
     std::fprintf(stderr, "%s\n", e.what());
     return 1;

@@ -60,7 +60,8 @@ def test_facade_matches_direct_abi(ctx, tmp_path):
                     f"-L{ROOT / 'nanomap_b200'}", "-lnanomap_b200", f"-Wl,-rpath,{ROOT / 'nanomap_b200'}",
                     "-o", str(exe)], check=True)
     out = subprocess.run([str(exe), str(cfg_dir / "config.txt"), str(fb), str(tmp_path / "mgr.bin"),
-                          str(tmp_path / "sim.bin"), str(tmp_path / "poses.bin")],
+                          str(tmp_path / "sim.bin"), str(tmp_path / "poses.bin"),
+                          str(tmp_path / "collisions.bin")],
                          capture_output=True, text=True)
     assert out.returncode == 0, out.stderr
     assert "gpu update time per loop:" in out.stdout
@@ -102,6 +103,22 @@ def test_facade_matches_direct_abi(ctx, tmp_path):
     errs = compare_maps(_read_map(tmp_path / "sim.bin"), simmap.export())
     assert not errs, "; ".join(errs[:5])
     assert simmap.stats()["rays"] > 0
+
+    # getAgentSimCollision (SimManager.h:141-168): the agent file's 80 observation rays and
+    # 0.5 m collision distance, cast from the moved agent position plus each delta
+    moved = np.array(struct.unpack_from("<3f", b, 8 + 32 * (cnt - 1)), np.float32)
+    c = (tmp_path / "collisions.bin").read_bytes()
+    nd = struct.unpack_from("<i", c, 0)[0]
+    rays = A.observation_sphere(80)
+    outcomes = []
+    for i in range(nd):
+        d = np.array(struct.unpack_from("<3f", c, 4 + 16 * i), np.float32)
+        got = struct.unpack_from("<i", c, 16 + 16 * i)[0]
+        dist = sim_file.cast_rays(np.tile(moved + d, (80, 1)), rays, 0.5)
+        expect = 0 if ((dist > 0) & (dist < 0.5)).any() else 1
+        assert got == expect, (d, got, dist[dist > 0])
+        outcomes.append(got)
+    assert nd == 75
 
 
 def test_vdb_sim_grid_is_refused(ctx, tmp_path):

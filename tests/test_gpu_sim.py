@@ -123,3 +123,51 @@ def test_noise_is_seeded(ctx):
     assert 0.01 < dropped < 0.03
     kept = a[a > 0] - 3.0
     assert abs(float(kept.std()) - 0.005 * 9.0) < 0.005
+
+
+def test_ray_casts_match_oracle(ctx):
+    """Agent observation / collision rays (SimManager.h:141-168): arbitrary origins and
+    directions against the sim map, first active voxel within range, bit-identical."""
+    sc, g, o = _maps(ctx, "plain_small")
+    rng = np.random.default_rng(21)
+    n_pos = 40
+    pos = np.stack([rng.uniform(0.5, 19.5, n_pos), rng.uniform(0.5, 19.5, n_pos),
+                    rng.uniform(0.3, 4.7, n_pos)], axis=1).astype(np.float32)
+    sphere = A.observation_sphere(64)
+    origins = np.repeat(pos, 64, axis=0)
+    dirs = np.tile(sphere, (n_pos, 1))
+    extra = rng.normal(size=(2000, 3)).astype(np.float32) * rng.uniform(0.1, 3.0, (2000, 1)).astype(np.float32)
+    extra[::97] = 0.0  # zero-length directions give no hit
+    extra[5::101, 0] = 0.0  # axis-parallel components
+    origins = np.concatenate([origins, np.repeat(pos[:1], 2000, axis=0)])
+    dirs = np.concatenate([dirs, extra]).astype(np.float32)
+    for max_range in (0.5, 5.0, 50.0):
+        gd = g.cast_rays(origins, dirs, max_range)
+        od = o.cast(origins, dirs, max_range)
+        assert np.array_equal(gd.view(np.uint32), od.view(np.uint32)), int((gd != od).sum())
+        assert (gd <= max_range).all()
+    assert (gd > 0).mean() > 0.3  # at 50 m many rays meet a box (the world has no walls)
+    import torch
+    td = g.cast_rays(torch.from_numpy(origins).cuda(), torch.from_numpy(dirs).cuda(), 5.0)
+    assert np.array_equal(td.cpu().numpy().view(np.uint32), g.cast_rays(origins, dirs, 5.0).view(np.uint32))
+
+
+def test_ray_cast_agrees_with_pixel_render(ctx):
+    """A laser pixel's ray cast as an arbitrary ray gives the rendered range (laser pixels have
+    unit directions, so the range limits agree)."""
+    import torch
+    sc, g, o = _maps(ctx, "plain_small")
+    desc = A.sensor_desc(type=1, hres=64, vres=16, hfov_deg=360.0, vfov_deg=30.0, max_range=8.0,
+                         frame_transform=S.OPTICAL_TO_BODY)
+    sensor = A.Sensor(ctx, desc)
+    pose = A.Pose((10.0, 10.0, 1.5), S.yaw_quaternion(0.3))
+    r = torch.zeros((16, 64), device="cuda")
+    g.render(sensor, pose, r)
+    osen = O.Sensor.from_desc(desc)
+    R = O.rotation(pose.orientation, list(desc.frame_transform))
+    d_s = osen.points(np.ones((16, 64), np.float32))  # unit-range points = pixel directions
+    d_w = (R.reshape(3, 3) @ d_s.T).T.astype(np.float32)
+    cast = g.cast_rays(np.tile(np.float32(pose.position), (len(d_w), 1)), d_w, 8.0)
+    rr = r.cpu().numpy().reshape(-1)
+    close = np.isclose(cast, rr, rtol=1e-5, atol=1e-5)
+    assert close.mean() > 0.99, close.mean()
