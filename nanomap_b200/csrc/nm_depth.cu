@@ -63,16 +63,29 @@ __device__ __forceinline__ float softplus(float x) {
   return x > 0.0f ? x + log1pf(expf(-x)) : log1pf(expf(x));
 }
 
-// (1 - exp(-sigma D)) / sigma: the segment's transmittance integral per unit entry transmittance.
-__device__ __forceinline__ float seg_integral(float sigma, float D) {
-  return sigma > 0.0f ? -expm1f(-sigma * D) / sigma : D;
+// g(u) = (u e^-u - 1 + e^-u) / u^2 given em1 = e^-u - 1; -1/2 at u = 0.
+__device__ __forceinline__ float seg_g(float u, float em1) {
+  if (u < 1e-2f) return -0.5f + u * (1.0f / 3.0f) - u * u * 0.125f;
+  return (u * (1.0f + em1) + em1) / (u * u);
 }
 
-// g(u) = (u e^-u - 1 + e^-u) / u^2, -1/2 at u = 0.
-__device__ __forceinline__ float seg_g(float u) {
-  if (u < 1e-2f) return -0.5f + u * (1.0f / 3.0f) - u * u * 0.125f;
-  return (u * expf(-u) + expm1f(-u)) / (u * u);
-}
+// Density of a log-odds value, memoised on the last value seen: along a ray most voxels share
+// a few values (the clamp of observed free space, 0 for unknown space), so the softplus and
+// sigmoid are mostly reused and each visit costs one expm1.
+struct DensityCache {
+  bool has = false;
+  float L = 0.0f;
+  float sg = 0.0f, sig = 0.5f;
+  __device__ __forceinline__ void at(const DepthParams& p, float l) {
+    if (!has || l != L) {
+      has = true;
+      L = l;
+      const float x = p.scale * l + p.bias;
+      sg = softplus(x);
+      sig = 1.0f / (1.0f + expf(-x));
+    }
+  }
+};
 
 // Visits every voxel of the ray after the start voxel: f(v, t_in, a_in, t_out, a_out), the
 // voxel entered at t_in < t_max across axis a_in and left at t_out = min(next crossing,
@@ -152,6 +165,7 @@ __device__ __forceinline__ float expected_index_depth(const DepthParams& p, cons
                                                       const float* vals, const double d[3],
                                                       float* t1_out, uint32_t* visits) {
   LeafCache c{kEmptyKey, -1};
+  DensityCache dc;
   float T = 1.0f, acc = 0.0f;
   double t1 = p.t_max;
   bool first = true;
@@ -159,15 +173,16 @@ __device__ __forceinline__ float expected_index_depth(const DepthParams& p, cons
   walk(p.eye, d, p.t_max, [&](const int v[3], double t_in, int, double t_out, int) {
     ++n;
     int slot, l;
-    const float L = voxel_logodds(m, vals, c, v, &slot, &l);
-    const float sg = softplus(p.scale * L + p.bias);
+    dc.at(p, voxel_logodds(m, vals, c, v, &slot, &l));
+    const float sg = dc.sg;
     const float Dk = (float)(t_out - t_in);
     if (first) {
       t1 = t_in;
       first = false;
     }
-    acc += T * seg_integral(sg, Dk);
-    T *= expf(-sg * Dk);
+    const float em1 = expm1f(-sg * Dk);
+    acc += T * (sg > 0.0f ? -em1 / sg : Dk);
+    T *= 1.0f + em1;
   });
   *t1_out = (float)t1;
   *visits += n;
@@ -181,6 +196,7 @@ __device__ __forceinline__ void replay_gradients(const DepthParams& p, const Map
                                                  float t1, float gd, float* grad_vals,
                                                  float g6[6], uint32_t* visits) {
   LeafCache c{kEmptyKey, -1};
+  DensityCache dc;
   uint32_t n = 0;
   float T = 1.0f, P = 0.0f, sg_prev = 0.0f;
   float ge[3] = {0.f, 0.f, 0.f}, gdir[3] = {0.f, 0.f, 0.f};
@@ -189,10 +205,9 @@ __device__ __forceinline__ void replay_gradients(const DepthParams& p, const Map
   const float tail0 = D - t1;
   walk(p.eye, d, p.t_max, [&](const int v[3], double t_in, int a_in, double t_out, int) {
     int slot, l;
-    const float L = voxel_logodds(m, vals, c, v, &slot, &l);
+    dc.at(p, voxel_logodds(m, vals, c, v, &slot, &l));
     ++n;
-    const float x = p.scale * L + p.bias;
-    const float sg = softplus(x);
+    const float sg = dc.sg;
     const float Dk = (float)(t_out - t_in);
     // entry crossing: the density steps from sg_prev to sg
     const float gc = (sg - sg_prev) * (tail0 - P) * (a_in == 0 ? inv_d[0] : (a_in == 1 ? inv_d[1] : inv_d[2]));
@@ -207,14 +222,15 @@ __device__ __forceinline__ void replay_gradients(const DepthParams& p, const Map
       ge[2] -= gc;
       gdir[2] -= gc * ti;
     }
-    const float Pn = P + T * seg_integral(sg, Dk);
+    const float u = sg * Dk;
+    const float em1 = expm1f(-u);
+    const float Pn = P + T * (sg > 0.0f ? -em1 / sg : Dk);
     if (grad_vals && slot >= 0) {
-      const float sig = 1.0f / (1.0f + expf(-x));
-      const float dsig = T * Dk * Dk * seg_g(sg * Dk) - Dk * (tail0 - Pn);
-      atomicAdd(&grad_vals[(size_t)slot * kLeafVoxels + l], gv * sig * dsig);
+      const float dsig = T * Dk * Dk * seg_g(u, em1) - Dk * (tail0 - Pn);
+      atomicAdd(&grad_vals[(size_t)slot * kLeafVoxels + l], gv * dc.sig * dsig);
     }
     P = Pn;
-    T *= expf(-sg * Dk);
+    T *= 1.0f + em1;
     sg_prev = sg;
   });
   *visits += n;
