@@ -13,9 +13,9 @@
 // Labels collect in a per-CTA shared-memory leaf table (hashed, 32 label words per leaf);
 // a leaf that finds no room goes straight to the device table.  After a tile, one warp per
 // cached leaf ORs its words into the device label buffer and puts the leaf on the touched
-// list.  Per step the walk compares the three crossing times as integers (they are never
-// negative), keeps the voxel as (leaf, local) coordinates, and probes the leaf table only
-// when the step leaves the current leaf.
+// list.  Per step the walk compares the three crossing times (non-negative doubles, one
+// compare per pair), keeps the voxel as (leaf, local) coordinates, and probes the leaf table
+// only when the step leaves the current leaf.
 #include <cfloat>
 #include <cstdint>
 
@@ -97,7 +97,7 @@ __device__ __forceinline__ bool setup_ray(const FrameParams& f, const float p[3]
         tn[a] = A::dmul(A::dadd((double)v[a], -f.eye[a]), inv);
         dl[a] = -inv;
       }
-      if (tn[a] == 0.0) tn[a] = 0.0;  // -0 -> +0 so the integer order matches the double order
+      if (tn[a] == 0.0) tn[a] = 0.0;  // canonical +0
     }
   }
   r.t0 = tn[0];
@@ -232,12 +232,11 @@ __device__ __forceinline__ void traverse_body(const TickWork<MaxF>& work, const 
         }
         continue;
       }
-      const long long i0 = __double_as_longlong(r.t0);
-      const long long i1 = __double_as_longlong(r.t1);
-      const long long i2 = __double_as_longlong(r.t2);
-      const int a = (i0 < i1) ? ((i0 < i2) ? 0 : 2) : ((i1 < i2) ? 1 : 2);
+      // crossing times are non-negative and never NaN (disabled axes hold DBL_MAX): one
+      // double compare per pair; ties go to the higher axis
+      const int a = (r.t0 < r.t1) ? ((r.t0 < r.t2) ? 0 : 2) : ((r.t1 < r.t2) ? 1 : 2);
       const double t = (a == 0) ? r.t0 : ((a == 1) ? r.t1 : r.t2);
-      if (!(__double_as_longlong(t) <= __double_as_longlong(r.len))) {
+      if (!(t <= r.len)) {
         if (t < (double)f.max_time) {
           label(kKindHit);
           visits += 1;
