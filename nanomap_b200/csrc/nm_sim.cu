@@ -258,15 +258,61 @@ __device__ __forceinline__ float sim_cast(const SimMapView& v, const float eye[3
     for (int iter = 0; iter < (1 << 22); ++iter) {
       int leaf = -1;
       const int lvl = sim_level(v, k[0], k[1], k[2], &leaf);
-      if (lvl == 0 && !first) {
-        const int l = ((k[0] & 7) << 6) | ((k[1] & 7) << 3) | (k[2] & 7);
-        if ((__ldg(&v.leaf_words[(size_t)leaf * 16 + (l >> 5)]) >> (l & 31)) & 1u) {
+      if (lvl == 0) {
+        // Voxel steps inside a leaf with active voxels: the leaf's words come from L1, and
+        // only the stepped axis's next crossing changes (each crossing is the closed form of
+        // its own plane, so the event sequence is the one the generic step takes).
+        const uint32_t* lw = v.leaf_words + (size_t)leaf * 16;
+        int k0 = k[0], k1 = k[1], k2 = k[2];
+        const int b0 = k0 & ~7, b1 = k1 & ~7, b2 = k2 & ~7;
+        float T0 = st[0] == 0 ? INFINITY : plane_time(st[0] > 0 ? k0 + 1 : k0, eye[0], inv[0]);
+        float T1 = st[1] == 0 ? INFINITY : plane_time(st[1] > 0 ? k1 + 1 : k1, eye[1], inv[1]);
+        float T2 = st[2] == 0 ? INFINITY : plane_time(st[2] > 0 ? k2 + 1 : k2, eye[2], inv[2]);
+        bool hit = false, done = false;
+        for (int it2 = 0; it2 < 24; ++it2) {
+          if (!first) {
+            const int l = ((k0 & 7) << 6) | ((k1 & 7) << 3) | (k2 & 7);
+            if ((__ldg(&lw[l >> 5]) >> (l & 31)) & 1u) {
+              hit = true;
+              break;
+            }
+          }
+          first = false;
+          const int ax = (T0 < T1) ? ((T0 < T2) ? 0 : 2) : ((T1 < T2) ? 1 : 2);
+          const float Tx = ax == 0 ? T0 : (ax == 1 ? T1 : T2);
+          if (!(Tx <= t_out)) {
+            done = true;
+            break;
+          }
+          t = Tx;
+          bool left;
+          if (ax == 0) {
+            k0 += st[0];
+            left = (k0 & ~7) != b0;
+            T0 = plane_time(st[0] > 0 ? k0 + 1 : k0, eye[0], inv[0]);
+          } else if (ax == 1) {
+            k1 += st[1];
+            left = (k1 & ~7) != b1;
+            T1 = plane_time(st[1] > 0 ? k1 + 1 : k1, eye[1], inv[1]);
+          } else {
+            k2 += st[2];
+            left = (k2 & ~7) != b2;
+            T2 = plane_time(st[2] > 0 ? k2 + 1 : k2, eye[2], inv[2]);
+          }
+          if (left) break;
+        }
+        k[0] = k0;
+        k[1] = k1;
+        k[2] = k2;
+        if (hit) {
           if (t >= tmin && t <= tmax) result = __fmul_rn(t, v.res);
           break;
         }
+        if (done) break;
+        continue;  // left the leaf: the outer walk takes the next level
       }
       first = false;
-      const int S = lvl == 2 ? 64 : (lvl == 1 ? 8 : 1);
+      const int S = lvl == 2 ? 64 : 8;
       int far[3];
       float T[3];
 #pragma unroll
