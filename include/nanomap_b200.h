@@ -365,6 +365,13 @@ int nm_simmap_export(nm_simmap sm, int32_t* origins, uint32_t* words, uint64_t m
 int nm_sim_render(nm_simmap sm, nm_sensor s, const nm_pose* pose, float* ranges,
                   uint32_t flags, void* stream);
 
+/* nm_sim_render and nm_ranges_add_noise in one launch (same ranges bit for bit): the range
+ * noise of the simulated sensors, sigma = sigma_coef * r^2 and drop probability drop_prob,
+ * counter-based per pixel from `seed`. */
+int nm_sim_render_noisy(nm_simmap sm, nm_sensor s, const nm_pose* pose, float* ranges,
+                        float sigma_coef, float drop_prob, uint64_t seed, uint32_t flags,
+                        void* stream);
+
 /* Ray casts against the sim map for agent observation and collision rays
  * (SimManager::getAgentSimCollision, SimManager.h:141-168): n rays from `origins` (metres,
  * 3 floats each) along `directions` (3 floats each, any length, normalised here); distances

@@ -447,6 +447,15 @@ class SimMap:
             flags |= N.NM_OUTPUT_HOST
         call("nm_sim_render", self.h, sensor.h, C.byref(pose.c()), p, flags, _stream(stream))
 
+    def render_noisy(self, sensor: Sensor, pose: Pose, out, sigma_coef: float, drop: float,
+                     seed: int, flags: int = 0, stream=None):
+        """render() with the range noise of Context.add_noise applied in the same launch."""
+        p, host = _ptr(out)
+        if host:
+            flags |= N.NM_OUTPUT_HOST
+        call("nm_sim_render_noisy", self.h, sensor.h, C.byref(pose.c()), p, sigma_coef, drop,
+             C.c_uint64(seed), flags, _stream(stream))
+
     def cast_rays(self, origins, directions, max_range: float, stream=None):
         """Distances (metres) to the first active voxel along each ray within max_range, 0 when
         none.  numpy inputs give a numpy result; CUDA tensors give a CUDA tensor."""

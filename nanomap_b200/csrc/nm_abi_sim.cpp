@@ -146,6 +146,51 @@ void release(nm_simmap sm) {
 }
 }  // namespace nm
 
+namespace {
+// Shared body of the two render entry points; noise (sigma coefficient, drop probability,
+// seed) is applied in the render kernel when `noise` is given.
+int render_impl(nm_simmap sm, nm_sensor s, const nm_pose* pose, float* ranges, uint32_t flags,
+                void* stream, const float* noise, uint64_t seed) {
+  if (!sm || !s || !pose || !ranges) return fail(NM_ERR_ARG, "null argument");
+  if (s->ctx != sm->ctx) return fail(NM_ERR_ARG, "sensor and sim map belong to different contexts");
+  for (int a = 0; a < 3; ++a)
+    if (!std::isfinite(pose->position[a])) return fail(NM_ERR_ARG, "pose position is not finite");
+  double qn = 0;
+  for (int a = 0; a < 4; ++a) qn += (double)pose->orientation[a] * pose->orientation[a];
+  if (!(qn > 1e-20) || !std::isfinite(qn)) return fail(NM_ERR_ARG, "orientation quaternion invalid");
+  if (noise && !(std::isfinite(noise[0]) && noise[1] >= 0.0f && noise[1] <= 1.0f))
+    return fail(NM_ERR_ARG, "noise parameters invalid");
+  nm_context ctx = sm->ctx;
+  NM_CUDA(cudaSetDevice(ctx->device));
+  cudaStream_t st = nm::pick(ctx, stream);
+  nm::SimRayParams rp;
+  nm::make_ray_params(s, *pose, &rp);
+  const size_t bytes = (size_t)rp.width * rp.height * 4;
+  float* dst = ranges;
+  if (flags & NM_OUTPUT_HOST) {
+    if (bytes > ctx->render_staging_bytes) {
+      cudaFree(ctx->render_staging);
+      ctx->render_staging = nullptr;
+      ctx->render_staging_bytes = 0;
+      NM_CUDA(cudaMalloc((void**)&ctx->render_staging, bytes));
+      ctx->render_staging_bytes = bytes;
+    }
+    dst = ctx->render_staging;
+  }
+  if (noise)
+    NM_CUDA(nm::launch_sim_render_noisy(sm->view, rp, dst, noise[0], noise[1], seed, st));
+  else
+    NM_CUDA(nm::launch_sim_render(sm->view, rp, dst, st));
+  if (flags & NM_OUTPUT_HOST) {
+    NM_CUDA(cudaMemcpyAsync(ranges, dst, bytes, cudaMemcpyDeviceToHost, st));
+    NM_CUDA(cudaStreamSynchronize(st));
+  } else if (flags & NM_SYNC) {
+    NM_CUDA(cudaStreamSynchronize(st));
+  }
+  return NM_OK;
+}
+}  // namespace
+
 extern "C" {
 
 int nm_simmap_create_primitives(nm_context ctx, float res, const int32_t vox_min[3],
@@ -293,40 +338,17 @@ int nm_simmap_export(nm_simmap sm, int32_t* origins, uint32_t* words, uint64_t m
   return NM_OK;
 }
 
+
 int nm_sim_render(nm_simmap sm, nm_sensor s, const nm_pose* pose, float* ranges, uint32_t flags,
                   void* stream) {
-  if (!sm || !s || !pose || !ranges) return fail(NM_ERR_ARG, "null argument");
-  if (s->ctx != sm->ctx) return fail(NM_ERR_ARG, "sensor and sim map belong to different contexts");
-  for (int a = 0; a < 3; ++a)
-    if (!std::isfinite(pose->position[a])) return fail(NM_ERR_ARG, "pose position is not finite");
-  double qn = 0;
-  for (int a = 0; a < 4; ++a) qn += (double)pose->orientation[a] * pose->orientation[a];
-  if (!(qn > 1e-20) || !std::isfinite(qn)) return fail(NM_ERR_ARG, "orientation quaternion invalid");
-  nm_context ctx = sm->ctx;
-  NM_CUDA(cudaSetDevice(ctx->device));
-  cudaStream_t st = pick(ctx, stream);
-  nm::SimRayParams rp;
-  nm::make_ray_params(s, *pose, &rp);
-  const size_t bytes = (size_t)rp.width * rp.height * 4;
-  float* dst = ranges;
-  if (flags & NM_OUTPUT_HOST) {
-    if (bytes > ctx->render_staging_bytes) {
-      cudaFree(ctx->render_staging);
-      ctx->render_staging = nullptr;
-      ctx->render_staging_bytes = 0;
-      NM_CUDA(cudaMalloc((void**)&ctx->render_staging, bytes));
-      ctx->render_staging_bytes = bytes;
-    }
-    dst = ctx->render_staging;
-  }
-  NM_CUDA(nm::launch_sim_render(sm->view, rp, dst, st));
-  if (flags & NM_OUTPUT_HOST) {
-    NM_CUDA(cudaMemcpyAsync(ranges, dst, bytes, cudaMemcpyDeviceToHost, st));
-    NM_CUDA(cudaStreamSynchronize(st));
-  } else if (flags & NM_SYNC) {
-    NM_CUDA(cudaStreamSynchronize(st));
-  }
-  return NM_OK;
+  return render_impl(sm, s, pose, ranges, flags, stream, nullptr, 0);
+}
+
+int nm_sim_render_noisy(nm_simmap sm, nm_sensor s, const nm_pose* pose, float* ranges,
+                        float sigma_coef, float drop_prob, uint64_t seed, uint32_t flags,
+                        void* stream) {
+  const float noise[2] = {sigma_coef, drop_prob};
+  return render_impl(sm, s, pose, ranges, flags, stream, noise, seed);
 }
 
 int nm_sim_cast_rays(nm_simmap sm, const float* origins, const float* directions, int64_t n,

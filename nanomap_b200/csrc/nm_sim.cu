@@ -435,6 +435,17 @@ __global__ void k_noise(float* r, long long n, float sigma_coef, float drop, uin
     r[i] = noisy(r[i], seed, i, sigma_coef, drop);
 }
 
+// Render and range noise in one pass: the same ranges as k_sim_render followed by k_noise.
+__global__ void __launch_bounds__(256) k_sim_render_noisy(SimMapView v, SimRayParams rp, float* out,
+                                                          float sigma_coef, float drop,
+                                                          uint64_t seed) {
+  const int w = blockIdx.x * 16 + (threadIdx.x & 15);
+  const int h = blockIdx.y * 16 + (threadIdx.x >> 4);
+  if (w >= rp.width || h >= rp.height) return;
+  const long long i = (long long)h * rp.width + w;
+  out[i] = noisy(sim_ray(v, rp, w, h), seed, i, sigma_coef, drop);
+}
+
 // All slots of a tick plan in one launch: one CTA per 16x16 tile of some slot.
 __global__ void __launch_bounds__(256) k_sim_render_batch(const RenderBatch* b, SimMapView v) {
   __shared__ SimRayParams s_rp;
@@ -485,6 +496,13 @@ cudaError_t launch_compact(const SimBuild& b, const SimMapView& v, uint32_t* d_c
 
 cudaError_t launch_fill_i32(int32_t* p, long long n, int32_t val, cudaStream_t s) {
   k_fill_i32<<<1184, 256, 0, s>>>(p, n, val);
+  return cudaGetLastError();
+}
+
+cudaError_t launch_sim_render_noisy(const SimMapView& v, const SimRayParams& rp, float* out,
+                                    float sigma_coef, float drop, uint64_t seed, cudaStream_t s) {
+  const dim3 grid((rp.width + 15) / 16, (rp.height + 15) / 16);
+  k_sim_render_noisy<<<grid, 256, 0, s>>>(v, rp, out, sigma_coef, drop, seed);
   return cudaGetLastError();
 }
 

@@ -62,6 +62,8 @@ cudaError_t launch_set_voxels(const SimBuild& b, const int32_t* d_ijk, long long
 cudaError_t launch_compact(const SimBuild& b, const SimMapView& v, uint32_t* d_count, int pass2,
                            int32_t* d_bbox, unsigned long long* d_nvox, cudaStream_t s);
 cudaError_t launch_fill_i32(int32_t* p, long long n, int32_t val, cudaStream_t s);
+cudaError_t launch_sim_render_noisy(const SimMapView& v, const SimRayParams& rp, float* out,
+                                    float sigma_coef, float drop, uint64_t seed, cudaStream_t s);
 cudaError_t launch_sim_render(const SimMapView& v, const SimRayParams& rp, float* out,
                               cudaStream_t s);
 cudaError_t launch_noise(float* r, long long n, float sigma_coef, float drop, uint64_t seed,

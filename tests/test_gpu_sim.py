@@ -171,3 +171,21 @@ def test_ray_cast_agrees_with_pixel_render(ctx):
     rr = r.cpu().numpy().reshape(-1)
     close = np.isclose(cast, rr, rtol=1e-5, atol=1e-5)
     assert close.mean() > 0.99, close.mean()
+
+
+def test_render_noisy_equals_render_then_noise(ctx):
+    """nm_sim_render_noisy is nm_sim_render followed by nm_ranges_add_noise, bit for bit."""
+    import torch
+    sc, g, o = _maps(ctx, "sim_headline")
+    spec = sc.spec
+    desc = camera_desc(spec)
+    sensor = A.Sensor(ctx, desc)
+    for k, (p, q) in enumerate(S.trajectory(sc, 3, seed=7)):
+        pose = A.Pose(p, q)
+        a = torch.zeros((spec.height, spec.width), device="cuda")
+        b = torch.zeros_like(a)
+        g.render(sensor, pose, a)
+        ctx.add_noise(a, spec.noise_coef, spec.drop, 77 + k)
+        g.render_noisy(sensor, pose, b, spec.noise_coef, spec.drop, 77 + k)
+        assert torch.equal(a.view(torch.int32), b.view(torch.int32))
+        assert (b == 0).float().mean() > spec.drop * 0.5
