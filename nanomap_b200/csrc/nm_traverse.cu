@@ -265,21 +265,26 @@ __device__ __forceinline__ void traverse_body(const TickWork<MaxF>& work, const 
     }
     __syncthreads();
 
-    // Flush the tile's leaf table: one warp per cached leaf, lane i carries word i.
-    for (int e = warp; e < nent; e += nwarps) {
+    // Flush the tile's leaf table: one lane per cached leaf, so the device-table lookups of
+    // up to 32 leaves overlap; word reads are rotated by lane to avoid bank conflicts.
+    for (int e = tid; e < nent; e += blockDim.x) {
       const unsigned long long key = s_keys[e];
       if (key == kEmptyKey) continue;
-      const uint32_t word = s_words[e * kLabelWords + lane];
-      if (__ballot_sync(kFull, word != 0u) == 0u) continue;
-      int g = -1;
-      if (lane == 0) {
-        g = map_find_or_insert(m, key);
-        if (g >= 0) mark_touched(m, g, f.epoch, plane);
-      }
-      g = __shfl_sync(kFull, g, 0);
+      const uint32_t* sw = s_words + e * kLabelWords;
+      bool has = false;
+#pragma unroll 4
+      for (int w = 0; w < kLabelWords; ++w) has |= sw[(w + lane) & (kLabelWords - 1)] != 0u;
+      if (!has) continue;
+      const int g = map_find_or_insert(m, key);
       if (g < 0) continue;
-      if (word)
-        atomicOr(&m.labels[((size_t)plane * m.capacity + (size_t)g) * kLabelWords + lane], word);
+      mark_touched(m, g, f.epoch, plane);
+      uint32_t* dst = &m.labels[((size_t)plane * m.capacity + (size_t)g) * kLabelWords];
+#pragma unroll 4
+      for (int w = 0; w < kLabelWords; ++w) {
+        const int wr = (w + lane) & (kLabelWords - 1);
+        const uint32_t word = sw[wr];
+        if (word) atomicOr(&dst[wr], word);
+      }
     }
     __syncthreads();
   }
