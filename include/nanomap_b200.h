@@ -391,6 +391,65 @@ int nm_observation_sphere(int32_t n, float* directions);
 int nm_ranges_add_noise(nm_context ctx, float* ranges, int64_t n, float sigma_coef,
                         float drop_prob, uint64_t seed, void* stream);
 
+/* ---- procedural cave generator (replaces nanomap::mapgen::CaveGen, CaveGen.h:32-68) ----
+ * The cave lives on a lattice of cells 8 voxels apart (CaveGen's LEAF_SIZE): with
+ * D = ceil(ceil(map_size / grid_res) / 2) voxels per half axis, cell (i, j, k) sits at voxel
+ * (-Dx + 8 + 8i, -Dy + 8 + 8j, -Dz + 8k) for k < nz, plus one ceiling plane k = nz at
+ * z = +Dz (setFloorAndCeil).  Each cell stands for the 8^3-voxel leaf that holds it. */
+typedef struct nm_cave_s* nm_cave;
+
+/* #cavegenconfig file (CaveGen::loadConfig, CaveGen.cpp:358-401). */
+typedef struct {
+  double map_size[3];      /* map_size (m) */
+  double grid_res;         /* grid_res (m) */
+  int32_t fill_percentage; /* fill_percentage: a cell starts on when rand() % 100 is below it */
+  int32_t smoothing_count; /* smoothing_count */
+  int32_t active_max;      /* active <max> <min>: on when more than max of the neighbours are */
+  int32_t active_min;      /* on, off when fewer than min are, unchanged otherwise */
+  int32_t time_seed;       /* random_seed 1: seeded from the clock */
+  uint32_t seed;           /* the value given to srand: std::hash of the seed string, or of
+                              the time, truncated to 32 bits as CaveGen's int _seed does */
+  char file_out[256];      /* file_out */
+} nm_cave_desc;
+
+#define NM_CAVE_2D 0x1u          /* columns: populateMap2D / smoothMapXY */
+#define NM_CAVE_COUNTER_RNG 0x2u /* fill from a counter-based generator on the device instead
+                                    of the C library's srand/rand sequence on the host */
+
+int nm_cave_config_load(const char* path, nm_cave_desc* out);
+int nm_cave_create(nm_context ctx, const nm_cave_desc* desc, nm_cave* out);
+int nm_cave_destroy(nm_cave c);
+/* half sizes D (voxels) and lattice size (cells along x, y; z planes below the ceiling) */
+int nm_cave_dims(nm_cave c, int32_t half[3], int32_t cells[3]);
+/* CaveGen::populateMap (CaveGen.cpp:13-47), or populateMap2D (:49-84) with NM_CAVE_2D: the
+ * cells are cleared and filled again. */
+int nm_cave_populate(nm_cave c, uint32_t flags);
+/* smoothing_count steps of CaveGen::smoothMap (:95-129: 26 neighbours), or smoothMapXY
+ * (:130-176: 8 neighbours in the floor plane, written to whole columns) with NM_CAVE_2D. */
+int nm_cave_smooth(nm_cave c, uint32_t flags);
+/* CaveGen::setFloorAndCeil (:86-94). */
+int nm_cave_floor_ceil(nm_cave c);
+/* CaveGen::getRegions (:178-240): 6-connected regions of on cells; their number and the
+ * size of the largest (either pointer may be NULL). */
+int nm_cave_regions(nm_cave c, int64_t* n_regions, int64_t* largest);
+/* CaveGen::keepLargestRegion (:242-252): only the largest region stays on; ties go to the
+ * region met first in OpenVDB's value order, as in the reference. */
+int nm_cave_keep_largest(nm_cave c);
+/* on cells as voxel coordinates (3 ints each, host), in OpenVDB value order */
+int nm_cave_cells(nm_cave c, int32_t* xyz, int64_t max_cells, int64_t* n);
+/* The cave as a sim map.  shell = 0: every voxel of the on cells' leaves (CaveGen::Save,
+ * :326-335); shell = 1: the narrow band of tools::topologyToLevelSet as invertAndSave calls
+ * it (:294-324): with the leaves' voxels T and face-neighbour morphology,
+ * M = erode^closing(dilate^closing(T)) and the active band is
+ * dilate^half_width(M) minus erode^half_width(M) (half_width 3, closing 1 in the reference). */
+int nm_cave_simmap(nm_cave c, int32_t shell, int32_t half_width, int32_t closing,
+                   nm_simmap* out);
+/* nm_cave_simmap written as an NMSIMv1 voxel list (the format nm_simmap_load reads) in
+ * place of the reference's .vdb file; a path ending in ".vdb" is written with ".nmsim"
+ * instead, and the name written is copied to written_path (may be NULL, 512 bytes). */
+int nm_cave_save(nm_cave c, int32_t shell, int32_t half_width, int32_t closing,
+                 const char* path, char* written_path);
+
 #ifdef __cplusplus
 }
 #endif

@@ -37,6 +37,8 @@ NM_SYNC = 0x4
 NM_OUTPUT_HOST = 0x8
 NM_FILTER_MEAN = 0x10
 NM_FILTER_CENTRE = 0x20
+NM_CAVE_2D = 0x1
+NM_CAVE_COUNTER_RNG = 0x2
 
 
 class NanomapError(RuntimeError):
@@ -104,6 +106,14 @@ class NmAgentInfo(C.Structure):
 
 class NmRayPose(C.Structure):
     _fields_ = [("position", C.c_double * 3), ("rotation", C.c_double * 9)]
+
+
+class NmCaveDesc(C.Structure):
+    _fields_ = [
+        ("map_size", C.c_double * 3), ("grid_res", C.c_double), ("fill_percentage", C.c_int32),
+        ("smoothing_count", C.c_int32), ("active_max", C.c_int32), ("active_min", C.c_int32),
+        ("time_seed", C.c_int32), ("seed", C.c_uint32), ("file_out", C.c_char * 256),
+    ]
 
 
 class NmFrame(C.Structure):
@@ -186,6 +196,18 @@ _SIGS = {
     "nm_simmap_export": (C.c_int, [_P, _PI32, _PU32, _U64, _PU64]),
     "nm_sim_render": (C.c_int, [_P, _P, C.POINTER(NmPose), _P, _U32, _P]),
     "nm_ranges_add_noise": (C.c_int, [_P, _P, _I64, _F, _F, _U64, _P]),
+    "nm_cave_config_load": (C.c_int, [C.c_char_p, C.POINTER(NmCaveDesc)]),
+    "nm_cave_create": (C.c_int, [_P, C.POINTER(NmCaveDesc), C.POINTER(_P)]),
+    "nm_cave_destroy": (C.c_int, [_P]),
+    "nm_cave_dims": (C.c_int, [_P, _PI32, _PI32]),
+    "nm_cave_populate": (C.c_int, [_P, _U32]),
+    "nm_cave_smooth": (C.c_int, [_P, _U32]),
+    "nm_cave_floor_ceil": (C.c_int, [_P]),
+    "nm_cave_regions": (C.c_int, [_P, C.POINTER(_I64), C.POINTER(_I64)]),
+    "nm_cave_keep_largest": (C.c_int, [_P]),
+    "nm_cave_cells": (C.c_int, [_P, _PI32, _I64, C.POINTER(_I64)]),
+    "nm_cave_simmap": (C.c_int, [_P, _I32, _I32, _I32, C.POINTER(_P)]),
+    "nm_cave_save": (C.c_int, [_P, _I32, _I32, _I32, C.c_char_p, C.c_char_p]),
 }
 
 _lib = None

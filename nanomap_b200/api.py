@@ -474,6 +474,14 @@ class SimMap:
              out.ctypes.data, N.NM_INPUT_HOST | N.NM_OUTPUT_HOST, _stream(stream))
         return out
 
+    @classmethod
+    def _adopt(cls, ctx: Context, res: float, handle: C.c_void_p) -> "SimMap":
+        sm = cls.__new__(cls)
+        sm.ctx = ctx
+        sm.res = res
+        sm.h = handle
+        return sm
+
     def close(self):
         if self.h:
             call("nm_simmap_destroy", self.h)
@@ -486,5 +494,104 @@ class SimMap:
             pass
 
 
-__all__ = ["Pose", "Context", "Sensor", "Map", "SimMap", "sensor_desc", "map_desc",
-           "frame_params", "NanomapError", "lib"]
+def cave_desc(map_size=(50.0, 50.0, 3.5), grid_res=0.1, fill_percentage=56, smoothing_count=4,
+              active_max=4, active_min=4, seed=1, file_out="") -> N.NmCaveDesc:
+    """A cave-generator description (the keys of a #cavegenconfig file); `seed` is the value
+    srand receives."""
+    d = N.NmCaveDesc()
+    for a in range(3):
+        d.map_size[a] = map_size[a]
+    d.grid_res = grid_res
+    d.fill_percentage = fill_percentage
+    d.smoothing_count = smoothing_count
+    d.active_max = active_max
+    d.active_min = active_min
+    d.seed = seed & 0xFFFFFFFF
+    d.file_out = file_out.encode()
+    return d
+
+
+def load_cave_config(path) -> N.NmCaveDesc:
+    d = N.NmCaveDesc()
+    call("nm_cave_config_load", str(path).encode(), C.byref(d))
+    return d
+
+
+class Cave:
+    """Procedural cave generator on the device (nanomap::mapgen::CaveGen)."""
+
+    def __init__(self, ctx: Context, desc: N.NmCaveDesc):
+        self.ctx = ctx
+        self.desc = desc
+        h = C.c_void_p()
+        call("nm_cave_create", ctx.h, C.byref(desc), C.byref(h))
+        self.h = h
+
+    def dims(self):
+        half = (C.c_int32 * 3)()
+        cells = (C.c_int32 * 3)()
+        call("nm_cave_dims", self.h, half, cells)
+        return tuple(half[:]), tuple(cells[:])
+
+    def populate(self, mode_2d=False, counter_rng=False):
+        call("nm_cave_populate", self.h, (N.NM_CAVE_2D if mode_2d else 0) |
+             (N.NM_CAVE_COUNTER_RNG if counter_rng else 0))
+
+    def smooth(self, mode_2d=False):
+        call("nm_cave_smooth", self.h, N.NM_CAVE_2D if mode_2d else 0)
+
+    def floor_ceil(self):
+        call("nm_cave_floor_ceil", self.h)
+
+    def regions(self):
+        n, big = C.c_int64(), C.c_int64()
+        call("nm_cave_regions", self.h, C.byref(n), C.byref(big))
+        return n.value, big.value
+
+    def keep_largest(self):
+        call("nm_cave_keep_largest", self.h)
+
+    def cells(self) -> np.ndarray:
+        n = C.c_int64()
+        call("nm_cave_cells", self.h, None, 0, C.byref(n))
+        out = np.zeros((max(n.value, 1), 3), np.int32)
+        call("nm_cave_cells", self.h, out.ctypes.data_as(N._PI32), n.value, C.byref(n))
+        return out[:n.value]
+
+    def simmap(self, shell=True, half_width=3, closing=1) -> SimMap:
+        h = C.c_void_p()
+        call("nm_cave_simmap", self.h, int(shell), half_width, closing, C.byref(h))
+        return SimMap._adopt(self.ctx, self.desc.grid_res, h)
+
+    def save(self, path, shell=True, half_width=3, closing=1) -> str:
+        written = C.create_string_buffer(512)
+        call("nm_cave_save", self.h, int(shell), half_width, closing, str(path).encode(), written)
+        return written.value.decode()
+
+    def close(self):
+        if self.h:
+            call("nm_cave_destroy", self.h)
+            self.h = None
+
+    def __del__(self):
+        try:
+            self.close()
+        except Exception:
+            pass
+
+
+def simmap_voxels(sm: SimMap) -> np.ndarray:
+    """Active voxels of a sim map, sorted by (x, y, z)."""
+    o, w = sm.export()
+    if len(o) == 0:
+        return np.zeros((0, 3), np.int32)
+    bits = np.unpackbits(w.view(np.uint8).reshape(len(o), 64), axis=1, bitorder="little")
+    leaf, l = np.nonzero(bits)
+    v = np.stack([o[leaf, 0] + (l >> 6), o[leaf, 1] + ((l >> 3) & 7), o[leaf, 2] + (l & 7)], 1)
+    idx = np.lexsort((v[:, 2], v[:, 1], v[:, 0]))
+    return v[idx].astype(np.int32)
+
+
+__all__ = ["Pose", "Context", "Sensor", "Map", "SimMap", "Cave", "cave_desc",
+           "load_cave_config", "simmap_voxels", "sensor_desc", "map_desc", "frame_params",
+           "NanomapError", "lib"]

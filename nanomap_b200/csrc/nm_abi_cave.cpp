@@ -1,0 +1,416 @@
+// nm_abi_cave.cpp -- C ABI of the procedural cave generator (replaces
+// nanomap::mapgen::CaveGen, CaveGen.h:32-68 / CaveGen.cpp).
+//
+// The cell lattice stays on the device between stages.  The reference's fill draws
+// rand() % 100 per cell after srand(seed) in x, y, z loop order (CaveGen.cpp:31-42, 66-79);
+// that sequence is drawn here with the C library's reentrant generator (initstate_r with a
+// 128-byte state, the state size behind srand/rand) so that the same seed gives the same cave
+// without touching the caller's rand() state.  NM_CAVE_COUNTER_RNG fills on the device
+// instead.  Every later stage runs on the device; the result is a device sim map.
+#include <algorithm>
+#include <array>
+#include <cfenv>
+#include <climits>
+#include <cmath>
+#include <cstdio>
+#include <cstdlib>
+#include <cstring>
+#include <memory>
+#include <string>
+#include <vector>
+
+#include "nm_cave.h"
+#include "nm_objects.h"
+
+using nm::fail;
+
+struct nm_cave_s {
+  std::atomic<int> refs{1};
+  nm_context ctx = nullptr;
+  nm_cave_desc desc{};
+  nm::CaveLattice L{};
+  uint8_t* d_cells[2] = {nullptr, nullptr};
+  int cur = 0;
+  int32_t* d_parent = nullptr;
+  uint32_t* d_size = nullptr;
+  unsigned long long* d_min_key = nullptr;
+  nm::CaveStats* d_stats = nullptr;
+};
+
+namespace nm {
+void release(nm_cave c) {
+  if (!c || c->refs.fetch_sub(1, std::memory_order_acq_rel) != 1) return;
+  nm_context ctx = c->ctx;
+  cudaSetDevice(ctx->device);
+  cudaDeviceSynchronize();
+  cudaFree(c->d_cells[0]);
+  cudaFree(c->d_cells[1]);
+  cudaFree(c->d_parent);
+  cudaFree(c->d_size);
+  cudaFree(c->d_min_key);
+  cudaFree(c->d_stats);
+  delete c;
+  release(ctx);
+}
+}  // namespace nm
+
+namespace {
+
+int floor_div8(int v) { return v >> 3; }  // arithmetic shift: floor for negatives
+
+// CaveGen::populateMap's dimensions (CaveGen.cpp:17-30): ceil(size / res) voxels, halved
+// rounding up, evaluated in double under round-to-nearest.
+int lattice_from_desc(const nm_cave_desc& d, nm::CaveLattice* L) {
+  const int saved = std::fegetround();
+  std::fesetround(FE_TONEAREST);
+  double full[3];
+  for (int a = 0; a < 3; ++a) full[a] = std::ceil(d.map_size[a] / d.grid_res);
+  std::fesetround(saved);
+  for (int a = 0; a < 3; ++a) {
+    if (!(full[a] >= 1.0) || full[a] > (double)(1 << 21))
+      return fail(NM_ERR_ARG, "map_size / grid_res on axis %d gives %g voxels (1 .. 2^21)", a,
+                  full[a]);
+    const int n = (int)full[a];
+    L->half[a] = (n % 2 != 0) ? (n + 1) / 2 : n / 2;
+  }
+  const int Dx = L->half[0], Dy = L->half[1], Dz = L->half[2];
+  L->nx = (2 * Dx - 16 > 0) ? (2 * Dx - 16 + 7) / 8 : 0;
+  L->ny = (2 * Dy - 16 > 0) ? (2 * Dy - 16 + 7) / 8 : 0;
+  L->nz = (2 * Dz + 7) / 8;
+  L->kf = (2 * Dz - 8 > 0) ? (2 * Dz - 8 + 7) / 8 : 0;
+  L->ceil_adjacent = ((2 * Dz) % 8 == 0) ? 1 : 0;
+  const long long n = nm::cave_cell_count(*L);
+  if (n >= (1ll << 31)) return fail(NM_ERR_CAPACITY, "cave lattice has %lld cells", n);
+  return NM_OK;
+}
+
+nm::CaveLattice current(nm_cave c) {
+  nm::CaveLattice L = c->L;
+  L.cells = c->d_cells[c->cur];
+  return L;
+}
+
+// Leaf box of the cells' leaves, widened by `margin` leaves on every side.
+void cave_leaf_box(const nm::CaveLattice& L, int margin, int32_t llo[3], int32_t ldim[3]) {
+  int lo[3], hi[3];
+  nm::cave_cell_xyz(L, 0, 0, 0, &lo[0], &lo[1], &lo[2]);
+  nm::cave_cell_xyz(L, std::max(L.nx - 1, 0), std::max(L.ny - 1, 0), L.nz, &hi[0], &hi[1],
+                    &hi[2]);
+  for (int a = 0; a < 3; ++a) {
+    llo[a] = floor_div8(lo[a]) - margin;
+    ldim[a] = floor_div8(hi[a]) + margin - llo[a] + 1;
+  }
+}
+
+int build_cave_simmap(nm_cave c, int shell, int half_width, int closing, nm_simmap* out) {
+  if (!c || !out) return fail(NM_ERR_ARG, "null argument");
+  *out = nullptr;
+  if (shell && (half_width < 1 || half_width > 64 || closing < 0 || closing > 64))
+    return fail(NM_ERR_ARG, "half_width must be in [1, 64] and closing in [0, 64]");
+  nm_context ctx = c->ctx;
+  NM_CUDA(cudaSetDevice(ctx->device));
+  cudaStream_t s = ctx->stream;
+  const int reach = shell ? closing + half_width : 0;
+  int32_t llo[3], ldim[3], vmin[3], vmax[3];
+  cave_leaf_box(c->L, reach / 8 + 1, llo, ldim);
+  for (int a = 0; a < 3; ++a) {
+    vmin[a] = llo[a] * 8;
+    vmax[a] = (llo[a] + ldim[a]) * 8;
+  }
+  std::unique_ptr<nm_simmap_s> sm(new nm_simmap_s());
+  sm->ctx = ctx;
+  nm::SimBuild b{};
+  int rc = nm::begin_build((float)c->desc.grid_res, vmin, vmax, &b, s);
+  if (rc != NM_OK) return rc;
+  NM_CUDA(nm::launch_cave_tiles(current(c), b.dense, b.llo, b.ldim, s));
+  if (shell) {
+    const long long nleaf = (long long)b.ldim[0] * b.ldim[1] * b.ldim[2];
+    uint32_t* buf[3] = {b.dense, nullptr, nullptr};
+    for (int i = 1; i < 3; ++i) {
+      const cudaError_t e = cudaMalloc((void**)&buf[i], (size_t)nleaf * 64);
+      if (e != cudaSuccess) {
+        cudaFree(buf[1]);
+        cudaFree(b.dense);
+        return fail(NM_ERR_CUDA, "cave shell buffers (%lld leaves): %s", nleaf,
+                    cudaGetErrorString(e));
+      }
+    }
+    cudaError_t e = cudaSuccess;
+    // closing: M = erode^c(dilate^c(T)), ping-pong between buf[0] and buf[1]; 2c steps end
+    // in buf[0]
+    int m = 0;
+    for (int i = 0; i < 2 * closing && e == cudaSuccess; ++i) {
+      e = nm::launch_leaf_morph(buf[m], buf[1 - m], b.ldim, i >= closing, s);
+      m = 1 - m;
+    }
+    // E = erode^h(M) into buf[1] / buf[2]; D = dilate^h(M) through the buffer E left free
+    // and buf[0] (M is not needed after D's first step); band = D & ~E
+    int e_buf = 1;
+    for (int i = 0; i < half_width && e == cudaSuccess; ++i) {
+      const int src = (i == 0) ? 0 : e_buf;
+      const int dst = (i == 0) ? 1 : 3 - e_buf;
+      e = nm::launch_leaf_morph(buf[src], buf[dst], b.ldim, 1, s);
+      e_buf = dst;
+    }
+    const int free_buf = 3 - e_buf;
+    int d_buf = 0;
+    for (int i = 0; i < half_width && e == cudaSuccess; ++i) {
+      const int dst = (d_buf == 0) ? free_buf : 0;
+      e = nm::launch_leaf_morph(buf[d_buf], buf[dst], b.ldim, 0, s);
+      d_buf = dst;
+    }
+    if (e == cudaSuccess) e = nm::launch_leaf_andnot(buf[d_buf], buf[e_buf], buf[d_buf], nleaf, s);
+    if (e != cudaSuccess) {
+      for (int i = 0; i < 3; ++i) cudaFree(buf[i]);
+      return fail(NM_ERR_CUDA, "cave shell: %s", cudaGetErrorString(e));
+    }
+    // the band buffer becomes the build buffer; the others go once the stream has used them
+    const cudaError_t se = cudaStreamSynchronize(s);
+    for (int i = 0; i < 3; ++i)
+      if (i != d_buf) cudaFree(buf[i]);
+    b.dense = buf[d_buf];
+    if (se != cudaSuccess) {
+      cudaFree(b.dense);
+      return fail(NM_ERR_CUDA, "cave shell: %s", cudaGetErrorString(se));
+    }
+  }
+  rc = nm::finish_build(ctx, b, sm.get(), s);
+  if (rc != NM_OK) return rc;
+  nm::retain(ctx);
+  *out = sm.release();
+  return NM_OK;
+}
+
+int check_cave(nm_cave c) {
+  if (!c) return fail(NM_ERR_ARG, "cave is null");
+  NM_CUDA(cudaSetDevice(c->ctx->device));
+  return NM_OK;
+}
+
+int run_regions(nm_cave c, nm::CaveStats* st) {
+  cudaStream_t s = c->ctx->stream;
+  NM_CUDA(nm::launch_cave_regions(current(c), c->d_parent, c->d_size, c->d_min_key, c->d_stats,
+                                  s));
+  NM_CUDA(cudaMemcpyAsync(st, c->d_stats, sizeof(*st), cudaMemcpyDeviceToHost, s));
+  NM_CUDA(cudaStreamSynchronize(s));
+  if (st->error) return fail(NM_ERR_TIMEOUT, "cave regions: a union gave up after its limit");
+  return NM_OK;
+}
+
+}  // namespace
+
+extern "C" {
+
+int nm_cave_create(nm_context ctx, const nm_cave_desc* desc, nm_cave* out) {
+  if (!ctx || !desc || !out) return fail(NM_ERR_ARG, "null argument");
+  *out = nullptr;
+  if (!(desc->grid_res > 0.0) || !std::isfinite(desc->grid_res))
+    return fail(NM_ERR_ARG, "grid_res must be positive");
+  for (int a = 0; a < 3; ++a)
+    if (!(desc->map_size[a] > 0.0) || !std::isfinite(desc->map_size[a]))
+      return fail(NM_ERR_ARG, "map_size must be positive");
+  if (desc->smoothing_count < 0 || desc->smoothing_count > 1000000)
+    return fail(NM_ERR_ARG, "smoothing_count out of range");
+  nm::CaveLattice L{};
+  int rc = lattice_from_desc(*desc, &L);
+  if (rc != NM_OK) return rc;
+  NM_CUDA(cudaSetDevice(ctx->device));
+  nm_cave c = new nm_cave_s();
+  c->ctx = nm::retain(ctx);
+  c->desc = *desc;
+  c->desc.file_out[sizeof(c->desc.file_out) - 1] = '\0';
+  c->L = L;
+  const long long n = std::max<long long>(nm::cave_cell_count(L), 1);
+  cudaError_t e = cudaMalloc((void**)&c->d_cells[0], (size_t)n);
+  if (e == cudaSuccess) e = cudaMalloc((void**)&c->d_cells[1], (size_t)n);
+  if (e == cudaSuccess) e = cudaMalloc((void**)&c->d_parent, (size_t)n * 4);
+  if (e == cudaSuccess) e = cudaMalloc((void**)&c->d_size, (size_t)n * 4);
+  if (e == cudaSuccess) e = cudaMalloc((void**)&c->d_min_key, (size_t)n * 8);
+  if (e == cudaSuccess) e = cudaMalloc((void**)&c->d_stats, sizeof(nm::CaveStats));
+  if (e == cudaSuccess) e = cudaMemsetAsync(c->d_cells[0], 0, (size_t)n, ctx->stream);
+  if (e == cudaSuccess) e = cudaStreamSynchronize(ctx->stream);
+  if (e != cudaSuccess) {
+    nm::release(c);  // frees what was allocated and the context reference
+    return fail(NM_ERR_CUDA, "cave buffers (%lld cells): %s", n, cudaGetErrorString(e));
+  }
+  *out = c;
+  return NM_OK;
+}
+
+int nm_cave_destroy(nm_cave c) {
+  nm::release(c);
+  return NM_OK;
+}
+
+int nm_cave_dims(nm_cave c, int32_t half[3], int32_t cells[3]) {
+  if (!c) return fail(NM_ERR_ARG, "cave is null");
+  if (half)
+    for (int a = 0; a < 3; ++a) half[a] = c->L.half[a];
+  if (cells) {
+    cells[0] = c->L.nx;
+    cells[1] = c->L.ny;
+    cells[2] = c->L.nz;
+  }
+  return NM_OK;
+}
+
+int nm_cave_populate(nm_cave c, uint32_t flags) {
+  int rc = check_cave(c);
+  if (rc != NM_OK) return rc;
+  cudaStream_t s = c->ctx->stream;
+  const int mode_2d = (flags & NM_CAVE_2D) ? 1 : 0;
+  c->cur = 0;
+  const nm::CaveLattice L = current(c);
+  if (flags & NM_CAVE_COUNTER_RNG) {
+    NM_CUDA(nm::launch_cave_fill(L, c->desc.seed, c->desc.fill_percentage, mode_2d, s));
+    NM_CUDA(cudaStreamSynchronize(s));
+    return NM_OK;
+  }
+  const long long n = nm::cave_cell_count(L);
+  std::vector<uint8_t> cells((size_t)std::max<long long>(n, 1), 0);
+  struct random_data rd;
+  std::memset(&rd, 0, sizeof(rd));
+  alignas(8) char state[128];
+  std::memset(state, 0, sizeof(state));
+  if (initstate_r(c->desc.seed, state, sizeof(state), &rd) != 0)
+    return fail(NM_ERR_STATE, "initstate_r failed");
+  const int nzp = L.nz + 1;
+  for (int i = 0; i < L.nx; ++i)
+    for (int j = 0; j < L.ny; ++j) {
+      const size_t col = ((size_t)i * L.ny + j) * nzp;
+      if (mode_2d) {
+        int32_t r = 0;
+        random_r(&rd, &r);
+        const uint8_t v = (r % 100 < c->desc.fill_percentage) ? 1 : 0;
+        for (int k = 0; k < L.nz; ++k) cells[col + k] = v;
+      } else {
+        for (int k = 1; k < L.kf; ++k) {
+          int32_t r = 0;
+          random_r(&rd, &r);
+          cells[col + k] = (r % 100 < c->desc.fill_percentage) ? 1 : 0;
+        }
+      }
+    }
+  NM_CUDA(cudaMemcpyAsync(L.cells, cells.data(), cells.size(), cudaMemcpyHostToDevice, s));
+  NM_CUDA(cudaStreamSynchronize(s));
+  return NM_OK;
+}
+
+int nm_cave_smooth(nm_cave c, uint32_t flags) {
+  int rc = check_cave(c);
+  if (rc != NM_OK) return rc;
+  cudaStream_t s = c->ctx->stream;
+  const int mode_2d = (flags & NM_CAVE_2D) ? 1 : 0;
+  for (int it = 0; it < c->desc.smoothing_count; ++it) {
+    const nm::CaveLattice L = current(c);
+    NM_CUDA(nm::launch_cave_smooth(L, L.cells, c->d_cells[1 - c->cur], c->desc.active_max,
+                                   c->desc.active_min, mode_2d, s));
+    c->cur = 1 - c->cur;
+  }
+  NM_CUDA(cudaStreamSynchronize(s));
+  return NM_OK;
+}
+
+int nm_cave_floor_ceil(nm_cave c) {
+  int rc = check_cave(c);
+  if (rc != NM_OK) return rc;
+  NM_CUDA(nm::launch_cave_floor_ceil(current(c), c->ctx->stream));
+  NM_CUDA(cudaStreamSynchronize(c->ctx->stream));
+  return NM_OK;
+}
+
+int nm_cave_regions(nm_cave c, int64_t* n_regions, int64_t* largest) {
+  int rc = check_cave(c);
+  if (rc != NM_OK) return rc;
+  nm::CaveStats st{};
+  rc = run_regions(c, &st);
+  if (rc != NM_OK) return rc;
+  if (n_regions) *n_regions = st.n_regions;
+  if (largest) *largest = st.largest;
+  return NM_OK;
+}
+
+int nm_cave_keep_largest(nm_cave c) {
+  int rc = check_cave(c);
+  if (rc != NM_OK) return rc;
+  nm::CaveStats st{};
+  rc = run_regions(c, &st);
+  if (rc != NM_OK) return rc;
+  NM_CUDA(nm::launch_cave_keep(current(c), c->d_parent, c->d_min_key, c->d_stats,
+                               c->ctx->stream));
+  NM_CUDA(cudaStreamSynchronize(c->ctx->stream));
+  return NM_OK;
+}
+
+int nm_cave_cells(nm_cave c, int32_t* xyz, int64_t max_cells, int64_t* n) {
+  int rc = check_cave(c);
+  if (rc != NM_OK) return rc;
+  if (!n || (max_cells > 0 && !xyz)) return fail(NM_ERR_ARG, "null argument");
+  const nm::CaveLattice L = current(c);
+  const long long total = nm::cave_cell_count(L);
+  std::vector<uint8_t> cells((size_t)std::max<long long>(total, 1));
+  if (total > 0) NM_CUDA(cudaMemcpy(cells.data(), L.cells, (size_t)total, cudaMemcpyDeviceToHost));
+  std::vector<std::pair<unsigned long long, std::array<int32_t, 3>>> on;
+  const int nzp = L.nz + 1;
+  for (long long idx = 0; idx < total; ++idx) {
+    if (!cells[(size_t)idx]) continue;
+    const int k = (int)(idx % nzp), j = (int)((idx / nzp) % L.ny), i = (int)(idx / nzp / L.ny);
+    int x, y, z;
+    nm::cave_cell_xyz(L, i, j, k, &x, &y, &z);
+    on.push_back({nm::vdb_order_key(x, y, z), {x, y, z}});
+  }
+  std::sort(on.begin(), on.end(),
+            [](const auto& a, const auto& b) { return a.first < b.first; });
+  *n = (int64_t)on.size();
+  const size_t m = std::min<size_t>(on.size(), (size_t)std::max<int64_t>(max_cells, 0));
+  for (size_t q = 0; q < m; ++q)
+    for (int a = 0; a < 3; ++a) xyz[3 * q + a] = on[q].second[a];
+  return NM_OK;
+}
+
+int nm_cave_simmap(nm_cave c, int32_t shell, int32_t half_width, int32_t closing,
+                   nm_simmap* out) {
+  return build_cave_simmap(c, shell, half_width, closing, out);
+}
+
+int nm_cave_save(nm_cave c, int32_t shell, int32_t half_width, int32_t closing,
+                 const char* path, char* written_path) {
+  if (!c || !path) return fail(NM_ERR_ARG, "null argument");
+  std::string name(path);
+  if (name.size() >= 4 && name.compare(name.size() - 4, 4, ".vdb") == 0)
+    name = name.substr(0, name.size() - 4) + ".nmsim";
+  if (name.size() >= 512) return fail(NM_ERR_ARG, "output path too long");
+  nm_simmap sm = nullptr;
+  int rc = build_cave_simmap(c, shell, half_width, closing, &sm);
+  if (rc != NM_OK) return rc;
+  uint64_t nleaves = 0;
+  nm_simmap_info(sm, nullptr, nullptr, &nleaves);
+  std::vector<int32_t> origins((size_t)nleaves * 3 + 3);
+  std::vector<uint32_t> words((size_t)nleaves * 16 + 16);
+  uint64_t got = 0;
+  rc = nm_simmap_export(sm, origins.data(), words.data(), nleaves, &got);
+  nm::release(sm);
+  if (rc != NM_OK) return rc;
+  std::vector<int32_t> ijk;
+  for (uint64_t q = 0; q < got; ++q)
+    for (int l = 0; l < 512; ++l)
+      if (words[q * 16 + (l >> 5)] >> (l & 31) & 1u) {
+        ijk.push_back(origins[3 * q] + (l >> 6));
+        ijk.push_back(origins[3 * q + 1] + ((l >> 3) & 7));
+        ijk.push_back(origins[3 * q + 2] + (l & 7));
+      }
+  FILE* f = std::fopen(name.c_str(), "wb");
+  if (!f) return fail(NM_ERR_IO, "cannot write '%s'", name.c_str());
+  const char magic[8] = {'N', 'M', 'S', 'I', 'M', 'v', '1', '\0'};
+  const float res = (float)c->desc.grid_res;
+  const int64_t count = (int64_t)(ijk.size() / 3);
+  bool ok = std::fwrite(magic, 1, 8, f) == 8 && std::fwrite(&res, 4, 1, f) == 1 &&
+            std::fwrite(&count, 8, 1, f) == 1 &&
+            (count == 0 || std::fwrite(ijk.data(), 12, (size_t)count, f) == (size_t)count);
+  ok = (std::fclose(f) == 0) && ok;
+  if (!ok) return fail(NM_ERR_IO, "short write to '%s'", name.c_str());
+  if (written_path) std::snprintf(written_path, 512, "%s", name.c_str());
+  return NM_OK;
+}
+
+}  // extern "C"

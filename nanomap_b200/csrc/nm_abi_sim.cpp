@@ -13,13 +13,19 @@
 #include "nm_host.h"
 #include "nm_objects.h"
 
+using nm::begin_build;
 using nm::fail;
+using nm::finish_build;
 
 namespace {
 
 int floor_div(int v, int d) { return (v >= 0) ? v / d : -((-v + d - 1) / d); }
 
-// Shared tail of both builders: compact the dense leaf buffer into the sparse view.
+}  // namespace
+
+namespace nm {
+
+// Shared tail of the builders: compact the dense leaf buffer into the sparse view.
 int finish_build(nm_context ctx, nm::SimBuild& b, nm_simmap sm, cudaStream_t s) {
   nm::SimMapView& v = sm->view;
   v.res = b.res;
@@ -97,6 +103,10 @@ int begin_build(float res, const int32_t vmin[3], const int32_t vmax[3], nm::Sim
   NM_CUDA(cudaMemsetAsync(b->dense, 0, (size_t)prod * 64, s));
   return NM_OK;
 }
+
+}  // namespace nm
+
+namespace {
 
 cudaStream_t pick(nm_context ctx, void* stream) {
   return stream ? static_cast<cudaStream_t>(stream) : ctx->stream;

@@ -1,0 +1,377 @@
+// nm_cave.cu -- procedural cave generation on the device (replaces CaveGen.cpp).
+//
+// Every stage of the reference's generator is one or a few grid-stride kernels over the cell
+// lattice (a few thousand to a few million one-byte cells), and the level-set shell is
+// face-neighbour morphology on 8^3 leaf bit masks in the sim map's build layout, so the
+// result goes into a device sim map without a host round trip:
+//   k_cave_fill        counter-based fill (the C library sequence is drawn on the host)
+//   k_cave_smooth3d/2d one cellular-automaton step (CaveGen::smoothMap / smoothMapXY)
+//   k_cc_*             6-connected regions by lock-free union-find (CaveGen::getRegions)
+//   k_cave_tiles       cells -> whole leaves (addTile(1, ...) + voxelizeActiveTiles)
+//   k_leaf_morph       one dilation or erosion step on 64-bit x-slices of the leaves
+#include <climits>
+#include <cstdint>
+
+#include "nm_cave.h"
+
+namespace nm {
+
+namespace {
+
+constexpr int kGrid = 1184;  // 148 SMs x 8 resident blocks of 256 threads
+constexpr int kUnionIters = 1 << 20;
+
+__host__ __device__ inline unsigned long long splitmix64(unsigned long long z) {
+  z += 0x9e3779b97f4a7c15ull;
+  z = (z ^ (z >> 30)) * 0xbf58476d1ce4e5b9ull;
+  z = (z ^ (z >> 27)) * 0x94d049bb133111ebull;
+  return z ^ (z >> 31);
+}
+
+__device__ __forceinline__ long long cell_index(const CaveLattice& L, int i, int j, int k) {
+  return ((long long)i * L.ny + j) * (L.nz + 1) + k;
+}
+
+__device__ __forceinline__ void cell_ijk(const CaveLattice& L, long long c, int* i, int* j,
+                                         int* k) {
+  const int nzp = L.nz + 1;
+  *k = (int)(c % nzp);
+  const long long r = c / nzp;
+  *j = (int)(r % L.ny);
+  *i = (int)(r / L.ny);
+}
+
+// Counter-based fill: one draw per cell (3-D) or per column (2-D), splitmix64 of the seed and
+// the cell's lattice position.
+__global__ void k_cave_fill(CaveLattice L, uint32_t seed, int pct, int mode_2d) {
+  const long long n = cave_cell_count(L);
+  for (long long c = (long long)blockIdx.x * blockDim.x + threadIdx.x; c < n;
+       c += (long long)gridDim.x * blockDim.x) {
+    int i, j, k;
+    cell_ijk(L, c, &i, &j, &k);
+    bool on = false;
+    if (mode_2d ? (k < L.nz) : (k >= 1 && k < L.kf)) {
+      const unsigned long long pos = ((unsigned long long)i << 42) |
+                                     ((unsigned long long)j << 21) |
+                                     (unsigned long long)(mode_2d ? 0 : k);
+      const unsigned long long h = splitmix64(((unsigned long long)seed << 32) ^ pos);
+      on = (int)((uint32_t)(h >> 32) % 100u) < pct;
+    }
+    L.cells[c] = on ? 1 : 0;
+  }
+}
+
+// One step of CaveGen::smoothMap: 26-neighbour count on the lattice (planes below the ceiling,
+// and the ceiling plane where it is a face neighbour); more than amax -> on, fewer than amin
+// -> off, else unchanged.  The ceiling plane is not part of the step's output (off after).
+__global__ void k_cave_smooth3d(CaveLattice L, const uint8_t* __restrict__ cur,
+                                uint8_t* __restrict__ next, int amax, int amin) {
+  const long long n = cave_cell_count(L);
+  const int ktop = L.ceil_adjacent ? L.nz : L.nz - 1;  // highest plane a neighbour can be in
+  for (long long c = (long long)blockIdx.x * blockDim.x + threadIdx.x; c < n;
+       c += (long long)gridDim.x * blockDim.x) {
+    int i, j, k;
+    cell_ijk(L, c, &i, &j, &k);
+    if (k >= L.nz) {
+      next[c] = 0;
+      continue;
+    }
+    int cnt = 0;
+    for (int dx = -1; dx <= 1; ++dx) {
+      const int ii = i + dx;
+      if (ii < 0 || ii >= L.nx) continue;
+      for (int dy = -1; dy <= 1; ++dy) {
+        const int jj = j + dy;
+        if (jj < 0 || jj >= L.ny) continue;
+        const long long base = ((long long)ii * L.ny + jj) * (L.nz + 1);
+        for (int dz = -1; dz <= 1; ++dz) {
+          const int kk = k + dz;
+          if (kk < 0 || kk > ktop || (dx == 0 && dy == 0 && dz == 0)) continue;
+          cnt += cur[base + kk];
+        }
+      }
+    }
+    next[c] = cnt > amax ? 1 : (cnt < amin ? 0 : cur[c]);
+  }
+}
+
+// One step of CaveGen::smoothMapXY: 8-neighbour count in the floor plane (k = 0), the result
+// written to the whole column below the ceiling.
+__global__ void k_cave_smooth2d(CaveLattice L, const uint8_t* __restrict__ cur,
+                                uint8_t* __restrict__ next, int amax, int amin) {
+  const long long ncol = (long long)L.nx * L.ny;
+  const int nzp = L.nz + 1;
+  for (long long col = (long long)blockIdx.x * blockDim.x + threadIdx.x; col < ncol;
+       col += (long long)gridDim.x * blockDim.x) {
+    const int i = (int)(col / L.ny), j = (int)(col % L.ny);
+    int cnt = 0;
+    for (int dx = -1; dx <= 1; ++dx) {
+      const int ii = i + dx;
+      if (ii < 0 || ii >= L.nx) continue;
+      for (int dy = -1; dy <= 1; ++dy) {
+        const int jj = j + dy;
+        if (jj < 0 || jj >= L.ny || (dx == 0 && dy == 0)) continue;
+        cnt += cur[((long long)ii * L.ny + jj) * nzp];
+      }
+    }
+    const uint8_t v = cnt > amax ? 1 : (cnt < amin ? 0 : cur[col * nzp]);
+    for (int k = 0; k < L.nz; ++k) next[col * nzp + k] = v;
+    next[col * nzp + L.nz] = 0;
+  }
+}
+
+__global__ void k_cave_floor_ceil(CaveLattice L) {
+  const long long ncol = (long long)L.nx * L.ny;
+  const int nzp = L.nz + 1;
+  for (long long col = (long long)blockIdx.x * blockDim.x + threadIdx.x; col < ncol;
+       col += (long long)gridDim.x * blockDim.x) {
+    L.cells[col * nzp] = 1;
+    L.cells[col * nzp + L.nz] = 1;
+  }
+}
+
+// ---- regions: union-find with roots linked toward the smaller cell index ----------------
+// parent[x] <= x always holds, so every find ends; a union retries only when another thread
+// linked one of its roots meanwhile, and gives up (error flag) after kUnionIters tries.
+
+__device__ __forceinline__ int cc_find(int32_t* parent, int x) {
+  for (;;) {
+    const int p = __ldcg(&parent[x]);
+    if (p == x) return x;
+    const int g = __ldcg(&parent[p]);
+    if (g != p) parent[x] = g;  // path halving; any ancestor is a valid parent
+    x = g;
+  }
+}
+
+__device__ void cc_union(int32_t* parent, int a, int b, unsigned int* err) {
+  for (int it = 0; it < kUnionIters; ++it) {
+    a = cc_find(parent, a);
+    b = cc_find(parent, b);
+    if (a == b) return;
+    if (a < b) {
+      const int t = a;
+      a = b;
+      b = t;
+    }
+    if (atomicCAS(&parent[a], a, b) == a) return;
+  }
+  atomicOr(err, 1u);
+}
+
+__global__ void k_cc_init(CaveLattice L, int32_t* parent, uint32_t* size,
+                          unsigned long long* min_key, CaveStats* stats) {
+  const long long n = cave_cell_count(L);
+  if (blockIdx.x == 0 && threadIdx.x == 0) {
+    stats->n_regions = 0;
+    stats->largest = 0;
+    stats->best_key = ~0ull;
+    stats->error = 0;
+  }
+  for (long long c = (long long)blockIdx.x * blockDim.x + threadIdx.x; c < n;
+       c += (long long)gridDim.x * blockDim.x) {
+    parent[c] = L.cells[c] ? (int)c : -1;
+    size[c] = 0;
+    min_key[c] = ~0ull;
+  }
+}
+
+__global__ void k_cc_union(CaveLattice L, int32_t* parent, CaveStats* stats) {
+  const long long n = cave_cell_count(L);
+  const int nzp = L.nz + 1;
+  for (long long c = (long long)blockIdx.x * blockDim.x + threadIdx.x; c < n;
+       c += (long long)gridDim.x * blockDim.x) {
+    if (!L.cells[c]) continue;
+    int i, j, k;
+    cell_ijk(L, c, &i, &j, &k);
+    if (i + 1 < L.nx && L.cells[c + (long long)L.ny * nzp])
+      cc_union(parent, (int)c, (int)(c + (long long)L.ny * nzp), &stats->error);
+    if (j + 1 < L.ny && L.cells[c + nzp]) cc_union(parent, (int)c, (int)(c + nzp), &stats->error);
+    const bool zn = (k + 1 < L.nz) || (k + 1 == L.nz && L.ceil_adjacent);
+    if (zn && L.cells[c + 1]) cc_union(parent, (int)c, (int)(c + 1), &stats->error);
+  }
+}
+
+__global__ void k_cc_flatten(CaveLattice L, int32_t* parent, uint32_t* size,
+                             unsigned long long* min_key) {
+  const long long n = cave_cell_count(L);
+  for (long long c = (long long)blockIdx.x * blockDim.x + threadIdx.x; c < n;
+       c += (long long)gridDim.x * blockDim.x) {
+    if (!L.cells[c]) continue;
+    const int r = cc_find(parent, (int)c);
+    int i, j, k, x, y, z;
+    cell_ijk(L, c, &i, &j, &k);
+    cave_cell_xyz(L, i, j, k, &x, &y, &z);
+    atomicAdd(&size[r], 1u);
+    atomicMin(&min_key[r], vdb_order_key(x, y, z));
+  }
+}
+
+// After k_cc_flatten every on cell's parent chain ends at its root; store the root itself.
+__global__ void k_cc_roots(CaveLattice L, int32_t* parent, const uint32_t* size,
+                           CaveStats* stats) {
+  const long long n = cave_cell_count(L);
+  for (long long c = (long long)blockIdx.x * blockDim.x + threadIdx.x; c < n;
+       c += (long long)gridDim.x * blockDim.x) {
+    if (!L.cells[c]) continue;
+    if (parent[c] == (int)c) {
+      atomicAdd(&stats->n_regions, 1u);
+      atomicMax(&stats->largest, size[c]);
+    } else {
+      parent[c] = cc_find(parent, (int)c);
+    }
+  }
+}
+
+__global__ void k_cc_best(CaveLattice L, const int32_t* parent, const uint32_t* size,
+                          const unsigned long long* min_key, CaveStats* stats) {
+  const long long n = cave_cell_count(L);
+  const uint32_t largest = stats->largest;
+  for (long long c = (long long)blockIdx.x * blockDim.x + threadIdx.x; c < n;
+       c += (long long)gridDim.x * blockDim.x)
+    if (L.cells[c] && parent[c] == (int)c && size[c] == largest)
+      atomicMin(&stats->best_key, min_key[c]);
+}
+
+__global__ void k_cave_keep(CaveLattice L, const int32_t* parent,
+                            const unsigned long long* min_key, const CaveStats* stats) {
+  const long long n = cave_cell_count(L);
+  const unsigned long long best = stats->best_key;
+  for (long long c = (long long)blockIdx.x * blockDim.x + threadIdx.x; c < n;
+       c += (long long)gridDim.x * blockDim.x)
+    if (L.cells[c]) L.cells[c] = (min_key[parent[c]] == best) ? 1 : 0;
+}
+
+// ---- leaves ------------------------------------------------------------------------------
+
+__global__ void k_cave_tiles(CaveLattice L, uint32_t* dense, int3 llo, int3 ldim) {
+  const long long n = cave_cell_count(L);
+  for (long long c = (long long)blockIdx.x * blockDim.x + threadIdx.x; c < n;
+       c += (long long)gridDim.x * blockDim.x) {
+    if (!L.cells[c]) continue;
+    int i, j, k, x, y, z;
+    cell_ijk(L, c, &i, &j, &k);
+    cave_cell_xyz(L, i, j, k, &x, &y, &z);
+    const long long lx = (x >> 3) - llo.x, ly = (y >> 3) - llo.y, lz = (z >> 3) - llo.z;
+    if (lx < 0 || lx >= ldim.x || ly < 0 || ly >= ldim.y || lz < 0 || lz >= ldim.z) continue;
+    uint4* w = reinterpret_cast<uint4*>(dense + ((lx * ldim.y + ly) * ldim.z + lz) * 16);
+    const uint4 ones = make_uint4(~0u, ~0u, ~0u, ~0u);
+    w[0] = ones;
+    w[1] = ones;
+    w[2] = ones;
+    w[3] = ones;
+  }
+}
+
+// Leaf bits: voxel (x, y, z) of a leaf is bit x*64 + y*8 + z, so x-slice x is the 64-bit word
+// x of the leaf with bit y*8 + z.  For each direction, the mask of voxels whose face
+// neighbour in that direction is on; dilation ORs them into the slice, erosion ANDs them.
+__global__ void __launch_bounds__(256) k_leaf_morph(const unsigned long long* __restrict__ src,
+                                                    unsigned long long* __restrict__ dst,
+                                                    int3 ldim, int erode) {
+  constexpr unsigned long long kZ0 = 0x0101010101010101ull, kZ7 = 0x8080808080808080ull;
+  const long long nleaf = (long long)ldim.x * ldim.y * ldim.z;
+  const long long n = nleaf * 8;
+  const long long sx = (long long)ldim.y * ldim.z, sy = ldim.z;
+  for (long long t = (long long)blockIdx.x * blockDim.x + threadIdx.x; t < n;
+       t += (long long)gridDim.x * blockDim.x) {
+    const long long pos = t >> 3;
+    const int x = (int)(t & 7);
+    const int lz = (int)(pos % ldim.z);
+    const int ly = (int)((pos / ldim.z) % ldim.y);
+    const int lx = (int)(pos / sx);
+    const unsigned long long s = __ldg(&src[t]);
+    const unsigned long long zp_l = lz + 1 < ldim.z ? __ldg(&src[t + 8]) : 0ull;
+    const unsigned long long zm_l = lz > 0 ? __ldg(&src[t - 8]) : 0ull;
+    const unsigned long long yp_l = ly + 1 < ldim.y ? __ldg(&src[t + 8 * sy]) : 0ull;
+    const unsigned long long ym_l = ly > 0 ? __ldg(&src[t - 8 * sy]) : 0ull;
+    unsigned long long xp, xm;
+    if (x < 7) xp = __ldg(&src[t + 1]);
+    else xp = lx + 1 < ldim.x ? __ldg(&src[(pos + sx) * 8]) : 0ull;
+    if (x > 0) xm = __ldg(&src[t - 1]);
+    else xm = lx > 0 ? __ldg(&src[(pos - sx) * 8 + 7]) : 0ull;
+    const unsigned long long zp = ((s >> 1) & ~kZ7) | ((zp_l << 7) & kZ7);
+    const unsigned long long zm = ((s << 1) & ~kZ0) | ((zm_l >> 7) & kZ0);
+    const unsigned long long yp = (s >> 8) | (yp_l << 56);
+    const unsigned long long ym = (s << 8) | (ym_l >> 56);
+    dst[t] = erode ? (s & zp & zm & yp & ym & xp & xm) : (s | zp | zm | yp | ym | xp | xm);
+  }
+}
+
+__global__ void k_leaf_andnot(const unsigned long long* a, const unsigned long long* b,
+                              unsigned long long* dst, long long n) {
+  for (long long t = (long long)blockIdx.x * blockDim.x + threadIdx.x; t < n;
+       t += (long long)gridDim.x * blockDim.x)
+    dst[t] = a[t] & ~b[t];
+}
+
+int grid_for(long long n) {
+  const long long g = (n + 255) / 256;
+  return (int)(g < 1 ? 1 : (g > kGrid ? kGrid : g));
+}
+
+}  // namespace
+
+cudaError_t launch_cave_fill(const CaveLattice& L, uint32_t seed, int pct, int mode_2d,
+                             cudaStream_t s) {
+  k_cave_fill<<<grid_for(cave_cell_count(L)), 256, 0, s>>>(L, seed, pct, mode_2d);
+  return cudaGetLastError();
+}
+
+cudaError_t launch_cave_smooth(const CaveLattice& L, const uint8_t* cur, uint8_t* next, int amax,
+                               int amin, int mode_2d, cudaStream_t s) {
+  if (mode_2d)
+    k_cave_smooth2d<<<grid_for((long long)L.nx * L.ny), 256, 0, s>>>(L, cur, next, amax, amin);
+  else
+    k_cave_smooth3d<<<grid_for(cave_cell_count(L)), 256, 0, s>>>(L, cur, next, amax, amin);
+  return cudaGetLastError();
+}
+
+cudaError_t launch_cave_floor_ceil(const CaveLattice& L, cudaStream_t s) {
+  k_cave_floor_ceil<<<grid_for((long long)L.nx * L.ny), 256, 0, s>>>(L);
+  return cudaGetLastError();
+}
+
+cudaError_t launch_cave_regions(const CaveLattice& L, int32_t* parent, uint32_t* size,
+                                unsigned long long* min_key, CaveStats* stats, cudaStream_t s) {
+  const int g = grid_for(cave_cell_count(L));
+  k_cc_init<<<g, 256, 0, s>>>(L, parent, size, min_key, stats);
+  k_cc_union<<<g, 256, 0, s>>>(L, parent, stats);
+  k_cc_flatten<<<g, 256, 0, s>>>(L, parent, size, min_key);
+  k_cc_roots<<<g, 256, 0, s>>>(L, parent, size, stats);
+  k_cc_best<<<g, 256, 0, s>>>(L, parent, size, min_key, stats);
+  return cudaGetLastError();
+}
+
+cudaError_t launch_cave_keep(const CaveLattice& L, const int32_t* parent,
+                             const unsigned long long* min_key, const CaveStats* stats,
+                             cudaStream_t s) {
+  k_cave_keep<<<grid_for(cave_cell_count(L)), 256, 0, s>>>(L, parent, min_key, stats);
+  return cudaGetLastError();
+}
+
+cudaError_t launch_cave_tiles(const CaveLattice& L, uint32_t* dense, const int32_t llo[3],
+                              const int32_t ldim[3], cudaStream_t s) {
+  k_cave_tiles<<<grid_for(cave_cell_count(L)), 256, 0, s>>>(
+      L, dense, make_int3(llo[0], llo[1], llo[2]), make_int3(ldim[0], ldim[1], ldim[2]));
+  return cudaGetLastError();
+}
+
+cudaError_t launch_leaf_morph(const uint32_t* src, uint32_t* dst, const int32_t ldim[3],
+                              int erode, cudaStream_t s) {
+  const long long n = (long long)ldim[0] * ldim[1] * ldim[2] * 8;
+  k_leaf_morph<<<grid_for(n), 256, 0, s>>>(reinterpret_cast<const unsigned long long*>(src),
+                                           reinterpret_cast<unsigned long long*>(dst),
+                                           make_int3(ldim[0], ldim[1], ldim[2]), erode);
+  return cudaGetLastError();
+}
+
+cudaError_t launch_leaf_andnot(const uint32_t* a, const uint32_t* b, uint32_t* dst, long long n,
+                               cudaStream_t s) {
+  k_leaf_andnot<<<grid_for(n * 8), 256, 0, s>>>(reinterpret_cast<const unsigned long long*>(a),
+                                                reinterpret_cast<const unsigned long long*>(b),
+                                                reinterpret_cast<unsigned long long*>(dst), n * 8);
+  return cudaGetLastError();
+}
+
+}  // namespace nm

@@ -5,6 +5,7 @@
 //   frustum sensor "#frustumconfig" ... "#endconfig"   (Config.cpp:226-264)
 //   laser sensor   "#laserconfig" ... "#endconfig"     (Config.cpp:185-225)
 //   agent          "#agentconfig" ... "#endconfig"     (Agent.h:63-125)
+//   cave generator "#cavegenconfig" ... "seed <s>"    (CaveGen.cpp:358-401)
 // Every key the reference reads is accepted with the same meaning.  Optional keys extend the
 // formats: main config ClampMin:, ClampMax:, UpdateMode: (label|accumulate), ClampOrder:
 // (always|crossing), Rounding: (down|nearest), PublishSensor: (the key the shipped config
@@ -14,7 +15,9 @@
 #include <cmath>
 #include <cstdio>
 #include <cstring>
+#include <ctime>
 #include <fstream>
+#include <functional>
 #include <memory>
 #include <sstream>
 #include <string>
@@ -347,6 +350,58 @@ int nm_config_map_desc(nm_config c, nm_map_desc* out) {
   out->update_mode = I.update_mode;
   out->rounding = I.rounding;
   out->max_agents = 1;
+  return NM_OK;
+}
+
+// CaveGen::loadConfig (CaveGen.cpp:358-401): keys are read in any order until "seed <s>";
+// random_seed 1 seeds from the clock, anything else from the seed string.  The seed is the
+// reference's: std::hash of the string (or of time(0)) stored in an int, i.e. its low 32 bits,
+// which srand receives.  A missing random_seed key counts as 0 (the reference leaves it
+// unset).
+int nm_cave_config_load(const char* path, nm_cave_desc* out) {
+  if (!path || !out) return fail(NM_ERR_ARG, "null argument");
+  std::memset(out, 0, sizeof(*out));
+  std::ifstream in(path, std::ios::in | std::ios::binary);
+  if (!in) return fail(NM_ERR_IO, "cannot open cave config '%s'", path);
+  std::string line;
+  in >> line;
+  if (line != "#cavegenconfig")
+    return fail(NM_ERR_IO, "%s: first token is [%s] instead of [#cavegenconfig]", path,
+                line.c_str());
+  std::string file_out, seed;
+  int random_seed = 0;
+  bool done = false;
+  while (in.good() && !done) {
+    if (!(in >> line)) break;
+    if (line == "file_out") {
+      in >> file_out;
+    } else if (line == "map_size") {
+      in >> out->map_size[0] >> out->map_size[1] >> out->map_size[2];
+    } else if (line == "grid_res") {
+      in >> out->grid_res;
+    } else if (line == "fill_percentage") {
+      in >> out->fill_percentage;
+    } else if (line == "smoothing_count") {
+      in >> out->smoothing_count;
+    } else if (line == "active") {
+      in >> out->active_max >> out->active_min;
+    } else if (line == "random_seed") {
+      in >> random_seed;
+    } else if (line == "seed") {
+      in >> seed;
+      done = true;
+    }
+  }
+  if (file_out.size() >= sizeof(out->file_out))
+    return fail(NM_ERR_IO, "%s: file_out is longer than %zu bytes", path,
+                sizeof(out->file_out) - 1);
+  std::snprintf(out->file_out, sizeof(out->file_out), "%s", file_out.c_str());
+  out->time_seed = (random_seed == 1) ? 1 : 0;
+  const size_t h = out->time_seed ? std::hash<std::time_t>{}(std::time(nullptr))
+                                  : std::hash<std::string>{}(seed);
+  out->seed = (uint32_t)h;
+  if (!(out->grid_res > 0.0))
+    return fail(NM_ERR_IO, "%s: grid_res missing or not positive", path);
   return NM_OK;
 }
 

@@ -107,6 +107,13 @@ void release(nm_context c);
 void release(nm_sensor s);
 void release(nm_map m);
 void release(nm_simmap sm);
+void release(nm_cave c);
+
+// Sim map construction: begin_build allocates the zeroed dense leaf buffer of the voxel
+// region [vmin, vmax); finish_build compacts it into `sm` and frees it.
+int begin_build(float res, const int32_t vmin[3], const int32_t vmax[3], SimBuild* b,
+                cudaStream_t s);
+int finish_build(nm_context ctx, SimBuild& b, nm_simmap sm, cudaStream_t s);
 
 cudaStream_t pick(nm_context ctx, void* stream);
 int make_frame(nm_map m, nm_sensor s, const nm_pose* pose, FrameParams* f);

@@ -94,6 +94,20 @@ def lib() -> C.CDLL:
         L.orc_depth.argtypes = [C.POINTER(OrcSensor), _PD, _PD, C.c_double, _PI32, _PF, C.c_int64,
                                 C.c_double, C.c_double, _PI32, C.c_int64, _PD, _PD,
                                 C.POINTER(C.c_uint64), _PD, _PD]
+        L.orc_cave_new.argtypes = [_PD, C.c_double, C.c_int, C.c_int, C.c_int, C.c_int, C.c_uint32]
+        L.orc_cave_new.restype = C.c_void_p
+        L.orc_cave_free.argtypes = [C.c_void_p]
+        L.orc_cave_dims.argtypes = [C.c_void_p, _PI32]
+        L.orc_cave_populate.argtypes = [C.c_void_p, C.c_int, C.c_int]
+        L.orc_cave_smooth.argtypes = [C.c_void_p, C.c_int]
+        L.orc_cave_floor_ceil.argtypes = [C.c_void_p]
+        L.orc_cave_set_cells.argtypes = [C.c_void_p, _PI32, C.c_int64]
+        L.orc_cave_regions.argtypes = [C.c_void_p, _PI64, _PI64]
+        L.orc_cave_keep_largest.argtypes = [C.c_void_p]
+        L.orc_cave_cells.argtypes = [C.c_void_p, _PI32, C.c_int64]
+        L.orc_cave_cells.restype = C.c_int64
+        L.orc_cave_voxels.argtypes = [C.c_void_p, C.c_int, C.c_int, C.c_int, _PI32, C.c_int64]
+        L.orc_cave_voxels.restype = C.c_int64
         _lib = L
     return _lib
 
@@ -345,3 +359,57 @@ def sort_leaves(origins, *arrays):
         return (origins,) + arrays
     idx = np.lexsort((origins[:, 2], origins[:, 1], origins[:, 0]))
     return (origins[idx],) + tuple(a[idx] for a in arrays)
+
+
+class Cave:
+    """CaveGen restated on a sparse coordinate set (oracle/nm_oracle_cave.cpp)."""
+
+    def __init__(self, map_size, grid_res, fill_percentage, smoothing_count, active_max,
+                 active_min, seed):
+        size = np.ascontiguousarray(map_size, np.float64)
+        self.h = lib().orc_cave_new(dp(size), C.c_double(grid_res), int(fill_percentage),
+                                    int(smoothing_count), int(active_max), int(active_min),
+                                    C.c_uint32(int(seed) & 0xFFFFFFFF))
+
+    def __del__(self):
+        if getattr(self, "h", None):
+            lib().orc_cave_free(self.h)
+            self.h = None
+
+    def dims(self):
+        d = np.zeros(3, np.int32)
+        lib().orc_cave_dims(self.h, d.ctypes.data_as(_PI32))
+        return tuple(int(v) for v in d)
+
+    def populate(self, mode_2d=False, counter=False):
+        lib().orc_cave_populate(self.h, int(mode_2d), int(counter))
+
+    def smooth(self, mode_2d=False):
+        lib().orc_cave_smooth(self.h, int(mode_2d))
+
+    def floor_ceil(self):
+        lib().orc_cave_floor_ceil(self.h)
+
+    def set_cells(self, xyz):
+        v = np.ascontiguousarray(xyz, np.int32).reshape(-1, 3)
+        lib().orc_cave_set_cells(self.h, v.ctypes.data_as(_PI32), len(v))
+
+    def regions(self):
+        n, big = C.c_int64(0), C.c_int64(0)
+        lib().orc_cave_regions(self.h, C.byref(n), C.byref(big))
+        return n.value, big.value
+
+    def keep_largest(self):
+        lib().orc_cave_keep_largest(self.h)
+
+    def cells(self) -> np.ndarray:
+        n = lib().orc_cave_cells(self.h, None, 0)
+        out = np.zeros((max(n, 1), 3), np.int32)
+        lib().orc_cave_cells(self.h, out.ctypes.data_as(_PI32), n)
+        return out[:n]
+
+    def voxels(self, shell=True, half_width=3, closing=1) -> np.ndarray:
+        n = lib().orc_cave_voxels(self.h, int(shell), half_width, closing, None, 0)
+        out = np.zeros((max(n, 1), 3), np.int32)
+        lib().orc_cave_voxels(self.h, int(shell), half_width, closing, out.ctypes.data_as(_PI32), n)
+        return out[:n]
