@@ -383,6 +383,8 @@ def run_ours(args, rank, world, local):
         line["batched"] = run_batched(args, rank, world, local, args.batched_ticks)
     if args.large:
         line["large"] = run_large_section(local)
+    if args.cave:
+        line["cave"] = run_cave_section(local, cpu=(rank == 0 and world == 1 and args.cpu_baseline_s > 0))
     if rank == 0 and world == 1 and args.cpu_baseline_s > 0:
         frames_host = []
         for k in range(30):
@@ -586,6 +588,99 @@ def run_large_section(local, frames=12, warmup=3):
     return out
 
 
+CAVE_WORKLOADS = {
+    # the shipped #cavegenconfig parameters (50 x 50 x 3.5 m at 0.1 m, fill 56 %, 4 smoothing
+    # steps, active 4 4) run through test3DCaveGen's stages
+    "shipped": dict(map_size=(50.0, 50.0, 3.5), grid_res=0.1, fill_percentage=56,
+                    smoothing_count=4, active_max=4, active_min=4, seed=1),
+    # a large cave: 200 x 200 x 20 m at 0.05 m, majority rule (active 13 13), 5 steps
+    "large": dict(map_size=(200.0, 200.0, 20.0), grid_res=0.05, fill_percentage=50,
+                  smoothing_count=5, active_max=13, active_min=13, seed=12345),
+}
+
+
+def cave_stages(g, timer):
+    """test3DCaveGen's stage order; `timer(name, fn)` runs and times each stage."""
+    timer("populate", g.populate)
+    timer("smooth", g.smooth)
+    timer("floor_ceil", g.floor_ceil)
+    timer("regions", g.regions)
+    timer("keep_largest", g.keep_largest)
+    return timer("shell_simmap", lambda: g.simmap(shell=True))
+
+
+def run_cave_section(local, cpu=True, reps=3):
+    """Procedural cave generation (CaveGen): every stage on the device from the fill to the
+    level-set band in a sim map, timed with CUDA events on the library's stream (the CUDA
+    default stream; each stage call waits for its work).  The shipped parameters are also run
+    through the oracle on one host core."""
+    import torch
+
+    from nanomap_b200 import api as A
+    from oracle import oracle as O
+    ctx = A.Context(local)
+    stream = torch.cuda.default_stream()
+    out = {}
+    for name, kw in CAVE_WORKLOADS.items():
+        g = A.Cave(ctx, A.cave_desc(**kw))
+        best = None
+        for _ in range(reps):
+            times = {}
+
+            def timer(stage, fn):
+                e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+                e0.record(stream)
+                r = fn()
+                e1.record(stream)
+                e1.synchronize()
+                times[stage] = e0.elapsed_time(e1)
+                return r
+
+            sm = cave_stages(g, timer)
+            total = sum(times.values())
+            if best is None or total < best[0]:
+                best = (total, dict(times), sm.info())
+            sm.close()
+        total, times, (bbox, nvox, nleaves) = best
+        half, cells = g.dims()
+        # leaf box of the band: the cells' leaves from the first cell to the ceiling, widened
+        # by one leaf on every side (the band reaches 4 voxels past the cells' leaves)
+        lo = (-half[0] + 8, -half[1] + 8, -half[2])
+        hi = (-half[0] + 8 + 8 * max(cells[0] - 1, 0), -half[1] + 8 + 8 * max(cells[1] - 1, 0),
+              half[2])
+        leaf_box = 1
+        for a in range(3):
+            leaf_box *= ((hi[a] >> 3) + 1) - ((lo[a] >> 3) - 1) + 1
+        # algorithmic bytes of the band: 8 face-neighbour steps (closing 1 + 1, half width
+        # 3 + 3) read and write 64 B per leaf, the band difference reads 128 B and writes 64 B
+        band_bytes = leaf_box * (8 * 128 + 192)
+        out[name] = {
+            "config": {k: (list(v) if isinstance(v, tuple) else v) for k, v in kw.items()},
+            "lattice_cells": int(cells[0] * cells[1] * (cells[2] + 1)),
+            "leaf_box": leaf_box, "band_voxels": int(nvox), "band_leaves": int(nleaves),
+            "stage_ms": times, "total_ms": total,
+            "shell_effective_gbs": band_bytes / (times["shell_simmap"] / 1e3) / 1e9,
+        }
+        g.close()
+    if cpu:
+        kw = CAVE_WORKLOADS["shipped"]
+        o = O.Cave(kw["map_size"], kw["grid_res"], kw["fill_percentage"], kw["smoothing_count"],
+                   kw["active_max"], kw["active_min"], kw["seed"])
+        t0 = time.perf_counter()
+        o.populate()
+        o.smooth()
+        o.floor_ceil()
+        o.regions()
+        o.keep_largest()
+        nv = len(o.voxels(shell=True))
+        cpu_ms = (time.perf_counter() - t0) * 1e3
+        out["shipped"]["cpu_oracle_ms"] = cpu_ms
+        out["shipped"]["cpu_oracle_band_voxels"] = nv
+        out["shipped"]["cpu_cores"] = 1
+    ctx.close()
+    return out
+
+
 def batched_agents(spec_small):
     """Sensor mix of the batched tick: (hres, vres, range m, type) per agent."""
     mix = [(320, 240, 5.0, 0)] * 6 + [(640, 480, 10.0, 0)] * 6 + [(1280, 720, 8.0, 0)] * 3 + [(1024, 64, 20.0, 1)]
@@ -731,6 +826,8 @@ def main():
                     help="ticks of the 16-agent batched comparison (0 = skip)")
     ap.add_argument("--large", type=int, default=1,
                     help="1 = also measure the large fine-resolution workload (0.02 m, 1280x720 at 15 m)")
+    ap.add_argument("--cave", type=int, default=1,
+                    help="1 = also measure procedural cave generation (shipped and large caves)")
     ap.add_argument("--extras", type=int, default=1,
                     help="1 = also measure the voxel-filtered insert, expected depth and refinement")
     ap.add_argument("--capacity-log2", type=int, default=21,

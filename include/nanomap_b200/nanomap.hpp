@@ -8,6 +8,7 @@
 //   nanomap::agent::Agent (updatePose, sensorPose, map)       Agent.h:49-210
 //   nanomap::manager::Manager::insertPointCloud               Manager.h:46-72
 //   nanomap::manager::SimManager::updateAgentViews([map])     SimManager.h:68-168
+//   nanomap::mapgen::CaveGen(std::string) and its stages      CaveGen.h:32-68
 // Eigen is not required: Vector3f / Quaternionf below keep Eigen's construction order
 // (Quaternionf(w, x, y, z)) and accessors.  Failures of the library raise nanomap::Error
 // (the reference reports nothing); an unknown sensor name in insertPointCloud is a no-op, as
@@ -22,6 +23,7 @@
 #include <memory>
 #include <stdexcept>
 #include <string>
+#include <unordered_set>
 #include <vector>
 
 #include "../nanomap_b200.h"
@@ -455,4 +457,102 @@ class SimManager {
 };
 
 }  // namespace manager
+
+namespace mapgen {
+
+// nanomap::mapgen::CaveGen (CaveGen.h:32-68) over nm_cave_*: the same stages in the same
+// order give the same cave for the same #cavegenconfig file (the fill reproduces the
+// reference's srand/rand draws without changing the caller's rand() state).  The cells stay
+// on the device; invertAndSave / Save write an NMSIMv1 voxel list (a file_out ending in
+// ".vdb" is written as ".nmsim"; writtenPath() names it) that SimManager's sim grid loader
+// reads, and simMap() hands the cave to a SimManager without a file.
+class CaveGen {
+ public:
+  explicit CaveGen(std::string config) { loadConfig(std::move(config)); }
+
+  // CaveGen::gen (CaveGen.cpp:337-342)
+  void gen() {
+    populateMap();
+    smoothMap();
+    getRegions();
+    invertAndSave();
+  }
+  void populateMap() { detail::check(nm_cave_populate(cave_.get(), 0)); }
+  void populateMap2D() { detail::check(nm_cave_populate(cave_.get(), NM_CAVE_2D)); }
+  void smoothMap() { detail::check(nm_cave_smooth(cave_.get(), 0)); }
+  void smoothMapXY() { detail::check(nm_cave_smooth(cave_.get(), NM_CAVE_2D)); }
+  void setFloorAndCeil() { detail::check(nm_cave_floor_ceil(cave_.get())); }
+  void getRegions() { detail::check(nm_cave_regions(cave_.get(), &regions_, &largest_)); }
+  void keepLargestRegion() { detail::check(nm_cave_keep_largest(cave_.get())); }
+  void addNoise() {}  // empty in the reference (CaveGen.cpp:254-256)
+  // level-set band with topologyToLevelSet's defaults (half width 3, closing 1)
+  void invertAndSave() { save(1); }
+  // the on cells' leaves, voxelised
+  void Save() { save(0); }
+  void loadConfig(std::string file_in) {
+    detail::check(nm_cave_config_load(file_in.c_str(), &desc_));
+    nm_cave c = nullptr;
+    detail::check(nm_cave_create(detail::context(), &desc_, &c));
+    cave_.reset(c, [](nm_cave p) { nm_cave_destroy(p); });
+  }
+  // CaveGen::getActiveNeighbourCount / get2DNeighbourCount (CaveGen.cpp:258-292): on cells
+  // among the 26 (8 in the floor plane) lattice neighbours of voxel (x, y, z) / (x, y).
+  int getActiveNeighbourCount(int x, int y, int z) {
+    const auto on = onCells();
+    int n = 0;
+    for (int dx = -8; dx <= 8; dx += 8)
+      for (int dy = -8; dy <= 8; dy += 8)
+        for (int dz = -8; dz <= 8; dz += 8)
+          if ((dx || dy || dz) && on.count(key(x + dx, y + dy, z + dz))) ++n;
+    return n;
+  }
+  int get2DNeighbourCount(int x, int y) {
+    int32_t half[3];
+    detail::check(nm_cave_dims(cave_.get(), half, nullptr));
+    const auto on = onCells();
+    int n = 0;
+    for (int dx = -8; dx <= 8; dx += 8)
+      for (int dy = -8; dy <= 8; dy += 8)
+        if ((dx || dy) && on.count(key(x + dx, y + dy, -half[2]))) ++n;
+    return n;
+  }
+
+  // additions
+  nm_simmap simMap(bool shell = true) {
+    nm_simmap sm = nullptr;
+    detail::check(nm_cave_simmap(cave_.get(), shell ? 1 : 0, 3, 1, &sm));
+    return sm;  // the caller destroys it (nm_simmap_destroy)
+  }
+  const std::string& writtenPath() const { return written_; }
+  int64_t regionCount() const { return regions_; }
+  int64_t largestRegion() const { return largest_; }
+  const nm_cave_desc& desc() const { return desc_; }
+
+ private:
+  static uint64_t key(int x, int y, int z) {
+    return ((uint64_t)(uint32_t)(x + (1 << 20)) << 42) | ((uint64_t)(uint32_t)(y + (1 << 20)) << 21) |
+           (uint64_t)(uint32_t)(z + (1 << 20));
+  }
+  std::unordered_set<uint64_t> onCells() {
+    int64_t n = 0;
+    detail::check(nm_cave_cells(cave_.get(), nullptr, 0, &n));
+    std::vector<int32_t> xyz((size_t)n * 3 + 3);
+    detail::check(nm_cave_cells(cave_.get(), xyz.data(), n, &n));
+    std::unordered_set<uint64_t> on;
+    for (int64_t q = 0; q < n; ++q) on.insert(key(xyz[3 * q], xyz[3 * q + 1], xyz[3 * q + 2]));
+    return on;
+  }
+  void save(int shell) {
+    char written[512] = {0};
+    detail::check(nm_cave_save(cave_.get(), shell, 3, 1, desc_.file_out, written));
+    written_ = written;
+  }
+
+  nm_cave_desc desc_{};
+  std::shared_ptr<nm_cave_s> cave_;
+  int64_t regions_ = 0, largest_ = 0;
+  std::string written_;
+};
+
+}  // namespace mapgen
 }  // namespace nanomap

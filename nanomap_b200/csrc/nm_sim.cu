@@ -98,65 +98,140 @@ __global__ void k_set_voxels(SimBuild b, const int32_t* ijk, long long n) {
     sim_build_set(b, ijk[3 * i], ijk[3 * i + 1], ijk[3 * i + 2]);
 }
 
-// Pass 1: count non-empty leaves.  Pass 2 (compact != null): give each a compact index,
-// copy its words, set its brick bit and fold its voxels into the active bounding box.
+// Voxel bounds of one 32-bit leaf word q (voxels x*64 + y*8 + z): x = q/2, the word's four
+// bytes are y = 4*(q&1) + 0..3, each byte's bits are z.  mn/mx are leaf-local.
+__device__ __forceinline__ void word_bounds(uint32_t w, int q, int mn[3], int mx[3]) {
+  if (!w) return;
+  const int x = q >> 1, y0 = (q & 1) << 2;
+  const uint32_t zor = (w | (w >> 8) | (w >> 16) | (w >> 24)) & 0xffu;
+  mn[0] = min(mn[0], x);
+  mx[0] = max(mx[0], x);
+  mn[1] = min(mn[1], y0 + ((__ffs(w) - 1) >> 3));
+  mx[1] = max(mx[1], y0 + ((31 - __clz(w)) >> 3));
+  mn[2] = min(mn[2], __ffs(zor) - 1);
+  mx[2] = max(mx[2], 31 - __clz(zor));
+}
+
+// Pass 1: count non-empty leaves (one atomic per block).  Pass 2: give each a compact index
+// (block-wide scan, one atomic per block and iteration), copy its words, set its brick bit
+// (one atomic per distinct brick word in a warp) and fold its voxels into the active bounding
+// box and voxel count (reduced per block, one set of atomics per block).  One thread per leaf.
 __global__ void __launch_bounds__(256) k_compact(SimBuild b, SimMapView v, uint32_t* count,
                                                  int pass2, int32_t* bbox,
                                                  unsigned long long* nvox) {
-  const int lane = threadIdx.x & 31;
-  const long long gw = ((long long)blockIdx.x * blockDim.x + threadIdx.x) >> 5;
-  const long long nw = ((long long)gridDim.x * blockDim.x) >> 5;
+  __shared__ uint32_t s_warp[8];
+  __shared__ uint32_t s_base;
+  __shared__ int s_red[8][6];
+  __shared__ unsigned long long s_cnt[8];
+  const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5;
   const long long total = (long long)b.ldim[0] * b.ldim[1] * b.ldim[2];
-  for (long long pos = gw; pos < total; pos += nw) {
-    const uint32_t w = (lane < 16) ? b.dense[pos * 16 + lane] : 0u;
-    if (__ballot_sync(kFull, w != 0u) == 0u) continue;
-    uint32_t idx = 0;
-    if (lane == 0) idx = atomicAdd(count, 1u);
-    idx = __shfl_sync(kFull, idx, 0);
-    if (!pass2) continue;
-    if (lane < 16) v.leaf_words[(size_t)idx * 16 + lane] = w;
-    const int lz = (int)(pos % b.ldim[2]);
-    const int ly = (int)((pos / b.ldim[2]) % b.ldim[1]);
-    const int lx = (int)(pos / ((long long)b.ldim[2] * b.ldim[1]));
-    const int ox = (b.llo[0] + lx) * 8, oy = (b.llo[1] + ly) * 8, oz = (b.llo[2] + lz) * 8;
-    unsigned cnt = (lane < 16) ? (unsigned)__popc(w) : 0u;
-    // voxel bounds of this leaf from its bits: word l>>5 holds voxel indices x*64+y*8+z
-    int mn[3] = {INT_MAX, INT_MAX, INT_MAX}, mx[3] = {INT_MIN, INT_MIN, INT_MIN};
-    if (lane < 16) {
-      uint32_t ww = w;
-      while (ww) {
-        const int bit = __ffs(ww) - 1;
-        ww &= ww - 1u;
-        const int l = lane * 32 + bit;
-        const int x = ox + (l >> 6), y = oy + ((l >> 3) & 7), z = oz + (l & 7);
-        mn[0] = min(mn[0], x);
-        mn[1] = min(mn[1], y);
-        mn[2] = min(mn[2], z);
-        mx[0] = max(mx[0], x);
-        mx[1] = max(mx[1], y);
-        mx[2] = max(mx[2], z);
-      }
-    }
+  const long long stride = (long long)gridDim.x * blockDim.x;
+  const uint4* src = reinterpret_cast<const uint4*>(b.dense);
+  int mn[3] = {INT_MAX, INT_MAX, INT_MAX}, mx[3] = {INT_MIN, INT_MIN, INT_MIN};
+  unsigned long long cnt = 0;
+  uint32_t nonempty = 0;
+  // every thread runs the same number of iterations so the block-wide scan stays uniform
+  for (long long base = (long long)blockIdx.x * blockDim.x; base < total; base += stride) {
+    const long long pos = base + threadIdx.x;
+    uint4 w[4] = {};
+    if (pos < total) {
 #pragma unroll
-    for (int o = 16; o > 0; o >>= 1) {
-      cnt += __shfl_xor_sync(kFull, cnt, o);
-#pragma unroll
-      for (int a = 0; a < 3; ++a) {
-        mn[a] = min(mn[a], __shfl_xor_sync(kFull, mn[a], o));
-        mx[a] = max(mx[a], __shfl_xor_sync(kFull, mx[a], o));
-      }
+      for (int i = 0; i < 4; ++i) w[i] = __ldg(&src[pos * 4 + i]);
     }
-    if (lane == 0) {
+    const bool any = (w[0].x | w[0].y | w[0].z | w[0].w | w[1].x | w[1].y | w[1].z | w[1].w |
+                      w[2].x | w[2].y | w[2].z | w[2].w | w[3].x | w[3].y | w[3].z | w[3].w) != 0u;
+    if (!pass2) {
+      nonempty += any ? 1u : 0u;
+      continue;
+    }
+    const unsigned ball = __ballot_sync(kFull, any);
+    if (lane == 0) s_warp[warp] = __popc(ball);
+    __syncthreads();
+    if (threadIdx.x == 0) {
+      uint32_t sum = 0;
+      for (int i = 0; i < 8; ++i) {
+        const uint32_t c = s_warp[i];
+        s_warp[i] = sum;
+        sum += c;
+      }
+      s_base = sum ? atomicAdd(count, sum) : 0u;
+    }
+    __syncthreads();
+    const uint32_t idx = s_base + s_warp[warp] + __popc(ball & ((1u << lane) - 1u));
+    __syncthreads();  // s_warp / s_base are rewritten by the next iteration
+    uint32_t bword = 0xffffffffu, bbit = 0u;
+    if (any) {
+      uint4* dst = reinterpret_cast<uint4*>(v.leaf_words) + (size_t)idx * 4;
+#pragma unroll
+      for (int i = 0; i < 4; ++i) dst[i] = w[i];
       v.leaf_index[pos] = (int32_t)idx;
+      const int lz = (int)(pos % b.ldim[2]);
+      const int ly = (int)((pos / b.ldim[2]) % b.ldim[1]);
+      const int lx = (int)(pos / ((long long)b.ldim[2] * b.ldim[1]));
       const int bx = lx + b.llo[0], by = ly + b.llo[1], bz = lz + b.llo[2];
       const long long bpos = ((long long)((bx >> 3) - v.blo[0]) * v.bdim[1] + ((by >> 3) - v.blo[1])) *
                                  v.bdim[2] + ((bz >> 3) - v.blo[2]);
-      atomicOr(&v.brick_bits[bpos >> 5], 1u << (bpos & 31));
-      for (int a = 0; a < 3; ++a) {
-        atomicMin(&bbox[a], mn[a]);
-        atomicMax(&bbox[3 + a], mx[a]);
+      bword = (uint32_t)(bpos >> 5);
+      bbit = 1u << (bpos & 31);
+      int lmn[3] = {8, 8, 8}, lmx[3] = {-1, -1, -1};
+      const uint32_t ww[16] = {w[0].x, w[0].y, w[0].z, w[0].w, w[1].x, w[1].y, w[1].z, w[1].w,
+                               w[2].x, w[2].y, w[2].z, w[2].w, w[3].x, w[3].y, w[3].z, w[3].w};
+#pragma unroll
+      for (int q = 0; q < 16; ++q) {
+        cnt += (unsigned)__popc(ww[q]);
+        word_bounds(ww[q], q, lmn, lmx);
       }
-      atomicAdd(nvox, (unsigned long long)cnt);
+      const int o[3] = {bx * 8, by * 8, bz * 8};
+#pragma unroll
+      for (int a = 0; a < 3; ++a) {
+        mn[a] = min(mn[a], o[a] + lmn[a]);
+        mx[a] = max(mx[a], o[a] + lmx[a]);
+      }
+    }
+    // brick bits: lanes of one warp that hit the same word OR their bits, the lowest sets them
+    const unsigned peers = __match_any_sync(kFull, bword);
+    const uint32_t bits = __reduce_or_sync(peers, bbit);
+    if (any && lane == __ffs(peers) - 1) atomicOr(&v.brick_bits[bword], bits);
+  }
+  if (!pass2) {
+#pragma unroll
+    for (int o = 16; o > 0; o >>= 1) nonempty += __shfl_xor_sync(kFull, nonempty, o);
+    if (lane == 0 && nonempty) atomicAdd(count, nonempty);
+    return;
+  }
+#pragma unroll
+  for (int o = 16; o > 0; o >>= 1) {
+    cnt += __shfl_xor_sync(kFull, cnt, o);
+#pragma unroll
+    for (int a = 0; a < 3; ++a) {
+      mn[a] = min(mn[a], __shfl_xor_sync(kFull, mn[a], o));
+      mx[a] = max(mx[a], __shfl_xor_sync(kFull, mx[a], o));
+    }
+  }
+  if (lane == 0) {
+    s_cnt[warp] = cnt;
+    for (int a = 0; a < 3; ++a) {
+      s_red[warp][a] = mn[a];
+      s_red[warp][3 + a] = mx[a];
+    }
+  }
+  __syncthreads();
+  if (threadIdx.x == 0) {
+    unsigned long long c = 0;
+    int bmn[3] = {INT_MAX, INT_MAX, INT_MAX}, bmx[3] = {INT_MIN, INT_MIN, INT_MIN};
+    for (int i = 0; i < (int)(blockDim.x >> 5); ++i) {
+      c += s_cnt[i];
+      for (int a = 0; a < 3; ++a) {
+        bmn[a] = min(bmn[a], s_red[i][a]);
+        bmx[a] = max(bmx[a], s_red[i][3 + a]);
+      }
+    }
+    if (c) {
+      atomicAdd(nvox, c);
+      for (int a = 0; a < 3; ++a) {
+        atomicMin(&bbox[a], bmn[a]);
+        atomicMax(&bbox[3 + a], bmx[a]);
+      }
     }
   }
 }
@@ -490,7 +565,7 @@ cudaError_t launch_set_voxels(const SimBuild& b, const int32_t* d_ijk, long long
 
 cudaError_t launch_compact(const SimBuild& b, const SimMapView& v, uint32_t* d_count, int pass2,
                            int32_t* d_bbox, unsigned long long* d_nvox, cudaStream_t s) {
-  k_compact<<<2368, 256, 0, s>>>(b, v, d_count, pass2, d_bbox, d_nvox);
+  k_compact<<<1184, 256, 0, s>>>(b, v, d_count, pass2, d_bbox, d_nvox);
   return cudaGetLastError();
 }
 

@@ -152,3 +152,55 @@ def test_cave_raycast_from_inside(ctx):
     assert np.all(d >= 0)
     assert np.mean(d > 0) > 0.5
     sm.close()
+
+
+def read_nmsim(path):
+    import struct
+    with open(path, "rb") as f:
+        magic = f.read(8)
+        res, = struct.unpack("<f", f.read(4))
+        n, = struct.unpack("<q", f.read(8))
+        v = np.frombuffer(f.read(12 * n), np.int32).reshape(n, 3)
+    assert magic == b"NMSIMv1\0"
+    idx = np.lexsort((v[:, 2], v[:, 1], v[:, 0]))
+    return res, v[idx]
+
+
+@pytest.mark.parametrize("mode", ["3d", "2d", "gen"])
+def test_cavegen_facade_program(ctx, tmp_path, mode):
+    """The reference's generator mains, written against nanomap::mapgen::CaveGen, give the
+    oracle's cave for the same #cavegenconfig file (seed string hashed as the reference does)."""
+    import subprocess
+    from pathlib import Path
+    root = Path(__file__).resolve().parents[1]
+    cfg = tmp_path / "cave.txt"
+    active = "13 13" if mode == "3d" else "4 4"
+    cfg.write_text(f"#cavegenconfig\nfile_out {tmp_path / 'map1.vdb'}\nmap_size 16 12 3.2\n"
+                   f"grid_res 0.1\nfill_percentage 50\nsmoothing_count 4\nactive {active}\n"
+                   "random_seed 0\nseed nanomap\n")
+    exe = tmp_path / "cavegen_demo"
+    subprocess.run(["g++", "-std=c++17", "-O2", f"-I{root / 'include'}",
+                    str(root / "tests" / "cpp" / "cavegen_demo.cpp"), f"-L{root / 'nanomap_b200'}",
+                    "-lnanomap_b200", f"-Wl,-rpath,{root / 'nanomap_b200'}", "-o", str(exe)],
+                   check=True)
+    out = subprocess.run([str(exe), str(cfg), mode], capture_output=True, text=True)
+    assert out.returncode == 0, out.stderr
+    written, n_regions, largest = out.stdout.split()
+    assert written == str(tmp_path / "map1.nmsim")
+    d = A.load_cave_config(cfg)
+    o = O.Cave(list(d.map_size), d.grid_res, d.fill_percentage, d.smoothing_count,
+               d.active_max, d.active_min, d.seed)
+    if mode == "2d":
+        o.populate(mode_2d=True)
+        o.smooth(mode_2d=True)
+    else:
+        o.populate()
+        o.smooth()
+        if mode == "3d":
+            o.floor_ceil()
+    assert (int(n_regions), int(largest)) == o.regions()
+    if mode != "gen":
+        o.keep_largest()
+    res, v = read_nmsim(written)
+    assert res == np.float32(0.1)
+    assert np.array_equal(v, o.voxels(shell=True))
