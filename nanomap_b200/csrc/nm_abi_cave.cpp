@@ -2,11 +2,16 @@
 // nanomap::mapgen::CaveGen, CaveGen.h:32-68 / CaveGen.cpp).
 //
 // The cell lattice stays on the device between stages.  The reference's fill draws
-// rand() % 100 per cell after srand(seed) in x, y, z loop order (CaveGen.cpp:31-42, 66-79);
-// that sequence is drawn here with the C library's reentrant generator (initstate_r with a
-// 128-byte state, the state size behind srand/rand) so that the same seed gives the same cave
-// without touching the caller's rand() state.  NM_CAVE_COUNTER_RNG fills on the device
-// instead.  Every later stage runs on the device; the result is a device sim map.
+// rand() % 100 per cell after srand(seed) in x, y, z loop order (CaveGen.cpp:31-42, 66-79).
+// The C library's generator (glibc's default, a 128-byte state) is the additive feedback
+// generator r[i] = r[i-31] + r[i-3] mod 2^32 with output r[i] >> 1, seeded by
+// r[0] = seed (1 for 0), r[i] = 16807 r[i-1] mod (2^31 - 1) for i < 31, r[i] = r[i-31] for
+// i < 34, and 310 discarded draws.  It is linear, so the device draws it in parallel: the host
+// seeds it, checks its first draws against the C library's own reentrant generator
+// (initstate_r / random_r, which leaves the caller's rand() state alone) and builds jump
+// matrices; each device thread jumps to its chunk.  NM_CAVE_COUNTER_RNG fills from a
+// counter-based generator instead.  Every later stage runs on the device; the result is a
+// device sim map.
 #include <algorithm>
 #include <array>
 #include <cfenv>
@@ -35,6 +40,14 @@ struct nm_cave_s {
   uint32_t* d_size = nullptr;
   unsigned long long* d_min_key = nullptr;
   nm::CaveStats* d_stats = nullptr;
+  bool regions_valid = false;  // the region labels describe the current cells
+  nm::CaveStats stats{};
+  // scratch kept between calls: the shell's three leaf-box buffers and the fill's jump
+  // matrices (grown on demand, freed with the cave)
+  uint32_t* shell_buf[3] = {nullptr, nullptr, nullptr};
+  size_t shell_bytes[3] = {0, 0, 0};
+  uint32_t* fill_buf = nullptr;
+  size_t fill_bytes = 0;
 };
 
 namespace nm {
@@ -49,6 +62,8 @@ void release(nm_cave c) {
   cudaFree(c->d_size);
   cudaFree(c->d_min_key);
   cudaFree(c->d_stats);
+  for (int i = 0; i < 3; ++i) cudaFree(c->shell_buf[i]);
+  cudaFree(c->fill_buf);
   delete c;
   release(ctx);
 }
@@ -102,6 +117,17 @@ void cave_leaf_box(const nm::CaveLattice& L, int margin, int32_t llo[3], int32_t
   }
 }
 
+// Grow a scratch buffer to at least `bytes` (contents not kept).
+cudaError_t grow(uint32_t** buf, size_t* have, size_t bytes) {
+  if (*buf && *have >= bytes) return cudaSuccess;
+  cudaFree(*buf);
+  *buf = nullptr;
+  *have = 0;
+  const cudaError_t e = cudaMalloc((void**)buf, bytes);
+  if (e == cudaSuccess) *have = bytes;
+  return e;
+}
+
 int build_cave_simmap(nm_cave c, int shell, int half_width, int closing, nm_simmap* out) {
   if (!c || !out) return fail(NM_ERR_ARG, "null argument");
   *out = nullptr;
@@ -113,72 +139,125 @@ int build_cave_simmap(nm_cave c, int shell, int half_width, int closing, nm_simm
   const int reach = shell ? closing + half_width : 0;
   int32_t llo[3], ldim[3], vmin[3], vmax[3];
   cave_leaf_box(c->L, reach / 8 + 1, llo, ldim);
+  long long nleaf = 1;
   for (int a = 0; a < 3; ++a) {
     vmin[a] = llo[a] * 8;
     vmax[a] = (llo[a] + ldim[a]) * 8;
+    nleaf *= ldim[a];
   }
+  if (nleaf > (1ll << 32)) return fail(NM_ERR_CAPACITY, "cave leaf box has %lld leaves", nleaf);
+  // the tiles need one leaf-box buffer, the shell three
+  const size_t bytes = (size_t)nleaf * 64;
+  for (int i = 0; i < (shell ? 3 : 1); ++i) {
+    const cudaError_t e = grow(&c->shell_buf[i], &c->shell_bytes[i], bytes);
+    if (e != cudaSuccess)
+      return fail(NM_ERR_CUDA, "cave shell buffers (%lld leaves): %s", nleaf,
+                  cudaGetErrorString(e));
+  }
+  uint32_t* buf[3] = {c->shell_buf[0], c->shell_buf[1], c->shell_buf[2]};
   std::unique_ptr<nm_simmap_s> sm(new nm_simmap_s());
   sm->ctx = ctx;
   nm::SimBuild b{};
-  int rc = nm::begin_build((float)c->desc.grid_res, vmin, vmax, &b, s);
+  int rc = nm::begin_build((float)c->desc.grid_res, vmin, vmax, &b, s, buf[0]);
   if (rc != NM_OK) return rc;
   NM_CUDA(nm::launch_cave_tiles(current(c), b.dense, b.llo, b.ldim, s));
   if (shell) {
-    const long long nleaf = (long long)b.ldim[0] * b.ldim[1] * b.ldim[2];
-    uint32_t* buf[3] = {b.dense, nullptr, nullptr};
-    for (int i = 1; i < 3; ++i) {
-      const cudaError_t e = cudaMalloc((void**)&buf[i], (size_t)nleaf * 64);
-      if (e != cudaSuccess) {
-        cudaFree(buf[1]);
-        cudaFree(b.dense);
-        return fail(NM_ERR_CUDA, "cave shell buffers (%lld leaves): %s", nleaf,
-                    cudaGetErrorString(e));
-      }
-    }
-    cudaError_t e = cudaSuccess;
     // closing: M = erode^c(dilate^c(T)), ping-pong between buf[0] and buf[1]; 2c steps end
     // in buf[0]
     int m = 0;
-    for (int i = 0; i < 2 * closing && e == cudaSuccess; ++i) {
-      e = nm::launch_leaf_morph(buf[m], buf[1 - m], b.ldim, i >= closing, s);
+    for (int i = 0; i < 2 * closing; ++i) {
+      NM_CUDA(nm::launch_leaf_morph(buf[m], buf[1 - m], b.ldim, i >= closing, s));
       m = 1 - m;
     }
     // E = erode^h(M) into buf[1] / buf[2]; D = dilate^h(M) through the buffer E left free
     // and buf[0] (M is not needed after D's first step); band = D & ~E
     int e_buf = 1;
-    for (int i = 0; i < half_width && e == cudaSuccess; ++i) {
+    for (int i = 0; i < half_width; ++i) {
       const int src = (i == 0) ? 0 : e_buf;
       const int dst = (i == 0) ? 1 : 3 - e_buf;
-      e = nm::launch_leaf_morph(buf[src], buf[dst], b.ldim, 1, s);
+      NM_CUDA(nm::launch_leaf_morph(buf[src], buf[dst], b.ldim, 1, s));
       e_buf = dst;
     }
     const int free_buf = 3 - e_buf;
     int d_buf = 0;
-    for (int i = 0; i < half_width && e == cudaSuccess; ++i) {
+    for (int i = 0; i < half_width; ++i) {
       const int dst = (d_buf == 0) ? free_buf : 0;
-      e = nm::launch_leaf_morph(buf[d_buf], buf[dst], b.ldim, 0, s);
+      NM_CUDA(nm::launch_leaf_morph(buf[d_buf], buf[dst], b.ldim, 0, s));
       d_buf = dst;
     }
-    if (e == cudaSuccess) e = nm::launch_leaf_andnot(buf[d_buf], buf[e_buf], buf[d_buf], nleaf, s);
-    if (e != cudaSuccess) {
-      for (int i = 0; i < 3; ++i) cudaFree(buf[i]);
-      return fail(NM_ERR_CUDA, "cave shell: %s", cudaGetErrorString(e));
-    }
-    // the band buffer becomes the build buffer; the others go once the stream has used them
-    const cudaError_t se = cudaStreamSynchronize(s);
-    for (int i = 0; i < 3; ++i)
-      if (i != d_buf) cudaFree(buf[i]);
-    b.dense = buf[d_buf];
-    if (se != cudaSuccess) {
-      cudaFree(b.dense);
-      return fail(NM_ERR_CUDA, "cave shell: %s", cudaGetErrorString(se));
-    }
+    NM_CUDA(nm::launch_leaf_andnot(buf[d_buf], buf[e_buf], buf[d_buf], nleaf, s));
+    b.dense = buf[d_buf];  // still borrowed: the build compacts it and leaves it to the cave
   }
   rc = nm::finish_build(ctx, b, sm.get(), s);
   if (rc != NM_OK) return rc;
   nm::retain(ctx);
   *out = sm.release();
   return NM_OK;
+}
+
+// Seeded state of the C library generator: the 31 words before the first draw.
+void libc_state(uint32_t seed, uint32_t state[31]) {
+  int32_t r[344];
+  r[0] = (int32_t)(seed == 0 ? 1u : seed);
+  for (int i = 1; i < 31; ++i) {
+    long long v = (16807LL * r[i - 1]) % 2147483647LL;
+    if (v < 0) v += 2147483647LL;
+    r[i] = (int32_t)v;
+  }
+  for (int i = 31; i < 34; ++i) r[i] = r[i - 31];
+  for (int i = 34; i < 344; ++i) r[i] = (int32_t)((uint32_t)r[i - 31] + (uint32_t)r[i - 3]);
+  for (int q = 0; q < 31; ++q) state[q] = (uint32_t)r[313 + q];
+}
+
+// The first draws from `state` must equal the C library's for this seed.
+bool libc_state_matches(uint32_t seed, const uint32_t state[31]) {
+  struct random_data rd;
+  std::memset(&rd, 0, sizeof(rd));
+  alignas(8) char buf[128];
+  std::memset(buf, 0, sizeof(buf));
+  if (initstate_r(seed, buf, sizeof(buf), &rd) != 0) return false;
+  std::vector<uint32_t> r(state, state + 31);
+  for (int k = 0; k < 200; ++k) {
+    const uint32_t v = r[r.size() - 31] + r[r.size() - 3];
+    r.push_back(v);
+    int32_t want = 0;
+    random_r(&rd, &want);
+    if ((int32_t)(v >> 1) != want) return false;
+  }
+  return true;
+}
+
+using Mat31 = std::array<uint32_t, 961>;
+
+Mat31 mat_mul(const Mat31& X, const Mat31& Y) {
+  Mat31 Z{};
+  for (int a = 0; a < 31; ++a)
+    for (int c = 0; c < 31; ++c) {
+      const uint32_t x = X[a * 31 + c];
+      if (!x) continue;
+      for (int b = 0; b < 31; ++b) Z[a * 31 + b] += x * Y[c * 31 + b];
+    }
+  return Z;
+}
+
+// A^(kLibcChunk * 2^j) for j < n, A the one-draw step of the state (r[i-31] .. r[i-1]).
+std::vector<uint32_t> libc_jump_mats(int n) {
+  Mat31 A{};
+  for (int m = 0; m < 30; ++m) A[m * 31 + m + 1] = 1u;
+  A[30 * 31 + 0] = 1u;
+  A[30 * 31 + 28] = 1u;
+  Mat31 P{}, B = A;
+  for (int q = 0; q < 31; ++q) P[q * 31 + q] = 1u;
+  for (int e = nm::kLibcChunk; e > 0; e >>= 1) {
+    if (e & 1) P = mat_mul(P, B);
+    B = mat_mul(B, B);
+  }
+  std::vector<uint32_t> out((size_t)n * 961);
+  for (int j = 0; j < n; ++j) {
+    std::copy(P.begin(), P.end(), out.begin() + (size_t)j * 961);
+    P = mat_mul(P, P);
+  }
+  return out;
 }
 
 int check_cave(nm_cave c) {
@@ -188,12 +267,18 @@ int check_cave(nm_cave c) {
 }
 
 int run_regions(nm_cave c, nm::CaveStats* st) {
+  if (c->regions_valid) {
+    *st = c->stats;
+    return NM_OK;
+  }
   cudaStream_t s = c->ctx->stream;
   NM_CUDA(nm::launch_cave_regions(current(c), c->d_parent, c->d_size, c->d_min_key, c->d_stats,
                                   s));
   NM_CUDA(cudaMemcpyAsync(st, c->d_stats, sizeof(*st), cudaMemcpyDeviceToHost, s));
   NM_CUDA(cudaStreamSynchronize(s));
   if (st->error) return fail(NM_ERR_TIMEOUT, "cave regions: a union gave up after its limit");
+  c->stats = *st;
+  c->regions_valid = true;
   return NM_OK;
 }
 
@@ -257,6 +342,7 @@ int nm_cave_dims(nm_cave c, int32_t half[3], int32_t cells[3]) {
 int nm_cave_populate(nm_cave c, uint32_t flags) {
   int rc = check_cave(c);
   if (rc != NM_OK) return rc;
+  c->regions_valid = false;
   cudaStream_t s = c->ctx->stream;
   const int mode_2d = (flags & NM_CAVE_2D) ? 1 : 0;
   c->cur = 0;
@@ -267,31 +353,32 @@ int nm_cave_populate(nm_cave c, uint32_t flags) {
     return NM_OK;
   }
   const long long n = nm::cave_cell_count(L);
-  std::vector<uint8_t> cells((size_t)std::max<long long>(n, 1), 0);
-  struct random_data rd;
-  std::memset(&rd, 0, sizeof(rd));
-  alignas(8) char state[128];
-  std::memset(state, 0, sizeof(state));
-  if (initstate_r(c->desc.seed, state, sizeof(state), &rd) != 0)
-    return fail(NM_ERR_STATE, "initstate_r failed");
-  const int nzp = L.nz + 1;
-  for (int i = 0; i < L.nx; ++i)
-    for (int j = 0; j < L.ny; ++j) {
-      const size_t col = ((size_t)i * L.ny + j) * nzp;
-      if (mode_2d) {
-        int32_t r = 0;
-        random_r(&rd, &r);
-        const uint8_t v = (r % 100 < c->desc.fill_percentage) ? 1 : 0;
-        for (int k = 0; k < L.nz; ++k) cells[col + k] = v;
-      } else {
-        for (int k = 1; k < L.kf; ++k) {
-          int32_t r = 0;
-          random_r(&rd, &r);
-          cells[col + k] = (r % 100 < c->desc.fill_percentage) ? 1 : 0;
-        }
-      }
-    }
-  NM_CUDA(cudaMemcpyAsync(L.cells, cells.data(), cells.size(), cudaMemcpyHostToDevice, s));
+  const long long n_draws = mode_2d ? (long long)L.nx * L.ny
+                                    : (L.kf > 1 ? (long long)L.nx * L.ny * (L.kf - 1) : 0);
+  uint32_t state[31];
+  libc_state(c->desc.seed, state);
+  if (!libc_state_matches(c->desc.seed, state))
+    return fail(NM_ERR_UNSUPPORTED,
+                "the C library's rand() sequence is not the additive feedback generator this "
+                "fill reproduces; use NM_CAVE_COUNTER_RNG");
+  NM_CUDA(cudaMemsetAsync(L.cells, 0, (size_t)std::max<long long>(n, 1), s));
+  if (n_draws > 0) {
+    const long long nchunks = (n_draws + nm::kLibcChunk - 1) / nm::kLibcChunk;
+    int nmats = 1;
+    while ((1ll << nmats) < nchunks) ++nmats;
+    const std::vector<uint32_t> mats = libc_jump_mats(nmats);
+    cudaError_t e = grow(&c->fill_buf, &c->fill_bytes, (mats.size() + 31) * 4);
+    uint32_t* d_buf = c->fill_buf;
+    if (e == cudaSuccess)
+      e = cudaMemcpyAsync(d_buf, mats.data(), mats.size() * 4, cudaMemcpyHostToDevice, s);
+    if (e == cudaSuccess)
+      e = cudaMemcpyAsync(d_buf + mats.size(), state, 31 * 4, cudaMemcpyHostToDevice, s);
+    if (e == cudaSuccess)
+      e = nm::launch_cave_fill_libc(L, d_buf, nmats, d_buf + mats.size(), n_draws,
+                                    c->desc.fill_percentage, mode_2d, s);
+    if (e == cudaSuccess) e = cudaStreamSynchronize(s);
+    if (e != cudaSuccess) return fail(NM_ERR_CUDA, "cave fill: %s", cudaGetErrorString(e));
+  }
   NM_CUDA(cudaStreamSynchronize(s));
   return NM_OK;
 }
@@ -299,6 +386,7 @@ int nm_cave_populate(nm_cave c, uint32_t flags) {
 int nm_cave_smooth(nm_cave c, uint32_t flags) {
   int rc = check_cave(c);
   if (rc != NM_OK) return rc;
+  c->regions_valid = false;
   cudaStream_t s = c->ctx->stream;
   const int mode_2d = (flags & NM_CAVE_2D) ? 1 : 0;
   for (int it = 0; it < c->desc.smoothing_count; ++it) {
@@ -314,6 +402,7 @@ int nm_cave_smooth(nm_cave c, uint32_t flags) {
 int nm_cave_floor_ceil(nm_cave c) {
   int rc = check_cave(c);
   if (rc != NM_OK) return rc;
+  c->regions_valid = false;
   NM_CUDA(nm::launch_cave_floor_ceil(current(c), c->ctx->stream));
   NM_CUDA(cudaStreamSynchronize(c->ctx->stream));
   return NM_OK;
@@ -336,6 +425,7 @@ int nm_cave_keep_largest(nm_cave c) {
   nm::CaveStats st{};
   rc = run_regions(c, &st);
   if (rc != NM_OK) return rc;
+  c->regions_valid = false;
   NM_CUDA(nm::launch_cave_keep(current(c), c->d_parent, c->d_min_key, c->d_stats,
                                c->ctx->stream));
   NM_CUDA(cudaStreamSynchronize(c->ctx->stream));

@@ -65,7 +65,7 @@ int finish_build(nm_context ctx, nm::SimBuild& b, nm_simmap sm, cudaStream_t s) 
   cudaFree(d_count);
   cudaFree(d_bbox);
   cudaFree(d_nvox);
-  cudaFree(b.dense);
+  if (!b.borrowed) cudaFree(b.dense);
   b.dense = nullptr;
   sm->leaves = nleaves;
   sm->active_voxels = nvox;
@@ -84,7 +84,7 @@ int finish_build(nm_context ctx, nm::SimBuild& b, nm_simmap sm, cudaStream_t s) 
 }
 
 int begin_build(float res, const int32_t vmin[3], const int32_t vmax[3], nm::SimBuild* b,
-                cudaStream_t s) {
+                cudaStream_t s, uint32_t* buffer) {
   b->res = res;
   long long prod = 1;
   for (int a = 0; a < 3; ++a) {
@@ -98,8 +98,9 @@ int begin_build(float res, const int32_t vmin[3], const int32_t vmax[3], nm::Sim
     prod *= b->ldim[a];
   }
   if (prod > (1ll << 32)) return fail(NM_ERR_CAPACITY, "voxel region has %lld leaves", prod);
-  b->dense = nullptr;
-  NM_CUDA(cudaMalloc((void**)&b->dense, (size_t)prod * 64));
+  b->dense = buffer;
+  b->borrowed = buffer ? 1 : 0;
+  if (!buffer) NM_CUDA(cudaMalloc((void**)&b->dense, (size_t)prod * 64));
   NM_CUDA(cudaMemsetAsync(b->dense, 0, (size_t)prod * 64, s));
   return NM_OK;
 }

@@ -9,6 +9,7 @@
 //   k_cc_*             6-connected regions by lock-free union-find (CaveGen::getRegions)
 //   k_cave_tiles       cells -> whole leaves (addTile(1, ...) + voxelizeActiveTiles)
 //   k_leaf_morph       one dilation or erosion step on 64-bit x-slices of the leaves
+//   k_compact (nm_sim.cu) compacts the band into the sim map
 #include <climits>
 #include <cstdint>
 
@@ -58,6 +59,59 @@ __global__ void k_cave_fill(CaveLattice L, uint32_t seed, int pct, int mode_2d) 
       on = (int)((uint32_t)(h >> 32) % 100u) < pct;
     }
     L.cells[c] = on ? 1 : 0;
+  }
+}
+
+// Draw d of the reference's fill loops: 3-D, d = ((i * ny) + j) * (kf - 1) + (k - 1) over the
+// fill planes k in [1, kf); 2-D, d = i * ny + j for the whole column below the ceiling.  The
+// cells start cleared.
+__global__ void k_cave_fill_libc(CaveLattice L, const uint32_t* __restrict__ mats, int nmats,
+                                 const uint32_t* __restrict__ state0, long long n_draws, int pct,
+                                 int mode_2d) {
+  const long long nchunks = (n_draws + kLibcChunk - 1) / kLibcChunk;
+  const int nzp = L.nz + 1;
+  const int nfill = L.kf - 1;
+  for (long long t = (long long)blockIdx.x * blockDim.x + threadIdx.x; t < nchunks;
+       t += (long long)gridDim.x * blockDim.x) {
+    uint32_t r[31];
+#pragma unroll
+    for (int q = 0; q < 31; ++q) r[q] = __ldg(&state0[q]);
+    for (int j = 0; j < nmats; ++j) {
+      if (!((t >> j) & 1)) continue;
+      const uint32_t* M = mats + (size_t)j * 961;
+      uint32_t y[31];
+#pragma unroll
+      for (int a = 0; a < 31; ++a) {
+        uint32_t acc = 0u;
+#pragma unroll
+        for (int b = 0; b < 31; ++b) acc += __ldg(&M[a * 31 + b]) * r[b];
+        y[a] = acc;
+      }
+#pragma unroll
+      for (int q = 0; q < 31; ++q) r[q] = y[q];
+    }
+    // r[q] holds the word 31 - q draws back; the oldest word sits at slot p and is replaced by
+    // the new one, with slot (p + 28) mod 31 holding the word 3 back
+    long long d = t * kLibcChunk;
+    for (int g = 0; g < kLibcChunk / 31; ++g) {
+#pragma unroll
+      for (int p = 0; p < 31; ++p) {
+        const uint32_t v = r[p] + r[(p + 28) % 31];
+        r[p] = v;
+        const long long dd = d + p;
+        if (dd < n_draws) {
+          const uint8_t on = ((int)((v >> 1) % 100u) < pct) ? 1 : 0;
+          if (mode_2d) {
+            uint8_t* col = L.cells + dd * nzp;
+            for (int k = 0; k < L.nz; ++k) col[k] = on;
+          } else {
+            const long long c = (dd / nfill) * nzp + 1 + (dd % nfill);
+            L.cells[c] = on;
+          }
+        }
+      }
+      d += 31;
+    }
   }
 }
 
@@ -170,9 +224,32 @@ __global__ void k_cc_init(CaveLattice L, int32_t* parent, uint32_t* size,
   }
   for (long long c = (long long)blockIdx.x * blockDim.x + threadIdx.x; c < n;
        c += (long long)gridDim.x * blockDim.x) {
-    parent[c] = L.cells[c] ? (int)c : -1;
     size[c] = 0;
     min_key[c] = ~0ull;
+  }
+}
+
+// One thread per column: every on cell is linked to the lowest cell of its vertical run (the
+// ceiling joins the run below it only where it is a face neighbour), so runs are depth-1
+// trees and the unions below are needed along x and y only.
+__global__ void k_cc_columns(CaveLattice L, int32_t* parent) {
+  const long long ncol = (long long)L.nx * L.ny;
+  const int nzp = L.nz + 1;
+  for (long long col = (long long)blockIdx.x * blockDim.x + threadIdx.x; col < ncol;
+       col += (long long)gridDim.x * blockDim.x) {
+    const long long c0 = col * nzp;
+    int bottom = -1;
+    for (int k = 0; k < nzp; ++k) {
+      const long long c = c0 + k;
+      const bool joins = k > 0 && (k < L.nz || L.ceil_adjacent);
+      if (!L.cells[c]) {
+        parent[c] = -1;
+        bottom = -1;
+        continue;
+      }
+      if (bottom < 0 || !joins) bottom = (int)c;
+      parent[c] = bottom;
+    }
   }
 }
 
@@ -187,23 +264,37 @@ __global__ void k_cc_union(CaveLattice L, int32_t* parent, CaveStats* stats) {
     if (i + 1 < L.nx && L.cells[c + (long long)L.ny * nzp])
       cc_union(parent, (int)c, (int)(c + (long long)L.ny * nzp), &stats->error);
     if (j + 1 < L.ny && L.cells[c + nzp]) cc_union(parent, (int)c, (int)(c + nzp), &stats->error);
-    const bool zn = (k + 1 < L.nz) || (k + 1 == L.nz && L.ceil_adjacent);
-    if (zn && L.cells[c + 1]) cc_union(parent, (int)c, (int)(c + 1), &stats->error);
   }
 }
 
+// Region sizes and smallest order keys.  Neighbouring cells mostly share a root, so the lanes
+// of a warp with the same root combine their count and key before one lane updates the root.
 __global__ void k_cc_flatten(CaveLattice L, int32_t* parent, uint32_t* size,
                              unsigned long long* min_key) {
   const long long n = cave_cell_count(L);
-  for (long long c = (long long)blockIdx.x * blockDim.x + threadIdx.x; c < n;
-       c += (long long)gridDim.x * blockDim.x) {
-    if (!L.cells[c]) continue;
-    const int r = cc_find(parent, (int)c);
-    int i, j, k, x, y, z;
-    cell_ijk(L, c, &i, &j, &k);
-    cave_cell_xyz(L, i, j, k, &x, &y, &z);
-    atomicAdd(&size[r], 1u);
-    atomicMin(&min_key[r], vdb_order_key(x, y, z));
+  const long long stride = (long long)gridDim.x * blockDim.x;
+  const int lane = threadIdx.x & 31;
+  for (long long base = (long long)blockIdx.x * blockDim.x; base < n; base += stride) {
+    const long long c = base + threadIdx.x;
+    const bool on = c < n && L.cells[c];
+    int r = -1;
+    uint32_t hi = 0xffffffffu, lo = 0xffffffffu;
+    if (on) {
+      r = cc_find(parent, (int)c);
+      int i, j, k, x, y, z;
+      cell_ijk(L, c, &i, &j, &k);
+      cave_cell_xyz(L, i, j, k, &x, &y, &z);
+      const unsigned long long key = vdb_order_key(x, y, z);
+      hi = (uint32_t)(key >> 32);
+      lo = (uint32_t)key;
+    }
+    const unsigned peers = __match_any_sync(0xffffffffu, r);
+    const uint32_t mhi = __reduce_min_sync(peers, hi);
+    const uint32_t mlo = __reduce_min_sync(peers, hi == mhi ? lo : 0xffffffffu);
+    if (on && lane == __ffs(peers) - 1) {
+      atomicAdd(&size[r], (uint32_t)__popc(peers));
+      atomicMin(&min_key[r], ((unsigned long long)mhi << 32) | mlo);
+    }
   }
 }
 
@@ -266,21 +357,20 @@ __global__ void k_cave_tiles(CaveLattice L, uint32_t* dense, int3 llo, int3 ldim
 // Leaf bits: voxel (x, y, z) of a leaf is bit x*64 + y*8 + z, so x-slice x is the 64-bit word
 // x of the leaf with bit y*8 + z.  For each direction, the mask of voxels whose face
 // neighbour in that direction is on; dilation ORs them into the slice, erosion ANDs them.
-// One thread per leaf: its 64 bytes and the four face-neighbour leaves along y and z are
-// loaded as 16-byte vectors (five leaves in flight per thread), the x neighbours' edge slices
-// as 8-byte words.
-__device__ __forceinline__ void load_leaf(const ulonglong2* src, long long pos, bool ok,
-                                          unsigned long long s[8]) {
+// Two adjacent lanes per leaf, each with four x-slices (h = 0: x 0..3, h = 1: x 4..7): a lane
+// loads its half of the leaf and of the four face-neighbour leaves along y and z as 16-byte
+// vectors, swaps the middle slices with its partner, and reads the x neighbour's edge slice.
+__device__ __forceinline__ void load_half(const ulonglong2* src, long long pos, int h, bool ok,
+                                          unsigned long long s[4]) {
   if (ok) {
-#pragma unroll
-    for (int i = 0; i < 4; ++i) {
-      const ulonglong2 v = __ldg(&src[pos * 4 + i]);
-      s[2 * i] = v.x;
-      s[2 * i + 1] = v.y;
-    }
+    const ulonglong2 a = __ldg(&src[pos * 4 + 2 * h]);
+    const ulonglong2 b = __ldg(&src[pos * 4 + 2 * h + 1]);
+    s[0] = a.x;
+    s[1] = a.y;
+    s[2] = b.x;
+    s[3] = b.y;
   } else {
-#pragma unroll
-    for (int i = 0; i < 8; ++i) s[i] = 0ull;
+    s[0] = s[1] = s[2] = s[3] = 0ull;
   }
 }
 
@@ -289,37 +379,51 @@ __global__ void __launch_bounds__(256) k_leaf_morph(const unsigned long long* __
                                                     int3 ldim, int erode) {
   constexpr unsigned long long kZ0 = 0x0101010101010101ull, kZ7 = 0x8080808080808080ull;
   const long long nleaf = (long long)ldim.x * ldim.y * ldim.z;
+  const long long n = nleaf * 2;
   const long long sx = (long long)ldim.y * ldim.z, sy = ldim.z;
   const ulonglong2* v2 = reinterpret_cast<const ulonglong2*>(src);
   ulonglong2* d2 = reinterpret_cast<ulonglong2*>(dst);
-  for (long long pos = (long long)blockIdx.x * blockDim.x + threadIdx.x; pos < nleaf;
-       pos += (long long)gridDim.x * blockDim.x) {
+  const long long stride = (long long)gridDim.x * blockDim.x;
+  // a warp-uniform loop: the partner exchange needs both lanes of every pair
+  for (long long base = (long long)blockIdx.x * blockDim.x; base < n; base += stride) {
+    const long long t = base + threadIdx.x;
+    const bool live = t < n;
+    const long long pos = live ? (t >> 1) : 0;
+    const int h = (int)(t & 1);
     const int lz = (int)(pos % ldim.z);
     const int ly = (int)((pos / ldim.z) % ldim.y);
     const int lx = (int)(pos / sx);
-    unsigned long long s[8], zp[8], zm[8], yp[8], ym[8];
-    load_leaf(v2, pos, true, s);
-    load_leaf(v2, pos + 1, lz + 1 < ldim.z, zp);
-    load_leaf(v2, pos - 1, lz > 0, zm);
-    load_leaf(v2, pos + sy, ly + 1 < ldim.y, yp);
-    load_leaf(v2, pos - sy, ly > 0, ym);
-    const unsigned long long xp7 = lx + 1 < ldim.x ? __ldg(&src[(pos + sx) * 8]) : 0ull;
-    const unsigned long long xm0 = lx > 0 ? __ldg(&src[(pos - sx) * 8 + 7]) : 0ull;
-    unsigned long long out[8];
+    unsigned long long s[4], zp[4], zm[4], yp[4], ym[4];
+    load_half(v2, pos, h, live, s);
+    load_half(v2, pos + 1, h, live && lz + 1 < ldim.z, zp);
+    load_half(v2, pos - 1, h, live && lz > 0, zm);
+    load_half(v2, pos + sy, h, live && ly + 1 < ldim.y, yp);
+    load_half(v2, pos - sy, h, live && ly > 0, ym);
+    // outer edge: x = -1 of this leaf (h = 0) or x = 8 (h = 1) from the x neighbour leaf
+    unsigned long long edge = 0ull;
+    if (live && h == 0 && lx > 0) edge = __ldg(&src[(pos - sx) * 8 + 7]);
+    if (live && h == 1 && lx + 1 < ldim.x) edge = __ldg(&src[(pos + sx) * 8]);
+    // inner edge: h = 0 needs slice 4 and h = 1 slice 3, each from the partner lane, so each
+    // lane sends the slice next to the middle (3 from h = 0, 4 from h = 1)
+    const unsigned long long mine = h == 0 ? s[3] : s[0];
+    const unsigned long long other = __shfl_xor_sync(0xffffffffu, mine, 1);
+    unsigned long long out[4];
 #pragma unroll
-    for (int x = 0; x < 8; ++x) {
-      const unsigned long long c = s[x];
-      const unsigned long long nzp = ((c >> 1) & ~kZ7) | ((zp[x] << 7) & kZ7);
-      const unsigned long long nzm = ((c << 1) & ~kZ0) | ((zm[x] >> 7) & kZ0);
-      const unsigned long long nyp = (c >> 8) | (yp[x] << 56);
-      const unsigned long long nym = (c << 8) | (ym[x] >> 56);
-      const unsigned long long nxp = x < 7 ? s[x + 1] : xp7;
-      const unsigned long long nxm = x > 0 ? s[x - 1] : xm0;
-      out[x] = erode ? (c & nzp & nzm & nyp & nym & nxp & nxm)
+    for (int i = 0; i < 4; ++i) {
+      const unsigned long long c = s[i];
+      const unsigned long long nzp = ((c >> 1) & ~kZ7) | ((zp[i] << 7) & kZ7);
+      const unsigned long long nzm = ((c << 1) & ~kZ0) | ((zm[i] >> 7) & kZ0);
+      const unsigned long long nyp = (c >> 8) | (yp[i] << 56);
+      const unsigned long long nym = (c << 8) | (ym[i] >> 56);
+      const unsigned long long nxp = i < 3 ? s[i + 1] : (h == 0 ? other : edge);
+      const unsigned long long nxm = i > 0 ? s[i - 1] : (h == 0 ? edge : other);
+      out[i] = erode ? (c & nzp & nzm & nyp & nym & nxp & nxm)
                      : (c | nzp | nzm | nyp | nym | nxp | nxm);
     }
-#pragma unroll
-    for (int i = 0; i < 4; ++i) d2[pos * 4 + i] = make_ulonglong2(out[2 * i], out[2 * i + 1]);
+    if (live) {
+      d2[pos * 4 + 2 * h] = make_ulonglong2(out[0], out[1]);
+      d2[pos * 4 + 2 * h + 1] = make_ulonglong2(out[2], out[3]);
+    }
   }
 }
 
@@ -343,6 +447,16 @@ cudaError_t launch_cave_fill(const CaveLattice& L, uint32_t seed, int pct, int m
   return cudaGetLastError();
 }
 
+cudaError_t launch_cave_fill_libc(const CaveLattice& L, const uint32_t* mats, int nmats,
+                                  const uint32_t* state0, long long n_draws, int pct, int mode_2d,
+                                  cudaStream_t s) {
+  const long long nchunks = (n_draws + kLibcChunk - 1) / kLibcChunk;
+  if (nchunks > 0)
+    k_cave_fill_libc<<<grid_for(nchunks), 256, 0, s>>>(L, mats, nmats, state0, n_draws, pct,
+                                                       mode_2d);
+  return cudaGetLastError();
+}
+
 cudaError_t launch_cave_smooth(const CaveLattice& L, const uint8_t* cur, uint8_t* next, int amax,
                                int amin, int mode_2d, cudaStream_t s) {
   if (mode_2d)
@@ -361,6 +475,7 @@ cudaError_t launch_cave_regions(const CaveLattice& L, int32_t* parent, uint32_t*
                                 unsigned long long* min_key, CaveStats* stats, cudaStream_t s) {
   const int g = grid_for(cave_cell_count(L));
   k_cc_init<<<g, 256, 0, s>>>(L, parent, size, min_key, stats);
+  k_cc_columns<<<grid_for((long long)L.nx * L.ny), 256, 0, s>>>(L, parent);
   k_cc_union<<<g, 256, 0, s>>>(L, parent, stats);
   k_cc_flatten<<<g, 256, 0, s>>>(L, parent, size, min_key);
   k_cc_roots<<<g, 256, 0, s>>>(L, parent, size, stats);
@@ -384,7 +499,7 @@ cudaError_t launch_cave_tiles(const CaveLattice& L, uint32_t* dense, const int32
 
 cudaError_t launch_leaf_morph(const uint32_t* src, uint32_t* dst, const int32_t ldim[3],
                               int erode, cudaStream_t s) {
-  const long long n = (long long)ldim[0] * ldim[1] * ldim[2];
+  const long long n = (long long)ldim[0] * ldim[1] * ldim[2] * 2;
   k_leaf_morph<<<grid_for(n), 256, 0, s>>>(reinterpret_cast<const unsigned long long*>(src),
                                            reinterpret_cast<unsigned long long*>(dst),
                                            make_int3(ldim[0], ldim[1], ldim[2]), erode);

@@ -60,6 +60,15 @@ struct CaveStats {
 
 cudaError_t launch_cave_fill(const CaveLattice& L, uint32_t seed, int pct, int mode_2d,
                              cudaStream_t s);
+// The C library's rand() sequence as the reference's fill draws it, generated on the device:
+// an additive feedback generator r[i] = r[i-31] + r[i-3] (mod 2^32), output r[i] >> 1.
+// Thread t starts from state0 (the 31 words before the first draw) advanced by
+// kLibcChunk * t draws with the jump matrices mats[j] = A^(kLibcChunk * 2^j) (31 x 31, row
+// major) for the set bits j of t, and makes draws [t * kLibcChunk, (t + 1) * kLibcChunk).
+constexpr int kLibcChunk = 31 * 32;
+cudaError_t launch_cave_fill_libc(const CaveLattice& L, const uint32_t* mats, int nmats,
+                                  const uint32_t* state0, long long n_draws, int pct, int mode_2d,
+                                  cudaStream_t s);
 cudaError_t launch_cave_smooth(const CaveLattice& L, const uint8_t* cur, uint8_t* next, int amax,
                                int amin, int mode_2d, cudaStream_t s);
 cudaError_t launch_cave_floor_ceil(const CaveLattice& L, cudaStream_t s);

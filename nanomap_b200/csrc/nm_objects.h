@@ -109,10 +109,11 @@ void release(nm_map m);
 void release(nm_simmap sm);
 void release(nm_cave c);
 
-// Sim map construction: begin_build allocates the zeroed dense leaf buffer of the voxel
-// region [vmin, vmax); finish_build compacts it into `sm` and frees it.
+// Sim map construction: begin_build allocates (or, given `buffer` of at least 64 bytes per
+// leaf, borrows) the zeroed dense leaf buffer of the voxel region [vmin, vmax); finish_build
+// compacts it into `sm` and frees it unless borrowed.
 int begin_build(float res, const int32_t vmin[3], const int32_t vmax[3], SimBuild* b,
-                cudaStream_t s);
+                cudaStream_t s, uint32_t* buffer = nullptr);
 int finish_build(nm_context ctx, SimBuild& b, nm_simmap sm, cudaStream_t s);
 
 cudaStream_t pick(nm_context ctx, void* stream);

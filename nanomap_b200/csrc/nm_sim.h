@@ -15,6 +15,7 @@ struct SimBuild {
   int32_t vmin[3], vmax[3];  // voxel region [vmin, vmax)
   int32_t llo[3], ldim[3];   // leaf box origin (leaf coordinates) and size
   uint32_t* dense;
+  int32_t borrowed;          // dense belongs to the caller (not freed by the build)
 };
 
 struct SimMapView {

@@ -204,3 +204,15 @@ def test_cavegen_facade_program(ctx, tmp_path, mode):
     res, v = read_nmsim(written)
     assert res == np.float32(0.1)
     assert np.array_equal(v, o.voxels(shell=True))
+
+
+@pytest.mark.parametrize("seed", [0, 1, 2**31 - 1, 2**31, 2**32 - 1, 0x9E3779B9])
+@pytest.mark.parametrize("mode_2d", [False, True])
+def test_cave_fill_reproduces_c_library_rand(ctx, seed, mode_2d):
+    """The device draws the C library's rand() sequence after srand(seed) in the reference's
+    loop order (several jump chunks: 48 x 48 columns, 3 fill planes)."""
+    g = A.Cave(ctx, A.cave_desc((40.0, 40.0, 4.0), 0.1, 50, 0, 4, 4, seed))
+    o = O.Cave((40.0, 40.0, 4.0), 0.1, 50, 0, 4, 4, seed)
+    g.populate(mode_2d=mode_2d)
+    o.populate(mode_2d=mode_2d)
+    assert np.array_equal(g.cells(), o.cells())
