@@ -372,6 +372,17 @@ int nm_sim_render_noisy(nm_simmap sm, nm_sensor s, const nm_pose* pose, float* r
                         float sigma_coef, float drop_prob, uint64_t seed, uint32_t flags,
                         void* stream);
 
+/* SimHandler::processPointCloud for one sensor (SimHandler.cpp:234-280: generateCloud, then
+ * the insertion): the simulated range image of `s` at `pose` over the sim map, with the
+ * simulated sensors' range noise as nm_sim_render_noisy applies it (sigma_coef = drop_prob = 0
+ * for none), inserted into `m`.  In label mode one launch does both: each tile of pixels is
+ * rendered into on-chip memory and walked from there.  The ranges and the map are those of
+ * nm_sim_render_noisy followed by nm_map_insert_ranges.  `ranges` (device, hres*vres floats,
+ * or host with NM_OUTPUT_HOST; may be NULL) receives the image.  Flags: NM_DEFER_INTEGRATE,
+ * NM_SYNC, NM_OUTPUT_HOST and the voxel-filter flags (which render first, then insert). */
+int nm_sim_insert(nm_simmap sm, nm_map m, nm_sensor s, const nm_pose* pose, float sigma_coef,
+                  float drop_prob, uint64_t seed, float* ranges, uint32_t flags, void* stream);
+
 /* Ray casts against the sim map for agent observation and collision rays
  * (SimManager::getAgentSimCollision, SimManager.h:141-168): n rays from `origins` (metres,
  * 3 floats each) along `directions` (3 floats each, any length, normalised here); distances

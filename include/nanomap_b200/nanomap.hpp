@@ -419,41 +419,22 @@ class SimManager {
     for (int i = 0; i < config_->agentCount(); ++i)
       agents_.push_back(std::make_shared<agent::Agent>(*config_, i));
   }
-  // Device range buffer shared by the agents' sensors: each render writes it and the insert
-  // that follows on the same stream reads it.
-  float* buffer(size_t floats) {
-    if (floats > buf_floats_) {
-      float* p = nullptr;
-      if (buf_) nm_free_device(buf_);
-      buf_ = nullptr;
-      detail::check(nm_alloc_device(detail::context(), floats * sizeof(float), (void**)&p));
-      buf_ = p;
-      buf_floats_ = floats;
-    }
-    return buf_;
-  }
+  // SimHandler::processPointCloud per sensor (SimHandler.cpp:234-280): render and insert in
+  // one launch, without a range-image buffer.
   void view(agent::Agent& a, std::shared_ptr<Map> map) {
     const auto names = a.sensorNames();
     for (size_t j = 0; j < names.size(); ++j) {
       auto s = config_->sensorData(names[j]);
       if (!s) continue;
-      float* r = buffer((size_t)s->hRes() * s->vRes());
       const nm_pose p = a.sensorPose((int)j).c();
-      detail::check(nm_sim_render(sim_.get(), s->handle(), &p, r, 0, nullptr));
-      detail::check(nm_map_insert_ranges(map->handle(), s->handle(), &p, r, 0, nullptr));
+      detail::check(nm_sim_insert(sim_.get(), map->handle(), s->handle(), &p, 0.0f, 0.0f, 0,
+                                  nullptr, 0, nullptr));
     }
   }
 
   std::shared_ptr<config::Config> config_;
   std::shared_ptr<nm_simmap_s> sim_;
   std::vector<std::shared_ptr<agent::Agent>> agents_;
-  float* buf_ = nullptr;
-  size_t buf_floats_ = 0;
-
- public:
-  ~SimManager() {
-    if (buf_) nm_free_device(buf_);
-  }
 };
 
 }  // namespace manager

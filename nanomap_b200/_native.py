@@ -162,6 +162,7 @@ _SIGS = {
     "nm_map_insert_points": (C.c_int, [_P, _P, C.POINTER(NmPose), _P, _I32, _I32, _I32, _U32, _P]),
     "nm_sim_render_noisy": (C.c_int, [_P, _P, C.POINTER(NmPose), _P, _F, _F, _U64, _U32, _P]),
     "nm_sim_cast_rays": (C.c_int, [_P, _P, _P, _I64, _F, _P, _U32, _P]),
+    "nm_sim_insert": (C.c_int, [_P, _P, _P, C.POINTER(NmPose), _F, _F, _U64, _P, _U32, _P]),
     "nm_observation_sphere": (C.c_int, [_I32, _PF]),
     "nm_ray_pose_from_pose": (C.c_int, [_P, C.POINTER(NmPose), C.POINTER(NmRayPose)]),
     "nm_map_values_copy": (C.c_int, [_P, _P, _U64, _PU64, _P]),

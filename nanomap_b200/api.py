@@ -456,6 +456,18 @@ class SimMap:
         call("nm_sim_render_noisy", self.h, sensor.h, C.byref(pose.c()), p, sigma_coef, drop,
              C.c_uint64(seed), flags, _stream(stream))
 
+    def insert(self, m: "Map", sensor: Sensor, pose: Pose, sigma_coef: float = 0.0,
+               drop: float = 0.0, seed: int = 0, out=None, flags: int = 0, stream=None):
+        """Render this sensor's noisy range image and insert it into `m` (one launch in label
+        mode); `out` (optional) receives the image."""
+        p = None
+        if out is not None:
+            p, host = _ptr(out)
+            if host:
+                flags |= N.NM_OUTPUT_HOST
+        call("nm_sim_insert", self.h, m.h, sensor.h, C.byref(pose.c()), sigma_coef, drop,
+             C.c_uint64(seed), p, flags, _stream(stream))
+
     def cast_rays(self, origins, directions, max_range: float, stream=None):
         """Distances (metres) to the first active voxel along each ray within max_range, 0 when
         none.  numpy inputs give a numpy result; CUDA tensors give a CUDA tensor."""

@@ -450,7 +450,7 @@ int apply_filter(nm_map m, nm::FrameParams& f, uint32_t flags, cudaStream_t s0) 
 
 // One frame through traverse (+ integrate unless deferred).
 int run_frame(nm_map m, nm_sensor s, nm::FrameParams& f, uint32_t flags, cudaStream_t s0,
-              uint64_t bound) {
+              uint64_t bound, const nm::SimRender* sim) {
   int rc = ensure_capacity(m, bound, s0);
   if (rc != NM_OK) return rc;
   rc = set_plane_constants(m, 0, s);
@@ -476,7 +476,12 @@ int run_frame(nm_map m, nm_sensor s, nm::FrameParams& f, uint32_t flags, cudaStr
     w.tile_start[1] = (uint32_t)(w.tiles_x[0] * tiles_y);
     w.total_tiles = w.tile_start[1];
     w.fr[0] = f;
-    if (w.total_tiles > 0) NM_CUDA(nm::launch_traverse_labels<1>(w, m->view, m->desc.rounding, s0));
+    if (w.total_tiles > 0) {
+      if (sim)
+        NM_CUDA(nm::launch_traverse_render(w, m->view, *sim, m->desc.rounding, s0));
+      else
+        NM_CUDA(nm::launch_traverse_labels<1>(w, m->view, m->desc.rounding, s0));
+    }
   } else {
     NM_CUDA(nm::launch_traverse_counts(f, m->view, m->desc.rounding, s0));
   }
@@ -742,7 +747,7 @@ int nm_map_insert_points(nm_map m, nm_sensor s, const nm_pose* pose, const void*
     rc = apply_filter(m, f, flags, s0);
     if (rc != NM_OK) return rc;
   }
-  return run_frame(m, s, f, flags, s0, bound);
+  return run_frame(m, s, f, flags, s0, bound, nullptr);
 }
 
 int nm_map_insert_ranges(nm_map m, nm_sensor s, const nm_pose* pose, const float* ranges,
@@ -766,7 +771,66 @@ int nm_map_insert_ranges(nm_map m, nm_sensor s, const nm_pose* pose, const float
     rc = apply_filter(m, f, flags, s0);
     if (rc != NM_OK) return rc;
   }
-  return run_frame(m, s, f, flags, s0, bound);
+  return run_frame(m, s, f, flags, s0, bound, nullptr);
+}
+
+int nm_sim_insert(nm_simmap sm, nm_map m, nm_sensor s, const nm_pose* pose, float sigma_coef,
+                  float drop_prob, uint64_t seed, float* ranges, uint32_t flags, void* stream) {
+  if (!sm || !m || !s || !pose) return fail(NM_ERR_ARG, "null argument");
+  if (sm->ctx != m->ctx || s->ctx != m->ctx)
+    return fail(NM_ERR_ARG, "sim map, map and sensor belong to different contexts");
+  if (!(std::isfinite(sigma_coef) && drop_prob >= 0.0f && drop_prob <= 1.0f))
+    return fail(NM_ERR_ARG, "noise parameters invalid");
+  if (flags & NM_INPUT_HOST) return fail(NM_ERR_ARG, "NM_INPUT_HOST does not apply (no input)");
+  int rc = validate_pose(pose);
+  if (rc != NM_OK) return rc;
+  NM_CUDA(cudaSetDevice(m->ctx->device));
+  cudaStream_t s0 = pick(m->ctx, stream);
+  const int64_t n = (int64_t)s->desc.hres * s->desc.vres;
+  const bool host_out = (flags & NM_OUTPUT_HOST) && ranges;
+  float* out = host_out ? nullptr : ranges;
+  // the voxel filter and per-ray sums need the whole image first: render, then insert
+  const bool two_pass = (flags & (NM_FILTER_MEAN | NM_FILTER_CENTRE)) ||
+                        m->desc.update_mode != NM_UPDATE_LABEL;
+  if (host_out || (two_pass && !out)) {
+    nm_context c = m->ctx;
+    if ((size_t)n * 4 > c->render_staging_bytes) {
+      cudaFree(c->render_staging);
+      c->render_staging = nullptr;
+      c->render_staging_bytes = 0;
+      NM_CUDA(cudaMalloc((void**)&c->render_staging, (size_t)n * 4));
+      c->render_staging_bytes = (size_t)n * 4;
+    }
+    out = c->render_staging;
+  }
+  const uint32_t pass = flags & ~(NM_OUTPUT_HOST | NM_SYNC);
+  if (two_pass) {
+    rc = nm_sim_render_noisy(sm, s, pose, out, sigma_coef, drop_prob, seed, 0, s0);
+    if (rc == NM_OK) rc = nm_map_insert_ranges(m, s, pose, out, pass | (flags & NM_SYNC), s0);
+  } else {
+    nm::FrameParams f;
+    rc = make_frame(m, s, pose, &f);
+    if (rc != NM_OK) return rc;
+    f.input_kind = 1;
+    f.ranges = nullptr;
+    nm::SimRender sr;
+    std::memset(&sr, 0, sizeof(sr));
+    sr.v = sm->view;
+    nm::make_ray_params(s, *pose, &sr.rp);
+    sr.sigma_coef = sigma_coef;
+    sr.drop = drop_prob;
+    sr.seed = seed;
+    sr.noise = (sigma_coef != 0.0f || drop_prob != 0.0f) ? 1 : 0;
+    sr.out = out;
+    const uint64_t bound = frame_leaf_bound(m, s, *pose, f.R, true, (uint64_t)n);
+    rc = run_frame(m, s, f, pass | (flags & NM_SYNC), s0, bound, &sr);
+  }
+  if (rc != NM_OK) return rc;
+  if (host_out) {
+    NM_CUDA(cudaMemcpyAsync(ranges, out, (size_t)n * 4, cudaMemcpyDeviceToHost, s0));
+    NM_CUDA(cudaStreamSynchronize(s0));
+  }
+  return NM_OK;
 }
 
 int nm_map_filter_points(nm_map m, nm_sensor s, const nm_pose* pose, const void* input,

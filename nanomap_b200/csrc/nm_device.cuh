@@ -114,8 +114,8 @@ __device__ __forceinline__ int local_index(int x, int y, int z) {
 
 // Range image -> sensor-frame point, round to nearest (same operation order as the oracle's
 // orc_ranges_to_points).  Returns false for pixels without a return.
-__device__ __forceinline__ bool range_point(const FrameParams& f, int w, int h, float p[3]) {
-  const float r = __ldg(&f.ranges[(size_t)h * f.width + w]);
+__device__ __forceinline__ bool range_point_r(const FrameParams& f, int w, int h, float r,
+                                              float p[3]) {
   if (!(r > 0.0f)) return false;
   if (f.type == NM_SENSOR_FRUSTUM) {
     const float u = __fmul_rn((float)w, f.su);
@@ -135,6 +135,10 @@ __device__ __forceinline__ bool range_point(const FrameParams& f, int w, int h, 
     p[2] = __fmul_rn(__fmul_rn(cu, cv), r);
   }
   return true;
+}
+
+__device__ __forceinline__ bool range_point(const FrameParams& f, int w, int h, float p[3]) {
+  return range_point_r(f, w, h, __ldg(&f.ranges[(size_t)h * f.width + w]), p);
 }
 
 __device__ __forceinline__ bool xyz_point(const FrameParams& f, int w, int h, float p[3]) {

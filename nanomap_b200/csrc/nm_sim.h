@@ -6,6 +6,7 @@
 #include <cuda_runtime.h>
 
 #include "nanomap_b200.h"
+#include "nm_internal.h"
 
 namespace nm {
 
@@ -40,6 +41,22 @@ struct SimRayParams {
   float pos[3];
   float min_range, max_range;
 };
+
+// Fused simulated frame: the traversal renders each tile's ranges from the sim map (with the
+// simulated sensors' range noise when `noise` is set) into shared memory and walks them; the
+// ranges also go to `out` when it is set.  Passed by value to the kernel.
+struct SimRender {
+  SimMapView v;
+  SimRayParams rp;
+  float sigma_coef, drop;
+  uint64_t seed;
+  int32_t noise;
+  int32_t pad;
+  float* out;
+};
+
+cudaError_t launch_traverse_render(const TickWork<1>& w, const MapView& m, const SimRender& sr,
+                                   int rounding, cudaStream_t s);
 
 constexpr int kMaxRenderSlots = 32;
 

@@ -21,6 +21,7 @@
 
 #include "nm_device.cuh"
 #include "nm_internal.h"
+#include "nm_sim_device.cuh"
 
 namespace nm {
 
@@ -120,13 +121,15 @@ __device__ __forceinline__ bool pixel_point(const FrameParams& f, int w, int h, 
   return xyz_point(f, w, h, p);
 }
 
-template <int RM, int MaxF>
-__device__ __forceinline__ void traverse_body(const TickWork<MaxF>& work, const MapView& m) {
+template <int RM, int MaxF, bool Render = false>
+__device__ __forceinline__ void traverse_body(const TickWork<MaxF>& work, const MapView& m,
+                                              const SimRender* sr = nullptr) {
   extern __shared__ __align__(16) unsigned char smem[];
   const uint32_t smask = work.smask;
   const int nent = (int)smask + 1;
   unsigned long long* s_keys = reinterpret_cast<unsigned long long*>(smem);
   uint32_t* s_words = reinterpret_cast<uint32_t*>(s_keys + nent);
+  float* s_rng = reinterpret_cast<float*>(s_words + nent * kLabelWords);  // Render: tile ranges
   __shared__ FrameParams s_f;
   __shared__ uint32_t s_tile;
   __shared__ int s_frame;
@@ -168,6 +171,21 @@ __device__ __forceinline__ void traverse_body(const TickWork<MaxF>& work, const 
     }
     for (int i = tid; i < nent; i += blockDim.x) s_keys[i] = kEmptyKey;
     for (int i = tid; i < nent * kLabelWords; i += blockDim.x) s_words[i] = 0u;
+    if constexpr (Render) {
+      // the tile's ranges: the sim map's first active voxel per pixel, then the range noise
+      // (the same values nm_sim_render_noisy writes)
+      for (int t = tid; t < nrays; t += blockDim.x) {
+        const int px = x0 + t % work.tile_w, py = y0 + t / work.tile_w;
+        float rr = 0.0f;
+        if (px < f.width && py < f.height) {
+          rr = sim_ray(sr->v, sr->rp, px, py);
+          const long long i = (long long)py * f.width + px;
+          if (sr->noise) rr = noisy(rr, sr->seed, i, sr->sigma_coef, sr->drop);
+          if (sr->out) sr->out[i] = rr;
+        }
+        s_rng[t] = rr;
+      }
+    }
     __syncthreads();
 
     Ray r;
@@ -224,7 +242,11 @@ __device__ __forceinline__ void traverse_body(const TickWork<MaxF>& work, const 
         const int px = x0 + (int)(k % (uint32_t)work.tile_w);
         const int py = y0 + (int)(k / (uint32_t)work.tile_w);
         float p[3];
-        if (px < f.width && py < f.height && pixel_point(f, px, py, p) && setup_ray<RM>(f, p, r)) {
+        // pixels of a tile that overhangs the image are skipped before any input is read
+        bool has_point = false;
+        if (px < f.width && py < f.height)
+          has_point = Render ? range_point_r(f, px, py, s_rng[k], p) : pixel_point(f, px, py, p);
+        if (has_point && setup_ray<RM>(f, p, r)) {
           active = true;
           rays += 1;
           cw_idx = -1;
@@ -308,6 +330,14 @@ __global__ void __launch_bounds__(256) k_traverse(const __grid_constant__ TickWo
   traverse_body<RM, MaxF>(work, m);
 }
 
+// One simulated frame rendered tile by tile inside the traversal (sim render + noise + insert).
+template <int RM>
+__global__ void __launch_bounds__(256) k_traverse_render(const __grid_constant__ TickWork<1> work,
+                                                         MapView m,
+                                                         const __grid_constant__ SimRender sr) {
+  traverse_body<RM, 1, true>(work, m, &sr);
+}
+
 // Work list read from device memory (tick plans replayed as CUDA graphs).
 template <int RM>
 __global__ void __launch_bounds__(256) k_traverse_dev(const TickWork<kMaxTickFrames>* work,
@@ -351,6 +381,44 @@ cudaError_t launch_traverse_labels(const TickWork<MaxF>& w, const MapView& m, in
     const int grid = min(persistent_grid<NM_ROUND_NEAREST, MaxF>(smem, block), (int)w.total_tiles);
     k_traverse<NM_ROUND_NEAREST, MaxF><<<grid, block, smem, s>>>(w, m);
   }
+  return cudaGetLastError();
+}
+
+cudaError_t launch_traverse_render(const TickWork<1>& w, const MapView& m, const SimRender& sr,
+                                   int rounding, cudaStream_t s) {
+  const int nrays = w.tile_w * w.tile_h;
+  const size_t smem = (size_t)(w.smask + 1) * (8 + kLabelWords * 4) + (size_t)nrays * 4;
+  const int block = min(256, nrays);
+  static int cached[2] = {0, 0};
+  static size_t cached_smem[2] = {0, 0};
+  static int cached_block[2] = {0, 0};
+  static int sms = 0;
+  const int ri = rounding == NM_ROUND_DOWN ? 1 : 0;
+  if (!cached[ri] || cached_smem[ri] != smem || cached_block[ri] != block) {
+    int dev = 0;
+    cudaGetDevice(&dev);
+    cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, dev);
+    int blocks = 0;
+    if (ri) {
+      cudaFuncSetAttribute(k_traverse_render<NM_ROUND_DOWN>,
+                           cudaFuncAttributeMaxDynamicSharedMemorySize, 160 * 1024);
+      cudaOccupancyMaxActiveBlocksPerMultiprocessor(&blocks, k_traverse_render<NM_ROUND_DOWN>,
+                                                    block, smem);
+    } else {
+      cudaFuncSetAttribute(k_traverse_render<NM_ROUND_NEAREST>,
+                           cudaFuncAttributeMaxDynamicSharedMemorySize, 160 * 1024);
+      cudaOccupancyMaxActiveBlocksPerMultiprocessor(&blocks, k_traverse_render<NM_ROUND_NEAREST>,
+                                                    block, smem);
+    }
+    cached[ri] = blocks > 0 ? blocks : 1;
+    cached_smem[ri] = smem;
+    cached_block[ri] = block;
+  }
+  const int grid = min(sms * cached[ri], (int)w.total_tiles);
+  if (ri)
+    k_traverse_render<NM_ROUND_DOWN><<<grid, block, smem, s>>>(w, m, sr);
+  else
+    k_traverse_render<NM_ROUND_NEAREST><<<grid, block, smem, s>>>(w, m, sr);
   return cudaGetLastError();
 }
 

@@ -189,3 +189,60 @@ def test_render_noisy_equals_render_then_noise(ctx):
         g.render_noisy(sensor, pose, b, spec.noise_coef, spec.drop, 77 + k)
         assert torch.equal(a.view(torch.int32), b.view(torch.int32))
         assert (b == 0).float().mean() > spec.drop * 0.5
+
+
+def _same_maps(a, b):
+    ao, av, aa = a.export()
+    bo, bv, ba = b.export()
+    ia = np.lexsort((ao[:, 2], ao[:, 1], ao[:, 0]))
+    ib = np.lexsort((bo[:, 2], bo[:, 1], bo[:, 0]))
+    return (np.array_equal(ao[ia], bo[ib]) and np.array_equal(av[ia].view(np.uint32),
+                                                              bv[ib].view(np.uint32))
+            and np.array_equal(aa[ia], ba[ib]))
+
+
+@pytest.mark.parametrize("kind", ["camera", "odd_camera", "laser", "accumulate", "filtered"])
+def test_sim_insert_equals_render_then_insert(ctx, kind):
+    """nm_sim_insert (the fused render + insert in label mode; render then insert for the
+    per-ray sums and the voxel filter) gives the ranges and the map of nm_sim_render_noisy
+    followed by nm_map_insert_ranges."""
+    import torch
+    sc, g, o = _maps(ctx, "sim_headline" if kind != "laser" else "plain_small")
+    spec = sc.spec
+    if kind == "laser":
+        desc = A.sensor_desc(type=N.NM_SENSOR_LASER, hres=1024, vres=64, hfov_deg=360.0,
+                             vfov_deg=30.0, max_range=20.0, min_range=0.2,
+                             frame_transform=S.OPTICAL_TO_BODY)
+        H, W, res = 64, 1024, 0.05
+    elif kind == "odd_camera":
+        # 100 x 70 pixels: the 16 x 16 tiles overhang the image on both axes
+        desc = camera_desc(spec, hres=100, vres=70)
+        H, W, res = 70, 100, spec.map_res
+    else:
+        desc = camera_desc(spec)
+        H, W, res = spec.height, spec.width, spec.map_res
+    sensor = A.Sensor(ctx, desc)
+    mode = N.NM_UPDATE_ACCUMULATE if kind == "accumulate" else N.NM_UPDATE_LABEL
+    flags = N.NM_FILTER_MEAN if kind == "filtered" else 0
+    ma = A.Map(ctx, A.map_desc(res=res, clamp_min=-2.0, clamp_max=3.5, update_mode=mode))
+    mb = A.Map(ctx, A.map_desc(res=res, clamp_min=-2.0, clamp_max=3.5, update_mode=mode))
+    for k, (p, q) in enumerate(S.trajectory(sc, 3, seed=11)):
+        pose = A.Pose(p, q)
+        a = torch.zeros((H, W), device="cuda")
+        b = torch.zeros_like(a)
+        g.render_noisy(sensor, pose, a, 0.005, 0.02, 31 + k)
+        ma.insert_ranges(sensor, pose, a, flags=flags)
+        g.insert(mb, sensor, pose, 0.005, 0.02, 31 + k, out=b, flags=flags)
+        assert torch.equal(a.view(torch.int32), b.view(torch.int32))
+    torch.cuda.synchronize()
+    assert _same_maps(ma, mb)
+    sa, sb = ma.stats(), mb.stats()
+    assert sa["visits"] == sb["visits"] and sa["rays"] == sb["rays"] and sb["error_flags"] == 0
+    # without an output image, and with a host one
+    mc = A.Map(ctx, A.map_desc(res=res, clamp_min=-2.0, clamp_max=3.5, update_mode=mode))
+    host = np.zeros((H, W), np.float32)
+    for k, (p, q) in enumerate(S.trajectory(sc, 3, seed=11)):
+        g.insert(mc, sensor, A.Pose(p, q), 0.005, 0.02, 31 + k,
+                 out=host if k == 2 else None, flags=flags)
+    assert _same_maps(ma, mc)
+    assert np.array_equal(host.view(np.uint32), b.cpu().numpy().view(np.uint32))
