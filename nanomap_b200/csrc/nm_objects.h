@@ -49,6 +49,13 @@ struct nm_context_s {
   cudaStream_t stream = nullptr;
   float* render_staging = nullptr;
   size_t render_staging_bytes = 0;
+  // chunked host input (created on first use): one copy stream, one stream per chunk launch
+  bool chunk_ready = false;
+  cudaStream_t copy_stream = nullptr;
+  cudaStream_t chunk_stream[nm::kMaxChunks] = {};
+  cudaEvent_t ev_prev = nullptr;
+  cudaEvent_t ev_copied[nm::kMaxChunks] = {};
+  cudaEvent_t ev_done[nm::kMaxChunks] = {};
 };
 
 struct nm_sensor_s {

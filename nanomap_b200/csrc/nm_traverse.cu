@@ -141,13 +141,14 @@ __device__ __forceinline__ void traverse_body(const TickWork<MaxF>& work, const 
 
   for (;;) {
     if (tid == 0) {
-      const uint32_t t = atomicAdd(&m.ctr->tile_queue, 1u);
+      unsigned int* queue = work.queue ? &m.ctr->chunk_queue[work.queue - 1] : &m.ctr->tile_queue;
+      const uint32_t t = atomicAdd(queue, 1u);
       int fi = 0;
       while (fi + 1 < work.n_frames && work.tile_start[fi + 1] <= t) ++fi;
       s_tile = t;
       s_frame = fi;
       s_next = 0u;
-      if (t == work.total_tiles + gridDim.x - 1) m.ctr->tile_queue = 0u;  // last reader resets
+      if (t == work.total_tiles + gridDim.x - 1) *queue = 0u;  // last reader resets
     }
     __syncthreads();
     const uint32_t tile = s_tile;

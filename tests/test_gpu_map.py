@@ -50,8 +50,12 @@ def test_labels_and_map_bit_exact_plain_small(ctx, small, rounding):
     assert st["frames"] == len(frames) and st["error_flags"] == 0
 
 
-def test_xyz_records_host_and_device_inputs(ctx, small):
-    """insertPointCloud-style input: width*height records of `step` bytes, xyz at 0/4/8."""
+@pytest.mark.parametrize("cut", [0, 13])
+def test_xyz_records_host_and_device_inputs(ctx, small, cut):
+    """insertPointCloud-style input: width*height records of `step` bytes, xyz at 0/4/8.
+    Host records are copied in chunks of tile rows overlapped with the walk (four frames in a
+    row without a wait, so the staging buffer is reused while earlier frames run); `cut` drops
+    the last rows so that the last tile row is partial."""
     spec, scene, desc, frames = small
     res = spec.map_res
     sensor = A.Sensor(ctx, desc)
@@ -59,9 +63,9 @@ def test_xyz_records_host_and_device_inputs(ctx, small):
     m_host = A.Map(ctx, A.map_desc(res=res))
     m_dev = A.Map(ctx, A.map_desc(res=res))
     om = O.Map(res)
-    H, W = spec.height, spec.width
+    H, W = spec.height - cut, spec.width
     for i, (pose, ranges) in enumerate(frames[:4]):
-        pts = osen.points(ranges)
+        pts = osen.points(ranges)[: H * W]
         rec = np.zeros((H * W, 5), np.float32)  # step 20 bytes, like the reference's Point AoS
         rec[:, :3] = pts
         rec[:, 3] = 7.0
