@@ -6,6 +6,7 @@
 // CUDA device is usable.  Built with -frounding-math so the rounding-mode sections below are
 // evaluated at run time under the mode they select.
 #include <algorithm>
+#include <cstddef>
 #include <cfenv>
 #include <cmath>
 #include <cstdarg>
@@ -379,9 +380,12 @@ int do_integrate(nm_map m, cudaStream_t s) {
 
 int check_device_errors(nm_map m, cudaStream_t s) {
   NM_CUDA(cudaStreamSynchronize(s));
-  unsigned int flags = 0, lc = 0;
-  NM_CUDA(cudaMemcpy(&flags, &m->d_ctr->error_flags, 4, cudaMemcpyDeviceToHost));
-  NM_CUDA(cudaMemcpy(&lc, &m->d_ctr->leaf_count, 4, cudaMemcpyDeviceToHost));
+  // leaf_count, touched_count and error_flags are adjacent: one read
+  static_assert(offsetof(nm::MapCounters, error_flags) ==
+                    offsetof(nm::MapCounters, leaf_count) + 8, "counter layout");
+  unsigned int w[3] = {0, 0, 0};
+  NM_CUDA(cudaMemcpy(w, &m->d_ctr->leaf_count, sizeof(w), cudaMemcpyDeviceToHost));
+  const unsigned int lc = w[0], flags = w[2];
   m->known_leaves = lc;
   m->pending_bound = 0;
   if (flags & nm::kErrProbe)
