@@ -8,7 +8,8 @@
 //   k_cave_smooth3d/2d one cellular-automaton step (CaveGen::smoothMap / smoothMapXY)
 //   k_cc_*             6-connected regions by lock-free union-find (CaveGen::getRegions)
 //   k_cave_tiles       cells -> whole leaves (addTile(1, ...) + voxelizeActiveTiles)
-//   k_leaf_morph       one dilation or erosion step on 64-bit x-slices of the leaves
+//   k_leaf_morph       one dilation or erosion step on 64-bit x-slices, walking runs of
+//                      leaves along x
 //   k_compact (nm_sim.cu) compacts the band into the sim map
 #include <climits>
 #include <cstdint>
@@ -374,55 +375,75 @@ __device__ __forceinline__ void load_half(const ulonglong2* src, long long pos, 
   }
 }
 
+// A pair of lanes walks a run of kMorphRun leaves along x at one (y, z) leaf position: the next
+// leaf's half is loaded one step ahead (it is the x+ edge now and this lane's leaf next), and
+// the previous leaf's last slice is kept, so only the run's first leaf reads an x neighbour
+// from memory.  Leaves next to each other along z and y are walked by neighbouring lanes and
+// warps at about the same time, so those loads are served by L1 / L2.
+constexpr int kMorphRun = 16;
+
 __global__ void __launch_bounds__(256) k_leaf_morph(const unsigned long long* __restrict__ src,
                                                     unsigned long long* __restrict__ dst,
                                                     int3 ldim, int erode) {
   constexpr unsigned long long kZ0 = 0x0101010101010101ull, kZ7 = 0x8080808080808080ull;
-  const long long nleaf = (long long)ldim.x * ldim.y * ldim.z;
-  const long long n = nleaf * 2;
-  const long long sx = (long long)ldim.y * ldim.z, sy = ldim.z;
+  const long long syz = (long long)ldim.y * ldim.z, sy = ldim.z;
+  const long long nseg = (ldim.x + kMorphRun - 1) / kMorphRun;
+  const long long n = nseg * syz * 2;
   const ulonglong2* v2 = reinterpret_cast<const ulonglong2*>(src);
   ulonglong2* d2 = reinterpret_cast<ulonglong2*>(dst);
   const long long stride = (long long)gridDim.x * blockDim.x;
-  // a warp-uniform loop: the partner exchange needs both lanes of every pair
+  // a warp-uniform loop (and a fixed number of steps per run): the partner exchanges need
+  // both lanes of every pair
   for (long long base = (long long)blockIdx.x * blockDim.x; base < n; base += stride) {
     const long long t = base + threadIdx.x;
-    const bool live = t < n;
-    const long long pos = live ? (t >> 1) : 0;
+    const bool live0 = t < n;
+    const long long pr = live0 ? (t >> 1) : 0;
     const int h = (int)(t & 1);
-    const int lz = (int)(pos % ldim.z);
-    const int ly = (int)((pos / ldim.z) % ldim.y);
-    const int lx = (int)(pos / sx);
-    unsigned long long s[4], zp[4], zm[4], yp[4], ym[4];
-    load_half(v2, pos, h, live, s);
-    load_half(v2, pos + 1, h, live && lz + 1 < ldim.z, zp);
-    load_half(v2, pos - 1, h, live && lz > 0, zm);
-    load_half(v2, pos + sy, h, live && ly + 1 < ldim.y, yp);
-    load_half(v2, pos - sy, h, live && ly > 0, ym);
-    // outer edge: x = -1 of this leaf (h = 0) or x = 8 (h = 1) from the x neighbour leaf
-    unsigned long long edge = 0ull;
-    if (live && h == 0 && lx > 0) edge = __ldg(&src[(pos - sx) * 8 + 7]);
-    if (live && h == 1 && lx + 1 < ldim.x) edge = __ldg(&src[(pos + sx) * 8]);
-    // inner edge: h = 0 needs slice 4 and h = 1 slice 3, each from the partner lane, so each
-    // lane sends the slice next to the middle (3 from h = 0, 4 from h = 1)
-    const unsigned long long mine = h == 0 ? s[3] : s[0];
-    const unsigned long long other = __shfl_xor_sync(0xffffffffu, mine, 1);
-    unsigned long long out[4];
+    const long long yz = pr % syz;
+    const int x0 = (int)(pr / syz) * kMorphRun;
+    const int lz = (int)(yz % ldim.z);
+    const int ly = (int)(yz / ldim.z);
+    unsigned long long s[4];
+    load_half(v2, (long long)x0 * syz + yz, h, live0, s);
+    // x- edge of the run's first leaf (slice 7 of leaf x0 - 1), needed by h = 0
+    unsigned long long prev7 =
+        (live0 && h == 0 && x0 > 0) ? __ldg(&src[((long long)(x0 - 1) * syz + yz) * 8 + 7]) : 0ull;
+    for (int it = 0; it < kMorphRun; ++it) {
+      const int lx = x0 + it;
+      const bool live = live0 && lx < ldim.x;
+      const long long pos = (long long)lx * syz + yz;
+      unsigned long long nx[4], zp[4], zm[4], yp[4], ym[4];
+      load_half(v2, pos + syz, h, live && lx + 1 < ldim.x, nx);
+      load_half(v2, pos + 1, h, live && lz + 1 < ldim.z, zp);
+      load_half(v2, pos - 1, h, live && lz > 0, zm);
+      load_half(v2, pos + sy, h, live && ly + 1 < ldim.y, yp);
+      load_half(v2, pos - sy, h, live && ly > 0, ym);
+      // inner edges: h = 0 needs slice 4 (partner's s[0]), h = 1 slice 3 (partner's s[3])
+      const unsigned long long other = __shfl_xor_sync(0xffffffffu, h == 0 ? s[3] : s[0], 1);
+      // x+ edge for h = 1: slice 0 of the next leaf, which the h = 0 partner loaded
+      const unsigned long long next0 = __shfl_xor_sync(0xffffffffu, nx[0], 1);
+      const unsigned long long edge = h == 0 ? prev7 : next0;
+      unsigned long long out[4];
 #pragma unroll
-    for (int i = 0; i < 4; ++i) {
-      const unsigned long long c = s[i];
-      const unsigned long long nzp = ((c >> 1) & ~kZ7) | ((zp[i] << 7) & kZ7);
-      const unsigned long long nzm = ((c << 1) & ~kZ0) | ((zm[i] >> 7) & kZ0);
-      const unsigned long long nyp = (c >> 8) | (yp[i] << 56);
-      const unsigned long long nym = (c << 8) | (ym[i] >> 56);
-      const unsigned long long nxp = i < 3 ? s[i + 1] : (h == 0 ? other : edge);
-      const unsigned long long nxm = i > 0 ? s[i - 1] : (h == 0 ? edge : other);
-      out[i] = erode ? (c & nzp & nzm & nyp & nym & nxp & nxm)
-                     : (c | nzp | nzm | nyp | nym | nxp | nxm);
-    }
-    if (live) {
-      d2[pos * 4 + 2 * h] = make_ulonglong2(out[0], out[1]);
-      d2[pos * 4 + 2 * h + 1] = make_ulonglong2(out[2], out[3]);
+      for (int i = 0; i < 4; ++i) {
+        const unsigned long long c = s[i];
+        const unsigned long long nzp = ((c >> 1) & ~kZ7) | ((zp[i] << 7) & kZ7);
+        const unsigned long long nzm = ((c << 1) & ~kZ0) | ((zm[i] >> 7) & kZ0);
+        const unsigned long long nyp = (c >> 8) | (yp[i] << 56);
+        const unsigned long long nym = (c << 8) | (ym[i] >> 56);
+        const unsigned long long nxp = i < 3 ? s[i + 1] : (h == 0 ? other : edge);
+        const unsigned long long nxm = i > 0 ? s[i - 1] : (h == 0 ? edge : other);
+        out[i] = erode ? (c & nzp & nzm & nyp & nym & nxp & nxm)
+                       : (c | nzp | nzm | nyp | nym | nxp | nxm);
+      }
+      if (live) {
+        d2[pos * 4 + 2 * h] = make_ulonglong2(out[0], out[1]);
+        d2[pos * 4 + 2 * h + 1] = make_ulonglong2(out[2], out[3]);
+      }
+      // the next leaf's x- edge for h = 0 is this leaf's slice 7, held by the h = 1 partner
+      prev7 = __shfl_xor_sync(0xffffffffu, s[3], 1);
+#pragma unroll
+      for (int i = 0; i < 4; ++i) s[i] = nx[i];
     }
   }
 }
@@ -499,7 +520,7 @@ cudaError_t launch_cave_tiles(const CaveLattice& L, uint32_t* dense, const int32
 
 cudaError_t launch_leaf_morph(const uint32_t* src, uint32_t* dst, const int32_t ldim[3],
                               int erode, cudaStream_t s) {
-  const long long n = (long long)ldim[0] * ldim[1] * ldim[2] * 2;
+  const long long n = (long long)((ldim[0] + kMorphRun - 1) / kMorphRun) * ldim[1] * ldim[2] * 2;
   k_leaf_morph<<<grid_for(n), 256, 0, s>>>(reinterpret_cast<const unsigned long long*>(src),
                                            reinterpret_cast<unsigned long long*>(dst),
                                            make_int3(ldim[0], ldim[1], ldim[2]), erode);
