@@ -262,9 +262,14 @@ __global__ void k_cc_union(CaveLattice L, int32_t* parent, CaveStats* stats) {
     if (!L.cells[c]) continue;
     int i, j, k;
     cell_ijk(L, c, &i, &j, &k);
-    if (i + 1 < L.nx && L.cells[c + (long long)L.ny * nzp])
-      cc_union(parent, (int)c, (int)(c + (long long)L.ny * nzp), &stats->error);
-    if (j + 1 < L.ny && L.cells[c + nzp]) cc_union(parent, (int)c, (int)(c + nzp), &stats->error);
+    // a cell whose run continues below joins a neighbour's run only where that run does not
+    // continue below too: otherwise the pair below has joined the same two runs already
+    const bool below = k > 0 && (k < L.nz || L.ceil_adjacent) && L.cells[c - 1];
+    const long long cx = c + (long long)L.ny * nzp, cy = c + nzp;
+    if (i + 1 < L.nx && L.cells[cx] && !(below && L.cells[cx - 1]))
+      cc_union(parent, (int)c, (int)cx, &stats->error);
+    if (j + 1 < L.ny && L.cells[cy] && !(below && L.cells[cy - 1]))
+      cc_union(parent, (int)c, (int)cy, &stats->error);
   }
 }
 
