@@ -11,11 +11,19 @@
 // tile's next ray as soon as its own ends, so lanes stay busy until the tile runs dry.
 //
 // Labels collect in a per-CTA shared-memory leaf table (hashed, 32 label words per leaf);
-// a leaf that finds no room goes straight to the device table.  After a tile, one warp per
+// a leaf that finds no room goes straight to the device table.  After a tile, one lane per
 // cached leaf ORs its words into the device label buffer and puts the leaf on the touched
-// list.  Per step the walk compares the three crossing times (non-negative doubles, one
-// compare per pair), keeps the voxel as (leaf, local) coordinates, and probes the leaf table
-// only when the step leaves the current leaf.
+// list (the device-table lookups of a warp's leaves overlap).
+//
+// Host xyz records may arrive in chunks of tile rows: each chunk is then its own launch on
+// its own stream and tile counter (TickWork::queue), started when its rows have arrived.
+//
+// Per step the walk compares the three crossing times (non-negative doubles, one compare per
+// pair), keeps the voxel as (leaf, local) coordinates, and probes the leaf table only when the
+// step leaves the current leaf.
+//
+// k_traverse_render renders each tile's ranges from the sim map into shared memory first
+// (nm_sim_insert), so one launch does the simulated frame and its insertion.
 #include <cfloat>
 #include <cstdint>
 
