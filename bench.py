@@ -582,9 +582,70 @@ def run_large_section(local, frames=12, warmup=3):
         "expected_depth_forward_ms": f0.elapsed_time(f1), "expected_depth_adjoint_ms_incl_host_sync": bwd_ms,
     }
     m.close()
+    out["with_two_agents"] = run_large_agents(ctx, sim, sensor, spec, scene, poses, frames, warmup)
     sim.close()
     sensor.close()
     ctx.close()
+    return out
+
+
+def run_large_agents(ctx, sim, camera, spec, scene, poses, frames, warmup):
+    """The large workload's camera with two batched agents alongside it (640x480 87x58 deg
+    cameras at 10 m): one tick plan (render + noise + insert of all three frames, one shared
+    map at 0.02 m) per tick, L2 flushed between ticks."""
+    import torch
+
+    from nanomap_b200 import _native as N
+    from nanomap_b200 import api as A
+    from nanomap_b200 import scenes as S
+    agents = [A.Sensor(ctx, A.sensor_desc(type=0, hres=640, vres=480, hfov_deg=87.0,
+                                          vfov_deg=58.0, max_range=10.0, explicit_log_odds=1,
+                                          log_odds_hit=0.85, log_odds_miss=-0.4,
+                                          frame_transform=S.OPTICAL_TO_BODY)) for _ in range(2)]
+    trajs = [[A.Pose(p, q) for p, q in S.trajectory(scene, frames + warmup, seed=211 + 13 * a)]
+             for a in range(2)]
+    sensors = [camera] + agents
+    bufs = [torch.zeros(s.desc.vres, s.desc.hres, device="cuda") for s in sensors]
+    m = A.Map(ctx, A.map_desc(res=spec.map_res, clamp_min=spec.clamp[0], clamp_max=spec.clamp[1],
+                              rounding=N.NM_ROUND_DOWN, max_agents=3,
+                              initial_leaf_capacity=1 << 22))
+    plan = A.TickPlan(m, [(sensors[a], bufs[a], a) for a in range(3)], sim=sim)
+    stream = torch.cuda.current_stream()
+    flush = torch.empty(256 << 20, dtype=torch.uint8, device="cuda")
+
+    def set_tick(k):
+        plan.set_pose(0, poses[k])
+        for a in range(2):
+            plan.set_pose(1 + a, trajs[a][k])
+        plan.set_noise(spec.noise_coef, spec.drop, 7 * (k + 1))
+
+    for k in range(warmup):
+        set_tick(k)
+        plan.run(stream=stream)
+    torch.cuda.synchronize()
+    s0 = m.stats()
+    evs = []
+    for k in range(warmup, warmup + frames):
+        flush.fill_(k & 255)
+        set_tick(k)
+        e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+        e0.record(stream)
+        plan.run(stream=stream)
+        e1.record(stream)
+        evs.append((e0, e1))
+    torch.cuda.synchronize()
+    s1 = m.stats()
+    ms = sum(a.elapsed_time(b) for a, b in evs) / len(evs)
+    visits = (s1["visits"] - s0["visits"]) / len(evs)
+    out = {"workload": "the 1280x720 camera + 2 agents (640x480 87x58 deg at 10 m), one tick plan "
+                       "per tick into one shared 0.02 m map",
+           "ticks": len(evs), "ms_per_tick": ms, "visits_per_tick": visits,
+           "voxel_updates_per_s": visits / (ms / 1e3), "table_growths": s1["grow_count"],
+           "error_flags": s1["error_flags"]}
+    plan.close()
+    m.close()
+    for s in agents:
+        s.close()
     return out
 
 
