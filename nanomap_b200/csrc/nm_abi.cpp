@@ -925,7 +925,7 @@ int nm_sim_insert(nm_simmap sm, nm_map m, nm_sensor s, const nm_pose* pose, floa
     nm::SimRender sr;
     std::memset(&sr, 0, sizeof(sr));
     sr.v = sm->view;
-    nm::make_ray_params(s, *pose, &sr.rp);
+    nm::make_ray_params(s, *pose, sm->view.res, &sr.rp);
     sr.sigma_coef = sigma_coef;
     sr.drop = drop_prob;
     sr.seed = seed;

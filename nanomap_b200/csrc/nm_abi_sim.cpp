@@ -117,7 +117,7 @@ cudaStream_t pick(nm_context ctx, void* stream) {
 
 namespace nm {
 
-void make_ray_params(nm_sensor s, const nm_pose& pose, SimRayParams* rp) {
+void make_ray_params(nm_sensor s, const nm_pose& pose, float res, SimRayParams* rp) {
   std::memset(rp, 0, sizeof(*rp));
   rp->type = s->desc.type;
   rp->width = s->desc.hres;
@@ -138,6 +138,12 @@ void make_ray_params(nm_sensor s, const nm_pose& pose, SimRayParams* rp) {
   for (int a = 0; a < 3; ++a) rp->pos[a] = pose.position[a];
   rp->min_range = s->desc.min_range;
   rp->max_range = s->desc.max_range;
+  {
+    RoundScope rn(NM_ROUND_NEAREST);
+    for (int a = 0; a < 3; ++a) rp->eye[a] = rp->pos[a] / res;
+    rp->tmin = rp->min_range / res;
+    rp->tmax = rp->max_range / res;
+  }
 }
 
 }  // namespace nm
@@ -175,7 +181,7 @@ int render_impl(nm_simmap sm, nm_sensor s, const nm_pose* pose, float* ranges, u
   NM_CUDA(cudaSetDevice(ctx->device));
   cudaStream_t st = nm::pick(ctx, stream);
   nm::SimRayParams rp;
-  nm::make_ray_params(s, *pose, &rp);
+  nm::make_ray_params(s, *pose, sm->view.res, &rp);
   const size_t bytes = (size_t)rp.width * rp.height * 4;
   float* dst = ranges;
   if (flags & NM_OUTPUT_HOST) {

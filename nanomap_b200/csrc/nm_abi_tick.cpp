@@ -100,7 +100,7 @@ int fill_stage(nm_tick_plan p, TickStage* st, uint64_t* bound) {
     }
     cap += nm::ray_leaf_cap(m, fr.sensor, (uint64_t)fr.sensor->desc.hres * fr.sensor->desc.vres);
     if (p->sim) {
-      nm::make_ray_params(fr.sensor, fr.pose, &rb.rp[i]);
+      nm::make_ray_params(fr.sensor, fr.pose, p->sim->view.res, &rb.rp[i]);
       rb.out[i] = const_cast<float*>(fr.ranges);
       rb.tiles_x[i] = (fr.sensor->desc.hres + 15) / 16;
       rb.tile_start[i + 1] = rb.tile_start[i] + (uint32_t)(rb.tiles_x[i] * ((fr.sensor->desc.vres + 15) / 16));

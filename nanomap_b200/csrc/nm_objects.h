@@ -137,6 +137,7 @@ IntegrateParams integrate_params(nm_map m);
 int do_integrate(nm_map m, cudaStream_t s);
 int check_device_errors(nm_map m, cudaStream_t s);
 int validate_pose(const nm_pose* pose);
-void make_ray_params(nm_sensor s, const nm_pose& pose, SimRayParams* rp);
+// Ray parameters of a sensor at a pose over a sim map of voxel size `res`.
+void make_ray_params(nm_sensor s, const nm_pose& pose, float res, SimRayParams* rp);
 int check_launch_shape(int tile_w, int tile_h, int entries);
 }  // namespace nm

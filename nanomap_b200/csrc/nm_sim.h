@@ -40,6 +40,11 @@ struct SimRayParams {
   float R[9];
   float pos[3];
   float min_range, max_range;
+  // per-frame constants of every pixel's ray, divided on the host (IEEE round to nearest, the
+  // same values as dividing on the device): the eye in voxel units and the range limits
+  float eye[3];
+  float tmin, tmax;  // min_range / res, max_range / res
+  int32_t pad2;
 };
 
 // Fused simulated frame: the traversal renders each tile's ranges from the sim map (with the

@@ -214,15 +214,11 @@ __device__ __forceinline__ float sim_ray(const SimMapView& v, const SimRayParams
   const float m2 = __fadd_rn(__fadd_rn(__fmul_rn(R[6], d0), __fmul_rn(R[7], d1)), __fmul_rn(R[8], d2));
   const float norm = __fsqrt_rn(__fadd_rn(__fadd_rn(__fmul_rn(m0, m0), __fmul_rn(m1, m1)), __fmul_rn(m2, m2)));
   float dir[3] = {__fdiv_rn(m0, norm), __fdiv_rn(m1, norm), __fdiv_rn(m2, norm)};
-  const float eye[3] = {__fdiv_rn(rp.pos[0], v.res), __fdiv_rn(rp.pos[1], v.res),
-                        __fdiv_rn(rp.pos[2], v.res)};
-  float tmin, tmax;
+  const float eye[3] = {rp.eye[0], rp.eye[1], rp.eye[2]};  // pos / res
+  float tmin = rp.tmin, tmax = rp.tmax;                     // range limits / res
   if (rp.type == NM_SENSOR_FRUSTUM) {
-    tmin = __fmul_rn(__fdiv_rn(rp.min_range, v.res), norm);
-    tmax = __fmul_rn(__fdiv_rn(rp.max_range, v.res), norm);
-  } else {
-    tmin = __fdiv_rn(rp.min_range, v.res);
-    tmax = __fdiv_rn(rp.max_range, v.res);
+    tmin = __fmul_rn(tmin, norm);
+    tmax = __fmul_rn(tmax, norm);
   }
   return sim_cast(v, eye, dir, tmin, tmax);
 }
