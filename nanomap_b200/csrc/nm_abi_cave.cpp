@@ -391,8 +391,10 @@ int nm_cave_smooth(nm_cave c, uint32_t flags) {
   const int mode_2d = (flags & NM_CAVE_2D) ? 1 : 0;
   for (int it = 0; it < c->desc.smoothing_count; ++it) {
     const nm::CaveLattice L = current(c);
+    // the region labels' buffer (4 bytes per cell) is free while the cells change
     NM_CUDA(nm::launch_cave_smooth(L, L.cells, c->d_cells[1 - c->cur], c->desc.active_max,
-                                   c->desc.active_min, mode_2d, s));
+                                   c->desc.active_min, mode_2d,
+                                   reinterpret_cast<uint8_t*>(c->d_parent), s));
     c->cur = 1 - c->cur;
   }
   NM_CUDA(cudaStreamSynchronize(s));

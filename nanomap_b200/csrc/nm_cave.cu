@@ -150,6 +150,51 @@ __global__ void k_cave_smooth3d(CaveLattice L, const uint8_t* __restrict__ cur,
   }
 }
 
+// The 26-neighbour count of k_cave_smooth3d in two passes: the 3 x 3 in-plane sums of every
+// cell (all planes, the ceiling included), then per cell the sums of its plane and the planes
+// below and above it (where they are neighbours) minus the cell itself.
+__global__ void k_cave_plane_sums(CaveLattice L, const uint8_t* __restrict__ cur,
+                                  uint8_t* __restrict__ sums) {
+  const long long n = cave_cell_count(L);
+  const int nzp = L.nz + 1;
+  for (long long c = (long long)blockIdx.x * blockDim.x + threadIdx.x; c < n;
+       c += (long long)gridDim.x * blockDim.x) {
+    int i, j, k;
+    cell_ijk(L, c, &i, &j, &k);
+    int sum = 0;
+    for (int dx = -1; dx <= 1; ++dx) {
+      const int ii = i + dx;
+      if (ii < 0 || ii >= L.nx) continue;
+      for (int dy = -1; dy <= 1; ++dy) {
+        const int jj = j + dy;
+        if (jj < 0 || jj >= L.ny) continue;
+        sum += cur[((long long)ii * L.ny + jj) * nzp + k];
+      }
+    }
+    sums[c] = (uint8_t)sum;
+  }
+}
+
+__global__ void k_cave_smooth3d_sums(CaveLattice L, const uint8_t* __restrict__ cur,
+                                     const uint8_t* __restrict__ sums, uint8_t* __restrict__ next,
+                                     int amax, int amin) {
+  const long long n = cave_cell_count(L);
+  const int nzp = L.nz + 1;
+  const int ktop = L.ceil_adjacent ? L.nz : L.nz - 1;
+  for (long long c = (long long)blockIdx.x * blockDim.x + threadIdx.x; c < n;
+       c += (long long)gridDim.x * blockDim.x) {
+    const int k = (int)(c % nzp);
+    if (k >= L.nz) {
+      next[c] = 0;
+      continue;
+    }
+    int cnt = sums[c] - cur[c];
+    if (k > 0) cnt += sums[c - 1];
+    if (k + 1 <= ktop) cnt += sums[c + 1];
+    next[c] = cnt > amax ? 1 : (cnt < amin ? 0 : cur[c]);
+  }
+}
+
 // One step of CaveGen::smoothMapXY: 8-neighbour count in the floor plane (k = 0), the result
 // written to the whole column below the ceiling.
 __global__ void k_cave_smooth2d(CaveLattice L, const uint8_t* __restrict__ cur,
@@ -484,11 +529,16 @@ cudaError_t launch_cave_fill_libc(const CaveLattice& L, const uint32_t* mats, in
 }
 
 cudaError_t launch_cave_smooth(const CaveLattice& L, const uint8_t* cur, uint8_t* next, int amax,
-                               int amin, int mode_2d, cudaStream_t s) {
-  if (mode_2d)
+                               int amin, int mode_2d, uint8_t* scratch, cudaStream_t s) {
+  if (mode_2d) {
     k_cave_smooth2d<<<grid_for((long long)L.nx * L.ny), 256, 0, s>>>(L, cur, next, amax, amin);
-  else
+  } else if (scratch) {
+    const int g = grid_for(cave_cell_count(L));
+    k_cave_plane_sums<<<g, 256, 0, s>>>(L, cur, scratch);
+    k_cave_smooth3d_sums<<<g, 256, 0, s>>>(L, cur, scratch, next, amax, amin);
+  } else {
     k_cave_smooth3d<<<grid_for(cave_cell_count(L)), 256, 0, s>>>(L, cur, next, amax, amin);
+  }
   return cudaGetLastError();
 }
 

@@ -69,8 +69,10 @@ constexpr int kLibcChunk = 31 * 32;
 cudaError_t launch_cave_fill_libc(const CaveLattice& L, const uint32_t* mats, int nmats,
                                   const uint32_t* state0, long long n_draws, int pct, int mode_2d,
                                   cudaStream_t s);
+// One smoothing step; `scratch` (one byte per cell, may be null) holds the in-plane sums of
+// the two-pass 3-D form.
 cudaError_t launch_cave_smooth(const CaveLattice& L, const uint8_t* cur, uint8_t* next, int amax,
-                               int amin, int mode_2d, cudaStream_t s);
+                               int amin, int mode_2d, uint8_t* scratch, cudaStream_t s);
 cudaError_t launch_cave_floor_ceil(const CaveLattice& L, cudaStream_t s);
 // Regions: labels (one int per cell), sizes and minimum order keys per root, statistics.
 cudaError_t launch_cave_regions(const CaveLattice& L, int32_t* parent, uint32_t* size,
