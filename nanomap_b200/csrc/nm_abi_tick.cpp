@@ -102,8 +102,9 @@ int fill_stage(nm_tick_plan p, TickStage* st, uint64_t* bound) {
     if (p->sim) {
       nm::make_ray_params(fr.sensor, fr.pose, p->sim->view.res, &rb.rp[i]);
       rb.out[i] = const_cast<float*>(fr.ranges);
-      rb.tiles_x[i] = (fr.sensor->desc.hres + 15) / 16;
-      rb.tile_start[i + 1] = rb.tile_start[i] + (uint32_t)(rb.tiles_x[i] * ((fr.sensor->desc.vres + 15) / 16));
+      constexpr int T = nm::kRenderTile;
+      rb.tiles_x[i] = (fr.sensor->desc.hres + T - 1) / T;
+      rb.tile_start[i + 1] = rb.tile_start[i] + (uint32_t)(rb.tiles_x[i] * ((fr.sensor->desc.vres + T - 1) / T));
       rb.noise_seed[i] = p->seed ^ (0x9E3779B97F4A7C15ull * (p->tick + 1)) ^ (0xBF58476D1CE4E5B9ull * (uint64_t)(i + 1));
     }
   }

@@ -287,8 +287,9 @@ __global__ void __launch_bounds__(64) k_sim_render_noisy(SimMapView v, SimRayPar
   out[i] = noisy(sim_ray(v, rp, w, h), seed, i, sigma_coef, drop);
 }
 
-// All slots of a tick plan in one launch: one CTA per 16x16 tile of some slot.
-__global__ void __launch_bounds__(256) k_sim_render_batch(const RenderBatch* b, SimMapView v) {
+// All slots of a tick plan in one launch: one CTA per kRenderTile^2-pixel tile of some slot.
+__global__ void __launch_bounds__(kRenderTile * kRenderTile) k_sim_render_batch(const RenderBatch* b,
+                                                                            SimMapView v) {
   __shared__ SimRayParams s_rp;
   __shared__ int s_slot;
   const uint32_t tile = blockIdx.x;
@@ -307,7 +308,8 @@ __global__ void __launch_bounds__(256) k_sim_render_batch(const RenderBatch* b, 
   __syncthreads();
   const uint32_t lt = tile - b->tile_start[sl];
   const int tx = (int)(lt % (uint32_t)b->tiles_x[sl]), ty = (int)(lt / (uint32_t)b->tiles_x[sl]);
-  const int w = tx * 16 + (threadIdx.x & 15), h = ty * 16 + (threadIdx.x >> 4);
+  const int w = tx * kRenderTile + (int)(threadIdx.x % kRenderTile);
+  const int h = ty * kRenderTile + (int)(threadIdx.x / kRenderTile);
   if (w >= s_rp.width || h >= s_rp.height) return;
   float x = sim_ray(v, s_rp, w, h);
   const long long i = (long long)h * s_rp.width + w;
@@ -363,7 +365,8 @@ cudaError_t launch_sim_cast(const SimMapView& v, const float* origins, const flo
 
 cudaError_t launch_render_batch(const RenderBatch* d_batch, uint32_t total_tiles,
                                 const SimMapView& v, cudaStream_t s) {
-  if (total_tiles > 0) k_sim_render_batch<<<total_tiles, 256, 0, s>>>(d_batch, v);
+  if (total_tiles > 0)
+    k_sim_render_batch<<<total_tiles, kRenderTile * kRenderTile, 0, s>>>(d_batch, v);
   return cudaGetLastError();
 }
 

@@ -64,6 +64,8 @@ cudaError_t launch_traverse_render(const TickWork<1>& w, const MapView& m, const
                                    int rounding, cudaStream_t s);
 
 constexpr int kMaxRenderSlots = 32;
+// Pixels per side of a batched render tile (one CTA of kRenderTile^2 threads per tile).
+constexpr int kRenderTile = 8;
 
 // Every slot of a tick plan rendered (and optionally noised) in one launch.
 struct RenderBatch {
