@@ -15,6 +15,7 @@
 // in the reference's name scan (Manager.h:55-57).
 #pragma once
 
+#include <array>
 #include <chrono>
 #include <cmath>
 #include <cstdint>
@@ -153,6 +154,20 @@ class Config {
       detail::check(nm_config_sensor(c, i, &d, name, sizeof(name)));
       sensors_.push_back(std::make_shared<sensor::SensorData>(name, d));
     }
+    leaf_volume_ = info_.leaf_edge * info_.leaf_edge * info_.leaf_edge;
+    for (const auto& sd : sensors_) {
+      const nm_sensor_desc& d = sd->desc();
+      const int pcl = d.hres * d.vres;
+      max_pcl_ = std::max(max_pcl_, pcl);
+      if (d.type == NM_SENSOR_FRUSTUM) {
+        frustum_pcl_ = std::max(frustum_pcl_, pcl);
+        const double leaf = (double)info_.mapping_res * info_.leaf_edge;
+        const int n = leaf > 0.0 ? (int)std::ceil(2.0 * d.max_range / leaf) + 2 : 0;
+        frustum_leaf_buffer_ = std::max(frustum_leaf_buffer_, n * n * n);
+      } else if (d.type == NM_SENSOR_LASER) {
+        laser_pcl_ = std::max(laser_pcl_, pcl);
+      }
+    }
   }
   std::vector<std::shared_ptr<sensor::SensorData>>& sensorData() { return sensors_; }
   std::shared_ptr<sensor::SensorData> sensorData(int index, bool searchById = false) {
@@ -179,6 +194,23 @@ class Config {
   float& probHitThres() { return info_.prob_hit_thres; }
   float& probMissThres() { return info_.prob_miss_thres; }
   float& frustumAllocationFactor() { return info_.frustum_allocation_factor; }
+  // Keys the reference's reader never reads (Config.cpp:60-113): they keep their defaults.
+  int& exploreType() { return explore_type_; }
+  int& simType() { return sim_type_; }
+  bool& serialUpdate() { return serial_update_; }
+  float& laserAllocationFactor() { return laser_allocation_factor_; }
+  // Derived as in Config::init (Config.cpp:24-58): leaf volume and the largest point cloud of
+  // all, of the frustum and of the laser sensors.  frustumLeafBufferSize is an upper bound of
+  // the leaves any rotation of a frustum sensor covers, the leaf box of its range sphere (the
+  // reference searches 5.8 M rotations for the exact worst case; this library bounds each
+  // frame's leaves from its pose instead).  laserVoxelBufferSize is left at 0, as the
+  // reference leaves it unset.
+  int& leafVolume() { return leaf_volume_; }
+  int& maxPCLSize() { return max_pcl_; }
+  int& frustumPCLSize() { return frustum_pcl_; }
+  int& laserPCLSize() { return laser_pcl_; }
+  int& frustumLeafBufferSize() { return frustum_leaf_buffer_; }
+  int& laserVoxelBufferSize() { return laser_voxel_buffer_; }
   std::string& config() { return file_; }
   std::string simGrid() const { return info_.sim_grid; }
   int agentCount() const { return info_.n_agents; }
@@ -194,6 +226,11 @@ class Config {
   std::shared_ptr<nm_config_s> cfg_;
   nm_config_info info_{};
   std::vector<std::shared_ptr<sensor::SensorData>> sensors_;
+  int explore_type_ = 0, sim_type_ = 0;
+  bool serial_update_ = false;
+  float laser_allocation_factor_ = 0.f;
+  int leaf_volume_ = 0, max_pcl_ = 0, frustum_pcl_ = 0, laser_pcl_ = 0;
+  int frustum_leaf_buffer_ = 0, laser_voxel_buffer_ = 0;
 };
 }  // namespace config
 
@@ -262,7 +299,7 @@ class Agent {
  public:
   // Agent `index` of the config (Agent.h:49-135): fixed spawn position, the reference's fixed
   // body rotation (columns (0,-1,0), (1,0,0), (0,0,1)), sensors with mount poses.
-  Agent(config::Config& cfg, int index, std::shared_ptr<map::Map> map = nullptr) {
+  Agent(config::Config& cfg, int index, std::shared_ptr<map::Map> map = nullptr) : id_(index) {
     nm_agent_info a;
     detail::check(nm_config_agent(cfg.handle(), index, &a));
     if (a.spawn_random)
@@ -313,8 +350,27 @@ class Agent {
   const std::vector<Vector3f>& observationRays() const { return obs_rays_; }
   float collisionDist() const { return collision_dist_; }
   float observationLength() const { return len_obs_; }
+  // Agent.h:181-192: (collision distance, observation length) for each observation ray.
+  std::vector<std::array<float, 2>> observationNorms() const {
+    return std::vector<std::array<float, 2>>(obs_rays_.size(), {collision_dist_, len_obs_});
+  }
+  // Agent.h:198-207
+  void clearSensors() {
+    poses_.clear();
+    names_.clear();
+    origins_.clear();
+  }
+  void clearObservationRays() { obs_rays_.clear(); }
+  void resetAgent() {
+    clearSensors();
+    clearObservationRays();
+  }
+  // The reference never sets its agent id and name; here the id is the config index.
+  int getId() const { return id_; }
+  std::string getName() const { return std::string(); }
 
  private:
+  int id_ = 0;
   int num_obs_ = 0;
   float len_obs_ = 0.f, collision_dist_ = 0.f;
   std::vector<Vector3f> obs_rays_;
@@ -413,6 +469,9 @@ class SimManager {
   std::shared_ptr<agent::Agent> agent(int index) { return agents_[index]; }
   nm_simmap simMap() { return sim_.get(); }
   void closeHandler() {}
+  // empty in the reference (SimManager.h:137-139)
+  void step() {}
+  void updateObservations() {}
 
  private:
   void load_agents() {

@@ -115,3 +115,32 @@ def test_malformed_configs_fail_with_io_errors(tmp_path, text, needle):
 def test_missing_config_and_vdb_grid(tmp_path):
     h = C.c_void_p()
     assert N.lib().nm_config_load(str(tmp_path / "none.txt").encode(), C.byref(h)) == N.NM_ERR_IO
+
+
+def test_facade_config_and_agent_accessors(tmp_path):
+    """nanomap::config::Config's derived sizes (Config.cpp:24-58) and the Agent accessors of
+    Agent.h:181-214 through the C++ facade, on the host only."""
+    import subprocess
+    root = Path(__file__).resolve().parents[1]
+    exe = tmp_path / "config_demo"
+    subprocess.run(["g++", "-std=c++17", "-O1", f"-I{root / 'include'}",
+                    str(root / "tests" / "cpp" / "config_demo.cpp"), f"-L{root / 'nanomap_b200'}",
+                    "-lnanomap_b200", f"-Wl,-rpath,{root / 'nanomap_b200'}", "-o", str(exe)],
+                   check=True)
+    out = subprocess.run([str(exe), str(HEADLINE)], capture_output=True, text=True)
+    assert out.returncode == 0, out.stderr
+    v = {}
+    for line in out.stdout.splitlines():
+        k, *rest = line.split()
+        v[k] = rest
+    assert v["leafVolume"] == ["512"]
+    # the 640x480 camera and the 64x1024 spinning laser of the headline config
+    assert v["maxPCLSize"] == ["307200"] and v["frustumPCLSize"] == ["307200"]
+    assert v["laserPCLSize"] == ["65536"]
+    # leaf box of the camera's 10 m range sphere at 0.05 m x 8: (ceil(20 / 0.4) + 2)^3
+    assert v["frustumLeafBufferSize"] == [str(52 ** 3)]
+    assert v["processType"] == ["1"] and v["laserVoxelBufferSize"] == ["0"]
+    assert v["exploreType"] == ["0"] and v["simType"] == ["0"] and v["serialUpdate"] == ["0"]
+    assert v["agentId"] == ["0"] and int(v["sensors"][0]) >= 1
+    assert v["observationRays"] == ["80"] and v["observationNorms"] == ["80", "0.5", "20"]
+    assert v["sensorsAfterReset"] == ["0"] and v["raysAfterReset"] == ["0"]
