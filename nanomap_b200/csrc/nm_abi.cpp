@@ -762,6 +762,7 @@ int nm_map_create(nm_context ctx, const nm_map_desc* d, nm_map* out) {
     return rc;
   }
   NM_CUDA(cudaStreamSynchronize(ctx->stream));
+  nm::prepare_integrate();
   for (int i = 0; i < nm::kMaxPlanes; ++i) m->pending_lh[i] = m->pending_lm[i] = 0.f;
   nm::retain(ctx);
   *out = m.release();

@@ -189,6 +189,8 @@ cudaError_t launch_traverse_counts(const FrameParams& f, const MapView& m, int r
                                    cudaStream_t s);
 cudaError_t launch_integrate(const MapView& m, const IntegrateParams& p, int update_mode,
                              int rounding, int sm_count, cudaStream_t s);
+// Queries the integration kernels' resident blocks per SM ahead of any stream capture.
+void prepare_integrate();
 cudaError_t launch_rehash(const MapView& from, const MapView& to, uint32_t cur_epoch,
                           int update_mode, cudaStream_t s);
 cudaError_t launch_export(const MapView& m, int32_t* origins, float* values, uint32_t* active,

@@ -3,6 +3,7 @@
 //
 // Replaces frustumCastCloud.cu:84-294 (leaf pass, CUB compaction, voxel pass with per-visit
 // fp32 atomics, int8 quantisation) and the host map update of Handler.cpp:134-182.
+#include <atomic>
 #include <cfloat>
 #include <cstdint>
 
@@ -84,33 +85,48 @@ __global__ void __launch_bounds__(256) k_traverse_count(FrameParams f, MapView m
 
 // ---- integration (Handler.cpp:88-122 / SimHandler.cpp:88-122) ------------------------------
 
-template <int RM>
+// Update of one voxel by `temp` (Handler.cpp:99-104 when Always: clamp, then set or clear
+// the active bit by the thresholds; SimHandler.cpp:100-110 otherwise: clamp only on the side
+// whose threshold was crossed).  `temp` == 0 leaves the voxel as it is.  Written with selects,
+// so lanes with different outcomes take no divergent branches.
+template <int RM, bool Always>
 __device__ __forceinline__ float update_voxel(float v, uint32_t& abit, float temp,
                                               const IntegrateParams& p) {
-  if (temp != 0.0f) {
-    v = Ar<RM>::fadd(v, temp);
-    if (p.clamp_mode == NM_CLAMP_ALWAYS) {
-      if (v > p.clamp_max) {
-        v = p.clamp_max;
-      } else if (v < p.clamp_min) {
-        v = p.clamp_min;
-      }
-      if (v > p.thres_hit) {
-        abit = 1u;
-      } else if (v < p.thres_miss) {
-        abit = 0u;
-      }
-    } else {
-      if (v > p.thres_hit) {
-        abit = 1u;
-        if (v > p.clamp_max) v = p.clamp_max;
-      } else if (v < p.thres_miss) {
-        abit = 0u;
-        if (v < p.clamp_min) v = p.clamp_min;
-      }
-    }
+  const float s = Ar<RM>::fadd(v, temp);
+  float c;
+  uint32_t a;
+  if (Always) {
+    c = s > p.clamp_max ? p.clamp_max : (s < p.clamp_min ? p.clamp_min : s);
+    a = c > p.thres_hit ? 1u : (c < p.thres_miss ? 0u : abit);
+  } else {
+    const bool up = s > p.thres_hit;
+    const bool down = !up && s < p.thres_miss;
+    c = (up && s > p.clamp_max) ? p.clamp_max : ((down && s < p.clamp_min) ? p.clamp_min : s);
+    a = up ? 1u : (down ? 0u : abit);
   }
-  return v;
+  const bool apply = temp != 0.0f;
+  abit = apply ? a : abit;
+  return apply ? c : v;
+}
+
+// The frame's touched-leaf count and the probe error bit, read once per block: every warp
+// reading the counter word itself queues thousands of requests on one L2 line.
+__device__ __forceinline__ void read_integrate_counters(const MapCounters* ctr, uint32_t* n,
+                                                        bool* fatal) {
+  __shared__ uint32_t s_n, s_err;
+  if (threadIdx.x == 0) {
+    s_n = *(const volatile unsigned int*)&ctr->touched_count;
+    s_err = *(const volatile unsigned int*)&ctr->error_flags;
+  }
+  __syncthreads();
+  *n = s_n;
+  *fatal = (s_err & kErrProbe) != 0u;
+}
+
+// Warp of the integration grid that takes touched leaf i: leaf i goes to block i % grid, so
+// the leaves of a small frame spread over all SMs instead of filling the first blocks.
+__device__ __forceinline__ uint32_t integrate_warp() {
+  return (threadIdx.x >> 5) * gridDim.x + blockIdx.x;
 }
 
 // The last CTA to finish resets the per-frame list and folds it into the totals.
@@ -141,13 +157,14 @@ __device__ __forceinline__ void integrate_epilogue(MapCounters* ctr, uint32_t n_
 // One warp per touched leaf.  Lane i owns float4 i, i+32, i+64, i+96 of the leaf's 512
 // log-odds (voxels 4q..4q+3 of float4 q); label and active words are shared through
 // shuffles.  Labels are cleared as they are consumed, so the next frame starts from zero.
-template <int RM>
+template <int RM, bool Always>
 __global__ void __launch_bounds__(256) k_integrate_label(MapView m, IntegrateParams p) {
   const int lane = threadIdx.x & 31;
-  const uint32_t gw = (blockIdx.x * blockDim.x + threadIdx.x) >> 5;
+  const uint32_t gw = integrate_warp();
   const uint32_t nw = (gridDim.x * blockDim.x) >> 5;
-  const uint32_t n = *(volatile unsigned int*)&m.ctr->touched_count;
-  const bool fatal = (*(volatile unsigned int*)&m.ctr->error_flags & kErrProbe) != 0u;
+  uint32_t n;
+  bool fatal;
+  read_integrate_counters(m.ctr, &n, &fatal);
   unsigned long long uniq = 0;
   for (uint32_t i = gw; i < n; i += nw) {
     const uint32_t slot = m.touched[i];
@@ -183,16 +200,14 @@ __global__ void __launch_bounds__(256) k_integrate_label(MapView m, IntegratePar
         const uint32_t hn = (__shfl_sync(kFull, myw, w) >> sh) & 0xFu;
         const uint32_t mn = (__shfl_sync(kFull, myw, 16 + w) >> sh) & 0xFu;
         const uint32_t tn = hn | mn;
-        if (tn) {
-          touched_any[k] |= tn;
-          uint32_t a0 = anib[k] & 1u, a1 = (anib[k] >> 1) & 1u, a2 = (anib[k] >> 2) & 1u,
-                   a3 = (anib[k] >> 3) & 1u;
-          if (tn & 1u) v[k].x = update_voxel<RM>(v[k].x, a0, (hn & 1u) ? lh : lm, p);
-          if (tn & 2u) v[k].y = update_voxel<RM>(v[k].y, a1, (hn & 2u) ? lh : lm, p);
-          if (tn & 4u) v[k].z = update_voxel<RM>(v[k].z, a2, (hn & 4u) ? lh : lm, p);
-          if (tn & 8u) v[k].w = update_voxel<RM>(v[k].w, a3, (hn & 8u) ? lh : lm, p);
-          anib[k] = a0 | (a1 << 1) | (a2 << 2) | (a3 << 3);
-        }
+        touched_any[k] |= tn;
+        uint32_t a0 = anib[k] & 1u, a1 = (anib[k] >> 1) & 1u, a2 = (anib[k] >> 2) & 1u,
+                 a3 = (anib[k] >> 3) & 1u;
+        v[k].x = update_voxel<RM, Always>(v[k].x, a0, (tn & 1u) ? ((hn & 1u) ? lh : lm) : 0.0f, p);
+        v[k].y = update_voxel<RM, Always>(v[k].y, a1, (tn & 2u) ? ((hn & 2u) ? lh : lm) : 0.0f, p);
+        v[k].z = update_voxel<RM, Always>(v[k].z, a2, (tn & 4u) ? ((hn & 4u) ? lh : lm) : 0.0f, p);
+        v[k].w = update_voxel<RM, Always>(v[k].w, a3, (tn & 8u) ? ((hn & 8u) ? lh : lm) : 0.0f, p);
+        anib[k] = a0 | (a1 << 1) | (a2 << 2) | (a3 << 3);
       }
     }
     if (fatal) continue;
@@ -218,13 +233,14 @@ __global__ void __launch_bounds__(256) k_integrate_label(MapView m, IntegratePar
   integrate_epilogue(m.ctr, n, uniq);
 }
 
-template <int RM>
+template <int RM, bool Always>
 __global__ void __launch_bounds__(256) k_integrate_count(MapView m, IntegrateParams p) {
   const int lane = threadIdx.x & 31;
-  const uint32_t gw = (blockIdx.x * blockDim.x + threadIdx.x) >> 5;
+  const uint32_t gw = integrate_warp();
   const uint32_t nw = (gridDim.x * blockDim.x) >> 5;
-  const uint32_t n = *(volatile unsigned int*)&m.ctr->touched_count;
-  const bool fatal = (*(volatile unsigned int*)&m.ctr->error_flags & kErrProbe) != 0u;
+  uint32_t n;
+  bool fatal;
+  read_integrate_counters(m.ctr, &n, &fatal);
   unsigned long long uniq = 0;
   const float lh = p.lh[0], lm = p.lm[0];
   for (uint32_t i = gw; i < n; i += nw) {
@@ -242,7 +258,7 @@ __global__ void __launch_bounds__(256) k_integrate_count(MapView m, IntegratePar
         cnt[512 + l] = 0u;
         if (!fatal) {
           const float temp = Ar<RM>::fadd(Ar<RM>::fmul((float)nm_, lm), Ar<RM>::fmul((float)nh, lh));
-          val[l] = update_voxel<RM>(val[l], abit, temp, p);
+          val[l] = update_voxel<RM, Always>(val[l], abit, temp, p);
           uniq += 1;
         }
       }
@@ -367,21 +383,63 @@ cudaError_t launch_traverse_counts(const FrameParams& f, const MapView& m, int r
   return cudaGetLastError();
 }
 
+namespace {
+
+// Integration grids hold exactly the blocks that are resident at once (one wave): a second
+// wave of blocks would only add block launches and counter traffic after the first finishes.
+std::atomic<int> g_integrate_blocks_per_sm[8];
+
+template <typename Kernel>
+int integrate_blocks_per_sm(Kernel kernel, int variant) {
+  int b = g_integrate_blocks_per_sm[variant].load(std::memory_order_relaxed);
+  if (b == 0) {
+    if (cudaOccupancyMaxActiveBlocksPerMultiprocessor(&b, kernel, 256, 0) != cudaSuccess || b < 1) {
+      cudaGetLastError();
+      b = 1;
+    }
+    g_integrate_blocks_per_sm[variant].store(b, std::memory_order_relaxed);
+  }
+  return b;
+}
+
+template <typename Kernel>
+cudaError_t launch_integrate_kernel(Kernel kernel, int variant, const MapView& m,
+                                    const IntegrateParams& p, int sm_count, cudaStream_t s) {
+  const int blocks = sm_count * integrate_blocks_per_sm(kernel, variant);
+  kernel<<<blocks, 256, 0, s>>>(m, p);
+  return cudaGetLastError();
+}
+
+template <int RM, bool Always>
+cudaError_t launch_integrate_t(const MapView& m, const IntegrateParams& p, bool label,
+                               int sm_count, cudaStream_t s) {
+  const int variant = (label ? 4 : 0) + (RM == NM_ROUND_DOWN ? 2 : 0) + (Always ? 1 : 0);
+  if (label) return launch_integrate_kernel(k_integrate_label<RM, Always>, variant, m, p, sm_count, s);
+  return launch_integrate_kernel(k_integrate_count<RM, Always>, variant, m, p, sm_count, s);
+}
+
+}  // namespace
+
 cudaError_t launch_integrate(const MapView& m, const IntegrateParams& p, int update_mode,
                              int rounding, int sm_count, cudaStream_t s) {
-  const dim3 grid(sm_count * 8), block(256);
-  if (update_mode == NM_UPDATE_LABEL) {
-    if (rounding == NM_ROUND_DOWN)
-      k_integrate_label<NM_ROUND_DOWN><<<grid, block, 0, s>>>(m, p);
-    else
-      k_integrate_label<NM_ROUND_NEAREST><<<grid, block, 0, s>>>(m, p);
-  } else {
-    if (rounding == NM_ROUND_DOWN)
-      k_integrate_count<NM_ROUND_DOWN><<<grid, block, 0, s>>>(m, p);
-    else
-      k_integrate_count<NM_ROUND_NEAREST><<<grid, block, 0, s>>>(m, p);
-  }
-  return cudaGetLastError();
+  const bool label = update_mode == NM_UPDATE_LABEL;
+  const bool always = p.clamp_mode == NM_CLAMP_ALWAYS;
+  if (rounding == NM_ROUND_DOWN)
+    return always ? launch_integrate_t<NM_ROUND_DOWN, true>(m, p, label, sm_count, s)
+                  : launch_integrate_t<NM_ROUND_DOWN, false>(m, p, label, sm_count, s);
+  return always ? launch_integrate_t<NM_ROUND_NEAREST, true>(m, p, label, sm_count, s)
+                : launch_integrate_t<NM_ROUND_NEAREST, false>(m, p, label, sm_count, s);
+}
+
+void prepare_integrate() {
+  integrate_blocks_per_sm(k_integrate_label<NM_ROUND_DOWN, true>, 7);
+  integrate_blocks_per_sm(k_integrate_label<NM_ROUND_DOWN, false>, 6);
+  integrate_blocks_per_sm(k_integrate_label<NM_ROUND_NEAREST, true>, 5);
+  integrate_blocks_per_sm(k_integrate_label<NM_ROUND_NEAREST, false>, 4);
+  integrate_blocks_per_sm(k_integrate_count<NM_ROUND_DOWN, true>, 3);
+  integrate_blocks_per_sm(k_integrate_count<NM_ROUND_DOWN, false>, 2);
+  integrate_blocks_per_sm(k_integrate_count<NM_ROUND_NEAREST, true>, 1);
+  integrate_blocks_per_sm(k_integrate_count<NM_ROUND_NEAREST, false>, 0);
 }
 
 cudaError_t launch_rehash(const MapView& from, const MapView& to, uint32_t cur_epoch,
