@@ -30,10 +30,6 @@ __host__ __device__ inline unsigned long long splitmix64(unsigned long long z) {
   return z ^ (z >> 31);
 }
 
-__device__ __forceinline__ long long cell_index(const CaveLattice& L, int i, int j, int k) {
-  return ((long long)i * L.ny + j) * (L.nz + 1) + k;
-}
-
 __device__ __forceinline__ void cell_ijk(const CaveLattice& L, long long c, int* i, int* j,
                                          int* k) {
   const int nzp = L.nz + 1;

@@ -143,7 +143,7 @@ __device__ __forceinline__ void traverse_body(const TickWork<MaxF>& work, const 
   __shared__ int s_frame;
   __shared__ uint32_t s_next;
   const int tid = threadIdx.x;
-  const int lane = tid & 31, warp = tid >> 5, nwarps = blockDim.x >> 5;
+  const int lane = tid & 31, nwarps = blockDim.x >> 5;
   const int nrays = work.tile_w * work.tile_h;
   uint32_t visits = 0, rays = 0;
 
