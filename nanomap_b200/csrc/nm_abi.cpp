@@ -379,12 +379,15 @@ int do_integrate(nm_map m, cudaStream_t s) {
 }
 
 int check_device_errors(nm_map m, cudaStream_t s) {
-  NM_CUDA(cudaStreamSynchronize(s));
   // leaf_count, touched_count and error_flags are adjacent: one read
   static_assert(offsetof(nm::MapCounters, error_flags) ==
                     offsetof(nm::MapCounters, leaf_count) + 8, "counter layout");
-  unsigned int w[3] = {0, 0, 0};
-  NM_CUDA(cudaMemcpy(w, &m->d_ctr->leaf_count, sizeof(w), cudaMemcpyDeviceToHost));
+  // one round trip: the status words are copied into page-locked memory on the map's
+  // stream, then the stream is waited for
+  unsigned int* w = m->h_status;
+  NM_CUDA(cudaMemcpyAsync(w, &m->d_ctr->leaf_count, 3 * sizeof(unsigned int),
+                          cudaMemcpyDeviceToHost, s));
+  NM_CUDA(cudaStreamSynchronize(s));
   const unsigned int lc = w[0], flags = w[2];
   m->known_leaves = lc;
   m->pending_bound = 0;
@@ -620,6 +623,7 @@ void release(nm_map m) {
   free_view(m->view);
   cudaFree(m->d_ctr);
   cudaFree(m->d_scratch_u32);
+  cudaFreeHost(m->h_status);
   cudaFree(m->staging);
   filter_release(&m->filter);
   cudaFree(m->depth_scratch);
@@ -751,17 +755,32 @@ int nm_map_create(nm_context ctx, const nm_map_desc* d, nm_map* out) {
   std::unique_ptr<nm_map_s> m(new nm_map_s());
   m->ctx = ctx;
   m->desc = *d;
-  NM_CUDA(cudaMalloc((void**)&m->d_ctr, sizeof(nm::MapCounters)));
-  NM_CUDA(cudaMemsetAsync(m->d_ctr, 0, sizeof(nm::MapCounters), ctx->stream));
-  NM_CUDA(cudaMalloc((void**)&m->d_scratch_u32, 64));
+  auto free_small = [&]() {
+    cudaFree(m->d_ctr);
+    cudaFree(m->d_scratch_u32);
+    cudaFreeHost(m->h_status);
+  };
+  cudaError_t e = cudaMalloc((void**)&m->d_ctr, sizeof(nm::MapCounters));
+  if (e == cudaSuccess) e = cudaMemsetAsync(m->d_ctr, 0, sizeof(nm::MapCounters), ctx->stream);
+  if (e == cudaSuccess) e = cudaMalloc((void**)&m->d_scratch_u32, 64);
+  if (e == cudaSuccess) e = cudaHostAlloc((void**)&m->h_status, 16, cudaHostAllocDefault);
+  if (e != cudaSuccess) {
+    free_small();
+    cudaGetLastError();
+    return fail(NM_ERR_CUDA, "map counters: %s", cudaGetErrorString(e));
+  }
   const uint32_t cap = next_pow2(std::max<uint64_t>(d->initial_leaf_capacity ? d->initial_leaf_capacity : (1u << 18), 1024));
   const int rc = alloc_view(m.get(), cap, &m->view, ctx->stream);
   if (rc != NM_OK) {
-    cudaFree(m->d_ctr);
-    cudaFree(m->d_scratch_u32);
+    free_small();
     return rc;
   }
-  NM_CUDA(cudaStreamSynchronize(ctx->stream));
+  e = cudaStreamSynchronize(ctx->stream);
+  if (e != cudaSuccess) {
+    free_view(m->view);
+    free_small();
+    return fail(NM_ERR_CUDA, "map set-up: %s", cudaGetErrorString(e));
+  }
   nm::prepare_integrate();
   for (int i = 0; i < nm::kMaxPlanes; ++i) m->pending_lh[i] = m->pending_lm[i] = 0.f;
   nm::retain(ctx);

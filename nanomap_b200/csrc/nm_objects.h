@@ -84,6 +84,7 @@ struct nm_map_s {
   unsigned char* staging = nullptr;  // device copy of host input
   size_t staging_bytes = 0;
   uint32_t* d_scratch_u32 = nullptr;  // export counters
+  unsigned int* h_status = nullptr;   // page-locked copy of the map's status words
   int tile_w = 16, tile_h = 16, smem_entries = 128;
   nm::FilterBuffers filter{};  // voxel-filter buffers, grown on first filtered insert
   double* depth_scratch = nullptr;  // expected-depth partial sums (grown on demand)
