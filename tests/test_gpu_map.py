@@ -78,15 +78,22 @@ def test_xyz_records_host_and_device_inputs(ctx, small, cut):
     assert not compare_maps(m_dev.export(), oe)
 
 
+@pytest.mark.parametrize("update_mode", [N.NM_UPDATE_LABEL, N.NM_UPDATE_ACCUMULATE])
 @pytest.mark.parametrize("clamp_mode", [N.NM_CLAMP_ALWAYS, N.NM_CLAMP_ON_CROSSING])
-def test_accumulate_mode_and_clamp_orders(ctx, small, clamp_mode):
+@pytest.mark.parametrize("thres", [(0.3, -0.2), (1.6, -1.1)])
+def test_update_modes_and_clamp_orders(ctx, small, update_mode, clamp_mode, thres):
+    """Both integration kernels under both clamp orders (Handler.cpp:99-104 clamps every
+    update; SimHandler.cpp:100-110 only on a threshold crossing), with clamps that five
+    frames reach.  Thresholds inside the clamp range give both orders the same map;
+    thresholds outside it make them differ (values past a clamp, active bits)."""
     spec, scene, desc, frames = small
     res = spec.map_res
     sensor = A.Sensor(ctx, desc)
     osen = O.Sensor.from_desc(desc)
-    kw = dict(clamp_min=-1.0, clamp_max=1.5, thres_hit=0.3, thres_miss=-0.2)
-    m = A.Map(ctx, A.map_desc(res=res, update_mode=N.NM_UPDATE_ACCUMULATE, clamp_mode=clamp_mode, **kw))
-    om = O.Map(res, update_mode=1, clamp_mode=clamp_mode, **kw)
+    kw = dict(clamp_min=-1.0, clamp_max=1.5, thres_hit=thres[0], thres_miss=thres[1])
+    m = A.Map(ctx, A.map_desc(res=res, update_mode=update_mode, clamp_mode=clamp_mode, **kw))
+    om = O.Map(res, update_mode=1 if update_mode == N.NM_UPDATE_ACCUMULATE else 0,
+               clamp_mode=clamp_mode, **kw)
     for pose, ranges in frames[:5]:
         m.insert_ranges(sensor, pose, _torch(ranges))
         R, eye, mt = oracle_frame(desc, pose, res, 1)
