@@ -201,7 +201,8 @@ def _same_maps(a, b):
             and np.array_equal(aa[ia], ba[ib]))
 
 
-@pytest.mark.parametrize("kind", ["camera", "odd_camera", "laser", "accumulate", "filtered"])
+@pytest.mark.parametrize("kind", ["camera", "camera_nearest", "odd_camera", "laser", "accumulate",
+                                  "filtered"])
 def test_sim_insert_equals_render_then_insert(ctx, kind):
     """nm_sim_insert (the fused render + insert in label mode; render then insert for the
     per-ray sums and the voxel filter) gives the ranges and the map of nm_sim_render_noisy
@@ -224,8 +225,11 @@ def test_sim_insert_equals_render_then_insert(ctx, kind):
     sensor = A.Sensor(ctx, desc)
     mode = N.NM_UPDATE_ACCUMULATE if kind == "accumulate" else N.NM_UPDATE_LABEL
     flags = N.NM_FILTER_MEAN if kind == "filtered" else 0
-    ma = A.Map(ctx, A.map_desc(res=res, clamp_min=-2.0, clamp_max=3.5, update_mode=mode))
-    mb = A.Map(ctx, A.map_desc(res=res, clamp_min=-2.0, clamp_max=3.5, update_mode=mode))
+    rnd = N.NM_ROUND_NEAREST if kind == "camera_nearest" else N.NM_ROUND_DOWN
+    ma = A.Map(ctx, A.map_desc(res=res, clamp_min=-2.0, clamp_max=3.5, update_mode=mode,
+                               rounding=rnd))
+    mb = A.Map(ctx, A.map_desc(res=res, clamp_min=-2.0, clamp_max=3.5, update_mode=mode,
+                               rounding=rnd))
     for k, (p, q) in enumerate(S.trajectory(sc, 3, seed=11)):
         pose = A.Pose(p, q)
         a = torch.zeros((H, W), device="cuda")
@@ -239,7 +243,8 @@ def test_sim_insert_equals_render_then_insert(ctx, kind):
     sa, sb = ma.stats(), mb.stats()
     assert sa["visits"] == sb["visits"] and sa["rays"] == sb["rays"] and sb["error_flags"] == 0
     # without an output image, and with a host one
-    mc = A.Map(ctx, A.map_desc(res=res, clamp_min=-2.0, clamp_max=3.5, update_mode=mode))
+    mc = A.Map(ctx, A.map_desc(res=res, clamp_min=-2.0, clamp_max=3.5, update_mode=mode,
+                               rounding=rnd))
     host = np.zeros((H, W), np.float32)
     for k, (p, q) in enumerate(S.trajectory(sc, 3, seed=11)):
         g.insert(mc, sensor, A.Pose(p, q), 0.005, 0.02, 31 + k,

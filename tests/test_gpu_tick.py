@@ -54,12 +54,18 @@ def test_tick_labels_match_solo_runs(ctx):
     m.integrate()
 
 
-def test_tick_map_equals_sequential_solo(ctx):
-    """The shared map after ticks equals inserting every agent's frame in agent order."""
+@pytest.mark.parametrize("variant", ["down_always", "nearest_crossing"])
+def test_tick_map_equals_sequential_solo(ctx, variant):
+    """The shared map after ticks equals inserting every agent's frame in agent order (both
+    roundings; the clamp-on-crossing order with thresholds outside the clamp range)."""
     sim, sensors, agents = _agents(ctx)
     n = len(sensors)
-    batched = A.Map(ctx, A.map_desc(res=0.05, max_agents=n))
-    sequential = A.Map(ctx, A.map_desc(res=0.05))
+    kw = dict(res=0.05)
+    if variant == "nearest_crossing":
+        kw.update(rounding=N.NM_ROUND_NEAREST, clamp_mode=N.NM_CLAMP_ON_CROSSING, clamp_min=-1.0,
+                  clamp_max=1.5, thres_hit=1.6, thres_miss=-1.1)
+    batched = A.Map(ctx, A.map_desc(max_agents=n, **kw))
+    sequential = A.Map(ctx, A.map_desc(**kw))
     for t in range(3):
         batched.tick([(sensors[a], agents[a][t][0], agents[a][t][1], a) for a in range(n)])
         for a in range(n):
