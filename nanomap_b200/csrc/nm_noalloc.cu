@@ -10,11 +10,15 @@
 // framework's pool already owns the device memory the library would otherwise take.
 //
 // Limits: a frame of at most kStaticMaxPixels pixels, at most kStaticLeafSlots / 2 distinct
-// leaves labelled per call.  The array (about 9 MiB) is held by every GPU that loads the
-// library until the process exits.  Every call shares it and it keeps the last call's
-// contents, so each call first clears what must start at zero; calls that overlap on the GPU
-// (different streams, or different host threads) race on it and must be serialised by the
-// caller.
+// leaves labelled per call (checked on the device after the walk; more is NM_ERR_CAPACITY).
+// The array (about 9 MiB) belongs to this file's device module.  CUDA loads modules lazily by
+// default, so the driver places the array in a GPU's memory when the module is first used on
+// that GPU: the first call on each device (which also looks up the array's device address)
+// is the start-up warm-up, and should come before the caller's no-allocation phase and before
+// any stream capture.  From then on the array stays resident until the process exits.  Every
+// call shares it and it keeps the last call's contents, so each call first clears what must
+// start at zero; calls that overlap on the GPU (different streams, or different host threads)
+// race on it and must be serialised by the caller.
 #include <cmath>
 #include <cstdint>
 #include <cstring>
@@ -31,6 +35,7 @@ namespace {
 constexpr uint32_t kStaticLeafSlots = 1u << 16;
 constexpr int64_t kStaticMaxPixels = 1ll << 23;
 constexpr uint32_t kErrOutputFull = 8u;  // more labelled leaves than the caller's max_leaves
+constexpr uint32_t kErrLeafLimit = 16u;  // more labelled leaves than kStaticLeafSlots / 2
 
 struct StaticScratch {
   MapCounters ctr;
@@ -81,7 +86,8 @@ __global__ void __launch_bounds__(256) k_static_export(const StaticScratch* s, i
   }
   if (blockIdx.x == 0 && threadIdx.x == 0) {
     status[0] = n;
-    status[1] = s->ctr.error_flags | (n > max_leaves ? kErrOutputFull : 0u);
+    status[1] = s->ctr.error_flags | (n > max_leaves ? kErrOutputFull : 0u) |
+                (n > kStaticLeafSlots / 2 ? kErrLeafLimit : 0u);
   }
 }
 
@@ -115,7 +121,8 @@ extern "C" int nm_label_frame_static(nm_sensor s, const nm_pose* pose, const flo
     return fail(NM_ERR_ARG, "null argument");
   int rc = validate_pose(pose);
   if (rc != NM_OK) return rc;
-  if (!(res > 0.0f)) return fail(NM_ERR_ARG, "resolution must be positive");
+  if (!(std::isfinite(res) && res > 0.0f))
+    return fail(NM_ERR_ARG, "resolution must be positive and finite");
   if (rounding != NM_ROUND_NEAREST && rounding != NM_ROUND_DOWN)
     return fail(NM_ERR_ARG, "unknown rounding %d", rounding);
   const int64_t pixels = (int64_t)s->desc.hres * s->desc.vres;
@@ -185,9 +192,12 @@ extern "C" int nm_label_frame_static(nm_sensor s, const nm_pose* pose, const flo
     NM_CUDA(cudaStreamSynchronize(st));
     uint32_t hs[2] = {0u, 0u};
     NM_CUDA(cudaMemcpy(hs, status, sizeof(hs), cudaMemcpyDeviceToHost));
+    if (hs[1] & kErrLeafLimit)
+      return fail(NM_ERR_CAPACITY, "frame labels %u leaves, more than the static-scratch limit of %u",
+                  hs[0], kStaticLeafSlots / 2);
     if (hs[1] & kErrProbe)
-      return fail(NM_ERR_CAPACITY, "frame labels more than %u leaves (static-scratch limit)",
-                  kStaticLeafSlots / 2);
+      return fail(NM_ERR_CAPACITY, "static-scratch leaf table of %u slots: probe limit reached, "
+                  "frame labels more than %u leaves", kStaticLeafSlots, kStaticLeafSlots / 2);
     if (hs[1] & kErrOutputFull)
       return fail(NM_ERR_CAPACITY, "%u labelled leaves exceed max_leaves = %u", hs[0], max_leaves);
   }
