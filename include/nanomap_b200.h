@@ -228,8 +228,10 @@ int nm_map_tick(nm_map m, const nm_frame* frames, int32_t n_frames, uint32_t fla
  * replayed as a CUDA graph each tick: upload of the per-frame constants derived from the
  * slots' poses, one launch rendering (and noising) every slot from `sim` when it is given,
  * one persistent traversal over all slots, and one integration of all planes in agent order.
- * At most 32 slots.  Always integrates (no NM_DEFER_INTEGRATE).  Replaces the per-agent loop
- * of SimManager::updateAgentViews(map) (SimManager.h:114-127). */
+ * At most 32 slots.  nm_tick_plan_run with NM_DEFER_INTEGRATE replays a graph without the
+ * integration: every slot's labels stay in its agent plane (nm_map_export_labels reads them)
+ * until nm_map_integrate applies them.  Replaces the per-agent loop of
+ * SimManager::updateAgentViews(map) (SimManager.h:114-127). */
 int nm_tick_plan_create(nm_map m, nm_simmap sim, const nm_frame* slots, int32_t n_slots,
                         nm_tick_plan* out);
 int nm_tick_plan_destroy(nm_tick_plan p);
@@ -238,10 +240,11 @@ int nm_tick_plan_set_pose(nm_tick_plan p, int32_t slot, const nm_pose* pose);
 int nm_tick_plan_set_noise(nm_tick_plan p, float sigma_coef, float drop_prob, uint64_t seed);
 int nm_tick_plan_set_launch(nm_tick_plan p, int32_t tile_w, int32_t tile_h, int32_t entries);
 int nm_tick_plan_run(nm_tick_plan p, uint32_t flags, void* stream);
-/* Autotuner: times candidate traversal shapes (tile, leaf-table entries) on a scratch map with
- * the plan's slots and poses, applies the fastest to the plan, and appends it to cache_path
- * (reused on later calls with the same device and slot shapes).  best = tile_w, tile_h,
- * entries. */
+/* Autotuner: times candidate traversal shapes on a scratch map with the plan's slots and
+ * poses: the tile (rays per warp: one ray per thread for tiles of up to 256 pixels, two or four
+ * for 512 and 1024), the shared leaf-table entries; applies the fastest to the plan, and
+ * appends it to cache_path (reused on later calls with the same device and slot shapes).
+ * best = tile_w, tile_h, entries. */
 int nm_tick_plan_autotune(nm_tick_plan p, const char* cache_path, int32_t best[3], float* best_us);
 
 /* Leaves of the map (any order): origins (3 ints per leaf, voxel units), 512 log-odds per
@@ -271,16 +274,20 @@ int nm_frame_params(const nm_sensor_desc* desc, const nm_pose* pose, float res, 
  * an addition for callers that cannot allocate device memory while they run, such as
  * real-time loops that forbid allocation after start-up, or hosts whose memory pool owns the
  * device).  Same traversal and labels as nm_map_insert_ranges + NM_DEFER_INTEGRATE on a map
- * of resolution `res` and rounding `rounding`, but the working memory is a fixed static
- * device array of about 9 MiB that every GPU loading the library holds until exit.  Inputs
- * and outputs are device memory owned by the caller: `ranges` (hres*vres floats),
- * `origins` (3 ints per leaf), `words` (32 label words per leaf, as nm_map_export_labels),
- * `status` (2 uints: labelled leaf count, error bits).  Limits: at most 8388608 pixels per
- * frame (larger frames are rejected with NM_ERR_ARG) and at most 32768 labelled leaves per
- * call (more is reported as NM_ERR_CAPACITY under NM_SYNC, else in status[1]).  The first
- * call on a device looks up the array's device address; make that first call before any
- * stream capture.  Every call shares the array and first clears it; calls that overlap on
- * the GPU race on it. */
+ * of resolution `res` (positive, finite) and rounding `rounding`, but the working memory is
+ * a fixed static device array of about 9 MiB.  Inputs and outputs are device memory owned by
+ * the caller: `ranges` (hres*vres floats), `origins` (3 ints per leaf), `words` (32 label
+ * words per leaf, as nm_map_export_labels), `status` (2 uints: labelled leaf count, error
+ * bits).  Limits: at most 8388608 pixels per frame (larger frames are rejected with
+ * NM_ERR_ARG) and at most 32768 labelled leaves per call (more is reported as
+ * NM_ERR_CAPACITY under NM_SYNC, else as bit 16 of status[1]); a frame with more labelled
+ * leaves than `max_leaves` writes the first `max_leaves` and reports NM_ERR_CAPACITY (bit 8),
+ * with the full count in status[0].  The array is loaded with the library's module on each
+ * GPU when that module is first used there (lazy loading, CUDA's default), so the first call
+ * on each device is the start-up warm-up: it makes the array resident and looks up its device
+ * address.  Make it before the phase that must not allocate and before any stream capture;
+ * the array then stays resident until the process exits.  Every call shares the array and
+ * first clears it; calls that overlap on the GPU race on it. */
 int nm_label_frame_static(nm_sensor s, const nm_pose* pose, const float* ranges, float res,
                           int32_t rounding, int32_t* origins, uint32_t* words,
                           uint32_t max_leaves, uint32_t* status, uint32_t flags, void* stream);
