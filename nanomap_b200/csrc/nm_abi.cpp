@@ -297,7 +297,10 @@ int ensure_capacity(nm_map m, uint64_t bound, cudaStream_t s) {
   m->known_leaves = lc;
   m->pending_bound = 0;
   uint64_t cap = m->view.capacity;
-  while (m->known_leaves + bound > cap / 2 && cap < (1ull << 30)) cap <<= 1;
+  while (m->known_leaves + bound > cap / 2 && cap < nm::kMaxLeafCapacity) cap <<= 1;
+  if (m->known_leaves + bound > cap / 2 && m->known_leaves >= cap / 2)
+    return fail(NM_ERR_CAPACITY, "map holds %llu leaves; the leaf table stops at %llu slots",
+                (unsigned long long)m->known_leaves, (unsigned long long)nm::kMaxLeafCapacity);
   if (cap != m->view.capacity) {
     const int rc = grow_map(m, (uint32_t)cap, s);
     if (rc != NM_OK) return rc;
@@ -751,6 +754,9 @@ int nm_map_create(nm_context ctx, const nm_map_desc* d, nm_map* out) {
     return fail(NM_ERR_ARG, "max_agents must be 1..%d", nm::kMaxPlanes);
   if (d->update_mode == NM_UPDATE_ACCUMULATE && d->max_agents != 1)
     return fail(NM_ERR_UNSUPPORTED, "accumulate mode keeps one label plane");
+  if (d->initial_leaf_capacity > nm::kMaxLeafCapacity)
+    return fail(NM_ERR_CAPACITY, "initial leaf capacity %u above %llu slots", d->initial_leaf_capacity,
+                (unsigned long long)nm::kMaxLeafCapacity);
   NM_CUDA(cudaSetDevice(ctx->device));
   std::unique_ptr<nm_map_s> m(new nm_map_s());
   m->ctx = ctx;
@@ -918,9 +924,13 @@ int nm_sim_insert(nm_simmap sm, nm_map m, nm_sensor s, const nm_pose* pose, floa
   const int64_t n = (int64_t)s->desc.hres * s->desc.vres;
   const bool host_out = (flags & NM_OUTPUT_HOST) && ranges;
   float* out = host_out ? nullptr : ranges;
-  // the voxel filter and per-ray sums need the whole image first: render, then insert
+  nm::FrameParams f;
+  rc = make_frame(m, s, pose, &f);
+  if (rc != NM_OK) return rc;
+  // the voxel filter and per-ray sums need the whole image first, and so do frames that reach
+  // beyond the fused kernel's leaf code: render, then insert
   const bool two_pass = (flags & (NM_FILTER_MEAN | NM_FILTER_CENTRE)) ||
-                        m->desc.update_mode != NM_UPDATE_LABEL;
+                        m->desc.update_mode != NM_UPDATE_LABEL || !nm::traverse_render_fits(f);
   if (host_out || (two_pass && !out)) {
     nm_context c = m->ctx;
     if ((size_t)n * 4 > c->render_staging_bytes) {
@@ -937,9 +947,6 @@ int nm_sim_insert(nm_simmap sm, nm_map m, nm_sensor s, const nm_pose* pose, floa
     rc = nm_sim_render_noisy(sm, s, pose, out, sigma_coef, drop_prob, seed, 0, s0);
     if (rc == NM_OK) rc = nm_map_insert_ranges(m, s, pose, out, pass | (flags & NM_SYNC), s0);
   } else {
-    nm::FrameParams f;
-    rc = make_frame(m, s, pose, &f);
-    if (rc != NM_OK) return rc;
     f.input_kind = 1;
     f.ranges = nullptr;
     nm::SimRender sr;

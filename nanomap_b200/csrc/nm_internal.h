@@ -25,6 +25,8 @@ constexpr int kLabelWords = 32;
 constexpr int kActiveWords = 16;
 constexpr int kMaxPlanes = 32;
 constexpr uint32_t kMaxProbe = 4096;
+// Largest leaf-table capacity (slots): at >2 KB per slot, 2^26 slots fill a 180 GB GPU.
+constexpr uint64_t kMaxLeafCapacity = 1ull << 26;
 
 // Device-side error bits (sticky until read by nm_map_stats).
 constexpr uint32_t kErrProbe = 1u;     // leaf table probe limit reached: labels were lost
@@ -90,6 +92,11 @@ struct FrameParams {
 };
 
 constexpr int kMaxTickFrames = 32;
+
+// Frames with max_range / res below this many voxels reach at most 501 leaves from the eye on
+// every axis, inside the range where the traversal's 32-bit leaf code is one-to-one; farther
+// reaching frames take the traversal without the shared leaf table.
+constexpr float kNarrowMaxTime = 4000.0f;
 
 // Work list of one traversal launch: frames and the prefix sum of their tile counts.
 // Passed by value as a __grid_constant__ kernel parameter (no host-to-device copy, so a
@@ -181,10 +188,14 @@ struct DepthParams {
 template <int MaxF>
 cudaError_t launch_traverse_labels(const TickWork<MaxF>& w, const MapView& m, int rounding,
                                    cudaStream_t s);
-cudaError_t prepare_traverse_dev(int tile_w, int tile_h, uint32_t smask, int rounding);
+// Dynamic shared memory of one traversal CTA (leaf table, ray order, rendered ranges).
+size_t traverse_smem_bytes(int tile_w, int tile_h, uint32_t smask, bool render);
+// Whether a frame fits the fused render + traversal (reach within the leaf code's range).
+bool traverse_render_fits(const FrameParams& f);
+cudaError_t prepare_traverse_dev(int tile_w, int tile_h, uint32_t smask, int rounding, bool wide);
 cudaError_t launch_traverse_labels_dev(const TickWork<kMaxTickFrames>* d_work, uint32_t total_tiles,
                                        int tile_w, int tile_h, uint32_t smask, const MapView& m,
-                                       int rounding, cudaStream_t s);
+                                       int rounding, bool wide, cudaStream_t s);
 cudaError_t launch_traverse_counts(const FrameParams& f, const MapView& m, int rounding,
                                    cudaStream_t s);
 cudaError_t launch_integrate(const MapView& m, const IntegrateParams& p, int update_mode,

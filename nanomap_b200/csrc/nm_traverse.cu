@@ -5,27 +5,38 @@
 // DDA of Handler.cpp:58-85 and records one label per voxel (hit overrides miss), allocating
 // map leaves on the fly.
 //
-// Work distribution: CTAs stay resident and take 16x16-pixel tiles from a device counter,
-// so the cost of a tile (set by its longest rays) no longer decides when an SM goes idle.
-// A tile holds several rays per thread; every lane walks one ray at a time and takes the
-// tile's next ray as soon as its own ends, so lanes stay busy until the tile runs dry.
+// Work distribution: CTAs stay resident and take tiles of neighbouring pixels from a device
+// counter, so the cost of a tile (set by its longest rays) no longer decides when an SM goes
+// idle.  A tile holds one or more rays per thread.  Before the walk the tile's rays are
+// ordered by range (a counting sort on 32 range buckets, longest first), so the 32 lanes of a
+// warp walk rays of about the same length and finish together; with several rays per
+// thread the rounds alternate direction, so every warp gets long and short rays.
 //
-// Labels collect in a per-CTA shared-memory leaf table (hashed, 32 label words per leaf);
-// a leaf that finds no room goes straight to the device table.  After a tile, one lane per
-// cached leaf ORs its words into the device label buffer and puts the leaf on the touched
-// list (the device-table lookups of a warp's leaves overlap).
+// Per step the walk compares the three crossing times (non-negative doubles, one compare per
+// pair, ties to the higher axis), advances the chosen axis with one rounded double add, and
+// keeps the voxel as (leaf code, index inside the leaf).  The leaf code lx*2^20 + ly*2^10 + lz
+// (mod 2^32) moves by one add per leaf crossing and is one-to-one over every leaf a frame can
+// reach while max_range / res stays below kNarrowMaxTime voxels; it is both the tag and the
+// hash source of a per-CTA shared-memory leaf table (32 label words per leaf).  A leaf that
+// finds no room in the table goes straight to the device table.
+//
+// Labels collect per 32-voxel word in a register and go to shared memory when the walk leaves
+// the word, with a shared atomic only when they add bits the word does not hold yet.  After a
+// tile, one lane per cached leaf ORs its words into the device label buffer and puts the leaf
+// on the touched list (the device-table lookups of a warp's leaves overlap).
+//
+// Frames whose reach exceeds the code's range (max_range / res >= kNarrowMaxTime) take
+// k_traverse_wide: one thread per ray with device-table lookups and label atomics.
 //
 // Host xyz records may arrive in chunks of tile rows: each chunk is then its own launch on
 // its own stream and tile counter (TickWork::queue), started when its rows have arrived.
 //
-// Per step the walk compares the three crossing times (non-negative doubles, one compare per
-// pair), keeps the voxel as (leaf, local) coordinates, and probes the leaf table only when the
-// step leaves the current leaf.
-//
 // k_traverse_render renders each tile's ranges from the sim map into shared memory first
 // (nm_sim_insert), so one launch does the simulated frame and its insertion.
 #include <cfloat>
+#include <climits>
 #include <cstdint>
+#include <mutex>
 
 #include "nm_device.cuh"
 #include "nm_internal.h"
@@ -36,27 +47,104 @@ namespace nm {
 namespace {
 
 constexpr unsigned kFull = 0xffffffffu;
+constexpr int kSortBuckets = 32;
+// Word index of a leaf whose labels were lost (device table full): flushes skip it.
+constexpr int kLostWord = INT_MIN;
+// Word indices at or above kGlobFloor and below 0 name a device-table leaf g as
+// -(g + 1) * 16 + w (w = miss word 0..15); capacities are at most 2^26 slots.
+constexpr int kGlobFloor = -(1 << 30);
 
-__device__ __noinline__ int smem_lookup_slow(unsigned long long* s_keys, uint32_t smask,
-                                            unsigned long long key, uint32_t h) {
-  h &= smask;
-  const uint32_t limit = (smask + 1) < 16u ? (smask + 1) : 16u;
-  for (uint32_t i = 0; i < limit; ++i) {
-    const unsigned long long k = ((volatile unsigned long long*)s_keys)[h];
-    if (k == key) return (int)h;
-    if (k == kEmptyKey) {
-      const unsigned long long old = atomicCAS(&s_keys[h], kEmptyKey, key);
-      if (old == kEmptyKey || old == key) return (int)h;
-    }
-    h = (h + 1) & smask;
-  }
-  return -1;
+__device__ __forceinline__ uint32_t leaf_code(int lx, int ly, int lz) {
+  return ((uint32_t)lx << 20) + ((uint32_t)ly << 10) + (uint32_t)lz;
 }
 
-// Shared-table slot of a leaf: Fibonacci hashing of the packed key (high product bits), which
-// spreads neighbouring leaves of a ray cone over the table.
-__device__ __forceinline__ uint32_t leaf_hash(unsigned long long key) {
-  return (uint32_t)((key * 0x9E3779B97F4A7C15ull) >> 40);
+// Table position of a leaf code: Fibonacci hashing, top bits (`sh` = 32 - log2 entries).
+__device__ __forceinline__ uint32_t code_slot(uint32_t code, int sh) {
+  return (code * 0x9E3779B1u) >> sh;
+}
+
+__device__ __forceinline__ int sext(uint32_t v, int bits) {
+  return (int)(v << (32 - bits)) >> (32 - bits);
+}
+
+// Absolute leaf key of a code near the eye's leaf (every reachable leaf lies within 511 leaves
+// of it on each axis, where the code is one-to-one).
+__device__ __forceinline__ unsigned long long code_key(uint32_t code, uint32_t ecode, int elx,
+                                                       int ely, int elz) {
+  const uint32_t c = code - ecode;  // dx*2^20 + dy*2^10 + dz (mod 2^32)
+  const int dz = sext(c & 0x3FFu, 10);
+  const uint32_t c1 = (c - (uint32_t)dz) >> 10;
+  const int dy = sext(c1 & 0x3FFu, 10);
+  const int dx = sext(((c1 - (uint32_t)dy) >> 10) & 0xFFFu, 12);
+  return leaf_key(elx + dx, ely + dy, elz + dz);
+}
+
+// Per-tile constants of the shared leaf table.
+struct TileTable {
+  unsigned long long* keys;  // absolute key per entry (valid where tags != sentinel)
+  uint32_t* tags;            // leaf code per entry, `sentinel` = empty
+  uint32_t* words;           // 32 label words per entry: 0..15 hit, 16..31 miss
+  uint32_t smask;
+  int sh;
+  uint32_t sentinel;
+  uint32_t ecode;
+  int elx, ely, elz;
+};
+
+// Probe / insert of a code the inline probe missed.  Returns the miss-word base of the leaf:
+// e * 32 + 16 for table entry e, -(g + 1) * 16 for device-table slot g, kLostWord when the
+// device table is full.
+__device__ __noinline__ int leaf_base_slow(const TileTable& tt, const MapView& m, uint32_t code,
+                                           uint32_t epoch, int plane) {
+  uint32_t h = code_slot(code, tt.sh);
+  const uint32_t limit = (tt.smask + 1) < 16u ? (tt.smask + 1) : 16u;
+  for (uint32_t i = 0; i < limit; ++i) {
+    const uint32_t k = ((volatile uint32_t*)tt.tags)[h];
+    if (k == code) return (int)(h * kLabelWords + 16);
+    if (k == tt.sentinel) {
+      const uint32_t old = atomicCAS(&tt.tags[h], tt.sentinel, code);
+      if (old == tt.sentinel) {
+        tt.keys[h] = code_key(code, tt.ecode, tt.elx, tt.ely, tt.elz);
+        return (int)(h * kLabelWords + 16);
+      }
+      if (old == code) return (int)(h * kLabelWords + 16);
+    }
+    h = (h + 1) & tt.smask;
+  }
+  const int g = map_find_or_insert(m, code_key(code, tt.ecode, tt.elx, tt.ely, tt.elz));
+  if (g < 0) return kLostWord;
+  mark_touched(m, g, epoch, plane);
+  return -(g + 1) * 16;
+}
+
+__device__ __forceinline__ int leaf_base(const TileTable& tt, const MapView& m, uint32_t code,
+                                         uint32_t epoch, int plane) {
+  const uint32_t e = code_slot(code, tt.sh);
+  if (((volatile uint32_t*)tt.tags)[e] == code) return (int)(e * kLabelWords + 16);
+  return leaf_base_slow(tt, m, code, epoch, plane);
+}
+
+// OR `bits` into label word `cw` (a table word, a device-table miss word, or lost).
+__device__ __noinline__ void flush_device_word(const MapView& m, int cw, uint32_t bits, int plane) {
+  if (cw < kGlobFloor) return;
+  const uint32_t x = (uint32_t)(-cw - 1);
+  const uint32_t g = x >> 4, w = 15u - (x & 15u);
+  atomicOr(&m.labels[((size_t)plane * m.capacity + g) * kLabelWords + 16 + w], bits);
+}
+
+__device__ __forceinline__ void flush_word(uint32_t* s_words, const MapView& m, int cw,
+                                           uint32_t bits, int plane) {
+  if (cw >= 0)
+    atomicOr(&s_words[cw], bits);
+  else
+    flush_device_word(m, cw, bits, plane);
+}
+
+// Hit label of voxel `l` of the leaf whose miss-word base is `wbase`.
+__device__ __noinline__ void hit_device(const MapView& m, int wbase, int l, int plane) {
+  if (wbase < kGlobFloor) return;
+  const uint32_t g = (uint32_t)(-wbase / 16 - 1);
+  atomicOr(&m.labels[((size_t)plane * m.capacity + g) * kLabelWords + (l >> 5)], 1u << (l & 31));
 }
 
 struct Ray {
@@ -65,7 +153,8 @@ struct Ray {
   double len;         // ray length in voxels
   int ds0, ds1, ds2;  // step of the voxel index inside the leaf per axis: +-64, +-8, +-1 or 0
   int l;              // voxel index inside the leaf, x*64 + y*8 + z
-  unsigned long long key;  // packed leaf coordinate
+  uint32_t hs0, hs1, hs2;  // leaf-code step per axis: +-2^20, +-2^10, +-1 or 0
+  uint32_t code;           // leaf code of the current voxel
 };
 
 // Ray set-up of the insertion DDA (Handler.cpp:64-76 restated; see trace_point in
@@ -118,8 +207,11 @@ __device__ __forceinline__ bool setup_ray(const FrameParams& f, const float p[3]
   r.ds0 = st[0] * 64;
   r.ds1 = st[1] * 8;
   r.ds2 = st[2];
+  r.hs0 = (uint32_t)st[0] << 20;
+  r.hs1 = (uint32_t)st[1] << 10;
+  r.hs2 = (uint32_t)st[2];
   r.l = ((v[0] & 7) << 6) | ((v[1] & 7) << 3) | (v[2] & 7);
-  r.key = leaf_key(v[0] >> 3, v[1] >> 3, v[2] >> 3);
+  r.code = leaf_code(v[0] >> 3, v[1] >> 3, v[2] >> 3);
   return true;
 }
 
@@ -129,22 +221,96 @@ __device__ __forceinline__ bool pixel_point(const FrameParams& f, int w, int h, 
   return xyz_point(f, w, h, p);
 }
 
+// Walk one ray from its set-up to its end, labelling every voxel it leaves as a miss and its
+// end voxel as a hit (when the crossing that leaves it lies below max_time).  Returns the
+// number of label events.
+template <int RM>
+__device__ __forceinline__ uint32_t walk_ray(const Ray& r, const TileTable& tt, const MapView& m,
+                                             double max_time, uint32_t epoch, int plane) {
+  using A = Ar<RM>;
+  double t0 = r.t0, t1 = r.t1, t2 = r.t2;
+  const double d0 = r.d0, d1 = r.d1, d2 = r.d2, len = r.len;
+  int l = r.l;
+  uint32_t code = r.code;
+  int wbase = leaf_base(tt, m, code, epoch, plane);
+  int cw = kLostWord;  // word the pending bits belong to
+  uint32_t acc = 0u;   // pending miss bits of word cw
+  uint32_t known = 0u; // bits word cw held when the walk entered it
+  uint32_t n = 0u;
+  double t;
+  for (;;) {
+    const bool c01 = t0 < t1, c02 = t0 < t2, c12 = t1 < t2;
+    const bool is0 = c01 && c02;
+    const bool is1 = !c01 && c12;
+    t = is0 ? t0 : (is1 ? t1 : t2);
+    if (!(t <= len)) break;
+    // miss label of the voxel being left
+    const int wi = wbase + (l >> 5);
+    if (wi != cw) {
+      if (acc & ~known) flush_word(tt.words, m, cw, acc, plane);
+      cw = wi;
+      acc = 0u;
+      known = wi >= 0 ? ((volatile uint32_t*)tt.words)[wi] : 0u;
+    }
+    acc |= 1u << (l & 31);
+    ++n;
+    // advance along the chosen axis: crossing time, index inside the leaf, leaf on wrap
+    const double dstep = is0 ? d0 : (is1 ? d1 : d2);
+    const double tn = A::dadd(t, dstep);
+    if (is0) t0 = tn;
+    if (is1) t1 = tn;
+    if (!is0 && !is1) t2 = tn;
+    const int msk = is0 ? 0x1C0 : (is1 ? 0x38 : 0x7);
+    const int ds = is0 ? r.ds0 : (is1 ? r.ds1 : r.ds2);
+    const int vv = (l & msk) + ds;
+    l = (l & ~msk) | (vv & msk);
+    if ((unsigned)vv > (unsigned)msk) {
+      code += is0 ? r.hs0 : (is1 ? r.hs1 : r.hs2);
+      wbase = leaf_base(tt, m, code, epoch, plane);
+    }
+  }
+  if (acc & ~known) flush_word(tt.words, m, cw, acc, plane);
+  if (t < max_time) {
+    if (wbase >= 0)
+      atomicOr(&tt.words[wbase - 16 + (l >> 5)], 1u << (l & 31));
+    else
+      hit_device(m, wbase, l, plane);
+    ++n;
+  }
+  return n;
+}
+
+// Range bucket of a pixel for the tile's ray order: 0 = longest rays, kSortBuckets - 1 =
+// shortest and rays without a return.
+// `qs` = kSortBuckets / max_range (metres): the bucket is the range's fraction of max range.
+__device__ __forceinline__ int range_bucket(float r_m, float qs) {
+  if (!(r_m > 0.0f)) return kSortBuckets - 1;
+  const float q = r_m * qs;
+  const int k = q < (float)kSortBuckets ? (int)q : kSortBuckets - 1;
+  return kSortBuckets - 1 - k;
+}
+
 template <int RM, int MaxF, bool Render = false>
 __device__ __forceinline__ void traverse_body(const TickWork<MaxF>& work, const MapView& m,
                                               const SimRender* sr = nullptr) {
   extern __shared__ __align__(16) unsigned char smem[];
   const uint32_t smask = work.smask;
   const int nent = (int)smask + 1;
+  const int nrays = work.tile_w * work.tile_h;
   unsigned long long* s_keys = reinterpret_cast<unsigned long long*>(smem);
   uint32_t* s_words = reinterpret_cast<uint32_t*>(s_keys + nent);
-  float* s_rng = reinterpret_cast<float*>(s_words + nent * kLabelWords);  // Render: tile ranges
+  uint32_t* s_tags = s_words + nent * kLabelWords;
+  uint16_t* s_order = reinterpret_cast<uint16_t*>(s_tags + nent);
+  uint8_t* s_bkt = reinterpret_cast<uint8_t*>(s_order + nrays);
+  float* s_rng = reinterpret_cast<float*>(s_bkt + nrays);  // Render: the tile's ranges
   __shared__ FrameParams s_f;
   __shared__ uint32_t s_tile;
   __shared__ int s_frame;
-  __shared__ uint32_t s_next;
+  __shared__ uint32_t s_hist[kSortBuckets];
   const int tid = threadIdx.x;
-  const int lane = tid & 31, nwarps = blockDim.x >> 5;
-  const int nrays = work.tile_w * work.tile_h;
+  const int lane = tid & 31;
+  const int nthreads = blockDim.x;
+  const int rounds = nrays / nthreads;
   uint32_t visits = 0, rays = 0;
 
   for (;;) {
@@ -155,7 +321,6 @@ __device__ __forceinline__ void traverse_body(const TickWork<MaxF>& work, const 
       while (fi + 1 < work.n_frames && work.tile_start[fi + 1] <= t) ++fi;
       s_tile = t;
       s_frame = fi;
-      s_next = 0u;
       if (t == work.total_tiles + gridDim.x - 1) *queue = 0u;  // last reader resets
     }
     __syncthreads();
@@ -165,8 +330,9 @@ __device__ __forceinline__ void traverse_body(const TickWork<MaxF>& work, const 
     {
       const uint32_t* src = reinterpret_cast<const uint32_t*>(&work.fr[fi]);
       uint32_t* dst = reinterpret_cast<uint32_t*>(&s_f);
-      for (int i = tid; i < (int)(sizeof(FrameParams) / 4); i += blockDim.x) dst[i] = src[i];
+      for (int i = tid; i < (int)(sizeof(FrameParams) / 4); i += nthreads) dst[i] = src[i];
     }
+    if (tid < kSortBuckets) s_hist[tid] = 0u;
     __syncthreads();
     const FrameParams& f = s_f;
     const uint32_t lt = tile - work.tile_start[fi];
@@ -178,137 +344,101 @@ __device__ __forceinline__ void traverse_body(const TickWork<MaxF>& work, const 
       __syncthreads();
       continue;
     }
-    for (int i = tid; i < nent; i += blockDim.x) s_keys[i] = kEmptyKey;
-    for (int i = tid; i < nent * kLabelWords; i += blockDim.x) s_words[i] = 0u;
-    if constexpr (Render) {
-      // the tile's ranges: the sim map's first active voxel per pixel, then the range noise
-      // (the same values nm_sim_render_noisy writes)
-      for (int t = tid; t < nrays; t += blockDim.x) {
-        const int px = x0 + t % work.tile_w, py = y0 + t / work.tile_w;
-        float rr = 0.0f;
-        if (px < f.width && py < f.height) {
-          rr = sim_ray(sr->v, sr->rp, px, py);
+    TileTable tt;
+    tt.keys = s_keys;
+    tt.tags = s_tags;
+    tt.words = s_words;
+    tt.smask = smask;
+    tt.sh = __clz((int)smask);
+    tt.elx = (int)floor(f.eye[0]) >> 3;
+    tt.ely = (int)floor(f.eye[1]) >> 3;
+    tt.elz = (int)floor(f.eye[2]) >> 3;
+    tt.ecode = leaf_code(tt.elx, tt.ely, tt.elz);
+    tt.sentinel = tt.ecode + (1536u << 20);  // the code of no leaf within reach
+    for (int i = tid; i < nent; i += nthreads) s_tags[i] = tt.sentinel;
+    for (int i = tid; i < nent * kLabelWords; i += nthreads) s_words[i] = 0u;
+
+    // the tile's ranges (Render: from the sim map, with the range noise), bucketed by length;
+    // every thread runs the same number of iterations (nrays is a multiple of the block)
+    const float qs = (float)kSortBuckets / (f.max_time * (float)f.res_d);
+    for (int k = tid; k < nrays; k += nthreads) {
+      const int px = x0 + k % work.tile_w, py = y0 + k / work.tile_w;
+      float rm = 0.0f;  // range in metres, 0 = no point
+      if (px < f.width && py < f.height) {
+        if constexpr (Render) {
+          float rr = sim_ray(sr->v, sr->rp, px, py);
           const long long i = (long long)py * f.width + px;
           if (sr->noise) rr = noisy(rr, sr->seed, i, sr->sigma_coef, sr->drop);
           if (sr->out) sr->out[i] = rr;
+          s_rng[k] = rr;
+          rm = rr;
+        } else if (f.input_kind == 1) {
+          rm = __ldg(&f.ranges[(size_t)py * f.width + px]);
+        } else {
+          float p[3];
+          if (pixel_point(f, px, py, p)) rm = sqrtf(p[0] * p[0] + p[1] * p[1] + p[2] * p[2]);
         }
-        s_rng[t] = rr;
       }
+      const int b = range_bucket(rm, qs);
+      s_bkt[k] = (uint8_t)b;
+      const unsigned peers = __match_any_sync(kFull, b);
+      if (lane == __ffs(peers) - 1) atomicAdd(&s_hist[b], (uint32_t)__popc(peers));
+    }
+    __syncthreads();
+    if (tid < 32) {  // exclusive prefix over the buckets
+      const uint32_t v = s_hist[lane];
+      uint32_t incl = v;
+#pragma unroll
+      for (int o = 1; o < 32; o <<= 1) {
+        const uint32_t u = __shfl_up_sync(kFull, incl, o);
+        if (lane >= o) incl += u;
+      }
+      s_hist[lane] = incl - v;
+    }
+    __syncthreads();
+    for (int k = tid; k < nrays; k += nthreads) {
+      const int b = s_bkt[k];
+      const unsigned peers = __match_any_sync(kFull, b);
+      const int leader = __ffs(peers) - 1;
+      uint32_t base = 0;
+      if (lane == leader) base = atomicAdd(&s_hist[b], (uint32_t)__popc(peers));
+      base = __shfl_sync(peers, base, leader);
+      s_order[base + __popc(peers & ((1u << lane) - 1u))] = (uint16_t)k;
     }
     __syncthreads();
 
-    Ray r;
-    bool active = false;
-    bool glob = false;
-    int slot = -1;
-    int cw_idx = -1;
-    uint32_t cw_bits = 0u;
     const int plane = f.plane;
-
-    // Leaf lookup after a crossing (or at ray start): one inline probe finds leaves already
-    // in the tile's table; a miss probes / inserts (or falls back to the device table).
-    auto resolve = [&]() {
-      const uint32_t hh = leaf_hash(r.key);
-      const uint32_t h = hh & smask;
-      if (((volatile unsigned long long*)s_keys)[h] == r.key) {
-        glob = false;
-        slot = (int)h;
-        return;
-      }
-      const int sl = smem_lookup_slow(s_keys, smask, r.key, hh);
-      if (sl >= 0) {
-        glob = false;
-        slot = sl;
-      } else {
-        glob = true;
-        slot = map_find_or_insert(m, r.key);
-        if (slot >= 0) mark_touched(m, slot, f.epoch, plane);
-      }
-    };
-    auto label = [&](int kind) {
-      const uint32_t bit = 1u << (r.l & 31);
-      const int wi = (kind == kKindHit ? 0 : 16) + (r.l >> 5);
-      if (!glob) {
-        const int idx = slot * kLabelWords + wi;
-        if (idx != cw_idx) {
-          cw_idx = idx;
-          cw_bits = ((volatile uint32_t*)s_words)[idx];
-        }
-        if (!(cw_bits & bit)) {
-          atomicOr(&s_words[idx], bit);
-          cw_bits |= bit;
-        }
-      } else if (slot >= 0) {
-        uint32_t* wp = &m.labels[((size_t)plane * m.capacity + (size_t)slot) * kLabelWords + wi];
-        if (!(__ldcg(wp) & bit)) atomicOr(wp, bit);
-      }
-    };
-
-    for (;;) {
-      if (!active) {
-        const uint32_t k = atomicAdd(&s_next, 1u);
-        if (k >= (uint32_t)nrays) break;
-        const int px = x0 + (int)(k % (uint32_t)work.tile_w);
-        const int py = y0 + (int)(k / (uint32_t)work.tile_w);
-        float p[3];
-        // pixels of a tile that overhangs the image are skipped before any input is read
-        bool has_point = false;
-        if (px < f.width && py < f.height)
-          has_point = Render ? range_point_r(f, px, py, s_rng[k], p) : pixel_point(f, px, py, p);
-        if (has_point && setup_ray<RM>(f, p, r)) {
-          active = true;
-          rays += 1;
-          cw_idx = -1;
-          resolve();
-        }
-        continue;
-      }
-      // crossing times are non-negative and never NaN (disabled axes hold DBL_MAX): one
-      // double compare per pair; ties go to the higher axis
-      const int a = (r.t0 < r.t1) ? ((r.t0 < r.t2) ? 0 : 2) : ((r.t1 < r.t2) ? 1 : 2);
-      const double t = (a == 0) ? r.t0 : ((a == 1) ? r.t1 : r.t2);
-      if (!(t <= r.len)) {
-        if (t < (double)f.max_time) {
-          label(kKindHit);
-          visits += 1;
-        }
-        active = false;
-        continue;
-      }
-      label(kKindMiss);
-      visits += 1;
-      // advance along axis a: crossing time, voxel index inside the leaf, leaf on wrap
-      const double dstep = (a == 0) ? r.d0 : ((a == 1) ? r.d1 : r.d2);
-      const double tnext = Ar<RM>::dadd(t, dstep);
-      r.t0 = (a == 0) ? tnext : r.t0;
-      r.t1 = (a == 1) ? tnext : r.t1;
-      r.t2 = (a == 2) ? tnext : r.t2;
-      const int msk = (a == 0) ? 0x1C0 : ((a == 1) ? 0x38 : 0x7);
-      const int ds = (a == 0) ? r.ds0 : ((a == 1) ? r.ds1 : r.ds2);
-      const int vv = (r.l & msk) + ds;
-      const bool cross = (unsigned)vv > (unsigned)msk;
-      r.l = (r.l & ~msk) | (vv & msk);
-      if (cross) {
-        const int sh = (a == 0) ? 42 : ((a == 1) ? 21 : 0);
-        r.key += (unsigned long long)(long long)(ds > 0 ? 1 : -1) << sh;
-        resolve();
+    const uint32_t epoch = f.epoch;
+    const double max_time = (double)f.max_time;
+    for (int j = 0; j < rounds; ++j) {
+      // alternate directions so every warp gets long and short rays
+      const int pos = (j & 1) ? (j + 1) * nthreads - 1 - tid : j * nthreads + tid;
+      const int k = s_order[pos];
+      const int px = x0 + k % work.tile_w, py = y0 + k / work.tile_w;
+      float p[3];
+      bool has_point = false;
+      if (px < f.width && py < f.height)
+        has_point = Render ? range_point_r(f, px, py, s_rng[k], p) : pixel_point(f, px, py, p);
+      Ray r;
+      if (has_point && setup_ray<RM>(f, p, r)) {
+        rays += 1;
+        visits += walk_ray<RM>(r, tt, m, max_time, epoch, plane);
       }
     }
     __syncthreads();
 
     // Flush the tile's leaf table: one lane per cached leaf, so the device-table lookups of
     // up to 32 leaves overlap; word reads are rotated by lane to avoid bank conflicts.
-    for (int e = tid; e < nent; e += blockDim.x) {
-      const unsigned long long key = s_keys[e];
-      if (key == kEmptyKey) continue;
+    for (int e = tid; e < nent; e += nthreads) {
+      if (s_tags[e] == tt.sentinel) continue;
       const uint32_t* sw = s_words + e * kLabelWords;
       bool has = false;
 #pragma unroll 4
       for (int w = 0; w < kLabelWords; ++w) has |= sw[(w + lane) & (kLabelWords - 1)] != 0u;
       if (!has) continue;
-      const int g = map_find_or_insert(m, key);
+      const int g = map_find_or_insert(m, s_keys[e]);
       if (g < 0) continue;
-      mark_touched(m, g, f.epoch, plane);
+      mark_touched(m, g, epoch, plane);
       uint32_t* dst = &m.labels[((size_t)plane * m.capacity + (size_t)g) * kLabelWords];
 #pragma unroll 4
       for (int w = 0; w < kLabelWords; ++w) {
@@ -327,6 +457,69 @@ __device__ __forceinline__ void traverse_body(const TickWork<MaxF>& work, const 
     rr += __shfl_xor_sync(kFull, rr, o);
   }
   if (lane == 0 && (vv | rr)) {
+    atomicAdd(&m.ctr->visits, vv);
+    atomicAdd(&m.ctr->rays, rr);
+  }
+}
+
+// Label sink of the wide-frame kernel: device-table lookups on leaf changes, one atomic per
+// new label bit.
+struct WideEmit {
+  const MapView* m;
+  uint32_t epoch;
+  int plane;
+  unsigned long long ckey;
+  int cslot;
+
+  __device__ __forceinline__ void operator()(int x, int y, int z, int kind) {
+    const unsigned long long key = leaf_key(x >> 3, y >> 3, z >> 3);
+    if (key != ckey) {
+      ckey = key;
+      cslot = map_find_or_insert(*m, key);
+      if (cslot >= 0) mark_touched(*m, cslot, epoch, plane);
+    }
+    if (cslot < 0) return;
+    const int l = local_index(x, y, z);
+    uint32_t* wp = &m->labels[((size_t)plane * m->capacity + (size_t)cslot) * kLabelWords +
+                              (kind == kKindHit ? 0 : 16) + (l >> 5)];
+    const uint32_t bit = 1u << (l & 31);
+    if (!(__ldcg(wp) & bit)) atomicOr(wp, bit);
+  }
+};
+
+// Frames whose reach is beyond the leaf code's range: one thread per ray over the work's
+// tiles (grid-stride), the same DDA and labels without the shared leaf table.
+template <int RM, int MaxF>
+__device__ __forceinline__ void traverse_wide_body(const TickWork<MaxF>& work, const MapView& m) {
+  const int nrays = work.tile_w * work.tile_h;
+  uint32_t visits = 0, rays = 0;
+  for (uint32_t tile = blockIdx.x; tile < work.total_tiles; tile += gridDim.x) {
+    int fi = 0;
+    while (fi + 1 < work.n_frames && work.tile_start[fi + 1] <= tile) ++fi;
+    const FrameParams& f = work.fr[fi];
+    const uint32_t lt = tile - work.tile_start[fi];
+    const int x0 = (int)(lt % (uint32_t)work.tiles_x[fi]) * work.tile_w;
+    const int y0 = (int)(lt / (uint32_t)work.tiles_x[fi]) * work.tile_h;
+    for (int k = threadIdx.x; k < nrays; k += blockDim.x) {
+      const int px = x0 + k % work.tile_w, py = y0 + k / work.tile_w;
+      float p[3];
+      if (px < f.width && py < f.height && pixel_point(f, px, py, p)) {
+        WideEmit em{&m, f.epoch, f.plane, kEmptyKey, -1};
+        const int n = trace_point<RM>(f, p[0], p[1], p[2], em);
+        if (n >= 0) {
+          visits += (uint32_t)n;
+          rays += 1;
+        }
+      }
+    }
+  }
+  unsigned long long vv = visits, rr = rays;
+#pragma unroll
+  for (int o = 16; o > 0; o >>= 1) {
+    vv += __shfl_xor_sync(kFull, vv, o);
+    rr += __shfl_xor_sync(kFull, rr, o);
+  }
+  if ((threadIdx.x & 31) == 0 && (vv | rr)) {
     atomicAdd(&m.ctr->visits, vv);
     atomicAdd(&m.ctr->rays, rr);
   }
@@ -354,77 +547,122 @@ __global__ void __launch_bounds__(256) k_traverse_dev(const TickWork<kMaxTickFra
   traverse_body<RM, kMaxTickFrames>(*work, m);
 }
 
-
 template <int RM, int MaxF>
-int persistent_grid(size_t smem_bytes, int block) {
-  static int cached_blocks = 0;
-  static size_t cached_smem = 0;
-  static int cached_block = 0;
-  static int sms = 0;
-  if (cached_blocks == 0 || cached_smem != smem_bytes || cached_block != block) {
-    cudaFuncSetAttribute(k_traverse<RM, MaxF>, cudaFuncAttributeMaxDynamicSharedMemorySize,
-                         160 * 1024);
+__global__ void __launch_bounds__(256) k_traverse_wide(const __grid_constant__ TickWork<MaxF> work,
+                                                       MapView m) {
+  traverse_wide_body<RM, MaxF>(work, m);
+}
+
+template <int RM>
+__global__ void __launch_bounds__(256) k_traverse_wide_dev(const TickWork<kMaxTickFrames>* work,
+                                                           MapView m) {
+  traverse_wide_body<RM, kMaxTickFrames>(*work, m);
+}
+
+// Resident CTAs of a traversal kernel for a block size and dynamic shared memory, queried
+// once per (kernel, shape) ahead of any stream capture.
+struct GridCache {
+  const void* fn = nullptr;
+  size_t smem = 0;
+  int block = 0;
+  int blocks = 0;
+};
+
+int g_sm_count = 0;
+constexpr int kGridCacheSize = 64;
+GridCache g_grid_cache[kGridCacheSize];
+int g_grid_next = 0;
+std::mutex g_grid_mutex;
+
+cudaError_t resident_grid(const void* fn, size_t smem, int block, int* grid) {
+  std::lock_guard<std::mutex> lock(g_grid_mutex);
+  for (GridCache& c : g_grid_cache)
+    if (c.fn == fn && c.smem == smem && c.block == block) {
+      *grid = g_sm_count * c.blocks;
+      return cudaSuccess;
+    }
+  cudaError_t e = cudaSuccess;
+  if (g_sm_count == 0) {
     int dev = 0;
-    cudaGetDevice(&dev);
-    cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, dev);
-    int blocks = 0;
-    cudaOccupancyMaxActiveBlocksPerMultiprocessor(&blocks, k_traverse<RM, MaxF>, block, smem_bytes);
-    cached_blocks = blocks > 0 ? blocks : 1;
-    cached_smem = smem_bytes;
-    cached_block = block;
+    e = cudaGetDevice(&dev);
+    if (e == cudaSuccess) e = cudaDeviceGetAttribute(&g_sm_count, cudaDevAttrMultiProcessorCount, dev);
+    if (e != cudaSuccess) return e;
   }
-  return sms * cached_blocks;
+  e = cudaFuncSetAttribute(fn, cudaFuncAttributeMaxDynamicSharedMemorySize, 160 * 1024);
+  int blocks = 0;
+  if (e == cudaSuccess) e = cudaOccupancyMaxActiveBlocksPerMultiprocessor(&blocks, fn, block, smem);
+  if (e != cudaSuccess) return e;
+  if (blocks < 1) blocks = 1;
+  GridCache& c = g_grid_cache[g_grid_next];
+  g_grid_next = (g_grid_next + 1) % kGridCacheSize;
+  c.fn = fn;
+  c.smem = smem;
+  c.block = block;
+  c.blocks = blocks;
+  *grid = g_sm_count * blocks;
+  return cudaSuccess;
+}
+
+bool work_is_wide(const FrameParams* fr, int n) {
+  for (int i = 0; i < n; ++i)
+    if (!(fr[i].max_time < kNarrowMaxTime)) return true;
+  return false;
 }
 
 }  // namespace
 
+size_t traverse_smem_bytes(int tile_w, int tile_h, uint32_t smask, bool render) {
+  const size_t nent = (size_t)smask + 1;
+  const size_t nrays = (size_t)tile_w * tile_h;
+  return nent * (8 + kLabelWords * 4 + 4) + nrays * (2 + 1) + (render ? nrays * 4 : 0);
+}
+
 template <int MaxF>
 cudaError_t launch_traverse_labels(const TickWork<MaxF>& w, const MapView& m, int rounding,
                                    cudaStream_t s) {
-  const size_t smem = (size_t)(w.smask + 1) * (8 + kLabelWords * 4);
   const int block = min(256, w.tile_w * w.tile_h);
-  if (rounding == NM_ROUND_DOWN) {
-    const int grid = min(persistent_grid<NM_ROUND_DOWN, MaxF>(smem, block), (int)w.total_tiles);
-    k_traverse<NM_ROUND_DOWN, MaxF><<<grid, block, smem, s>>>(w, m);
-  } else {
-    const int grid = min(persistent_grid<NM_ROUND_NEAREST, MaxF>(smem, block), (int)w.total_tiles);
-    k_traverse<NM_ROUND_NEAREST, MaxF><<<grid, block, smem, s>>>(w, m);
+  const bool down = rounding == NM_ROUND_DOWN;
+  int grid = 0;
+  if (work_is_wide(w.fr, w.n_frames)) {
+    const void* fn = down ? (const void*)k_traverse_wide<NM_ROUND_DOWN, MaxF>
+                          : (const void*)k_traverse_wide<NM_ROUND_NEAREST, MaxF>;
+    cudaError_t e = resident_grid(fn, 0, block, &grid);
+    if (e != cudaSuccess) return e;
+    grid = min(grid, (int)w.total_tiles);
+    if (down)
+      k_traverse_wide<NM_ROUND_DOWN, MaxF><<<grid, block, 0, s>>>(w, m);
+    else
+      k_traverse_wide<NM_ROUND_NEAREST, MaxF><<<grid, block, 0, s>>>(w, m);
+    return cudaGetLastError();
   }
+  const size_t smem = traverse_smem_bytes(w.tile_w, w.tile_h, w.smask, false);
+  const void* fn = down ? (const void*)k_traverse<NM_ROUND_DOWN, MaxF>
+                        : (const void*)k_traverse<NM_ROUND_NEAREST, MaxF>;
+  cudaError_t e = resident_grid(fn, smem, block, &grid);
+  if (e != cudaSuccess) return e;
+  grid = min(grid, (int)w.total_tiles);
+  if (down)
+    k_traverse<NM_ROUND_DOWN, MaxF><<<grid, block, smem, s>>>(w, m);
+  else
+    k_traverse<NM_ROUND_NEAREST, MaxF><<<grid, block, smem, s>>>(w, m);
   return cudaGetLastError();
 }
 
+bool traverse_render_fits(const FrameParams& f) { return f.max_time < kNarrowMaxTime; }
+
 cudaError_t launch_traverse_render(const TickWork<1>& w, const MapView& m, const SimRender& sr,
                                    int rounding, cudaStream_t s) {
-  const int nrays = w.tile_w * w.tile_h;
-  const size_t smem = (size_t)(w.smask + 1) * (8 + kLabelWords * 4) + (size_t)nrays * 4;
-  const int block = min(256, nrays);
-  static int cached[2] = {0, 0};
-  static size_t cached_smem[2] = {0, 0};
-  static int cached_block[2] = {0, 0};
-  static int sms = 0;
-  const int ri = rounding == NM_ROUND_DOWN ? 1 : 0;
-  if (!cached[ri] || cached_smem[ri] != smem || cached_block[ri] != block) {
-    int dev = 0;
-    cudaGetDevice(&dev);
-    cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, dev);
-    int blocks = 0;
-    if (ri) {
-      cudaFuncSetAttribute(k_traverse_render<NM_ROUND_DOWN>,
-                           cudaFuncAttributeMaxDynamicSharedMemorySize, 160 * 1024);
-      cudaOccupancyMaxActiveBlocksPerMultiprocessor(&blocks, k_traverse_render<NM_ROUND_DOWN>,
-                                                    block, smem);
-    } else {
-      cudaFuncSetAttribute(k_traverse_render<NM_ROUND_NEAREST>,
-                           cudaFuncAttributeMaxDynamicSharedMemorySize, 160 * 1024);
-      cudaOccupancyMaxActiveBlocksPerMultiprocessor(&blocks, k_traverse_render<NM_ROUND_NEAREST>,
-                                                    block, smem);
-    }
-    cached[ri] = blocks > 0 ? blocks : 1;
-    cached_smem[ri] = smem;
-    cached_block[ri] = block;
-  }
-  const int grid = min(sms * cached[ri], (int)w.total_tiles);
-  if (ri)
+  if (!traverse_render_fits(w.fr[0])) return cudaErrorInvalidValue;
+  const int block = min(256, w.tile_w * w.tile_h);
+  const size_t smem = traverse_smem_bytes(w.tile_w, w.tile_h, w.smask, true);
+  const bool down = rounding == NM_ROUND_DOWN;
+  const void* fn = down ? (const void*)k_traverse_render<NM_ROUND_DOWN>
+                        : (const void*)k_traverse_render<NM_ROUND_NEAREST>;
+  int grid = 0;
+  cudaError_t e = resident_grid(fn, smem, block, &grid);
+  if (e != cudaSuccess) return e;
+  grid = min(grid, (int)w.total_tiles);
+  if (down)
     k_traverse_render<NM_ROUND_DOWN><<<grid, block, smem, s>>>(w, m, sr);
   else
     k_traverse_render<NM_ROUND_NEAREST><<<grid, block, smem, s>>>(w, m, sr);
@@ -432,51 +670,43 @@ cudaError_t launch_traverse_render(const TickWork<1>& w, const MapView& m, const
 }
 
 namespace {
-struct DevGrid {
-  int blocks = 0;
-  size_t smem = 0;
-  int block = 0;
-  int sms = 0;
-};
-DevGrid g_dev_grid[2];
+const void* dev_kernel(int rounding, bool wide) {
+  if (wide)
+    return rounding == NM_ROUND_DOWN ? (const void*)k_traverse_wide_dev<NM_ROUND_DOWN>
+                                     : (const void*)k_traverse_wide_dev<NM_ROUND_NEAREST>;
+  return rounding == NM_ROUND_DOWN ? (const void*)k_traverse_dev<NM_ROUND_DOWN>
+                                   : (const void*)k_traverse_dev<NM_ROUND_NEAREST>;
+}
 }  // namespace
 
-cudaError_t prepare_traverse_dev(int tile_w, int tile_h, uint32_t smask, int rounding) {
-  const size_t smem = (size_t)(smask + 1) * (8 + kLabelWords * 4);
+cudaError_t prepare_traverse_dev(int tile_w, int tile_h, uint32_t smask, int rounding, bool wide) {
   const int block = min(256, tile_w * tile_h);
-  DevGrid& g = g_dev_grid[rounding == NM_ROUND_DOWN ? 1 : 0];
-  if (g.blocks && g.smem == smem && g.block == block) return cudaSuccess;
-  int dev = 0;
-  cudaError_t e = cudaGetDevice(&dev);
-  if (e == cudaSuccess) e = cudaDeviceGetAttribute(&g.sms, cudaDevAttrMultiProcessorCount, dev);
-  if (rounding == NM_ROUND_DOWN) {
-    if (e == cudaSuccess)
-      e = cudaFuncSetAttribute(k_traverse_dev<NM_ROUND_DOWN>, cudaFuncAttributeMaxDynamicSharedMemorySize, 160 * 1024);
-    if (e == cudaSuccess)
-      e = cudaOccupancyMaxActiveBlocksPerMultiprocessor(&g.blocks, k_traverse_dev<NM_ROUND_DOWN>, block, smem);
-  } else {
-    if (e == cudaSuccess)
-      e = cudaFuncSetAttribute(k_traverse_dev<NM_ROUND_NEAREST>, cudaFuncAttributeMaxDynamicSharedMemorySize, 160 * 1024);
-    if (e == cudaSuccess)
-      e = cudaOccupancyMaxActiveBlocksPerMultiprocessor(&g.blocks, k_traverse_dev<NM_ROUND_NEAREST>, block, smem);
-  }
-  if (g.blocks < 1) g.blocks = 1;
-  g.smem = smem;
-  g.block = block;
-  return e;
+  const size_t smem = wide ? 0 : traverse_smem_bytes(tile_w, tile_h, smask, false);
+  int grid = 0;
+  return resident_grid(dev_kernel(rounding, wide), smem, block, &grid);
 }
 
 cudaError_t launch_traverse_labels_dev(const TickWork<kMaxTickFrames>* d_work, uint32_t total_tiles,
                                        int tile_w, int tile_h, uint32_t smask, const MapView& m,
-                                       int rounding, cudaStream_t s) {
-  const cudaError_t e = prepare_traverse_dev(tile_w, tile_h, smask, rounding);
+                                       int rounding, bool wide, cudaStream_t s) {
+  const int block = min(256, tile_w * tile_h);
+  const size_t smem = wide ? 0 : traverse_smem_bytes(tile_w, tile_h, smask, false);
+  int grid = 0;
+  const cudaError_t e = resident_grid(dev_kernel(rounding, wide), smem, block, &grid);
   if (e != cudaSuccess) return e;
-  const DevGrid& g = g_dev_grid[rounding == NM_ROUND_DOWN ? 1 : 0];
-  const int grid = min(g.sms * g.blocks, (int)total_tiles);
-  if (rounding == NM_ROUND_DOWN)
-    k_traverse_dev<NM_ROUND_DOWN><<<grid, g.block, g.smem, s>>>(d_work, m);
-  else
-    k_traverse_dev<NM_ROUND_NEAREST><<<grid, g.block, g.smem, s>>>(d_work, m);
+  grid = min(grid, (int)total_tiles);
+  const bool down = rounding == NM_ROUND_DOWN;
+  if (wide) {
+    if (down)
+      k_traverse_wide_dev<NM_ROUND_DOWN><<<grid, block, 0, s>>>(d_work, m);
+    else
+      k_traverse_wide_dev<NM_ROUND_NEAREST><<<grid, block, 0, s>>>(d_work, m);
+  } else {
+    if (down)
+      k_traverse_dev<NM_ROUND_DOWN><<<grid, block, smem, s>>>(d_work, m);
+    else
+      k_traverse_dev<NM_ROUND_NEAREST><<<grid, block, smem, s>>>(d_work, m);
+  }
   return cudaGetLastError();
 }
 
