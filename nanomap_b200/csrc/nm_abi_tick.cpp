@@ -44,7 +44,8 @@ struct nm_tick_plan_s {
   TickStage* h_stage[2] = {nullptr, nullptr};  // pinned
   TickStage* d_stage = nullptr;
   cudaStream_t cap_stream = nullptr;
-  cudaGraphExec_t exec[2] = {nullptr, nullptr};
+  // graphs per staging buffer: [k] integrates the tick, [2 + k] leaves its labels in place
+  cudaGraphExec_t exec[4] = {nullptr, nullptr, nullptr, nullptr};
   cudaEvent_t done[2] = {nullptr, nullptr};
   bool launched[2] = {false, false};
   uint32_t captured_capacity = 0;
@@ -57,7 +58,7 @@ struct nm_tick_plan_s {
 namespace {
 
 void drop_graphs(nm_tick_plan p) {
-  for (int i = 0; i < 2; ++i) {
+  for (int i = 0; i < 4; ++i) {
     if (p->exec[i]) cudaGraphExecDestroy(p->exec[i]);
     p->exec[i] = nullptr;
   }
@@ -113,13 +114,19 @@ int fill_stage(nm_tick_plan p, TickStage* st, uint64_t* bound) {
   return NM_OK;
 }
 
-int capture(nm_tick_plan p, int k) {
+// Captures the graph of staging buffer k: stage copy, batched render (plans with a sim map),
+// the persistent traversal, and (unless `defer`) the integration of every label plane.
+int capture(nm_tick_plan p, int k, bool defer) {
   nm_map m = p->map;
   TickStage* h = p->h_stage[k];
   const uint32_t render_tiles = h->render.tile_start[p->n];
   const uint32_t total_tiles = h->work.total_tiles;
+  // frames that reach beyond the leaf code take the wide traversal (fixed per plan: the
+  // slots' sensors and the map resolution set max_range / res)
+  bool wide = false;
+  for (int i = 0; i < p->n; ++i) wide |= !(h->work.fr[i].max_time < nm::kNarrowMaxTime);
   // occupancy queries and attributes are settled before capture begins
-  NM_CUDA(nm::prepare_traverse_dev(p->tile_w, p->tile_h, (uint32_t)p->entries - 1u, m->desc.rounding));
+  NM_CUDA(nm::prepare_traverse_dev(p->tile_w, p->tile_h, (uint32_t)p->entries - 1u, m->desc.rounding, wide));
   NM_CUDA(cudaStreamBeginCapture(p->cap_stream, cudaStreamCaptureModeThreadLocal));
   cudaError_t e = cudaMemcpyAsync(p->d_stage, h, sizeof(TickStage), cudaMemcpyHostToDevice, p->cap_stream);
   if (e == cudaSuccess && p->sim)
@@ -127,8 +134,8 @@ int capture(nm_tick_plan p, int k) {
   if (e == cudaSuccess && total_tiles > 0)
     e = nm::launch_traverse_labels_dev(&p->d_stage->work, total_tiles, p->tile_w, p->tile_h,
                                        (uint32_t)p->entries - 1u, m->view, m->desc.rounding,
-                                       p->cap_stream);
-  if (e == cudaSuccess)
+                                       wide, p->cap_stream);
+  if (e == cudaSuccess && !defer)
     e = nm::launch_integrate(m->view, p->integ, m->desc.update_mode, m->desc.rounding,
                              m->ctx->sm_count, p->cap_stream);
   cudaGraph_t g = nullptr;
@@ -138,7 +145,7 @@ int capture(nm_tick_plan p, int k) {
     cudaGetLastError();
     return fail(NM_ERR_CUDA, "tick capture failed: %s", cudaGetErrorString(e != cudaSuccess ? e : e2));
   }
-  e = cudaGraphInstantiate(&p->exec[k], g, 0);
+  e = cudaGraphInstantiate(&p->exec[defer ? 2 + k : k], g, 0);
   cudaGraphDestroy(g);
   if (e != cudaSuccess) return fail(NM_ERR_CUDA, "tick instantiate: %s", cudaGetErrorString(e));
   return NM_OK;
@@ -162,18 +169,29 @@ int run_plan(nm_tick_plan p, uint32_t flags, cudaStream_t s) {
     p->captured_capacity = m->view.capacity;
     p->captured_keys = m->view.keys;
   }
+  const bool defer = (flags & NM_DEFER_INTEGRATE) != 0;
+  if (defer)  // the labels stay in their planes until nm_map_integrate applies them
+    for (int i = 0; i < p->n; ++i) {
+      rc = nm::set_plane_constants(m, p->slots[i].agent, p->slots[i].sensor);
+      if (rc != NM_OK) return rc;
+    }
   for (int i = 0; i < p->n; ++i) p->h_stage[k]->work.fr[i].epoch = m->epoch;
-  if (!p->exec[k]) {
-    rc = capture(p, k);
+  const int gi = defer ? 2 + k : k;
+  if (!p->exec[gi]) {
+    rc = capture(p, k, defer);
     if (rc != NM_OK) return rc;
   }
-  NM_CUDA(cudaGraphLaunch(p->exec[k], s));
+  NM_CUDA(cudaGraphLaunch(p->exec[gi], s));
   NM_CUDA(cudaEventRecord(p->done[k], s));
   p->launched[k] = true;
   p->parity ^= 1;
   p->tick += 1;
-  m->epoch += 1;
-  if (m->epoch == 0) m->epoch = 1;
+  if (defer) {
+    m->pending_labels = true;  // nm_map_integrate advances the epoch
+  } else {
+    m->epoch += 1;
+    if (m->epoch == 0) m->epoch = 1;
+  }
   if (flags & NM_SYNC) return nm::check_device_errors(m, s);
   return NM_OK;
 }
@@ -327,8 +345,10 @@ int nm_tick_plan_autotune(nm_tick_plan p, const char* cache_path, int32_t best[3
       }
     }
   }
-  const int cands[][3] = {{16, 16, 128}, {16, 16, 256}, {16, 8, 128}, {32, 8, 128},
-                          {32, 16, 128}, {32, 16, 256}, {8, 8, 64},   {16, 16, 64}};
+  // tile shape (rays per thread = tile area / 256 for tiles of 256 rays and more: 1, 2, 4)
+  // and shared leaf-table entries
+  const int cands[][3] = {{16, 16, 128}, {16, 16, 256}, {16, 8, 128},  {8, 8, 64},
+                          {32, 16, 128}, {32, 16, 256}, {32, 32, 256}, {64, 16, 256}};
   nm_map scratch = nullptr;
   nm_map_desc d = m->desc;
   d.initial_leaf_capacity = m->view.capacity;

@@ -209,6 +209,57 @@ def sensor_desc_kwargs(spec: SceneSpec) -> dict:
                 explicit_log_odds=1, frame_transform=OPTICAL_TO_BODY)
 
 
+# The batched multi-agent tick: the plain_small world mapped at 0.05 m into one shared map by
+# 16 agents of uneven sensors, as (type, hres, vres, hfov deg, vfov deg, max range m): six
+# 320x240 cameras at 5 m, six 640x480 at 10 m, three 1280x720 at 8 m (87 x 58 deg) and one
+# spinning 64-beam x 1024-column range sensor (360 x 30 deg) at 20 m.
+TICK_RES = 0.05
+TICK_AGENTS = ([(0, 320, 240, 87.0, 58.0, 5.0)] * 6 + [(0, 640, 480, 87.0, 58.0, 10.0)] * 6 +
+               [(0, 1280, 720, 87.0, 58.0, 8.0)] * 3 + [(1, 1024, 64, 360.0, 30.0, 20.0)])
+
+
+def tick_agent_desc_kwargs(agent: tuple) -> dict:
+    """Sensor parameters of one agent of the batched tick (explicit log-odds +0.85 / -0.4)."""
+    typ, w, h, hf, vf, rng = agent
+    return dict(type=typ, hres=w, vres=h, hfov_deg=hf, vfov_deg=vf, max_range=rng,
+                explicit_log_odds=1, log_odds_hit=0.85, log_odds_miss=-0.4,
+                frame_transform=OPTICAL_TO_BODY)
+
+
+def tick_sim_box(spec: SceneSpec, res: float = TICK_RES):
+    """Voxel box [0, size / res) of the batched tick's sim map."""
+    return (0, 0, 0), tuple(int(math.ceil(x / res)) for x in spec.size)
+
+
+def analytic_box_ranges(scene: Scene, pixel_model, width: int, height: int, max_range: float,
+                        pos, q) -> np.ndarray:
+    """Radial ranges (float32, 0 = no return) of a frustum camera against the scene's boxes by
+    exact FP64 ray-box intersection: pixel (w, h) looks along (w/W * 2hw - hw, h/H * 2hh - hh,
+    1) in the sensor frame (`pixel_model` = hw, hh, 2hw, 2hh, 1/W, 1/H)."""
+    hw, hh, c0, c1 = (float(v) for v in pixel_model[:4])
+    u = np.arange(width, dtype=np.float64) / width
+    v = np.arange(height, dtype=np.float64) / height
+    d = np.stack(np.broadcast_arrays(u[None, :] * c0 - hw, v[:, None] * c1 - hh, 1.0), axis=-1)
+    m = d.reshape(-1, 3) @ rotation_matrix(q).T
+    m /= np.linalg.norm(m, axis=1, keepdims=True)
+    p = np.asarray(pos, dtype=np.float64)
+    best = np.full(len(m), np.inf)
+    # boxes whose nearest point lies beyond max range cannot be hit
+    near = np.linalg.norm(np.maximum(np.maximum(scene.boxes[:, :3] - p, p - scene.boxes[:, 3:]), 0.0),
+                          axis=1) <= max_range
+    with np.errstate(divide="ignore", invalid="ignore"):
+        inv = 1.0 / m
+        for b in scene.boxes[near]:
+            ta = (b[:3] - p) * inv
+            tb = (b[3:] - p) * inv
+            t0 = np.nanmax(np.maximum(np.minimum(ta, tb), 0.0), axis=1)
+            t1 = np.nanmin(np.maximum(ta, tb), axis=1)
+            hit = t0 <= t1
+            best = np.where(hit & (t0 < best), t0, best)
+    out = np.where((best <= max_range) & (best > 0.0), best, 0.0)
+    return out.astype(np.float32).reshape(height, width)
+
+
 def rotation_matrix(q, F=OPTICAL_TO_BODY) -> np.ndarray:
     """World-from-sensor rotation in float64 (for analytic rendering; not bit-matched)."""
     w, x, y, z = q

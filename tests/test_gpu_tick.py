@@ -5,7 +5,8 @@ import pytest
 from nanomap_b200 import _native as N
 from nanomap_b200 import api as A
 from nanomap_b200 import scenes as S
-from tests.workloads import compare_labels, compare_maps
+from oracle import oracle as O
+from tests.workloads import compare_labels, compare_maps, oracle_frame
 
 pytestmark = pytest.mark.gpu
 
@@ -116,3 +117,62 @@ def test_tick_rejects_bad_slots(ctx):
         m.tick([(s, A.Pose((0, 0, 1), (1, 0, 0, 0)), r, 2)])
     with pytest.raises(N.NanomapError):
         m.tick([(s, A.Pose((0, 0, 1), (1, 0, 0, 0)), r, 0)] * 33)
+
+
+def test_sixteen_agent_plan_ticks_match_solo_sequential_and_oracle(ctx):
+    """The batched tick at its full size: 16 agents of uneven sensors (6 x 320x240 at 5 m,
+    6 x 640x480 at 10 m, 3 x 1280x720 at 8 m, one spinning 64 x 1024 at 20 m) in the 20 x 20 x 5
+    m world at 0.05 m, rendered with range noise and labelled by one graph-replayed tick plan per
+    tick.  Every tick, every agent's label plane equals its solo insert of the same ranges bit
+    for bit, and the spinning sensor's labels equal the oracle's; after the ticks the shared map
+    equals the agents' frames inserted one by one in agent order."""
+    import torch
+    spec = S.SCENES["plain_small"]
+    scene = S.make_scene(spec, 1)
+    lo, hi = S.tick_sim_box(spec)
+    sim = A.SimMap(ctx, S.TICK_RES, boxes=scene.boxes, cylinders=scene.cylinders, vox_min=lo,
+                   vox_max=hi)
+    sensors = [A.Sensor(ctx, A.sensor_desc(**S.tick_agent_desc_kwargs(a))) for a in S.TICK_AGENTS]
+    n = len(sensors)
+    assert n == 16
+    ticks = 3
+    trajs = [[A.Pose(p, q) for p, q in S.trajectory(scene, ticks, seed=101 + 37 * a)]
+             for a in range(n)]
+    bufs = [torch.zeros(s.desc.vres, s.desc.hres, device="cuda") for s in sensors]
+    kw = dict(res=S.TICK_RES, initial_leaf_capacity=1 << 20)
+    mb = A.Map(ctx, A.map_desc(max_agents=n, **kw))
+    plan = A.TickPlan(mb, [(sensors[a], bufs[a], a) for a in range(n)], sim=sim)
+    plan.set_noise(0.005, 0.02, 99)
+    seq = A.Map(ctx, A.map_desc(**kw))
+    solo = A.Map(ctx, A.map_desc(**kw))
+    laser = n - 1
+    assert sensors[laser].desc.type == N.NM_SENSOR_LASER
+    osen = O.Sensor.from_desc(sensors[laser].desc)
+    for t in range(ticks):
+        for a in range(n):
+            plan.set_pose(a, trajs[a][t])
+        plan.run(flags=N.NM_DEFER_INTEGRATE)
+        torch.cuda.synchronize()
+        for a in range(n):
+            solo.reset()
+            solo.insert_ranges(sensors[a], trajs[a][t], bufs[a], flags=N.NM_DEFER_INTEGRATE)
+            got = mb.export_labels(a)
+            assert len(got[0]) > 0, f"tick {t} agent {a}: no labels"
+            errs = compare_labels(got, solo.export_labels(0))
+            assert not errs, f"tick {t} agent {a} vs solo: " + "; ".join(errs[:3])
+            if a == laser:
+                R, eye, mt = oracle_frame(sensors[a].desc, trajs[a][t], S.TICK_RES, N.NM_ROUND_DOWN)
+                om = O.Map(S.TICK_RES, rounding=1)
+                d = sensors[a].desc
+                om.insert(R, eye, mt, d.log_odds_hit, d.log_odds_miss,
+                          osen.points(bufs[a].cpu().numpy()), threads=8, keep_labels=True)
+                errs = compare_labels(got, om.labels())
+                assert not errs, f"tick {t} laser vs oracle: " + "; ".join(errs[:3])
+        mb.integrate()
+        for a in range(n):
+            seq.insert_ranges(sensors[a], trajs[a][t], bufs[a])
+    errs = compare_maps(mb.export(), seq.export())
+    assert not errs, "; ".join(errs[:5])
+    sb, ss = mb.stats(), seq.stats()
+    assert sb["visits"] == ss["visits"] and sb["error_flags"] == 0 and ss["error_flags"] == 0
+    plan.close()
