@@ -1,17 +1,24 @@
-"""Benchmark of the B200 mapping + simulation path (one JSON line on rank 0).
+"""Benchmark of the B200 mapping path (one JSON line on rank 0).
 
 Workload (per GPU): the 40 x 40 x 10 m scene with 2000 boxes and 300 cylinders at 0.05 m, a
-640x480 frustum camera (87 x 58 deg, 10 m), a 100-frame seeded trajectory.  One step = one
-frame: simulated range image with range noise (sigma 0.005 d^2, 2 % dropped; one launch) ->
-traversal and per-frame labels -> integration into the device map (3 launches).  Inputs (sim map, poses) are resident
-when timing starts; L2 is flushed (256 MiB write) between steps, outside the per-step events.
+640x480 frustum camera (87 x 58 deg, 10 m), a seeded trajectory.  The frames are simulated
+ranges with range noise (sigma 0.005 d^2, 2 % dropped), given to the map as PointCloud2-style
+xyz records (16 bytes per pixel, NaN where no return), computed before timing starts.  One
+step = one frame inserted: traversal and per-frame labels, then integration into the device
+map (2 launches).  `value` times the step with the records resident in device memory; L2 is
+flushed (256 MiB write) between steps, outside the per-step events.
 
-`e2e` repeats the metric through the reference-facing call (nm_map_insert_points with
-PointCloud2-style xyz records in pinned host memory, copied to the device inside the call,
-and a synchronous read-back of the frame status).
+`e2e` repeats the metric through the reference-facing call (nm_map_insert_points with the
+records in pinned host memory, copied to the device inside the call, and a synchronous
+read-back of the frame status).
 
-`--impl reference` times the CPU path the reference runs (Handler::processPointCloudCPU,
-restated by the oracle, plus its simulated depth) on the host cores, rank 0 only.
+`--impl reference` times the same step on the host cores, rank 0 only: the reference's CPU
+insertion path (Handler::processPointCloudCPU, restated by the oracle) on the same kind of
+frames, computed beforehand.
+
+Sections beside the headline: the whole simulated frame (render + noise + insert), the small
+plain-mapping workload, the voxel filter, expected depth and pose refinement, the 16-agent
+batched tick, the large fine-resolution workload and procedural caves.
 
 Multi-GPU (torchrun): each rank maps its own agent's trajectory into its own map (weak
 scaling, no collective on the data path); `value` = all ranks' voxel updates / max time.
@@ -40,12 +47,14 @@ WORKLOAD = "sim_headline"
 
 def workload_config(spec):
     return {
-        "workload": (f"sim+map frame: {spec.size[0]:.0f}x{spec.size[1]:.0f}x{spec.size[2]:.0f} m, "
-                     f"{spec.n_boxes} boxes + {spec.n_cyl} cylinders, {spec.width}x{spec.height} "
-                     f"{spec.hfov:.0f}x{spec.vfov:.0f} deg, {spec.max_range:.0f} m range, "
-                     f"{spec.map_res} m voxels, label mode, round-down policy"),
+        "workload": (f"xyz-record insert of simulated frames: {spec.size[0]:.0f}x{spec.size[1]:.0f}x"
+                     f"{spec.size[2]:.0f} m, {spec.n_boxes} boxes + {spec.n_cyl} cylinders, "
+                     f"{spec.width}x{spec.height} {spec.hfov:.0f}x{spec.vfov:.0f} deg, "
+                     f"{spec.max_range:.0f} m range, {spec.map_res} m voxels, label mode, "
+                     f"round-down policy"),
         "frames_per_step": 1,
         "pixels_per_frame": spec.width * spec.height,
+        "input": "xyz records, 16 B per pixel, range noise sigma 0.005 d^2, 2 % dropped",
         "l2": "flushed between steps (256 MiB write outside the per-step CUDA events)",
     }
 
@@ -146,8 +155,48 @@ class ClockSampler:
                 "samples": len(sm)}
 
 
+def frame_records(ranges, pixel_model):
+    """PointCloud2-style xyz records (x, y, z, pad: 16 bytes) of a frustum range image, NaN
+    where the pixel has no return; works on torch tensors (device or host) and numpy arrays."""
+    import torch
+    r = ranges if isinstance(ranges, torch.Tensor) else torch.from_numpy(np.asarray(ranges))
+    H, W = r.shape
+    hw, hh, c0, c1, su, sv = (float(v) for v in pixel_model)
+    u = torch.arange(W, dtype=torch.float32, device=r.device) * su
+    v = torch.arange(H, dtype=torch.float32, device=r.device) * sv
+    dx = (u * c0 - hw)[None, :].expand(H, W)
+    dy = (v * c1 - hh)[:, None].expand(H, W)
+    sc = r / torch.sqrt(dx * dx + dy * dy + 1.0)
+    rec = torch.stack([dx * sc, dy * sc, sc, torch.zeros_like(sc)], dim=-1).reshape(H * W, 4)
+    rec[(r <= 0).reshape(-1), :3] = float("nan")
+    return rec.contiguous()
+
+
+def reference_frames(spec, scene, traj, desc, n, threads, seed=5):
+    """n frames of the workload computed on the host by the oracle: simulated ranges with range
+    noise (sigma = noise_coef d^2, drop fraction), as sensor-frame points; with the rotation,
+    eye and max time of each frame (outside any timed region)."""
+    from oracle import oracle as O
+    osen = O.Sensor.from_desc(desc)
+    sim = O.SimMap(spec.sim_res, scene.vox_min, scene.vox_max, scene.boxes, scene.cylinders)
+    rng = np.random.default_rng(seed)
+    out = []
+    for i in range(n):
+        pos, q = traj[i % len(traj)]
+        R = O.rotation(q, list(desc.frame_transform))
+        r = sim.render(osen, pos, R, threads=threads)
+        r = np.where(r > 0, r + rng.normal(0, 1, r.shape) * spec.noise_coef * r * r, 0).astype(np.float32)
+        r[rng.random(r.shape) < spec.drop] = 0
+        r[~(r > 0)] = 0
+        eye, mt = O.frame_setup(pos, spec.map_res, desc.max_range, 1)
+        out.append((R, eye, mt, osen.points(r)))
+    return out
+
+
 def run_reference(args, rank, world):
-    """CPU path of the reference (oracle restatement), rank 0 only."""
+    """The reference's CPU insertion path (Handler::processPointCloudCPU, restated by the
+    oracle) on the host cores, rank 0 only: each step inserts one frame's points (the
+    simulated, noised frames are computed beforehand, outside the timed region)."""
     if rank != 0:
         return None
     from nanomap_b200 import api as A
@@ -157,29 +206,17 @@ def run_reference(args, rank, world):
     scene = S.make_scene(spec, 1)
     traj = S.trajectory(scene, spec.frames, seed=7)
     desc = A.sensor_desc(**S.sensor_desc_kwargs(spec))
-    osen = O.Sensor.from_desc(desc)
-    sim = O.SimMap(spec.sim_res, scene.vox_min, scene.vox_max, scene.boxes, scene.cylinders)
-    om = O.Map(spec.map_res, clamp_min=spec.clamp[0], clamp_max=spec.clamp[1], rounding=1)
     threads = os.cpu_count() or 1
-    rng = np.random.default_rng(5)
-
-    def step(i):
-        pos, q = traj[i % len(traj)]
-        R = O.rotation(q, list(desc.frame_transform))
-        r = sim.render(osen, pos, R, threads=threads)
-        valid = r > 0
-        r = np.where(valid, r + rng.normal(0, 1, r.shape) * spec.noise_coef * r * r, 0).astype(np.float32)
-        r[rng.random(r.shape) < spec.drop] = 0
-        r[~(r > 0)] = 0
-        eye, mt = O.frame_setup(pos, spec.map_res, desc.max_range, 1)
-        om.insert(R, eye, mt, desc.log_odds_hit, desc.log_odds_miss, osen.points(r), threads=threads)
-
+    frames = reference_frames(spec, scene, traj, desc, args.warmup + args.steps, threads)
+    om = O.Map(spec.map_res, clamp_min=spec.clamp[0], clamp_max=spec.clamp[1], rounding=1)
     for i in range(args.warmup):
-        step(i)
+        R, eye, mt, pts = frames[i]
+        om.insert(R, eye, mt, desc.log_odds_hit, desc.log_odds_miss, pts, threads=threads)
     v0 = om.stats()["visits"]
     t0 = time.perf_counter()
     for i in range(args.steps):
-        step(args.warmup + i)
+        R, eye, mt, pts = frames[args.warmup + i]
+        om.insert(R, eye, mt, desc.log_odds_hit, desc.log_odds_miss, pts, threads=threads)
     dt = time.perf_counter() - t0
     visits = om.stats()["visits"] - v0
     value = visits / dt
@@ -191,29 +228,37 @@ def run_reference(args, rank, world):
         "higher_is_better": True, "scaling": "weak", "vs_baseline": None, "dtype": "f64",
         "data": "synthetic", "config": cfg,
         "cpu_baseline": {"value": value, "unit": UNIT, "cores": threads, "kind": "port",
-                         "sample": f"{args.steps} full frames (sim depth + insertion), oracle restatement of Handler::processPointCloudCPU"},
+                         "sample": (f"{args.steps} full frames: insertion of one frame's points "
+                                    "into the map (oracle restatement of "
+                                    "Handler::processPointCloudCPU), all host threads")},
         "e2e": {"value": value, "unit": UNIT, "h2d_bytes_per_step": 0, "d2h_bytes_per_step": 0},
     }
     return line
 
 
-def cpu_baseline(spec, desc, frames_host, budget_s=12.0):
-    """Single-thread oracle on a bounded sample of the same frames (rank 0, N=1)."""
+def cpu_baseline(spec, scene, traj, desc, budget_s=12.0):
+    """Single-thread oracle insertion on a bounded sample of the workload's frames (rank 0,
+    N=1); the frames are computed first, outside the timed region."""
     from oracle import oracle as O
-    osen = O.Sensor.from_desc(desc)
+    frames = reference_frames(spec, scene, traj, desc, 30, os.cpu_count() or 1, seed=6)
     om = O.Map(spec.map_res, clamp_min=spec.clamp[0], clamp_max=spec.clamp[1], rounding=1)
     t0 = time.perf_counter()
     n = 0
-    for pose, r in frames_host:
-        R = O.rotation(pose.orientation, list(desc.frame_transform))
-        eye, mt = O.frame_setup(pose.position, spec.map_res, desc.max_range, 1)
-        om.insert(R, eye, mt, desc.log_odds_hit, desc.log_odds_miss, osen.points(r), threads=1)
+    for R, eye, mt, pts in frames:
+        om.insert(R, eye, mt, desc.log_odds_hit, desc.log_odds_miss, pts, threads=1)
         n += 1
         if time.perf_counter() - t0 > budget_s:
             break
     dt = time.perf_counter() - t0
     return {"value": om.stats()["visits"] / dt, "unit": UNIT, "cores": 1, "kind": "port",
-            "sample": f"first {n} frames of the timed trajectory, single thread, includes range->point conversion"}
+            "sample": f"insertion of the first {n} frames of the workload's trajectory, single thread"}
+
+
+def load_profile_constants():
+    """Per-launch figures of the dominant kernel from an ncu capture of one headline frame
+    (committed with the profiles): DRAM bytes and warp instructions per voxel visit."""
+    tf = ROOT / "profiles" / "roofline_traffic.json"
+    return json.loads(tf.read_text()) if tf.exists() else {}
 
 
 def run_ours(args, rank, world, local):
@@ -235,12 +280,194 @@ def run_ours(args, rank, world, local):
                    vox_min=scene.vox_min, vox_max=scene.vox_max)
     mdesc = A.map_desc(res=spec.map_res, clamp_min=spec.clamp[0], clamp_max=spec.clamp[1],
                        rounding=N.NM_ROUND_DOWN, initial_leaf_capacity=1 << args.capacity_log2)
-    m = A.Map(ctx, mdesc)
     stream = torch.cuda.current_stream(dev)
     H, W = spec.height, spec.width
-    ranges = torch.zeros(H, W, device=dev)
-    flush = torch.empty(256 << 20, dtype=torch.uint8, device=dev)
     poses = [A.Pose(p, q) for p, q in traj]
+    pm = sensor.params()
+    flush = torch.empty(256 << 20, dtype=torch.uint8, device=dev)
+
+    # the frames: simulated ranges with range noise, as xyz records (outside any timed region)
+    n_frames = min(len(poses), max(20, args.warmup + 1))
+    ranges = torch.zeros(H, W, device=dev)
+    records = []
+    for k in range(n_frames):
+        sim.render_noisy(sensor, poses[k], ranges, spec.noise_coef, spec.drop, 1000003 * (k + 1),
+                         stream=stream)
+        records.append(frame_records(ranges, pm))
+    torch.cuda.synchronize()
+
+    m = A.Map(ctx, mdesc)
+
+    def step(i, ev=None):
+        k = i % n_frames
+        if ev:
+            ev[0].record(stream)
+        m.insert_points(sensor, poses[k], records[k], W, H, 16, flags=N.NM_DEFER_INTEGRATE,
+                        stream=stream)
+        if ev:
+            ev[1].record(stream)
+        m.integrate(stream=stream)
+        if ev:
+            ev[2].record(stream)
+
+    for i in range(args.warmup):
+        step(i)
+        flush.fill_(i & 0xFF)
+    torch.cuda.synchronize()
+    s0 = m.stats()
+    evs = [[torch.cuda.Event(enable_timing=True) for _ in range(3)] for _ in range(args.steps)]
+    clocks = ClockSampler(local)
+    clocks.start()
+    barrier()
+    torch.cuda.synchronize()
+    for k in range(args.steps):
+        step(args.warmup + k, evs[k])
+        flush.fill_(k & 0xFF)
+    torch.cuda.synchronize()
+    barrier()
+    clk = clocks.stop()
+    s1 = m.stats()
+    step_ms = [e[0].elapsed_time(e[2]) for e in evs]
+    trav_ms = [e[0].elapsed_time(e[1]) for e in evs]
+    integ_ms = [e[1].elapsed_time(e[2]) for e in evs]
+    local_time = sum(step_ms) / 1e3
+    visits = s1["visits"] - s0["visits"]
+    rays = s1["rays"] - s0["rays"]
+    uniq = s1["unique_voxels"] - s0["unique_voxels"]
+    leaves = s1["touched_leaves"] - s0["touched_leaves"]
+    assert s1["error_flags"] == 0, "device error during the timed region"
+    t_max = allreduce_max(local_time)
+    visits_all = allreduce_sum(visits)
+    value = visits_all / t_max
+
+    # e2e: the same inserts through the reference-facing call with the records in pinned host
+    # memory (copied inside the call) and a synchronous read-back of the frame status
+    e2e = None
+    if args.e2e_steps > 0:
+        host_recs = [r.cpu().pin_memory() for r in records]
+        m2 = A.Map(ctx, mdesc)
+        for k in range(3):
+            m2.insert_points(sensor, poses[k], host_recs[k], W, H, 16, flags=N.NM_SYNC)
+        e0 = m2.stats()
+        barrier()
+        torch.cuda.synchronize()
+        # each step: L2 flushed first (outside the timed call), then the synchronous insert of
+        # the host records, timed on the host clock from the call to its return
+        dt = 0.0
+        for k in range(args.e2e_steps):
+            i = (3 + k) % n_frames
+            flush.fill_(k & 0xFF)
+            torch.cuda.synchronize()
+            t0 = time.perf_counter()
+            m2.insert_points(sensor, poses[i], host_recs[i], W, H, 16, flags=N.NM_SYNC)
+            dt += time.perf_counter() - t0
+        barrier()
+        e1 = m2.stats()
+        dt = allreduce_max(dt)
+        ev_all = allreduce_sum(e1["visits"] - e0["visits"])
+        e2e = {"value": ev_all / dt, "unit": UNIT, "h2d_bytes_per_step": H * W * 16,
+               "d2h_bytes_per_step": 8, "steps": args.e2e_steps,
+               "ms_per_step": dt * 1e3 / args.e2e_steps,
+               "path": "nm_map_insert_points(host xyz records, step 16, NM_SYNC)",
+               "l2": "flushed before each step, outside the timed call"}
+        m2.close()
+
+    # roofline of the dominant kernel (the traversal): algorithmic bytes per launch =
+    # 12 B per pixel (xyz read) + 1 B per unique labelled voxel + 16 B per touched leaf
+    n_steps = args.steps
+    pix = H * W
+    u_vox = uniq / n_steps
+    u_leaf = leaves / n_steps
+    trav_bytes = 12 * pix + 1 * u_vox + 16 * u_leaf
+    integ_bytes = 9 * u_vox + 64 * u_leaf
+    peaks = json.loads((ROOT / "MEASURED_PEAKS.json").read_text()) if (ROOT / "MEASURED_PEAKS.json").exists() else {}
+    hbm = peaks.get("hbm_gbs", 6650.0)
+    t_trav = statistics.mean(trav_ms) / 1e3
+    t_integ = statistics.mean(integ_ms) / 1e3
+    dominant = "traverse" if t_trav >= t_integ else "integrate"
+    prof = load_profile_constants().get("k_" + dominant, {})
+    if dominant == "traverse":
+        ach = trav_bytes / t_trav / 1e9
+    else:
+        ach = integ_bytes / t_integ / 1e9
+    per_visit = visits / n_steps
+    roof = {"bound": "hbm", "kernel": f"k_{dominant}", "achieved": ach, "peak": hbm,
+            "unit": "GB/s", "frac": ach / hbm,
+            "peak_source": "measured (MEASURED_PEAKS.json hbm_gbs)" if peaks else "fallback (6650 GB/s)",
+            "algorithmic_bytes_per_launch": trav_bytes if dominant == "traverse" else integ_bytes,
+            "algorithmic_bytes": ("12 B per pixel (xyz record read) + 1 B per unique labelled voxel "
+                                  "+ 16 B per touched leaf" if dominant == "traverse" else
+                                  "9 B per unique voxel + 64 B per touched leaf")}
+    traffic = None
+    if prof.get("dram_bytes_per_visit"):
+        traffic = prof["dram_bytes_per_visit"] * per_visit
+        roof["traffic_source"] = ("ncu dram__bytes_read.sum + dram__bytes_write.sum of one launch on "
+                                  "a headline frame, scaled to this run's visits per launch")
+    roof["traffic"] = traffic
+    # issue roofline: the walk is bound by instruction issue, not by DRAM
+    inst = prof.get("warp_inst_per_visit")
+    if dominant == "traverse" and inst and clk.get("sm_mhz"):
+        issue_peak = 148 * 4 * clk["sm_mhz"] * 1e6  # warp instructions per second
+        issued = inst * per_visit / t_trav
+        roof["issue"] = {"warp_inst_per_visit": inst, "visits_per_s": per_visit / t_trav,
+                         "achieved_warp_inst_per_s": issued, "peak_warp_inst_per_s": issue_peak,
+                         "frac": issued / issue_peak,
+                         "source": "warp instructions per visit from an ncu capture of one launch; "
+                                   "peak = 148 SMs x 4 schedulers x median SM clock"}
+    line = {
+        "metric": METRIC, "value": value, "unit": UNIT, "n_gpus": world, "steps": args.steps,
+        "warmup": args.warmup, "ms_per_step": t_max * 1e3 / args.steps, "higher_is_better": True,
+        "scaling": "weak", "vs_baseline": None, "dtype": "f64", "data": "synthetic",
+        "config": workload_config(spec),
+        "frames_per_s": world * args.steps / t_max,
+        "rays_per_s": allreduce_sum(rays) / t_max,
+        "unique_voxel_updates_per_s": allreduce_sum(uniq) / t_max,
+        "per_frame": {"visits": per_visit, "rays": rays / n_steps, "unique_voxels": u_vox,
+                      "touched_leaves": u_leaf},
+        "stage_ms": {"traverse": statistics.mean(trav_ms), "integrate": statistics.mean(integ_ms)},
+        "gpu_launches": args.steps * 2,
+        "roofline": roof,
+        "e2e": e2e,
+        "clocks": clk,
+    }
+    m.close()
+    line["sim_frame"] = run_sim_frame_section(ctx, sensor, sim, mdesc, spec, poses, stream, flush,
+                                              args.warmup)
+    if args.extras:
+        line["plain_small"] = run_plain_small_section(local, args.warmup,
+                                                      cpu=(rank == 0 and world == 1 and args.cpu_baseline_s > 0))
+        line["voxel_filter"] = run_filter_section(ctx, sensor, sim, mdesc, spec, poses, ranges,
+                                                  stream, args.warmup)
+        mdepth = A.Map(ctx, mdesc)
+        for k in range(n_frames):
+            mdepth.insert_points(sensor, poses[k], records[k], W, H, 16, stream=stream)
+        line["expected_depth"] = run_depth_section(ctx, mdepth, sensor, sim, spec, poses, stream, hbm)
+        mdepth.close()
+    if args.batched_ticks > args.warmup:
+        line["batched"] = run_batched(args, rank, world, local, args.batched_ticks)
+    if args.large:
+        line["large"] = run_large_section(local)
+    if args.cave:
+        line["cave"] = run_cave_section(local, cpu=(rank == 0 and world == 1 and args.cpu_baseline_s > 0))
+    if rank == 0 and world == 1 and args.cpu_baseline_s > 0:
+        line["cpu_baseline"] = cpu_baseline(spec, scene, traj, desc, args.cpu_baseline_s)
+    sim.close()
+    sensor.close()
+    ctx.close()
+    return line
+
+
+def run_sim_frame_section(ctx, sensor, sim, mdesc, spec, poses, stream, flush, warmup, frames=20):
+    """The whole simulated frame of the workload per step: sim render with range noise (one
+    launch), traversal and labels, integration; device-timed with CUDA events, L2 flushed
+    between steps outside the events."""
+    import torch
+
+    from nanomap_b200 import _native as N
+    from nanomap_b200 import api as A
+    H, W = spec.height, spec.width
+    ranges = torch.zeros(H, W, device=flush.device)
+    m = A.Map(ctx, mdesc)
 
     def step(i, ev=None):
         pose = poses[i % len(poses)]
@@ -257,151 +484,104 @@ def run_ours(args, rank, world, local):
         if ev:
             ev[3].record(stream)
 
-    for i in range(args.warmup):
+    for i in range(warmup):
         step(i)
         flush.fill_(i & 0xFF)
     torch.cuda.synchronize()
     s0 = m.stats()
-    evs = [[torch.cuda.Event(enable_timing=True) for _ in range(4)] for _ in range(args.steps)]
-    clocks = ClockSampler(local)
-    clocks.start()
-    barrier()
-    torch.cuda.synchronize()
-    t_start = torch.cuda.Event(enable_timing=True)
-    t_end = torch.cuda.Event(enable_timing=True)
-    t_start.record(stream)
-    for k in range(args.steps):
-        step(args.warmup + k, evs[k])
+    evs = [[torch.cuda.Event(enable_timing=True) for _ in range(4)] for _ in range(frames)]
+    for k in range(frames):
+        step(warmup + k, evs[k])
         flush.fill_(k & 0xFF)
-    t_end.record(stream)
     torch.cuda.synchronize()
-    barrier()
-    clk = clocks.stop()
     s1 = m.stats()
-    step_ms = [e[0].elapsed_time(e[3]) for e in evs]
-    trav_ms = [e[1].elapsed_time(e[2]) for e in evs]
-    integ_ms = [e[2].elapsed_time(e[3]) for e in evs]
-    sim_ms = [e[0].elapsed_time(e[1]) for e in evs]
-    local_time = sum(step_ms) / 1e3
-    region_ms = t_start.elapsed_time(t_end)
-    visits = s1["visits"] - s0["visits"]
-    rays = s1["rays"] - s0["rays"]
-    uniq = s1["unique_voxels"] - s0["unique_voxels"]
-    leaves = s1["touched_leaves"] - s0["touched_leaves"]
-    assert s1["error_flags"] == 0, "device error during the timed region"
-    t_max = allreduce_max(local_time)
-    visits_all = allreduce_sum(visits)
-    value = visits_all / t_max
-
-    # e2e: reference-facing insert of pinned host xyz records (step 16 bytes)
-    e2e = None
-    if args.e2e_steps > 0:
-        frames_xyz = []
-        pm = sensor.params()
-        u = (np.arange(W, dtype=np.float32) * pm[4])[None, :]
-        v = (np.arange(H, dtype=np.float32) * pm[5])[:, None]
-        dx = u * pm[2] - pm[0]
-        dy = v * pm[3] - pm[1]
-        nrm = np.sqrt(dx * dx + dy * dy + 1.0).astype(np.float32)
-        for k in range(min(args.e2e_steps, 20)):
-            step(k)
-            r = ranges.cpu().numpy()
-            sc = r / nrm
-            rec = torch.zeros(H * W, 4, dtype=torch.float32).pin_memory()
-            xyz = np.stack([dx * sc, np.broadcast_to(dy, (H, W)) * sc, sc], axis=-1).reshape(-1, 3)
-            xyz[(r <= 0).reshape(-1)] = np.nan
-            rec[:, :3] = torch.from_numpy(xyz.astype(np.float32))
-            frames_xyz.append((poses[k % len(poses)], rec))
-        m2 = A.Map(ctx, mdesc)
-        for k in range(3):
-            pose, rec = frames_xyz[k % len(frames_xyz)]
-            m2.insert_points(sensor, pose, rec, W, H, 16, flags=N.NM_SYNC)
-        e0 = m2.stats()
-        barrier()
-        torch.cuda.synchronize()
-        # each step: L2 flushed first (outside the timed call), then the synchronous insert of
-        # the host records, timed on the host clock from the call to its return
-        dt = 0.0
-        for k in range(args.e2e_steps):
-            pose, rec = frames_xyz[k % len(frames_xyz)]
-            flush.fill_(k & 0xFF)
-            torch.cuda.synchronize()
-            t0 = time.perf_counter()
-            m2.insert_points(sensor, pose, rec, W, H, 16, flags=N.NM_SYNC)
-            dt += time.perf_counter() - t0
-        barrier()
-        e1 = m2.stats()
-        dt = allreduce_max(dt)
-        ev_all = allreduce_sum(e1["visits"] - e0["visits"])
-        e2e = {"value": ev_all / dt, "unit": UNIT, "h2d_bytes_per_step": H * W * 16,
-               "d2h_bytes_per_step": 8, "steps": args.e2e_steps,
-               "path": "nm_map_insert_points(host xyz records, step 16, NM_SYNC)",
-               "l2": "flushed before each step, outside the timed call"}
-        m2.close()
-
-    # roofline of the dominant kernel (traversal): algorithmic bytes per launch =
-    # 4 B per pixel (range read) + 1 B per unique labelled voxel + 16 B per touched leaf
-    n_steps = args.steps
-    pix = H * W
-    u_vox = uniq / n_steps
-    u_leaf = leaves / n_steps
-    trav_bytes = 4 * pix + 1 * u_vox + 16 * u_leaf
-    integ_bytes = 9 * u_vox + 64 * u_leaf
-    peaks = json.loads((ROOT / "MEASURED_PEAKS.json").read_text()) if (ROOT / "MEASURED_PEAKS.json").exists() else {}
-    hbm = peaks.get("hbm_gbs", 6650.0)
-    t_trav = statistics.mean(trav_ms) / 1e3
-    t_integ = statistics.mean(integ_ms) / 1e3
-    dominant = "traverse" if t_trav >= t_integ else "integrate"
-    traffic = None
-    tf = ROOT / "profiles" / "roofline_traffic.json"
-    if tf.exists():
-        traffic = json.loads(tf.read_text()).get("k_" + dominant, {}).get("dram_bytes_per_launch")
-    if dominant == "traverse":
-        ach = trav_bytes / t_trav / 1e9
-    else:
-        ach = integ_bytes / t_integ / 1e9
-    line = {
-        "metric": METRIC, "value": value, "unit": UNIT, "n_gpus": world, "steps": args.steps,
-        "warmup": args.warmup, "ms_per_step": t_max * 1e3 / args.steps, "higher_is_better": True,
-        "scaling": "weak", "vs_baseline": None, "dtype": "f64", "data": "synthetic",
-        "config": workload_config(spec),
-        "frames_per_s": world * args.steps / t_max,
-        "rays_per_s": allreduce_sum(rays) / t_max,
-        "unique_voxel_updates_per_s": allreduce_sum(uniq) / t_max,
-        "per_frame": {"visits": visits / n_steps, "rays": rays / n_steps, "unique_voxels": u_vox,
-                      "touched_leaves": u_leaf},
-        "stage_ms": {"sim_render+noise": statistics.mean(sim_ms), "traverse": statistics.mean(trav_ms),
-                     "integrate": statistics.mean(integ_ms), "timed_region_incl_flush": region_ms / args.steps},
-        "gpu_launches": args.steps * 3,
-        "roofline": {"bound": "hbm", "kernel": f"k_{dominant}", "achieved": ach, "peak": hbm,
-                     "unit": "GB/s", "frac": ach / hbm, "traffic": traffic,
-                     "peak_source": "measured (MEASURED_PEAKS.json hbm_gbs)" if peaks else "fallback",
-                     "traffic_source": "ncu dram bytes of one headline frame (profiles/k_traverse_sim_headline.md)",
-                     "algorithmic_bytes_per_launch": trav_bytes if dominant == "traverse" else integ_bytes},
-        "e2e": e2e,
-        "clocks": clk,
+    tot = [e[0].elapsed_time(e[3]) for e in evs]
+    out = {
+        "workload": "sim render + range noise, traversal + labels, integration of one headline frame per step",
+        "frames": frames, "ms_per_frame": statistics.mean(tot),
+        "voxel_updates_per_s": (s1["visits"] - s0["visits"]) / (sum(tot) / 1e3),
+        "frames_per_s": frames / (sum(tot) / 1e3),
+        "stage_ms": {"sim_render+noise": statistics.mean(e[0].elapsed_time(e[1]) for e in evs),
+                     "traverse": statistics.mean(e[1].elapsed_time(e[2]) for e in evs),
+                     "integrate": statistics.mean(e[2].elapsed_time(e[3]) for e in evs)},
+        "sim_rays_per_s": H * W / (statistics.mean(e[0].elapsed_time(e[1]) for e in evs) / 1e3),
+        "gpu_launches_per_frame": 3,
     }
-    if args.extras:
-        line["voxel_filter"] = run_filter_section(ctx, sensor, sim, mdesc, spec, poses, ranges,
-                                                  stream, args.warmup)
-        line["expected_depth"] = run_depth_section(ctx, m, sensor, sim, spec, poses, stream, hbm)
-    if args.batched_ticks > args.warmup:
-        line["batched"] = run_batched(args, rank, world, local, args.batched_ticks)
-    if args.large:
-        line["large"] = run_large_section(local)
-    if args.cave:
-        line["cave"] = run_cave_section(local, cpu=(rank == 0 and world == 1 and args.cpu_baseline_s > 0))
-    if rank == 0 and world == 1 and args.cpu_baseline_s > 0:
-        frames_host = []
-        for k in range(30):
-            step(k)
-            frames_host.append((poses[k % len(poses)], ranges.cpu().numpy().copy()))
-        line["cpu_baseline"] = cpu_baseline(spec, desc, frames_host, args.cpu_baseline_s)
     m.close()
-    sim.close()
+    return out
+
+
+def run_plain_small_section(local, warmup, cpu=True, frames=10):
+    """The small plain-mapping workload (20 x 20 x 5 m, 200 boxes, 320x240 87 x 58 deg camera at
+    5 m, mapping at 0.1 m): exact FP64 ray-box ranges + N(0, 0.01 m), inserted as range images
+    and integrated; device-timed, L2 flushed between frames; the oracle's insertion of the same
+    frames on one core and on every host core."""
+    import torch
+
+    from nanomap_b200 import _native as N
+    from nanomap_b200 import api as A
+    from nanomap_b200 import scenes as S
+    spec = S.SCENES["plain_small"]
+    scene = S.make_scene(spec, 1)
+    traj = S.trajectory(scene, frames, seed=7)
+    ctx = A.Context(local)
+    desc = A.sensor_desc(**S.sensor_desc_kwargs(spec))
+    sensor = A.Sensor(ctx, desc)
+    pm = sensor.params()
+    rng = np.random.default_rng(17)
+    host = []
+    for pos, q in traj:
+        r = S.analytic_box_ranges(scene, pm, spec.width, spec.height, spec.max_range, pos, q)
+        r = np.where(r > 0, r + rng.normal(0.0, spec.noise_sigma, r.shape), 0.0).astype(np.float32)
+        r[~(r > 0)] = 0.0
+        host.append((A.Pose(pos, q), r))
+    dev_r = [torch.from_numpy(r).cuda() for _, r in host]
+    m = A.Map(ctx, A.map_desc(res=spec.map_res, clamp_min=spec.clamp[0], clamp_max=spec.clamp[1],
+                              rounding=N.NM_ROUND_DOWN))
+    stream = torch.cuda.current_stream()
+    flush = torch.empty(256 << 20, dtype=torch.uint8, device="cuda")
+    for k in range(warmup):
+        m.insert_ranges(sensor, host[k % frames][0], dev_r[k % frames], stream=stream)
+    torch.cuda.synchronize()
+    s0 = m.stats()
+    evs = []
+    for k in range(frames):
+        flush.fill_(k & 255)
+        e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+        e0.record(stream)
+        m.insert_ranges(sensor, host[k][0], dev_r[k], stream=stream)
+        e1.record(stream)
+        evs.append((e0, e1))
+    torch.cuda.synchronize()
+    s1 = m.stats()
+    ms = statistics.mean(a.elapsed_time(b) for a, b in evs)
+    visits = (s1["visits"] - s0["visits"]) / frames
+    out = {"workload": ("20x20x5 m, 200 boxes, 320x240 87x58 deg camera at 5 m, 0.1 m voxels; exact "
+                        "ray-box ranges + N(0, 0.01 m); range-image insert + integration per frame"),
+           "frames": frames, "ms_per_frame": ms, "voxel_updates_per_s": visits / (ms / 1e3),
+           "frames_per_s": 1e3 / ms, "visits_per_frame": visits,
+           "rays_per_frame": (s1["rays"] - s0["rays"]) / frames, "gpu_launches_per_frame": 2}
+    if cpu:
+        from oracle import oracle as O
+        osen = O.Sensor.from_desc(desc)
+        for threads in (1, os.cpu_count() or 1):
+            om = O.Map(spec.map_res, clamp_min=spec.clamp[0], clamp_max=spec.clamp[1], rounding=1)
+            pts = []
+            for pose, r in host:
+                R = O.rotation(pose.orientation, list(desc.frame_transform))
+                eye, mt = O.frame_setup(pose.position, spec.map_res, desc.max_range, 1)
+                pts.append((R, eye, mt, osen.points(r)))
+            t0 = time.perf_counter()
+            for R, eye, mt, p in pts:
+                om.insert(R, eye, mt, desc.log_odds_hit, desc.log_odds_miss, p, threads=threads)
+            dt = time.perf_counter() - t0
+            out[f"cpu_oracle_{'1_core' if threads == 1 else 'all_cores'}"] = {
+                "voxel_updates_per_s": om.stats()["visits"] / dt, "ms_per_frame": dt * 1e3 / frames,
+                "cores": threads, "kind": "port"}
+    m.close()
     sensor.close()
     ctx.close()
-    return line
+    return out
 
 
 def run_filter_section(ctx, sensor, sim, mdesc, spec, poses, ranges, stream, warmup, frames=20):
@@ -748,15 +928,36 @@ def run_cave_section(local, cpu=True, reps=3):
     return out
 
 
-def batched_agents(spec_small):
-    """Sensor mix of the batched tick: (hres, vres, range m, type) per agent."""
-    mix = [(320, 240, 5.0, 0)] * 6 + [(640, 480, 10.0, 0)] * 6 + [(1280, 720, 8.0, 0)] * 3 + [(1024, 64, 20.0, 1)]
-    return mix
+def _leaf_dict(origins, *arrays):
+    return {tuple(int(v) for v in o): tuple(a[i] for a in arrays) for i, o in enumerate(origins)}
+
+
+def maps_equal(a, b) -> bool:
+    """Two map exports hold the same log-odds (bit for bit) and active bits on every leaf (a
+    leaf missing from one export counts as all zero)."""
+    A, B = _leaf_dict(*a), _leaf_dict(*b)
+    zero = (np.zeros(512, np.float32), np.zeros(16, np.uint32))
+    for k in set(A) | set(B):
+        va, aa = A.get(k, zero)
+        vb, ab = B.get(k, zero)
+        if not (np.array_equal(va.view(np.uint32), vb.view(np.uint32)) and np.array_equal(aa, ab)):
+            return False
+    return True
+
+
+def labels_equal(a, b) -> bool:
+    A, B = _leaf_dict(*a), _leaf_dict(*b)
+    zero = (np.zeros(32, np.uint32),)
+    return all(np.array_equal(A.get(k, zero)[0], B.get(k, zero)[0]) for k in set(A) | set(B))
 
 
 def run_batched(args, rank, world, local, ticks):
-    """16-agent tick (config-1 world at 0.05 m): one graph-replayed, autotuned tick per step,
-    against the same agents run one frame per launch (render + insert per agent)."""
+    """16-agent tick in the 20 x 20 x 5 m world at 0.05 m: one graph-replayed, autotuned tick
+    plan per tick (render + labels + integration of every agent) against the same agents run
+    one frame at a time (render + insert per agent); after the timed ticks, the two maps are
+    compared, and one more tick left unintegrated is compared agent by agent with solo inserts."""
+    import tempfile
+
     import torch
 
     from nanomap_b200 import _native as N
@@ -766,36 +967,38 @@ def run_batched(args, rank, world, local, ticks):
     dev = torch.device("cuda", local)
     spec = S.SCENES["plain_small"]
     scene = S.make_scene(spec, 1)
-    res = 0.05
+    res = S.TICK_RES
     ctx = A.Context(local)
-    sim = A.SimMap(ctx, res, boxes=scene.boxes, cylinders=scene.cylinders, vox_min=(0, 0, 0),
-                   vox_max=tuple(int(math.ceil(x / res)) for x in spec.size))
+    lo, hi = S.tick_sim_box(spec)
+    sim = A.SimMap(ctx, res, boxes=scene.boxes, cylinders=scene.cylinders, vox_min=lo, vox_max=hi)
     sensors, bufs, trajs = [], [], []
-    for a, (w, h, rng_m, typ) in enumerate(batched_agents(spec)):
-        if typ == 1:
-            d = A.sensor_desc(type=1, hres=w, vres=h, hfov_deg=360.0, vfov_deg=30.0, max_range=rng_m,
-                              explicit_log_odds=1, log_odds_hit=0.85, log_odds_miss=-0.4,
-                              frame_transform=S.OPTICAL_TO_BODY)
-        else:
-            d = A.sensor_desc(type=0, hres=w, vres=h, hfov_deg=87.0, vfov_deg=58.0, max_range=rng_m,
-                              explicit_log_odds=1, log_odds_hit=0.85, log_odds_miss=-0.4,
-                              frame_transform=S.OPTICAL_TO_BODY)
+    for a, agent in enumerate(S.TICK_AGENTS):
+        d = A.sensor_desc(**S.tick_agent_desc_kwargs(agent))
         sensors.append(A.Sensor(ctx, d))
-        bufs.append(torch.zeros(h, w, device=dev))
-        trajs.append([A.Pose(p, q) for p, q in S.trajectory(scene, ticks, seed=101 + 37 * a + 7919 * rank)])
+        bufs.append(torch.zeros(d.vres, d.hres, device=dev))
+        trajs.append([A.Pose(p, q) for p, q in S.trajectory(scene, ticks + 1, seed=101 + 37 * a + 7919 * rank)])
     n = len(sensors)
     rays_per_tick = sum(s.desc.hres * s.desc.vres for s in sensors)
     cap = 1 << 21
     stream = torch.cuda.current_stream(dev)
     flush = torch.empty(256 << 20, dtype=torch.uint8, device=dev)
+    timed = ticks - args.warmup
 
-    # batched: one tick plan (graph), autotuned on a scratch map
+    # batched: one tick plan (graph), autotuned on a scratch map; the second autotune call is
+    # served from the cache file the first one wrote
     mb = A.Map(ctx, A.map_desc(res=res, clamp_min=-2.0, clamp_max=3.5, max_agents=n,
                                rounding=N.NM_ROUND_DOWN, initial_leaf_capacity=cap))
     plan = A.TickPlan(mb, [(sensors[a], bufs[a], a) for a in range(n)], sim=sim)
     for a in range(n):
         plan.set_pose(a, trajs[a][0])
-    best, best_us = plan.autotune(None)
+    with tempfile.TemporaryDirectory() as td:
+        cache = str(Path(td) / "tick_tune.txt")
+        t0 = time.perf_counter()
+        best, best_us = plan.autotune(cache)
+        tune_s = time.perf_counter() - t0
+        t0 = time.perf_counter()
+        best2, _ = plan.autotune(cache)
+        cached_s = time.perf_counter() - t0
     for t in range(args.warmup):
         for a in range(n):
             plan.set_pose(a, trajs[a][t])
@@ -803,7 +1006,7 @@ def run_batched(args, rank, world, local, ticks):
     torch.cuda.synchronize()
     b0 = mb.stats()
     evs = []
-    for t in range(ticks - args.warmup):
+    for t in range(timed):
         e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
         flush.fill_(t & 255)
         for a in range(n):
@@ -815,7 +1018,6 @@ def run_batched(args, rank, world, local, ticks):
     torch.cuda.synchronize()
     b1 = mb.stats()
     tb = sum(e0.elapsed_time(e1) for e0, e1 in evs) / 1e3
-    nb = len(evs)
     vb = b1["visits"] - b0["visits"]
 
     # plain: the same frames, one render + one insert launch pair per agent frame
@@ -828,7 +1030,7 @@ def run_batched(args, rank, world, local, ticks):
     torch.cuda.synchronize()
     p0 = mp.stats()
     evp = []
-    for t in range(ticks - args.warmup):
+    for t in range(timed):
         e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
         flush.fill_(t & 255)
         e0.record(stream)
@@ -841,12 +1043,55 @@ def run_batched(args, rank, world, local, ticks):
     p1 = mp.stats()
     tp = sum(e0.elapsed_time(e1) for e0, e1 in evp) / 1e3
     vp = p1["visits"] - p0["visits"]
+    same_map = maps_equal(mb.export(), mp.export())
+
+    # one more tick, left unintegrated: every agent's labels against its solo insert
+    for a in range(n):
+        plan.set_pose(a, trajs[a][ticks])
+    plan.run(flags=N.NM_DEFER_INTEGRATE, stream=stream)
+    torch.cuda.synchronize()
+    solo = A.Map(ctx, A.map_desc(res=res, rounding=N.NM_ROUND_DOWN, initial_leaf_capacity=1 << 20))
+    agents_equal = 0
+    for a in range(n):
+        solo.reset()
+        solo.insert_ranges(sensors[a], trajs[a][ticks], bufs[a], flags=N.NM_DEFER_INTEGRATE)
+        agents_equal += int(labels_equal(mb.export_labels(a), solo.export_labels(0)))
+    mb.integrate()
+    solo.close()
+
+    # plain frames by sensor type (a separate pass with events around every agent's frame)
+    kinds = {}
+    mk = A.Map(ctx, A.map_desc(res=res, rounding=N.NM_ROUND_DOWN, initial_leaf_capacity=cap))
+    per = [[] for _ in range(n)]
+    for t in range(min(10, timed)):
+        flush.fill_(t & 255)
+        row = []
+        for a in range(n):
+            e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+            e0.record(stream)
+            sim.render(sensors[a], trajs[a][args.warmup + t], bufs[a], stream=stream)
+            mk.insert_ranges(sensors[a], trajs[a][args.warmup + t], bufs[a], stream=stream)
+            e1.record(stream)
+            row.append((e0, e1))
+        torch.cuda.synchronize()
+        for a, (e0, e1) in enumerate(row):
+            per[a].append(e0.elapsed_time(e1))
+    for a, agent in enumerate(S.TICK_AGENTS):
+        typ, w, h, _, _, rng = agent
+        key = f"{w}x{h}{' spinning' if typ == 1 else ''} at {rng:g} m"
+        k = kinds.setdefault(key, {"agents": 0, "ms_per_frame": 0.0,
+                                   "tiles_per_frame": ((w + 15) // 16) * ((h + 15) // 16)})
+        k["agents"] += 1
+        k["ms_per_frame"] += statistics.mean(per[a])
+    for k in kinds.values():
+        k["ms_per_frame"] /= k["agents"]
+    mk.close()
 
     # plain with a host round trip per frame (the reference's per-frame synchronous pipeline)
     mq = A.Map(ctx, A.map_desc(res=res, clamp_min=-2.0, clamp_max=3.5, rounding=N.NM_ROUND_DOWN,
                                initial_leaf_capacity=cap))
     q0 = mq.stats()
-    nq = min(5, ticks - args.warmup)
+    nq = min(5, timed)
     torch.cuda.synchronize()
     t0 = time.perf_counter()
     for t in range(nq):
@@ -861,18 +1106,24 @@ def run_batched(args, rank, world, local, ticks):
                      "6x640x480@10 m, 3x1280x720@8 m (87x58 deg), 1x1024x64 spinning@20 m; sim render "
                      "+ labels + integration per tick; L2 flushed between ticks"),
         "rays_per_tick": rays_per_tick,
-        "ticks": nb,
+        "ticks": timed, "warmup_ticks": args.warmup,
         "batched_voxel_updates_per_s": vb / tb,
-        "batched_ms_per_tick": tb * 1e3 / nb,
+        "batched_ms_per_tick": tb * 1e3 / timed,
         "plain_voxel_updates_per_s": vp / tp,
-        "plain_ms_per_tick": tp * 1e3 / nb,
+        "plain_ms_per_tick": tp * 1e3 / timed,
         "plain_synchronous_voxel_updates_per_s": vq / tq,
         "speedup_vs_plain": (vb / tb) / (vp / tp),
         "speedup_vs_plain_synchronous": (vb / tb) / (vq / tq),
-        "autotuned_launch": {"tile": [best[0], best[1]], "leaf_table_entries": best[2], "tick_us": best_us},
-        "maps_equal_visits": vb == vp,
+        "plain_by_sensor": kinds,
+        "autotuned_launch": {"tile": [best[0], best[1]], "leaf_table_entries": best[2],
+                             "rays_per_thread": best[0] * best[1] // min(256, best[0] * best[1]),
+                             "tick_us": best_us, "tune_s": tune_s,
+                             "cache_hit_same_choice": best2 == best, "cached_call_s": cached_s},
+        "maps_equal": same_map and vb == vp,
+        "labels_equal_solo": f"{agents_equal}/{n} agents",
         "table_growths": {"batched": b1["grow_count"], "plain": p1["grow_count"],
                           "plain_synchronous": q1["grow_count"]},
+        "error_flags": b1["error_flags"] | p1["error_flags"],
         "gpu_launches_per_tick": 4,
     }
     plan.close()
@@ -889,8 +1140,8 @@ def main():
     ap.add_argument("--impl", choices=["ours", "reference"], default="ours")
     ap.add_argument("--e2e-steps", type=int, default=30)
     ap.add_argument("--cpu-baseline-s", type=float, default=12.0)
-    ap.add_argument("--batched-ticks", type=int, default=40,
-                    help="ticks of the 16-agent batched comparison (0 = skip)")
+    ap.add_argument("--batched-ticks", type=int, default=200,
+                    help="ticks of the 16-agent batched comparison, warm-up included (0 = skip)")
     ap.add_argument("--large", type=int, default=1,
                     help="1 = also measure the large fine-resolution workload (0.02 m, 1280x720 at 15 m)")
     ap.add_argument("--cave", type=int, default=1,
