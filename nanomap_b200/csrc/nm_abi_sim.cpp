@@ -38,21 +38,27 @@ int finish_build(nm_context ctx, nm::SimBuild& b, nm_simmap sm, cudaStream_t s) 
   uint32_t* d_count = nullptr;
   int32_t* d_bbox = nullptr;
   unsigned long long* d_nvox = nullptr;
+  const long long bprod = (long long)v.bdim[0] * v.bdim[1] * v.bdim[2];
   NM_CUDA(cudaMalloc((void**)&d_count, 4));
   NM_CUDA(cudaMalloc((void**)&d_bbox, 24));
   NM_CUDA(cudaMalloc((void**)&d_nvox, 8));
+  NM_CUDA(cudaMalloc((void**)&v.brick_index, (size_t)bprod * 4));
+  NM_CUDA(cudaMemsetAsync(v.brick_index, 0, (size_t)bprod * 4, s));
   NM_CUDA(cudaMemsetAsync(d_count, 0, 4, s));
   NM_CUDA(nm::launch_compact(b, v, d_count, 0, d_bbox, d_nvox, s));
   uint32_t nleaves = 0;
+  std::vector<int32_t> bricks((size_t)bprod);
   NM_CUDA(cudaMemcpyAsync(&nleaves, d_count, 4, cudaMemcpyDeviceToHost, s));
+  NM_CUDA(cudaMemcpyAsync(bricks.data(), v.brick_index, (size_t)bprod * 4, cudaMemcpyDeviceToHost, s));
   NM_CUDA(cudaStreamSynchronize(s));
-  const long long lprod = (long long)b.ldim[0] * b.ldim[1] * b.ldim[2];
-  const long long bprod = (long long)v.bdim[0] * v.bdim[1] * v.bdim[2];
-  NM_CUDA(cudaMalloc((void**)&v.leaf_index, (size_t)lprod * 4));
+  // number the flagged bricks in brick-box order; the others are empty (-1)
+  int32_t nblocks = 0;
+  for (int32_t& x : bricks) x = x ? nblocks++ : -1;
+  NM_CUDA(cudaMemcpyAsync(v.brick_index, bricks.data(), (size_t)bprod * 4, cudaMemcpyHostToDevice, s));
+  NM_CUDA(cudaMalloc((void**)&v.brick_leaves, (size_t)std::max(nblocks, 1) * 512 * 4));
+  NM_CUDA(nm::launch_fill_i32(v.brick_leaves, (long long)std::max(nblocks, 1) * 512, -1, s));
   NM_CUDA(cudaMalloc((void**)&v.leaf_words, (size_t)std::max<uint32_t>(nleaves, 1) * 64));
-  NM_CUDA(cudaMalloc((void**)&v.brick_bits, (size_t)((bprod + 31) / 32) * 4));
-  NM_CUDA(nm::launch_fill_i32(v.leaf_index, lprod, -1, s));
-  NM_CUDA(cudaMemsetAsync(v.brick_bits, 0, (size_t)((bprod + 31) / 32) * 4, s));
+  sm->bricks = (uint64_t)nblocks;
   const int32_t init[6] = {INT_MAX, INT_MAX, INT_MAX, INT_MIN, INT_MIN, INT_MIN};
   NM_CUDA(cudaMemcpyAsync(d_bbox, init, 24, cudaMemcpyHostToDevice, s));
   NM_CUDA(cudaMemsetAsync(d_nvox, 0, 8, s));
@@ -154,9 +160,9 @@ void release(nm_simmap sm) {
   nm_context c = sm->ctx;
   cudaSetDevice(c->device);
   cudaDeviceSynchronize();
-  cudaFree(sm->view.leaf_index);
+  cudaFree(sm->view.brick_index);
+  cudaFree(sm->view.brick_leaves);
   cudaFree(sm->view.leaf_words);
-  cudaFree(sm->view.brick_bits);
   cudaFree(sm->cast_staging);
   delete sm;
   release(c);
@@ -331,26 +337,32 @@ int nm_simmap_export(nm_simmap sm, int32_t* origins, uint32_t* words, uint64_t m
   NM_CUDA(cudaSetDevice(sm->ctx->device));
   *n = sm->leaves;
   const nm::SimMapView& v = sm->view;
-  const long long lprod = (long long)v.ldim[0] * v.ldim[1] * v.ldim[2];
-  std::vector<int32_t> index((size_t)lprod);
-  NM_CUDA(cudaMemcpy(index.data(), v.leaf_index, (size_t)lprod * 4, cudaMemcpyDeviceToHost));
+  const long long bprod = (long long)v.bdim[0] * v.bdim[1] * v.bdim[2];
+  std::vector<int32_t> bricks((size_t)bprod);
+  std::vector<int32_t> blocks((size_t)std::max<uint64_t>(sm->bricks, 1) * 512);
+  NM_CUDA(cudaMemcpy(bricks.data(), v.brick_index, (size_t)bprod * 4, cudaMemcpyDeviceToHost));
+  NM_CUDA(cudaMemcpy(blocks.data(), v.brick_leaves, blocks.size() * 4, cudaMemcpyDeviceToHost));
   std::vector<uint32_t> all((size_t)sm->leaves * 16);
   if (sm->leaves)
     NM_CUDA(cudaMemcpy(all.data(), v.leaf_words, all.size() * 4, cudaMemcpyDeviceToHost));
   uint64_t o = 0;
-  for (long long pos = 0; pos < lprod && o < max_leaves; ++pos) {
-    const int32_t li = index[(size_t)pos];
-    if (li < 0) continue;
-    const int lz = (int)(pos % v.ldim[2]);
-    const int ly = (int)((pos / v.ldim[2]) % v.ldim[1]);
-    const int lx = (int)(pos / ((long long)v.ldim[2] * v.ldim[1]));
-    if (origins) {
-      origins[3 * o] = (v.llo[0] + lx) * 8;
-      origins[3 * o + 1] = (v.llo[1] + ly) * 8;
-      origins[3 * o + 2] = (v.llo[2] + lz) * 8;
+  for (long long bpos = 0; bpos < bprod && o < max_leaves; ++bpos) {
+    const int32_t blk = bricks[(size_t)bpos];
+    if (blk < 0) continue;
+    const int bz = (int)(bpos % v.bdim[2]) + v.blo[2];
+    const int by = (int)((bpos / v.bdim[2]) % v.bdim[1]) + v.blo[1];
+    const int bx = (int)(bpos / ((long long)v.bdim[2] * v.bdim[1])) + v.blo[0];
+    for (int e = 0; e < 512 && o < max_leaves; ++e) {
+      const int32_t li = blocks[(size_t)blk * 512 + e];
+      if (li < 0) continue;
+      if (origins) {
+        origins[3 * o] = (bx * 8 + (e >> 6)) * 8;
+        origins[3 * o + 1] = (by * 8 + ((e >> 3) & 7)) * 8;
+        origins[3 * o + 2] = (bz * 8 + (e & 7)) * 8;
+      }
+      if (words) std::memcpy(words + 16 * o, all.data() + (size_t)li * 16, 64);
+      ++o;
     }
-    if (words) std::memcpy(words + 16 * o, all.data() + (size_t)li * 16, 64);
-    ++o;
   }
   return NM_OK;
 }

@@ -98,6 +98,7 @@ struct nm_simmap_s {
   int32_t bbox[6] = {0, 0, 0, -1, -1, -1};
   uint64_t active_voxels = 0;
   uint64_t leaves = 0;
+  uint64_t bricks = 0;  // non-empty 64^3-voxel bricks (blocks of 512 leaf entries)
   float* cast_staging = nullptr;  // host-side ray casts: origins, directions, distances
   size_t cast_staging_bytes = 0;
 };

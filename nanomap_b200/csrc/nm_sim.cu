@@ -3,9 +3,9 @@
 // Replaces the NanoVDB sim grid upload (SimHandler.cpp:22-23) and generateCloud /
 // viewSimKernel / getActiveCrossing (generateCloud.cu:20-94).
 //
-// Sim map layout: a dense grid of leaf indices over the map's leaf box (-1 = empty leaf),
-// compact 8^3 bit leaves (16 words each), and one occupancy bit per 64^3-voxel brick for
-// long empty-space skips.
+// Sim map layout: a table over the brick box (64^3-voxel bricks) naming each non-empty brick's
+// block of 512 leaf entries, each entry the index of a compact 8^3 bit leaf (16 words) or -1;
+// empty bricks give the walk its long empty-space skips.
 //
 // The ray cast itself (sim_cast, sim_ray) and the range noise live in nm_sim_device.cuh,
 // shared with the traversal kernel's fused render.
@@ -108,10 +108,11 @@ __device__ __forceinline__ void word_bounds(uint32_t w, int q, int mn[3], int mx
   mx[2] = max(mx[2], 31 - __clz(zor));
 }
 
-// Pass 1: count non-empty leaves (one atomic per block).  Pass 2: give each a compact index
-// (block-wide scan, one atomic per block and iteration), copy its words, set its brick bit
-// (one atomic per distinct brick word in a warp) and fold its voxels into the active bounding
-// box and voxel count (reduced per block, one set of atomics per block).  One thread per leaf.
+// Pass 1: count non-empty leaves (one atomic per block) and flag their bricks in
+// v.brick_index (set to 1; the host then numbers the flagged bricks).  Pass 2: give each leaf
+// a compact index (block-wide scan, one atomic per block and iteration), copy its words, enter
+// it in its brick's block, and fold its voxels into the active bounding box and voxel count
+// (reduced per block, one set of atomics per block).  One thread per leaf of the build box.
 __global__ void __launch_bounds__(256) k_compact(SimBuild b, SimMapView v, uint32_t* count,
                                                  int pass2, int32_t* bbox,
                                                  unsigned long long* nvox) {
@@ -136,8 +137,21 @@ __global__ void __launch_bounds__(256) k_compact(SimBuild b, SimMapView v, uint3
     }
     const bool any = (w[0].x | w[0].y | w[0].z | w[0].w | w[1].x | w[1].y | w[1].z | w[1].w |
                       w[2].x | w[2].y | w[2].z | w[2].w | w[3].x | w[3].y | w[3].z | w[3].w) != 0u;
+    long long bpos = 0;
+    int bx = 0, by = 0, bz = 0;
+    if (any) {
+      const int lz = (int)(pos % b.ldim[2]);
+      const int ly = (int)((pos / b.ldim[2]) % b.ldim[1]);
+      const int lx = (int)(pos / ((long long)b.ldim[2] * b.ldim[1]));
+      bx = lx + b.llo[0];
+      by = ly + b.llo[1];
+      bz = lz + b.llo[2];
+      bpos = ((long long)((bx >> 3) - v.blo[0]) * v.bdim[1] + ((by >> 3) - v.blo[1])) * v.bdim[2] +
+             ((bz >> 3) - v.blo[2]);
+    }
     if (!pass2) {
       nonempty += any ? 1u : 0u;
+      if (any) v.brick_index[bpos] = 1;
       continue;
     }
     const unsigned ball = __ballot_sync(kFull, any);
@@ -155,20 +169,13 @@ __global__ void __launch_bounds__(256) k_compact(SimBuild b, SimMapView v, uint3
     __syncthreads();
     const uint32_t idx = s_base + s_warp[warp] + __popc(ball & ((1u << lane) - 1u));
     __syncthreads();  // s_warp / s_base are rewritten by the next iteration
-    uint32_t bword = 0xffffffffu, bbit = 0u;
     if (any) {
       uint4* dst = reinterpret_cast<uint4*>(v.leaf_words) + (size_t)idx * 4;
 #pragma unroll
       for (int i = 0; i < 4; ++i) dst[i] = w[i];
-      v.leaf_index[pos] = (int32_t)idx;
-      const int lz = (int)(pos % b.ldim[2]);
-      const int ly = (int)((pos / b.ldim[2]) % b.ldim[1]);
-      const int lx = (int)(pos / ((long long)b.ldim[2] * b.ldim[1]));
-      const int bx = lx + b.llo[0], by = ly + b.llo[1], bz = lz + b.llo[2];
-      const long long bpos = ((long long)((bx >> 3) - v.blo[0]) * v.bdim[1] + ((by >> 3) - v.blo[1])) *
-                                 v.bdim[2] + ((bz >> 3) - v.blo[2]);
-      bword = (uint32_t)(bpos >> 5);
-      bbit = 1u << (bpos & 31);
+      const int32_t blk = v.brick_index[bpos];
+      const int e = ((bx & 7) << 6) | ((by & 7) << 3) | (bz & 7);
+      v.brick_leaves[(size_t)blk * 512 + e] = (int32_t)idx;
       int lmn[3] = {8, 8, 8}, lmx[3] = {-1, -1, -1};
       const uint32_t ww[16] = {w[0].x, w[0].y, w[0].z, w[0].w, w[1].x, w[1].y, w[1].z, w[1].w,
                                w[2].x, w[2].y, w[2].z, w[2].w, w[3].x, w[3].y, w[3].z, w[3].w};
@@ -184,10 +191,6 @@ __global__ void __launch_bounds__(256) k_compact(SimBuild b, SimMapView v, uint3
         mx[a] = max(mx[a], o[a] + lmx[a]);
       }
     }
-    // brick bits: lanes of one warp that hit the same word OR their bits, the lowest sets them
-    const unsigned peers = __match_any_sync(kFull, bword);
-    const uint32_t bits = __reduce_or_sync(peers, bbit);
-    if (any && lane == __ffs(peers) - 1) atomicOr(&v.brick_bits[bword], bits);
   }
   if (!pass2) {
 #pragma unroll

@@ -19,14 +19,18 @@ struct SimBuild {
   int32_t borrowed;          // dense belongs to the caller (not freed by the build)
 };
 
+// Two-level index, like the upper levels of a NanoVDB tree: a table over the brick box (64^3
+// voxels per brick) names each non-empty brick's block of 512 leaf entries (its 8^3 leaves,
+// x*64 + y*8 + z), and each entry names a compact 64-byte bit leaf.  Memory follows the
+// occupied bricks and leaves, not the volume of the scene's box.
 struct SimMapView {
   float res;
   int32_t any;
   int32_t llo[3], ldim[3];   // leaf box
   int32_t blo[3], bdim[3];   // brick box (64^3-voxel bricks)
-  int32_t* leaf_index;       // ldim product entries, -1 = empty leaf
+  int32_t* brick_index;      // bdim product entries: block of the brick, -1 = empty brick
+  int32_t* brick_leaves;     // 512 entries per block: compact leaf index, -1 = empty leaf
   uint32_t* leaf_words;      // 16 words per non-empty leaf
-  uint32_t* brick_bits;      // one bit per brick
   float box_lo[3], box_hi[3];  // active voxel box in index space, [amin, amax + 1]
 };
 

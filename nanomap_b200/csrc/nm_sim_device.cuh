@@ -58,12 +58,10 @@ __device__ __forceinline__ int sim_level(const SimMapView& v, int x, int y, int 
       (unsigned)bz >= (unsigned)v.bdim[2])
     return 2;
   const long long bpos = ((long long)bx * v.bdim[1] + by) * v.bdim[2] + bz;
-  if (!((__ldg(&v.brick_bits[bpos >> 5]) >> (bpos & 31)) & 1u)) return 2;
-  const int lx = (x >> 3) - v.llo[0], ly = (y >> 3) - v.llo[1], lz = (z >> 3) - v.llo[2];
-  if ((unsigned)lx >= (unsigned)v.ldim[0] || (unsigned)ly >= (unsigned)v.ldim[1] ||
-      (unsigned)lz >= (unsigned)v.ldim[2])
-    return 1;
-  const int32_t li = __ldg(&v.leaf_index[((long long)lx * v.ldim[1] + ly) * v.ldim[2] + lz]);
+  const int32_t blk = __ldg(&v.brick_index[bpos]);
+  if (blk < 0) return 2;
+  const int e = (((x >> 3) & 7) << 6) | (((y >> 3) & 7) << 3) | ((z >> 3) & 7);
+  const int32_t li = __ldg(&v.brick_leaves[(size_t)blk * 512 + e]);
   if (li < 0) return 1;
   *leaf = li;
   return 0;

@@ -202,3 +202,60 @@ def test_handles_destroyed_in_any_order(small):
     sensor.close()
     sim.close()
     m.close()
+
+
+def _wide_frame(seed=3):
+    """A 32x24 camera at 10 m mapped at 2 mm: max_range / res = 5000 voxels, beyond the reach
+    of the traversal's shared leaf table (frames past 4000 voxels take the wide traversal)."""
+    rng = np.random.default_rng(seed)
+    desc = A.sensor_desc(hres=32, vres=24, hfov_deg=60.0, vfov_deg=45.0, max_range=10.0,
+                         explicit_log_odds=1, log_odds_hit=0.85, log_odds_miss=-0.4)
+    r = rng.uniform(0.5, 9.99, (24, 32)).astype(np.float32)
+    r[rng.random(r.shape) < 0.1] = 0.0       # no return
+    r[rng.random(r.shape) < 0.05] = 10.5     # beyond max range: dropped
+    return desc, r
+
+
+@pytest.mark.parametrize("rounding", [N.NM_ROUND_DOWN, N.NM_ROUND_NEAREST])
+def test_wide_frame_labels_and_map_match_oracle(ctx, rounding):
+    desc, r = _wide_frame()
+    res = 0.002
+    sensor = A.Sensor(ctx, desc)
+    pose = A.Pose((0.31, -0.27, 1.13), (0.9, 0.1, -0.2, 0.3))
+    m = A.Map(ctx, A.map_desc(res=res, rounding=rounding))
+    m.insert_ranges(sensor, pose, _torch(r), flags=N.NM_DEFER_INTEGRATE)
+    gl = m.export_labels()
+    R, eye, mt = oracle_frame(desc, pose, res, rounding)
+    assert mt >= 4000.0
+    om = O.Map(res, rounding=1 if rounding == N.NM_ROUND_DOWN else 0)
+    osen = O.Sensor.from_desc(desc)
+    om.insert(R, eye, mt, desc.log_odds_hit, desc.log_odds_miss, osen.points(r), keep_labels=True)
+    errs = compare_labels(gl, om.labels())
+    assert not errs, "; ".join(errs[:5])
+    m.integrate()
+    errs = compare_maps(m.export(), om.export())
+    assert not errs, "; ".join(errs[:5])
+    st = m.stats()
+    assert st["visits"] == om.stats()["visits"] and st["error_flags"] == 0
+
+
+def test_tick_with_a_wide_frame_matches_solo_runs(ctx, small):
+    """A one-shot tick mixing a wide frame (2 mm, 10 m) with a frame of the small camera runs
+    the wide traversal for both; each plane equals its solo insert."""
+    spec, scene, desc_small, frames = small
+    desc, r = _wide_frame(seed=5)
+    res = 0.002
+    wide = A.Sensor(ctx, desc)
+    cam = A.Sensor(ctx, desc_small)
+    pose_w = A.Pose((0.0, 0.0, 1.0), (1.0, 0.0, 0.0, 0.0))
+    pose_c, rc = frames[0]
+    rw, rcam = _torch(r), _torch(np.minimum(rc, 0.5).astype(np.float32))
+    m = A.Map(ctx, A.map_desc(res=res, max_agents=2))
+    m.tick([(wide, pose_w, rw, 0), (cam, pose_c, rcam, 1)], flags=N.NM_DEFER_INTEGRATE)
+    for plane, (s, p, rr) in enumerate([(wide, pose_w, rw), (cam, pose_c, rcam)]):
+        solo = A.Map(ctx, A.map_desc(res=res))
+        solo.insert_ranges(s, p, rr, flags=N.NM_DEFER_INTEGRATE)
+        errs = compare_labels(m.export_labels(plane), solo.export_labels(0))
+        assert not errs, f"plane {plane}: " + "; ".join(errs[:3])
+        solo.close()
+    m.integrate()
