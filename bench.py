@@ -443,6 +443,7 @@ def run_ours(args, rank, world, local):
             mdepth.insert_points(sensor, poses[k], records[k], W, H, 16, stream=stream)
         line["expected_depth"] = run_depth_section(ctx, mdepth, sensor, sim, spec, poses, stream, hbm)
         mdepth.close()
+        line["refine"] = run_refine_section(local)
     if args.batched_ticks > args.warmup:
         line["batched"] = run_batched(args, rank, world, local, args.batched_ticks)
     if args.large:
@@ -625,8 +626,8 @@ def run_filter_section(ctx, sensor, sim, mdesc, spec, poses, ranges, stream, war
 
 
 def run_depth_section(ctx, m, sensor, sim, spec, poses, stream, hbm, reps=10):
-    """Expected-depth forward and adjoint over the headline map after the timed run (640x480,
-    10 m, 0.05 m voxels), and scan-to-map refinement from a perturbed pose (50 Adam steps)."""
+    """Expected-depth forward and adjoint over a map of the workload's frames (640x480, 10 m,
+    0.05 m voxels) at a perturbed pose of the trajectory."""
     import torch
 
     from nanomap_b200 import api as A
@@ -677,29 +678,87 @@ def run_depth_section(ctx, m, sensor, sim, spec, poses, stream, hbm, reps=10):
                               "unit": "GB/s", "frac": bwd_bytes / (bwd_ms / 1e3) / 1e9 / hbm},
         "occupancy": f"sigmoid({scale} * log-odds + {bias}) per voxel length",
     }
-    # refinement: map-consistent scan (expected depth at the ground truth where the simulated
-    # sensor returns) and the simulated depth itself
-    sim_depth = torch.zeros(H, W, device=vals.device)
-    sim.render(sensor, gt, sim_depth, stream=stream)
-    scan = m.depth_render(sensor, gpos, gR, scale=scale, bias=bias)
-    scan = torch.where(sim_depth > 0, scan, torch.zeros_like(scan))
+    return out
 
-    def errors(p, Rm):
-        ang = math.degrees(math.acos(max(-1.0, min(1.0, (np.trace(Rm @ gR.T) - 1) / 2))))
-        return float(np.linalg.norm(p - gpos)), ang
 
-    t_start, a_start = errors(pos, R)
-    ref = {"start_error_m": t_start, "start_error_deg": a_start, "steps": 50}
-    for name, tgt in (("map_consistent_scan", scan), ("sim_depth", sim_depth)):
-        torch.cuda.synchronize()
-        t0 = time.perf_counter()
-        p1, R1, losses = m.pose_refine(sensor, pos, R, tgt, steps=50, lr_position=0.01,
-                                       lr_rotation=0.004, scale=scale, bias=bias, max_residual=0.3)
-        dt = time.perf_counter() - t0
-        te, ae = errors(p1, R1)
-        ref[name] = {"final_error_m": te, "final_error_deg": ae, "loss_first": float(losses[0]),
-                     "loss_last": float(losses[-1]), "ms_per_step": dt * 1e3 / 50}
-    out["refine"] = ref
+def run_refine_section(local, trials=3):
+    """Config 4: the small world mapped at 0.1 m from its 100-frame walk (exact ray-box ranges
+    + N(0, 0.01 m), fp32 log-odds); one 640x480 87 x 58 deg camera at 5 m starts at a pose of
+    the walk perturbed by U(+-5 cm), U(+-2 deg); 50 Adam steps on the L1 residual against the
+    simulated depth of the 0.1 m sim grid at the ground truth.  Three settings: the surface at
+    the voxel face the ray enters (occupancy scale 4), the surface at the middle of the ending
+    voxel (scale 12, silhouettes left out) started perturbed and started at the ground truth
+    (the objective's own minimum), and a map-consistent scan (the map's expected depth at the
+    ground truth) as the target."""
+    import torch
+
+    from nanomap_b200 import api as A
+    from nanomap_b200 import scenes as S
+    from nanomap_b200.diff import so3_exp
+    spec = S.SCENES["plain_small"]
+    scene = S.make_scene(spec, 1)
+    traj = S.trajectory(scene, 100, seed=7)
+    ctx = A.Context(local)
+    desc = A.sensor_desc(**S.sensor_desc_kwargs(spec))
+    sensor = A.Sensor(ctx, desc)
+    pm = sensor.params()
+    rng = np.random.default_rng(101)
+    m = A.Map(ctx, A.map_desc(res=spec.map_res, clamp_min=spec.clamp[0], clamp_max=spec.clamp[1]))
+    t0 = time.perf_counter()
+    for pos, q in traj:
+        r = S.analytic_box_ranges(scene, pm, spec.width, spec.height, spec.max_range, pos, q)
+        r = np.where(r > 0, r + rng.normal(0.0, spec.noise_sigma, r.shape), 0.0).astype(np.float32)
+        r[~(r > 0)] = 0.0
+        m.insert_ranges(sensor, A.Pose(pos, q), torch.from_numpy(r).cuda())
+    torch.cuda.synchronize()
+    build_s = time.perf_counter() - t0
+    cam = A.Sensor(ctx, A.sensor_desc(**dict(S.sensor_desc_kwargs(spec), hres=640, vres=480)))
+    sim = A.SimMap(ctx, spec.sim_res, boxes=scene.boxes, cylinders=scene.cylinders,
+                   vox_min=scene.vox_min, vox_max=scene.vox_max)
+    target = torch.zeros(480, 640, device="cuda")
+
+    def gap(p0, R0, p1, R1):
+        ang = math.degrees(math.acos(max(-1.0, min(1.0, (np.trace(R1 @ R0.T) - 1) / 2))))
+        return float(np.linalg.norm(p1 - p0)), ang
+
+    face = dict(steps=50, lr_position=0.01, lr_rotation=0.004, scale=4.0, bias=0.0, max_residual=0.3)
+    mid = dict(face, scale=12.0, surface_offset=0.5, edge_threshold=0.15)
+    out = {"workload": ("plain_small world mapped at 0.1 m from 100 frames; 640x480 camera at 5 m; "
+                        "target = 0.1 m sim depth at the ground truth; 50 Adam steps from "
+                        "U(+-5 cm), U(+-2 deg)"), "map_build_s": build_s, "trials": []}
+    for trial in range(trials):
+        gt = A.Pose(*traj[10 + 20 * trial])
+        gpos, gR = A.Map.ray_pose(cam, gt)
+        rr = np.random.default_rng(11 + trial)
+        pos = gpos + rr.uniform(-0.05, 0.05, 3)
+        R = so3_exp(np.radians(rr.uniform(-2.0, 2.0, 3))) @ gR
+        sim.render(cam, gt, target)
+        row = {"start_error": gap(gpos, gR, pos, R)}
+        runs = [("sim_depth_face_scale4", pos, R, target, face),
+                ("sim_depth_mid_voxel", pos, R, target, mid),
+                ("sim_depth_mid_voxel_from_truth", gpos, gR, target, mid)]
+        if trial == 0:
+            scan = m.depth_render(cam, gpos, gR, scale=4.0, bias=0.0)
+            scan = torch.where(target > 0, scan, torch.zeros_like(scan))
+            runs.append(("map_consistent_scan", pos, R, scan, face))
+        ends = {}
+        for name, p0, R0, tgt, kw in runs:
+            torch.cuda.synchronize()
+            t0 = time.perf_counter()
+            p1, R1, losses = m.pose_refine(cam, p0, R0, tgt, **kw)
+            dt = time.perf_counter() - t0
+            ends[name] = (p1, R1)
+            te, ae = gap(gpos, gR, p1, R1)
+            row[name] = {"final_error_m": te, "final_error_deg": ae, "loss_first": float(losses[0]),
+                         "loss_last": float(losses[-1]), "ms_per_step": dt * 1e3 / 50}
+        g = gap(*ends["sim_depth_mid_voxel"], *ends["sim_depth_mid_voxel_from_truth"])
+        row["mid_voxel_end_vs_minimum"] = {"m": g[0], "deg": g[1]}
+        out["trials"].append(row)
+    sim.close()
+    cam.close()
+    m.close()
+    sensor.close()
+    ctx.close()
     return out
 
 

@@ -346,6 +346,26 @@ int nm_pose_refine(nm_map m, nm_sensor s, nm_ray_pose* pose, const float* target
                    float bias, float max_residual, int32_t steps, float lr_position,
                    float lr_rotation, float* losses);
 
+/* Options of scan-to-map refinement.  surface_offset (0..1) places the predicted surface that
+ * fraction of a voxel past the face the ray enters the voxel it ends in (0 = at the face, as
+ * nm_pose_refine; 0.5 = at the middle of the voxel, the unbiased choice against a target
+ * rendered from a different voxel grid, whose surfaces lie 0 or 1 voxel past that face).
+ * edge_threshold (m, 0 = off) leaves out target pixels on silhouettes: a 4-neighbour without
+ * a return or with a range that differs by more than the threshold. */
+typedef struct nm_refine_desc {
+  float scale, bias;       /* occupancy = sigmoid(scale * log-odds + bias) */
+  float max_residual;      /* truncation of the L1 residual (m; 0 = plain L1) */
+  int32_t steps;
+  float lr_position;       /* m */
+  float lr_rotation;       /* rad */
+  float surface_offset;
+  float edge_threshold;
+} nm_refine_desc;
+
+/* nm_pose_refine with the options above. */
+int nm_pose_refine_desc(nm_map m, nm_sensor s, nm_ray_pose* pose, const float* target,
+                        const nm_refine_desc* desc, float* losses);
+
 /* ---- simulation map (replaces the NanoVDB sim grid, SimHandler.cpp:13-24) -------------- */
 /* Voxelise primitives into a sparse device map: boxes are 6 doubles (min xyz, max xyz, m);
  * cylinders are 5 doubles (cx, cy, radius, z0, z1, m).  A voxel is active when its centre is

@@ -108,6 +108,12 @@ class NmRayPose(C.Structure):
     _fields_ = [("position", C.c_double * 3), ("rotation", C.c_double * 9)]
 
 
+class NmRefineDesc(C.Structure):
+    _fields_ = [("scale", C.c_float), ("bias", C.c_float), ("max_residual", C.c_float),
+                ("steps", C.c_int32), ("lr_position", C.c_float), ("lr_rotation", C.c_float),
+                ("surface_offset", C.c_float), ("edge_threshold", C.c_float)]
+
+
 class NmCaveDesc(C.Structure):
     _fields_ = [
         ("map_size", C.c_double * 3), ("grid_res", C.c_double), ("fill_percentage", C.c_int32),
@@ -172,6 +178,8 @@ _SIGS = {
                                     _P]),
     "nm_pose_refine": (C.c_int, [_P, _P, C.POINTER(NmRayPose), _P, _F, _F, _F, _I32, _F, _F,
                                  _PF]),
+    "nm_pose_refine_desc": (C.c_int, [_P, _P, C.POINTER(NmRayPose), _P, C.POINTER(NmRefineDesc),
+                                      _PF]),
     "nm_map_filter_points": (C.c_int, [_P, _P, C.POINTER(NmPose), _P, _I32, _I32, _I32, _U32,
                                        _PF, _PU32, _U64, _PU64]),
     "nm_map_insert_ranges": (C.c_int, [_P, _P, C.POINTER(NmPose), _P, _U32, _P]),

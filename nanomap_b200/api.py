@@ -278,15 +278,18 @@ class Map:
 
     def pose_refine(self, sensor: Sensor, position, rotation, target, steps=50,
                     lr_position=0.005, lr_rotation=0.002, scale=1.0, bias=0.0,
-                    max_residual=0.0):
-        """Native Adam refinement; returns (position, rotation, losses (steps + 1,))."""
+                    max_residual=0.0, surface_offset=0.0, edge_threshold=0.0):
+        """Native Adam refinement (nm_pose_refine_desc); returns (position, rotation,
+        losses (steps + 1,))."""
         import torch
         torch.cuda.current_stream().synchronize()
         rp = _ray_pose(position, rotation)
         losses = np.zeros(steps + 1, np.float32)
         t = target.contiguous()
-        call("nm_pose_refine", self.h, sensor.h, C.byref(rp), C.c_void_p(t.data_ptr()), scale,
-             bias, max_residual, steps, lr_position, lr_rotation, losses.ctypes.data_as(N._PF))
+        d = N.NmRefineDesc(scale, bias, max_residual, steps, lr_position, lr_rotation,
+                           surface_offset, edge_threshold)
+        call("nm_pose_refine_desc", self.h, sensor.h, C.byref(rp), C.c_void_p(t.data_ptr()),
+             C.byref(d), losses.ctypes.data_as(N._PF))
         return np.array(rp.position[:]), np.array(rp.rotation[:]).reshape(3, 3), losses
 
     def set_launch(self, tile_w: int, tile_h: int, leaf_table_entries: int):

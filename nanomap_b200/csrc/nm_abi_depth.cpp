@@ -203,10 +203,30 @@ int nm_depth_backward(nm_map m, nm_sensor s, const nm_ray_pose* pose, const floa
 int nm_pose_refine(nm_map m, nm_sensor s, nm_ray_pose* pose, const float* target, float scale,
                    float bias, float max_residual, int32_t steps, float lr_position,
                    float lr_rotation, float* losses) {
-  if (!pose || !target) return fail(NM_ERR_ARG, "null argument");
+  nm_refine_desc d;
+  d.scale = scale;
+  d.bias = bias;
+  d.max_residual = max_residual;
+  d.steps = steps;
+  d.lr_position = lr_position;
+  d.lr_rotation = lr_rotation;
+  d.surface_offset = 0.0f;
+  d.edge_threshold = 0.0f;
+  return nm_pose_refine_desc(m, s, pose, target, &d, losses);
+}
+
+int nm_pose_refine_desc(nm_map m, nm_sensor s, nm_ray_pose* pose, const float* target,
+                        const nm_refine_desc* desc, float* losses) {
+  if (!pose || !target || !desc) return fail(NM_ERR_ARG, "null argument");
+  const float scale = desc->scale, bias = desc->bias, max_residual = desc->max_residual;
+  const int32_t steps = desc->steps;
+  const float lr_position = desc->lr_position, lr_rotation = desc->lr_rotation;
   if (!(max_residual >= 0.0f)) return fail(NM_ERR_ARG, "max_residual must be >= 0");
   if (steps < 0) return fail(NM_ERR_ARG, "steps must be >= 0");
   if (!(lr_position >= 0.0f) || !(lr_rotation >= 0.0f)) return fail(NM_ERR_ARG, "bad learning rate");
+  if (!(desc->surface_offset >= 0.0f && desc->surface_offset <= 1.0f))
+    return fail(NM_ERR_ARG, "surface_offset must lie in [0, 1]");
+  if (!(desc->edge_threshold >= 0.0f)) return fail(NM_ERR_ARG, "edge_threshold must be >= 0");
   nm::DepthParams p;
   int rc = make_depth_params(m, s, pose, scale, bias, &p);
   if (rc != NM_OK) return rc;
@@ -225,6 +245,7 @@ int nm_pose_refine(nm_map m, nm_sensor s, nm_ray_pose* pose, const float* target
     rc = make_depth_params(m, s, &cur, scale, bias, &p);
     if (rc != NM_OK) return rc;
     NM_CUDA(nm::launch_depth_refine(p, m->view, m->view.values, target, max_residual,
+                                    desc->surface_offset, desc->edge_threshold,
                                     m->depth_scratch, out8, s0));
     double h[8];
     NM_CUDA(cudaMemcpyAsync(h, out8, sizeof(h), cudaMemcpyDeviceToHost, s0));

@@ -162,17 +162,23 @@ __device__ __forceinline__ float voxel_logodds(const MapView& m, const float* va
   return c.slot >= 0 ? __ldg(&vals[(size_t)c.slot * kLeafVoxels + *l]) : 0.0f;
 }
 
-// Expected depth in index units (integral of the transmittance over [0, t_max]), FP32.
+// Expected depth in index units (integral of the transmittance over [0, t_max]), FP32.  With
+// `entry_step` given, also the mean, over where the ray ends, of the voxel step along the axis
+// it entered the ending voxel across (1 / |d_a|, index units): the depth the ray covers from
+// one face of that voxel to the opposite one.
 __device__ __forceinline__ float expected_index_depth(const DepthParams& p, const MapView& m,
                                                       const float* vals, const double d[3],
-                                                      float* t1_out, uint32_t* visits) {
+                                                      float* t1_out, uint32_t* visits,
+                                                      float* entry_step = nullptr) {
   LeafCache c{kEmptyKey, -1};
   DensityCache dc;
-  float T = 1.0f, acc = 0.0f;
+  float T = 1.0f, acc = 0.0f, W = 0.0f;
   double t1 = p.t_max;
   bool first = true;
   uint32_t n = 0;
-  walk(p.eye, d, p.t_max, [&](const int v[3], double t_in, int, double t_out, int) {
+  const float step[3] = {(float)(1.0 / fabs(d[0])), (float)(1.0 / fabs(d[1])),
+                         (float)(1.0 / fabs(d[2]))};
+  walk(p.eye, d, p.t_max, [&](const int v[3], double t_in, int a_in, double t_out, int) {
     ++n;
     int slot, l;
     dc.at(p, voxel_logodds(m, vals, c, v, &slot, &l));
@@ -184,10 +190,12 @@ __device__ __forceinline__ float expected_index_depth(const DepthParams& p, cons
     }
     const float em1 = expm1f(-sg * Dk);
     acc += T * (sg > 0.0f ? -em1 / sg : Dk);
+    if (entry_step) W -= T * em1 * step[a_in];
     T *= 1.0f + em1;
   });
   *t1_out = (float)t1;
   *visits += n;
+  if (entry_step) *entry_step = T < 1.0f ? W / (1.0f - T) : 0.0f;
   return (float)t1 + acc;
 }
 
@@ -316,25 +324,45 @@ __global__ void __launch_bounds__(kDepthTile * kDepthTile) k_depth_backward(
   block_partials<6>(acc, partials);
 }
 
+// Whether pixel (w, h) of the target lies on a silhouette: a 4-neighbour inside the image
+// without a return, or with a range more than `edge` metres away.
+__device__ __forceinline__ bool target_edge(const float* target, int W, int H, int w, int h,
+                                            float r, float edge) {
+  const int nx[4] = {w - 1, w + 1, w, w};
+  const int ny[4] = {h, h, h - 1, h + 1};
+#pragma unroll
+  for (int k = 0; k < 4; ++k) {
+    if (nx[k] < 0 || nx[k] >= W || ny[k] < 0 || ny[k] >= H) continue;
+    const float q = target[(size_t)ny[k] * W + nx[k]];
+    if (!(q > 0.0f && q < CUDART_INF_F) || fabsf(q - r) > edge) return true;
+  }
+  return false;
+}
+
 // One refinement step: L1 loss against `target` (metres; <= 0 or NaN = no return), truncated
 // at max_residual when it is positive (residuals beyond it add max_residual and no gradient),
-// its pose gradient, and the number of pixels that took part.  Partials: loss, count, 6
-// gradients.
+// its pose gradient, and the number of pixels that took part.  The prediction is the expected
+// depth plus `surface_offset` times the entry step of the voxel where the ray ends (0: the
+// surface at the face the ray enters; 0.5: at the middle of the voxel), the offset held fixed
+// for the gradient.  Silhouette pixels of the target are left out when edge > 0.  Partials:
+// loss, count, 6 gradients.
 __global__ void __launch_bounds__(kDepthTile * kDepthTile) k_depth_refine(
     DepthParams p, MapView m, const float* vals, const float* target, float max_residual,
-    double* partials) {
+    float surface_offset, float edge, double* partials) {
   const int w = blockIdx.x * kDepthTile + threadIdx.x;
   const int h = blockIdx.y * kDepthTile + threadIdx.y;
   double acc[8] = {0, 0, 0, 0, 0, 0, 0, 0};
   uint32_t n = 0;
   if (w < p.width && h < p.height) {
     const float r = target[(size_t)h * p.width + w];
-    if (r > 0.0f && r < CUDART_INF_F) {
+    if (r > 0.0f && r < CUDART_INF_F &&
+        !(edge > 0.0f && target_edge(target, p.width, p.height, w, h, r, edge))) {
       double d[3];
       pixel_dir(p, w, h, d);
-      float t1;
-      const float D = expected_index_depth(p, m, vals, d, &t1, &n);
-      const float res = D * (float)p.res - r;
+      float t1, step = 0.0f;
+      const float D = expected_index_depth(p, m, vals, d, &t1, &n,
+                                           surface_offset != 0.0f ? &step : nullptr);
+      const float res = (D + surface_offset * step) * (float)p.res - r;
       const bool clipped = max_residual > 0.0f && fabsf(res) > max_residual;
       acc[0] = clipped ? (double)max_residual : fabs((double)res);
       acc[1] = 1.0;
@@ -398,11 +426,11 @@ cudaError_t launch_depth_backward(const DepthParams& p, const MapView& m, const 
 }
 
 cudaError_t launch_depth_refine(const DepthParams& p, const MapView& m, const float* vals,
-                                const float* target, float max_residual, double* partials,
-                                double* out8, cudaStream_t s) {
+                                const float* target, float max_residual, float surface_offset,
+                                float edge, double* partials, double* out8, cudaStream_t s) {
   const dim3 g = depth_grid(p);
   k_depth_refine<<<g, dim3(kDepthTile, kDepthTile), 0, s>>>(p, m, vals, target, max_residual,
-                                                            partials);
+                                                            surface_offset, edge, partials);
   cudaError_t e = cudaGetLastError();
   if (e != cudaSuccess) return e;
   k_sum_partials<<<1, 256, 0, s>>>(partials, (int)(g.x * g.y), 8, out8);

@@ -217,8 +217,8 @@ cudaError_t launch_depth_backward(const DepthParams& p, const MapView& m, const 
                                   const float* grad_depth, float* grad_vals, double* partials,
                                   double* out6, cudaStream_t s);
 cudaError_t launch_depth_refine(const DepthParams& p, const MapView& m, const float* vals,
-                                const float* target, float max_residual, double* partials,
-                                double* out8, cudaStream_t s);
+                                const float* target, float max_residual, float surface_offset,
+                                float edge, double* partials, double* out8, cudaStream_t s);
 cudaError_t filter_reserve(FilterBuffers* b, int64_t n, cudaStream_t s);
 void filter_release(FilterBuffers* b);
 int filter_key_bits(float max_time);  // bits per axis of a filter key; 0 if out of range

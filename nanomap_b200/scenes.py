@@ -247,15 +247,19 @@ def analytic_box_ranges(scene: Scene, pixel_model, width: int, height: int, max_
     # boxes whose nearest point lies beyond max range cannot be hit
     near = np.linalg.norm(np.maximum(np.maximum(scene.boxes[:, :3] - p, p - scene.boxes[:, 3:]), 0.0),
                           axis=1) <= max_range
+    boxes = scene.boxes[near]
     with np.errstate(divide="ignore", invalid="ignore"):
         inv = 1.0 / m
-        for b in scene.boxes[near]:
-            ta = (b[:3] - p) * inv
-            tb = (b[3:] - p) * inv
-            t0 = np.nanmax(np.maximum(np.minimum(ta, tb), 0.0), axis=1)
-            t1 = np.nanmin(np.maximum(ta, tb), axis=1)
-            hit = t0 <= t1
-            best = np.where(hit & (t0 < best), t0, best)
+        for c in range(0, len(boxes), 64):  # slab tests of 64 boxes at a time
+            b = boxes[c:c + 64]
+            t0 = np.zeros((len(m), len(b)))
+            t1 = np.full((len(m), len(b)), np.inf)
+            for a in range(3):  # fmax / fmin skip the NaN of 0 * inf on a parallel axis
+                ta = (b[None, :, a] - p[a]) * inv[:, a, None]
+                tb = (b[None, :, 3 + a] - p[a]) * inv[:, a, None]
+                t0 = np.fmax(t0, np.fmin(ta, tb))
+                t1 = np.fmin(t1, np.fmax(ta, tb))
+            best = np.minimum(best, np.where(t0 <= t1, t0, np.inf).min(axis=1))
     out = np.where((best <= max_range) & (best > 0.0), best, 0.0)
     return out.astype(np.float32).reshape(height, width)
 

@@ -158,3 +158,40 @@ def test_scan_to_map_refinement(world, trial):
     t1, a1 = errors(p1, R1)
     assert losses[-1] < 0.2 * losses[0], losses[[0, -1]]
     assert t1 < 0.005 and a1 < 0.3, (t0, a0, t1, a1)
+
+
+def _pose_gap(p0, R0, p1, R1):
+    ang = math.degrees(math.acos(max(-1.0, min(1.0, (np.trace(R1 @ R0.T) - 1) / 2))))
+    return float(np.linalg.norm(p1 - p0)), ang
+
+
+@pytest.mark.parametrize("trial", [0, 1, 2])
+def test_refinement_converges_on_sim_depth(world, trial):
+    """The refinement against the simulated depth itself (config 4's target): the map (0.1 m,
+    from exact ray-box ranges) holds a surface in the voxel that contains it, the sim grid
+    (0.1 m, voxel active when its centre is inside a box) 0 or 1 voxel further on; the
+    prediction therefore puts the surface at the middle of the ending voxel (surface_offset
+    0.5), sharpens the occupancy (scale 12: weakly observed free voxels stop no rays) and
+    leaves out silhouette pixels.  Checked: 50 Adam steps from U(+-5 cm), U(+-2 deg) end within
+    4 cm / 0.75 deg of where the same refinement started at the ground truth ends (the
+    objective's own minimum), and within 8 cm / 1 deg of the ground truth (the quantisation
+    floor of two 0.1 m grids; an FP64 analysis of this workload puts the minimum 2-7 cm away)."""
+    import torch
+    w = world
+    m, cam = w["m"], w["cam"]
+    gt = w["frames"][10 + 20 * trial][0]
+    gpos, gR = A.Map.ray_pose(cam, gt)
+    rng = np.random.default_rng(11 + trial)
+    pos = gpos + rng.uniform(-0.05, 0.05, 3)
+    R = so3_exp(np.radians(rng.uniform(-2.0, 2.0, 3))) @ gR
+    sim_depth = torch.zeros((480, 640), dtype=torch.float32, device="cuda")
+    w["sim"].render(cam, gt, sim_depth)
+    kw = dict(steps=50, lr_position=0.01, lr_rotation=0.004, scale=12.0, bias=0.0,
+              max_residual=0.3, surface_offset=0.5, edge_threshold=0.15)
+    p1, R1, losses = m.pose_refine(cam, pos, R, sim_depth, **kw)
+    p0, R0, _ = m.pose_refine(cam, gpos, gR, sim_depth, **kw)
+    assert losses[-1] < losses[0], losses[[0, -1]]
+    gap = _pose_gap(p0, R0, p1, R1)
+    err = _pose_gap(gpos, gR, p1, R1)
+    assert gap[0] < 0.04 and gap[1] < 0.75, (gap, err)
+    assert err[0] < 0.08 and err[1] < 1.0, (gap, err)
