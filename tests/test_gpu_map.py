@@ -246,7 +246,12 @@ def test_tick_with_a_wide_frame_matches_solo_runs(ctx, small):
     desc, r = _wide_frame(seed=5)
     res = 0.002
     wide = A.Sensor(ctx, desc)
-    cam = A.Sensor(ctx, desc_small)
+    # the small camera with its range cut to 0.6 m (300 voxels at 2 mm), so its frames stay
+    # within the leaf code's reach and its leaf bound stays small
+    cam = A.Sensor(ctx, A.sensor_desc(hres=desc_small.hres, vres=desc_small.vres,
+                                      hfov_deg=desc_small.hfov_deg, vfov_deg=desc_small.vfov_deg,
+                                      max_range=0.6, explicit_log_odds=1, log_odds_hit=0.85,
+                                      log_odds_miss=-0.4))
     pose_w = A.Pose((0.0, 0.0, 1.0), (1.0, 0.0, 0.0, 0.0))
     pose_c, rc = frames[0]
     rw, rcam = _torch(r), _torch(np.minimum(rc, 0.5).astype(np.float32))
