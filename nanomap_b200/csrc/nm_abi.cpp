@@ -571,10 +571,21 @@ int run_frame(nm_map m, nm_sensor s, nm::FrameParams& f, uint32_t flags, cudaStr
     w.total_tiles = w.tile_start[1];
     w.fr[0] = f;
     if (w.total_tiles > 0) {
-      if (sim)
+      if (sim) {
         NM_CUDA(nm::launch_traverse_render(w, m->view, *sim, m->desc.rounding, s0));
-      else
+      } else {
+        // longest walks first (frames within the leaf code's reach; the others take the
+        // table-free traversal, which claims no tiles)
+        if (f.max_time < nm::kNarrowMaxTime) {
+          NM_CUDA(nm::tile_order_reserve(&m->tile_order, w.total_tiles, s0));
+          w.order_scale = nm::tile_order_scale<1>(w);
+          NM_CUDA(nm::launch_tile_order<1>(w, m->tile_order, s0));
+          w.order_counts = m->tile_order.counts;
+          w.order_lists = m->tile_order.lists;
+          w.order_cap = m->tile_order.capacity;
+        }
         NM_CUDA(nm::launch_traverse_labels<1>(w, m->view, m->desc.rounding, s0));
+      }
     }
   } else {
     NM_CUDA(nm::launch_traverse_counts(f, m->view, m->desc.rounding, s0));
@@ -629,6 +640,7 @@ void release(nm_map m) {
   cudaFreeHost(m->h_status);
   cudaFree(m->staging);
   filter_release(&m->filter);
+  nm::tile_order_release(&m->tile_order);
   cudaFree(m->depth_scratch);
   delete m;
   release(c);
@@ -1179,8 +1191,19 @@ int nm_map_tick(nm_map m, const nm_frame* frames, int32_t n_frames, uint32_t fla
   int rc = ensure_capacity(m, bound, s0);
   if (rc != NM_OK) return rc;
   for (int i = 0; i < n_frames; ++i) w->fr[i].epoch = m->epoch;
-  if (w->total_tiles > 0)
+  if (w->total_tiles > 0) {
+    bool wide = false;
+    for (int i = 0; i < n_frames; ++i) wide |= !(w->fr[i].max_time < nm::kNarrowMaxTime);
+    if (!wide) {  // longest walks first
+      NM_CUDA(nm::tile_order_reserve(&m->tile_order, w->total_tiles, s0));
+      w->order_scale = nm::tile_order_scale<nm::kMaxTickFrames>(*w);
+      NM_CUDA(nm::launch_tile_order<nm::kMaxTickFrames>(*w, m->tile_order, s0));
+      w->order_counts = m->tile_order.counts;
+      w->order_lists = m->tile_order.lists;
+      w->order_cap = m->tile_order.capacity;
+    }
     NM_CUDA(nm::launch_traverse_labels<nm::kMaxTickFrames>(*w, m->view, m->desc.rounding, s0));
+  }
   m->pending_labels = true;
   if (!(flags & NM_DEFER_INTEGRATE)) {
     rc = do_integrate(m, s0);

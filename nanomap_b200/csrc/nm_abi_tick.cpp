@@ -53,6 +53,7 @@ struct nm_tick_plan_s {
   int parity = 0;
   int tile_w = 16, tile_h = 16, entries = 128;
   nm::IntegrateParams integ{};
+  nm::TileOrderBuffers order{};  // claim order of the tick's tiles (fixed address per graph)
 };
 
 namespace {
@@ -131,6 +132,8 @@ int capture(nm_tick_plan p, int k, bool defer) {
   cudaError_t e = cudaMemcpyAsync(p->d_stage, h, sizeof(TickStage), cudaMemcpyHostToDevice, p->cap_stream);
   if (e == cudaSuccess && p->sim)
     e = nm::launch_render_batch(&p->d_stage->render, render_tiles, p->sim->view, p->cap_stream);
+  if (e == cudaSuccess && total_tiles > 0 && !wide)  // longest walks first
+    e = nm::launch_tile_order_dev(&p->d_stage->work, total_tiles, p->order, p->cap_stream);
   if (e == cudaSuccess && total_tiles > 0)
     e = nm::launch_traverse_labels_dev(&p->d_stage->work, total_tiles, p->tile_w, p->tile_h,
                                        (uint32_t)p->entries - 1u, m->view, m->desc.rounding,
@@ -163,6 +166,24 @@ int run_plan(nm_tick_plan p, uint32_t flags, cudaStream_t s) {
   if (rc != NM_OK) return rc;
   rc = nm::ensure_capacity(m, bound, s);
   if (rc != NM_OK) return rc;
+  const uint32_t tiles = p->h_stage[k]->work.total_tiles;
+  if (tiles > p->order.capacity) {  // the graphs hold the buffers' addresses
+    NM_CUDA(cudaStreamSynchronize(s));
+    NM_CUDA(cudaDeviceSynchronize());
+    drop_graphs(p);
+    NM_CUDA(nm::tile_order_reserve(&p->order, tiles, s));
+  }
+  {
+    auto& w = p->h_stage[k]->work;
+    bool wide = false;
+    for (int i = 0; i < p->n; ++i) wide |= !(w.fr[i].max_time < nm::kNarrowMaxTime);
+    if (!wide) {  // the graph files the tiles by walk length, then claims them longest first
+      w.order_counts = p->order.counts;
+      w.order_lists = p->order.lists;
+      w.order_cap = p->order.capacity;
+      w.order_scale = nm::tile_order_scale<nm::kMaxTickFrames>(w);
+    }
+  }
   if (m->view.capacity != p->captured_capacity || m->view.keys != p->captured_keys) {
     NM_CUDA(cudaStreamSynchronize(s));
     drop_graphs(p);
@@ -257,6 +278,7 @@ int nm_tick_plan_destroy(nm_tick_plan p) {
     if (p->done[k]) cudaEventDestroy(p->done[k]);
   }
   cudaFree(p->d_stage);
+  nm::tile_order_release(&p->order);
   if (p->cap_stream) cudaStreamDestroy(p->cap_stream);
   for (int i = 0; i < p->n; ++i) nm::release(p->slots[i].sensor);
   nm::release(p->sim);

@@ -108,6 +108,12 @@ struct TickWork {
   uint32_t smask;         // shared-memory leaf table entries - 1 (power of two)
   uint32_t total_tiles;
   uint32_t queue;         // 0: MapCounters::tile_queue; c + 1: chunk_queue[c]
+  // claim order of the tiles (longest walks first; null = tile order): the number of tiles in
+  // each of kOrderBuckets walk-length buckets, and bucket b's tiles at order_lists[b * order_cap]
+  const uint32_t* order_counts;
+  const uint32_t* order_lists;
+  uint32_t order_cap;
+  float order_scale;      // buckets per walk step: kOrderBuckets / (longest possible walk)
   uint32_t tile_start[MaxF + 1];
   int32_t tiles_x[MaxF];
   FrameParams fr[MaxF];
@@ -188,6 +194,27 @@ struct DepthParams {
 template <int MaxF>
 cudaError_t launch_traverse_labels(const TickWork<MaxF>& w, const MapView& m, int rounding,
                                    cudaStream_t s);
+// Claim order of a traversal's tiles, longest walks first: kOrderBuckets buckets of the tiles'
+// longest-ray walk estimates (bucket 0 = longest), each with its list of tiles.
+constexpr int kOrderBuckets = 64;
+struct TileOrderBuffers {
+  uint32_t* counts;  // kOrderBuckets words, cleared before each pass
+  uint32_t* lists;   // kOrderBuckets * capacity words
+  uint32_t capacity; // tiles per list
+};
+// Sizes (or grows) the buffers for `tiles` tiles.
+cudaError_t tile_order_reserve(TileOrderBuffers* b, uint32_t tiles, cudaStream_t s);
+void tile_order_release(TileOrderBuffers* b);
+// kOrderBuckets / the longest walk any ray of these frames can take (steps + set-up).
+template <int MaxF>
+float tile_order_scale(const TickWork<MaxF>& w);
+// Clears the counts and files every tile under the bucket of its longest ray's walk (|R p|_1
+// / res, the DDA's step count up to rounding, plus a set-up allowance).
+template <int MaxF>
+cudaError_t launch_tile_order(const TickWork<MaxF>& w, const TileOrderBuffers& b, cudaStream_t s);
+cudaError_t launch_tile_order_dev(const TickWork<kMaxTickFrames>* d_work, uint32_t total_tiles,
+                                  const TileOrderBuffers& b, cudaStream_t s);
+
 // Dynamic shared memory of one traversal CTA (leaf table, ray order, rendered ranges).
 size_t traverse_smem_bytes(int tile_w, int tile_h, uint32_t smask, bool render);
 // Whether a frame fits the fused render + traversal (reach within the leaf code's range).

@@ -87,6 +87,7 @@ struct nm_map_s {
   unsigned int* h_status = nullptr;   // page-locked copy of the map's status words
   int tile_w = 16, tile_h = 16, smem_entries = 128;
   nm::FilterBuffers filter{};  // voxel-filter buffers, grown on first filtered insert
+  nm::TileOrderBuffers tile_order{};  // claim order of traversal tiles, grown on demand
   double* depth_scratch = nullptr;  // expected-depth partial sums (grown on demand)
   size_t depth_scratch_n = 0;
 };

@@ -35,6 +35,7 @@
 // (nm_sim_insert), so one launch does the simulated frame and its insertion.
 #include <cfloat>
 #include <climits>
+#include <algorithm>
 #include <cstdint>
 #include <mutex>
 
@@ -312,14 +313,41 @@ __device__ __forceinline__ void traverse_body(const TickWork<MaxF>& work, const 
   const int nthreads = blockDim.x;
   const int rounds = nrays / nthreads;
   uint32_t visits = 0, rays = 0;
+  // claim order: the first tiles of the queue are those of bucket 0 (longest walks), ...
+  __shared__ uint32_t s_pre[kOrderBuckets + 1];
+  if (work.order_counts) {
+    if (tid < 32) {
+      const uint32_t c0 = __ldcg(&work.order_counts[2 * lane]);
+      const uint32_t c1 = __ldcg(&work.order_counts[2 * lane + 1]);
+      uint32_t incl = c0 + c1;
+#pragma unroll
+      for (int o = 1; o < 32; o <<= 1) {
+        const uint32_t u = __shfl_up_sync(kFull, incl, o);
+        if (lane >= o) incl += u;
+      }
+      s_pre[2 * lane] = incl - c0 - c1;
+      s_pre[2 * lane + 1] = incl - c1;
+      if (lane == 31) s_pre[kOrderBuckets] = incl;
+    }
+    __syncthreads();
+  }
 
   for (;;) {
     if (tid == 0) {
       unsigned int* queue = work.queue ? &m.ctr->chunk_queue[work.queue - 1] : &m.ctr->tile_queue;
       const uint32_t t = atomicAdd(queue, 1u);
+      uint32_t tl = t;
+      if (work.order_counts && t < s_pre[kOrderBuckets]) {
+        int lo = 0, hi = kOrderBuckets - 1;  // the bucket b with s_pre[b] <= t < s_pre[b + 1]
+        while (lo < hi) {
+          const int mid = (lo + hi + 1) >> 1;
+          if (s_pre[mid] <= t) lo = mid; else hi = mid - 1;
+        }
+        tl = __ldcg(&work.order_lists[(size_t)lo * work.order_cap + (t - s_pre[lo])]);
+      }
       int fi = 0;
-      while (fi + 1 < work.n_frames && work.tile_start[fi + 1] <= t) ++fi;
-      s_tile = t;
+      while (fi + 1 < work.n_frames && work.tile_start[fi + 1] <= tl) ++fi;
+      s_tile = tl;
       s_frame = fi;
       if (t == work.total_tiles + gridDim.x - 1) *queue = 0u;  // last reader resets
     }
@@ -460,6 +488,70 @@ __device__ __forceinline__ void traverse_body(const TickWork<MaxF>& work, const 
     atomicAdd(&m.ctr->visits, vv);
     atomicAdd(&m.ctr->rays, rr);
   }
+}
+
+// ---- tile order (longest walks first) --------------------------------------------------------
+//
+// A frame's walk is bounded by its longest rays: a step costs a warp ~70 instructions issued
+// at one per ~11 cycles while the SM's other warps run, so a 350-step ray takes most of a
+// frame's traversal.  Claiming the tiles in decreasing order of their longest ray starts those
+// rays first.  One warp per tile takes the largest |R p|_1 / res over the tile's rays (the
+// DDA's step count up to rounding) plus kSetupSteps, scales it to one of kOrderBuckets
+// buckets, and appends the tile to that bucket's list (order inside a bucket is arbitrary).
+constexpr float kSetupSteps = 8.0f;
+constexpr int kOrderThreads = 256;
+
+template <int MaxF>
+__device__ __forceinline__ void tile_order_body(const TickWork<MaxF>& work, TileOrderBuffers b) {
+  const int lane = threadIdx.x & 31;
+  const uint32_t tile = (blockIdx.x * blockDim.x + threadIdx.x) >> 5;
+  if (tile >= work.total_tiles) return;
+  const int nrays = work.tile_w * work.tile_h;
+  int fi = 0;
+  while (fi + 1 < work.n_frames && work.tile_start[fi + 1] <= tile) ++fi;
+  const FrameParams& f = work.fr[fi];
+  const uint32_t lt = tile - work.tile_start[fi];
+  const int x0 = (int)(lt % (uint32_t)work.tiles_x[fi]) * work.tile_w;
+  const int y0 = (int)(lt / (uint32_t)work.tiles_x[fi]) * work.tile_h;
+  const float inv_res = (float)(1.0 / f.res_d);
+  float longest = 0.0f;
+  for (int k = lane; k < nrays; k += 32) {
+    const int px = x0 + k % work.tile_w, py = y0 + k / work.tile_w;
+    float p[3];
+    if (px < f.width && py < f.height && pixel_point(f, px, py, p)) {
+      const float* R = f.R;
+      const float x = R[0] * p[0] + R[1] * p[1] + R[2] * p[2];
+      const float y = R[3] * p[0] + R[4] * p[1] + R[5] * p[2];
+      const float z = R[6] * p[0] + R[7] * p[1] + R[8] * p[2];
+      const float len = sqrtf(x * x + y * y + z * z) * inv_res;
+      if (len < f.max_time)
+        longest = fmaxf(longest, (fabsf(x) + fabsf(y) + fabsf(z)) * inv_res + kSetupSteps);
+    }
+  }
+#pragma unroll
+  for (int o = 16; o > 0; o >>= 1) longest = fmaxf(longest, __shfl_xor_sync(kFull, longest, o));
+  if (lane == 0) {
+    const float q = longest * work.order_scale;
+    const int bkt = kOrderBuckets - 1 - (q < (float)(kOrderBuckets - 1) ? (int)q : kOrderBuckets - 1);
+    const uint32_t r = atomicAdd(&b.counts[bkt], 1u);
+    b.lists[(size_t)bkt * b.capacity + r] = tile;
+  }
+}
+
+template <int MaxF>
+__global__ void __launch_bounds__(kOrderThreads) k_tile_order(const __grid_constant__ TickWork<MaxF> work,
+                                                              TileOrderBuffers b) {
+  tile_order_body<MaxF>(work, b);
+}
+
+__global__ void __launch_bounds__(kOrderThreads) k_tile_order_dev(const TickWork<kMaxTickFrames>* work,
+                                                                  TileOrderBuffers b) {
+  tile_order_body<kMaxTickFrames>(*work, b);
+}
+
+int order_grid(uint32_t total_tiles) {
+  const uint32_t warps = kOrderThreads / 32;
+  return (int)((total_tiles + warps - 1) / warps);
 }
 
 // Label sink of the wide-frame kernel: device-table lookups on leaf changes, one atomic per
@@ -710,6 +802,59 @@ cudaError_t launch_traverse_labels_dev(const TickWork<kMaxTickFrames>* d_work, u
   return cudaGetLastError();
 }
 
+cudaError_t tile_order_reserve(TileOrderBuffers* b, uint32_t tiles, cudaStream_t s) {
+  if (tiles <= b->capacity && b->counts) return cudaSuccess;
+  tile_order_release(b);
+  const uint32_t cap = std::max<uint32_t>(tiles, 4096u);
+  cudaError_t e = cudaMalloc((void**)&b->counts, kOrderBuckets * 4);
+  if (e == cudaSuccess) e = cudaMalloc((void**)&b->lists, (size_t)kOrderBuckets * cap * 4);
+  if (e == cudaSuccess) e = cudaMemsetAsync(b->counts, 0, kOrderBuckets * 4, s);
+  if (e != cudaSuccess) {
+    tile_order_release(b);
+    return e;
+  }
+  b->capacity = cap;
+  return cudaSuccess;
+}
+
+void tile_order_release(TileOrderBuffers* b) {
+  cudaFree(b->counts);
+  cudaFree(b->lists);
+  *b = TileOrderBuffers{};
+}
+
+template <int MaxF>
+float tile_order_scale(const TickWork<MaxF>& w) {
+  float longest = 0.0f;
+  for (int i = 0; i < w.n_frames; ++i) longest = std::max(longest, w.fr[i].max_time);
+  return (float)kOrderBuckets / (longest * 1.7320508f + kSetupSteps);
+}
+
+template <int MaxF>
+cudaError_t launch_tile_order(const TickWork<MaxF>& w, const TileOrderBuffers& b, cudaStream_t s) {
+  if (w.total_tiles == 0) return cudaSuccess;
+  if (w.total_tiles > b.capacity) return cudaErrorInvalidValue;
+  cudaError_t e = cudaMemsetAsync(b.counts, 0, kOrderBuckets * 4, s);
+  if (e != cudaSuccess) return e;
+  k_tile_order<MaxF><<<order_grid(w.total_tiles), kOrderThreads, 0, s>>>(w, b);
+  return cudaGetLastError();
+}
+
+cudaError_t launch_tile_order_dev(const TickWork<kMaxTickFrames>* d_work, uint32_t total_tiles,
+                                  const TileOrderBuffers& b, cudaStream_t s) {
+  if (total_tiles == 0) return cudaSuccess;
+  if (total_tiles > b.capacity) return cudaErrorInvalidValue;
+  cudaError_t e = cudaMemsetAsync(b.counts, 0, kOrderBuckets * 4, s);
+  if (e != cudaSuccess) return e;
+  k_tile_order_dev<<<order_grid(total_tiles), kOrderThreads, 0, s>>>(d_work, b);
+  return cudaGetLastError();
+}
+
+template float tile_order_scale<1>(const TickWork<1>&);
+template float tile_order_scale<kMaxTickFrames>(const TickWork<kMaxTickFrames>&);
+template cudaError_t launch_tile_order<1>(const TickWork<1>&, const TileOrderBuffers&, cudaStream_t);
+template cudaError_t launch_tile_order<kMaxTickFrames>(const TickWork<kMaxTickFrames>&,
+                                                       const TileOrderBuffers&, cudaStream_t);
 template cudaError_t launch_traverse_labels<1>(const TickWork<1>&, const MapView&, int, cudaStream_t);
 template cudaError_t launch_traverse_labels<kMaxTickFrames>(const TickWork<kMaxTickFrames>&,
                                                             const MapView&, int, cudaStream_t);
