@@ -1122,6 +1122,9 @@ def run_batched(args, rank, world, local, ticks):
     kinds = {}
     mk = A.Map(ctx, A.map_desc(res=res, rounding=N.NM_ROUND_DOWN, initial_leaf_capacity=cap))
     per = [[] for _ in range(n)]
+    for a in range(n):  # one untimed frame per agent first (the map's buffers grow here)
+        sim.render(sensors[a], trajs[a][0], bufs[a], stream=stream)
+        mk.insert_ranges(sensors[a], trajs[a][0], bufs[a], stream=stream)
     for t in range(min(10, timed)):
         flush.fill_(t & 255)
         row = []

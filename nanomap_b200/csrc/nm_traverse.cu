@@ -804,8 +804,10 @@ cudaError_t launch_traverse_labels_dev(const TickWork<kMaxTickFrames>* d_work, u
 
 cudaError_t tile_order_reserve(TileOrderBuffers* b, uint32_t tiles, cudaStream_t s) {
   if (tiles <= b->capacity && b->counts) return cudaSuccess;
+  // growth frees the old buffers (a device synchronisation): start at 16 K tiles (a 1280x720
+  // frame has 7200 tiles of 16x8) and double
+  const uint32_t cap = std::max<uint32_t>(tiles, std::max<uint32_t>(1u << 14, 2u * b->capacity));
   tile_order_release(b);
-  const uint32_t cap = std::max<uint32_t>(tiles, 4096u);
   cudaError_t e = cudaMalloc((void**)&b->counts, kOrderBuckets * 4);
   if (e == cudaSuccess) e = cudaMalloc((void**)&b->lists, (size_t)kOrderBuckets * cap * 4);
   if (e == cudaSuccess) e = cudaMemsetAsync(b->counts, 0, kOrderBuckets * 4, s);
