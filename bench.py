@@ -923,7 +923,6 @@ def run_cave_section(local, cpu=True, reps=3):
     import torch
 
     from nanomap_b200 import api as A
-    from oracle import oracle as O
     ctx = A.Context(local)
     stream = torch.cuda.default_stream()
     out = {}
@@ -969,6 +968,7 @@ def run_cave_section(local, cpu=True, reps=3):
         }
         g.close()
     if cpu:
+        from oracle import oracle as O
         kw = CAVE_WORKLOADS["shipped"]
         o = O.Cave(kw["map_size"], kw["grid_res"], kw["fill_percentage"], kw["smoothing_count"],
                    kw["active_max"], kw["active_min"], kw["seed"])
