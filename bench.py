@@ -365,11 +365,24 @@ def run_ours(args, rank, world, local):
         e1 = m2.stats()
         dt = allreduce_max(dt)
         ev_all = allreduce_sum(e1["visits"] - e0["visits"])
+        # the host link alone: one frame's records copied from pinned memory (outside the timing)
+        dev_buf = torch.empty_like(host_recs[0], device=dev)
+        lt = []
+        for k in range(10):
+            c0, c1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+            c0.record(stream)
+            dev_buf.copy_(host_recs[k % n_frames], non_blocking=True)
+            c1.record(stream)
+            torch.cuda.synchronize()
+            lt.append(c0.elapsed_time(c1))
+        link_ms = statistics.median(lt)
         e2e = {"value": ev_all / dt, "unit": UNIT, "h2d_bytes_per_step": H * W * 16,
                "d2h_bytes_per_step": 8, "steps": args.e2e_steps,
                "ms_per_step": dt * 1e3 / args.e2e_steps,
                "path": "nm_map_insert_points(host xyz records, step 16, NM_SYNC)",
-               "l2": "flushed before each step, outside the timed call"}
+               "l2": "flushed before each step, outside the timed call",
+               "host_link": {"copy_ms": link_ms, "gbs": H * W * 16 / (link_ms / 1e3) / 1e9,
+                             "what": "one frame's records (pinned host -> device), alone"}}
         m2.close()
 
     # roofline of the dominant kernel (the traversal): algorithmic bytes per launch =
