@@ -20,8 +20,9 @@
 // hash source of a per-CTA shared-memory leaf table (32 label words per leaf).  A leaf that
 // finds no room in the table goes straight to the device table.
 //
-// Labels collect per 32-voxel word in a register and go to shared memory when the walk leaves
-// the word, with a shared atomic only when they add bits the word does not hold yet.  After a
+// Labels collect per 32-voxel word in a register and go to shared memory with one shared atomic
+// when the walk leaves the word (reading the word first to skip atomics that add no bits was
+// measured slower: the read costs more than the atomics it saves).  After a
 // tile, one lane per cached leaf ORs its words into the device label buffer and puts the leaf
 // on the touched list (the device-table lookups of a warp's leaves overlap).
 //
@@ -236,7 +237,6 @@ __device__ __forceinline__ uint32_t walk_ray(const Ray& r, const TileTable& tt, 
   int wbase = leaf_base(tt, m, code, epoch, plane);
   int cw = kLostWord;  // word the pending bits belong to
   uint32_t acc = 0u;   // pending miss bits of word cw
-  uint32_t known = 0u; // bits word cw held when the walk entered it
   uint32_t n = 0u;
   double t;
   for (;;) {
@@ -248,10 +248,9 @@ __device__ __forceinline__ uint32_t walk_ray(const Ray& r, const TileTable& tt, 
     // miss label of the voxel being left
     const int wi = wbase + (l >> 5);
     if (wi != cw) {
-      if (acc & ~known) flush_word(tt.words, m, cw, acc, plane);
+      if (acc) flush_word(tt.words, m, cw, acc, plane);
       cw = wi;
       acc = 0u;
-      known = wi >= 0 ? ((volatile uint32_t*)tt.words)[wi] : 0u;
     }
     acc |= 1u << (l & 31);
     ++n;
@@ -270,7 +269,7 @@ __device__ __forceinline__ uint32_t walk_ray(const Ray& r, const TileTable& tt, 
       wbase = leaf_base(tt, m, code, epoch, plane);
     }
   }
-  if (acc & ~known) flush_word(tt.words, m, cw, acc, plane);
+  if (acc) flush_word(tt.words, m, cw, acc, plane);
   if (t < max_time) {
     if (wbase >= 0)
       atomicOr(&tt.words[wbase - 16 + (l >> 5)], 1u << (l & 31));
