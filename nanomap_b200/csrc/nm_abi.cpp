@@ -369,11 +369,11 @@ nm::IntegrateParams integrate_params(nm_map m) {
   return p;
 }
 
-int do_integrate(nm_map m, cudaStream_t s) {
+int do_integrate(nm_map m, cudaStream_t s, bool dependent) {
   if (!m->pending_labels) return NM_OK;
   const nm::IntegrateParams p = integrate_params(m);
   NM_CUDA(nm::launch_integrate(m->view, p, m->desc.update_mode, m->desc.rounding,
-                               m->ctx->sm_count, s));
+                               m->ctx->sm_count, s, dependent));
   m->pending_labels = false;
   m->pending_planes = 0;
   m->epoch += 1;
@@ -551,6 +551,7 @@ int run_frame(nm_map m, nm_sensor s, nm::FrameParams& f, uint32_t flags, cudaStr
   if (rc != NM_OK) return rc;
   f.epoch = m->epoch;
   f.plane = 0;
+  bool dependent_integrate = false;  // the integration directly follows a traversal kernel
   if (m->desc.update_mode == NM_UPDATE_LABEL) {
     nm::TickWork<1> w;
     std::memset(&w, 0, sizeof(w));
@@ -573,26 +574,32 @@ int run_frame(nm_map m, nm_sensor s, nm::FrameParams& f, uint32_t flags, cudaStr
     if (w.total_tiles > 0) {
       if (sim) {
         NM_CUDA(nm::launch_traverse_render(w, m->view, *sim, m->desc.rounding, s0));
+        dependent_integrate = true;
       } else {
         // longest walks first (frames within the leaf code's reach; the others take the
         // table-free traversal, which claims no tiles)
-        if (f.max_time < nm::kNarrowMaxTime) {
+        const bool ordered = f.max_time < nm::kNarrowMaxTime;
+        if (ordered) {
           NM_CUDA(nm::tile_order_reserve(&m->tile_order, w.total_tiles, s0));
           w.order_scale = nm::tile_order_scale<1>(w);
-          NM_CUDA(nm::launch_tile_order<1>(w, m->tile_order, s0));
+          NM_CUDA(nm::launch_tile_order<1>(w, &m->tile_order, s0));
           w.order_counts = m->tile_order.counts;
           w.order_lists = m->tile_order.lists;
           w.order_cap = m->tile_order.capacity;
         }
-        NM_CUDA(nm::launch_traverse_labels<1>(w, m->view, m->desc.rounding, s0));
+        // the walk's CTAs start while the order pass finishes
+        NM_CUDA(nm::launch_traverse_labels<1>(w, m->view, m->desc.rounding, s0, ordered));
+        if (ordered) m->tile_order.pending = false;
+        dependent_integrate = true;
       }
     }
   } else {
     NM_CUDA(nm::launch_traverse_counts(f, m->view, m->desc.rounding, s0));
+    dependent_integrate = true;
   }
   m->pending_labels = true;
   if (!(flags & NM_DEFER_INTEGRATE)) {
-    rc = do_integrate(m, s0);
+    rc = do_integrate(m, s0, dependent_integrate);
     if (rc != NM_OK) return rc;
   }
   if (flags & NM_SYNC) return check_device_errors(m, s0);
@@ -1197,16 +1204,17 @@ int nm_map_tick(nm_map m, const nm_frame* frames, int32_t n_frames, uint32_t fla
     if (!wide) {  // longest walks first
       NM_CUDA(nm::tile_order_reserve(&m->tile_order, w->total_tiles, s0));
       w->order_scale = nm::tile_order_scale<nm::kMaxTickFrames>(*w);
-      NM_CUDA(nm::launch_tile_order<nm::kMaxTickFrames>(*w, m->tile_order, s0));
+      NM_CUDA(nm::launch_tile_order<nm::kMaxTickFrames>(*w, &m->tile_order, s0));
       w->order_counts = m->tile_order.counts;
       w->order_lists = m->tile_order.lists;
       w->order_cap = m->tile_order.capacity;
     }
-    NM_CUDA(nm::launch_traverse_labels<nm::kMaxTickFrames>(*w, m->view, m->desc.rounding, s0));
+    NM_CUDA(nm::launch_traverse_labels<nm::kMaxTickFrames>(*w, m->view, m->desc.rounding, s0, !wide));
+    if (!wide) m->tile_order.pending = false;
   }
   m->pending_labels = true;
   if (!(flags & NM_DEFER_INTEGRATE)) {
-    rc = do_integrate(m, s0);
+    rc = do_integrate(m, s0, w->total_tiles > 0);
     if (rc != NM_OK) return rc;
   }
   if (flags & NM_SYNC) return check_device_errors(m, s0);

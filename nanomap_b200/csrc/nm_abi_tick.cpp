@@ -133,11 +133,13 @@ int capture(nm_tick_plan p, int k, bool defer) {
   if (e == cudaSuccess && p->sim)
     e = nm::launch_render_batch(&p->d_stage->render, render_tiles, p->sim->view, p->cap_stream);
   if (e == cudaSuccess && total_tiles > 0 && !wide)  // longest walks first
-    e = nm::launch_tile_order_dev(&p->d_stage->work, total_tiles, p->order, p->cap_stream);
+    e = nm::launch_tile_order_dev(&p->d_stage->work, total_tiles, &p->order, p->cap_stream);
   if (e == cudaSuccess && total_tiles > 0)
     e = nm::launch_traverse_labels_dev(&p->d_stage->work, total_tiles, p->tile_w, p->tile_h,
                                        (uint32_t)p->entries - 1u, m->view, m->desc.rounding,
                                        wide, p->cap_stream);
+  if (e == cudaSuccess && total_tiles > 0 && !wide)
+    p->order.pending = false;  // the graph's traversal clears the counts its order pass fills
   if (e == cudaSuccess && !defer)
     e = nm::launch_integrate(m->view, p->integ, m->desc.update_mode, m->desc.rounding,
                              m->ctx->sm_count, p->cap_stream);

@@ -9,6 +9,17 @@
 
 namespace nm {
 
+// Programmatic dependent launch.  A kernel launched with programmatic stream serialisation
+// may start while the kernel before it on the stream still runs; it calls wait_prior_grid()
+// before its first access to memory that kernel writes, which returns once that kernel has
+// finished and its writes are visible.  allow_dependent_launch() tells the hardware that this
+// CTA no longer needs to hold the dependent back.  Both are no-ops when the launch carries no
+// dependency.
+__device__ __forceinline__ void wait_prior_grid() { asm volatile("griddepcontrol.wait;" ::: "memory"); }
+__device__ __forceinline__ void allow_dependent_launch() {
+  asm volatile("griddepcontrol.launch_dependents;" ::: "memory");
+}
+
 // Arithmetic with an explicit rounding mode.  Every product and sum is rounded on its own
 // (the intrinsics are never contracted into fused multiply-adds), so the device reproduces
 // the CPU oracle bit for bit under the same policy.

@@ -109,8 +109,9 @@ struct TickWork {
   uint32_t total_tiles;
   uint32_t queue;         // 0: MapCounters::tile_queue; c + 1: chunk_queue[c]
   // claim order of the tiles (longest walks first; null = tile order): the number of tiles in
-  // each of kOrderBuckets walk-length buckets, and bucket b's tiles at order_lists[b * order_cap]
-  const uint32_t* order_counts;
+  // each of kOrderBuckets walk-length buckets, and bucket b's tiles at order_lists[b * order_cap];
+  // the traversal zeroes the counts once every CTA has read them, for the next order pass
+  uint32_t* order_counts;
   const uint32_t* order_lists;
   uint32_t order_cap;
   float order_scale;      // buckets per walk step: kOrderBuckets / (longest possible walk)
@@ -191,16 +192,20 @@ struct DepthParams {
 };
 
 // ---- kernel launchers (defined in the .cu files) -----------------------------------------
+// `dependent`: launched as a programmatic dependent of the preceding kernel on the stream (its
+// CTAs start while that kernel finishes and wait for it before reading anything); not for
+// stream capture.
 template <int MaxF>
 cudaError_t launch_traverse_labels(const TickWork<MaxF>& w, const MapView& m, int rounding,
-                                   cudaStream_t s);
+                                   cudaStream_t s, bool dependent = false);
 // Claim order of a traversal's tiles, longest walks first: kOrderBuckets buckets of the tiles'
 // longest-ray walk estimates (bucket 0 = longest), each with its list of tiles.
 constexpr int kOrderBuckets = 64;
 struct TileOrderBuffers {
-  uint32_t* counts;  // kOrderBuckets words, cleared before each pass
+  uint32_t* counts;  // kOrderBuckets words, zero between passes (the traversal clears them)
   uint32_t* lists;   // kOrderBuckets * capacity words
   uint32_t capacity; // tiles per list
+  bool pending;      // host side: a pass was launched and its traversal not (yet)
 };
 // Sizes (or grows) the buffers for `tiles` tiles.
 cudaError_t tile_order_reserve(TileOrderBuffers* b, uint32_t tiles, cudaStream_t s);
@@ -208,12 +213,14 @@ void tile_order_release(TileOrderBuffers* b);
 // kOrderBuckets / the longest walk any ray of these frames can take (steps + set-up).
 template <int MaxF>
 float tile_order_scale(const TickWork<MaxF>& w);
-// Clears the counts and files every tile under the bucket of its longest ray's walk (|R p|_1
-// / res, the DDA's step count up to rounding, plus a set-up allowance).
+// Files every tile under the bucket of its longest ray's walk (|R p|_1 / res, the DDA's step
+// count up to rounding, plus a set-up allowance).  The counts are zero on entry: the traversal
+// that reads a pass's lists clears them; `b.pending` (a pass whose traversal was never launched)
+// clears them first.
 template <int MaxF>
-cudaError_t launch_tile_order(const TickWork<MaxF>& w, const TileOrderBuffers& b, cudaStream_t s);
+cudaError_t launch_tile_order(const TickWork<MaxF>& w, TileOrderBuffers* b, cudaStream_t s);
 cudaError_t launch_tile_order_dev(const TickWork<kMaxTickFrames>* d_work, uint32_t total_tiles,
-                                  const TileOrderBuffers& b, cudaStream_t s);
+                                  TileOrderBuffers* b, cudaStream_t s);
 
 // Dynamic shared memory of one traversal CTA (leaf table, ray order, rendered ranges).
 size_t traverse_smem_bytes(int tile_w, int tile_h, uint32_t smask, bool render);
@@ -226,7 +233,7 @@ cudaError_t launch_traverse_labels_dev(const TickWork<kMaxTickFrames>* d_work, u
 cudaError_t launch_traverse_counts(const FrameParams& f, const MapView& m, int rounding,
                                    cudaStream_t s);
 cudaError_t launch_integrate(const MapView& m, const IntegrateParams& p, int update_mode,
-                             int rounding, int sm_count, cudaStream_t s);
+                             int rounding, int sm_count, cudaStream_t s, bool dependent = false);
 // Queries the integration kernels' resident blocks per SM ahead of any stream capture.
 void prepare_integrate();
 cudaError_t launch_rehash(const MapView& from, const MapView& to, uint32_t cur_epoch,

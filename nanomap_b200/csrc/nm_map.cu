@@ -114,6 +114,7 @@ __device__ __forceinline__ float update_voxel(float v, uint32_t& abit, float tem
 __device__ __forceinline__ void read_integrate_counters(const MapCounters* ctr, uint32_t* n,
                                                         bool* fatal) {
   __shared__ uint32_t s_n, s_err;
+  wait_prior_grid();  // the walk that fills the counters may still run at launch
   if (threadIdx.x == 0) {
     s_n = *(const volatile unsigned int*)&ctr->touched_count;
     s_err = *(const volatile unsigned int*)&ctr->error_flags;
@@ -404,31 +405,44 @@ int integrate_blocks_per_sm(Kernel kernel, int variant) {
 
 template <typename Kernel>
 cudaError_t launch_integrate_kernel(Kernel kernel, int variant, const MapView& m,
-                                    const IntegrateParams& p, int sm_count, cudaStream_t s) {
-  const int blocks = sm_count * integrate_blocks_per_sm(kernel, variant);
-  kernel<<<blocks, 256, 0, s>>>(m, p);
+                                    const IntegrateParams& p, int sm_count, cudaStream_t s,
+                                    bool dependent) {
+  cudaLaunchConfig_t cfg = {};
+  cfg.gridDim = dim3(sm_count * integrate_blocks_per_sm(kernel, variant));
+  cfg.blockDim = dim3(256);
+  cfg.stream = s;
+  cudaLaunchAttribute attr[1];
+  attr[0].id = cudaLaunchAttributeProgrammaticStreamSerialization;
+  attr[0].val.programmaticStreamSerializationAllowed = 1;
+  cfg.attrs = attr;
+  cfg.numAttrs = dependent ? 1 : 0;
+  const cudaError_t e = cudaLaunchKernelEx(&cfg, kernel, m, p);
+  if (e != cudaSuccess) return e;
   return cudaGetLastError();
 }
 
 template <int RM, bool Always>
 cudaError_t launch_integrate_t(const MapView& m, const IntegrateParams& p, bool label,
-                               int sm_count, cudaStream_t s) {
+                               int sm_count, cudaStream_t s, bool dependent) {
   const int variant = (label ? 4 : 0) + (RM == NM_ROUND_DOWN ? 2 : 0) + (Always ? 1 : 0);
-  if (label) return launch_integrate_kernel(k_integrate_label<RM, Always>, variant, m, p, sm_count, s);
-  return launch_integrate_kernel(k_integrate_count<RM, Always>, variant, m, p, sm_count, s);
+  if (label)
+    return launch_integrate_kernel(k_integrate_label<RM, Always>, variant, m, p, sm_count, s,
+                                   dependent);
+  return launch_integrate_kernel(k_integrate_count<RM, Always>, variant, m, p, sm_count, s,
+                                 dependent);
 }
 
 }  // namespace
 
 cudaError_t launch_integrate(const MapView& m, const IntegrateParams& p, int update_mode,
-                             int rounding, int sm_count, cudaStream_t s) {
+                             int rounding, int sm_count, cudaStream_t s, bool dependent) {
   const bool label = update_mode == NM_UPDATE_LABEL;
   const bool always = p.clamp_mode == NM_CLAMP_ALWAYS;
   if (rounding == NM_ROUND_DOWN)
-    return always ? launch_integrate_t<NM_ROUND_DOWN, true>(m, p, label, sm_count, s)
-                  : launch_integrate_t<NM_ROUND_DOWN, false>(m, p, label, sm_count, s);
-  return always ? launch_integrate_t<NM_ROUND_NEAREST, true>(m, p, label, sm_count, s)
-                : launch_integrate_t<NM_ROUND_NEAREST, false>(m, p, label, sm_count, s);
+    return always ? launch_integrate_t<NM_ROUND_DOWN, true>(m, p, label, sm_count, s, dependent)
+                  : launch_integrate_t<NM_ROUND_DOWN, false>(m, p, label, sm_count, s, dependent);
+  return always ? launch_integrate_t<NM_ROUND_NEAREST, true>(m, p, label, sm_count, s, dependent)
+                : launch_integrate_t<NM_ROUND_NEAREST, false>(m, p, label, sm_count, s, dependent);
 }
 
 void prepare_integrate() {

@@ -137,7 +137,9 @@ double ray_leaf_cap(nm_map m, nm_sensor s, uint64_t n_rays);
 int ensure_capacity(nm_map m, uint64_t bound, cudaStream_t s);
 int set_plane_constants(nm_map m, int plane, nm_sensor s);
 IntegrateParams integrate_params(nm_map m);
-int do_integrate(nm_map m, cudaStream_t s);
+// `dependent`: the last operation on `s` is a traversal kernel, so the integration may be
+// launched as its programmatic dependent.
+int do_integrate(nm_map m, cudaStream_t s, bool dependent = false);
 int check_device_errors(nm_map m, cudaStream_t s);
 int validate_pose(const nm_pose* pose);
 // Ray parameters of a sensor at a pose over a sim map of voxel size `res`.

@@ -312,6 +312,7 @@ __device__ __forceinline__ void traverse_body(const TickWork<MaxF>& work, const 
   const int nthreads = blockDim.x;
   const int rounds = nrays / nthreads;
   uint32_t visits = 0, rays = 0;
+  wait_prior_grid();
   // claim order: the first tiles of the queue are those of bucket 0 (longest walks), ...
   __shared__ uint32_t s_pre[kOrderBuckets + 1];
   if (work.order_counts) {
@@ -348,11 +349,19 @@ __device__ __forceinline__ void traverse_body(const TickWork<MaxF>& work, const 
       while (fi + 1 < work.n_frames && work.tile_start[fi + 1] <= tl) ++fi;
       s_tile = tl;
       s_frame = fi;
-      if (t == work.total_tiles + gridDim.x - 1) *queue = 0u;  // last reader resets
+      if (t == work.total_tiles + gridDim.x - 1) {  // last reader resets
+        *queue = 0u;
+        // every CTA read the counts before its first claim: clear them for the next pass
+        if (work.order_counts)
+          for (int b = 0; b < kOrderBuckets; ++b) work.order_counts[b] = 0u;
+      }
     }
     __syncthreads();
     const uint32_t tile = s_tile;
-    if (tile >= work.total_tiles) break;
+    if (tile >= work.total_tiles) {
+      allow_dependent_launch();  // the integration may start its CTAs on freed SMs
+      break;
+    }
     const int fi = s_frame;
     {
       const uint32_t* src = reinterpret_cast<const uint32_t*>(&work.fr[fi]);
@@ -502,6 +511,7 @@ constexpr int kOrderThreads = 256;
 
 template <int MaxF>
 __device__ __forceinline__ void tile_order_body(const TickWork<MaxF>& work, TileOrderBuffers b) {
+  allow_dependent_launch();  // the walk's CTAs launch now and wait for this pass to finish
   const int lane = threadIdx.x & 31;
   const uint32_t tile = (blockIdx.x * blockDim.x + threadIdx.x) >> 5;
   if (tile >= work.total_tiles) return;
@@ -533,7 +543,7 @@ __device__ __forceinline__ void tile_order_body(const TickWork<MaxF>& work, Tile
     const float q = longest * work.order_scale;
     const int bkt = kOrderBuckets - 1 - (q < (float)(kOrderBuckets - 1) ? (int)q : kOrderBuckets - 1);
     const uint32_t r = atomicAdd(&b.counts[bkt], 1u);
-    b.lists[(size_t)bkt * b.capacity + r] = tile;
+    if (r < b.capacity) b.lists[(size_t)bkt * b.capacity + r] = tile;
   }
 }
 
@@ -710,7 +720,7 @@ size_t traverse_smem_bytes(int tile_w, int tile_h, uint32_t smask, bool render) 
 
 template <int MaxF>
 cudaError_t launch_traverse_labels(const TickWork<MaxF>& w, const MapView& m, int rounding,
-                                   cudaStream_t s) {
+                                   cudaStream_t s, bool dependent) {
   const int block = min(256, w.tile_w * w.tile_h);
   const bool down = rounding == NM_ROUND_DOWN;
   int grid = 0;
@@ -732,10 +742,21 @@ cudaError_t launch_traverse_labels(const TickWork<MaxF>& w, const MapView& m, in
   cudaError_t e = resident_grid(fn, smem, block, &grid);
   if (e != cudaSuccess) return e;
   grid = min(grid, (int)w.total_tiles);
+  cudaLaunchConfig_t cfg = {};
+  cfg.gridDim = dim3(grid);
+  cfg.blockDim = dim3(block);
+  cfg.dynamicSmemBytes = smem;
+  cfg.stream = s;
+  cudaLaunchAttribute attr[1];
+  attr[0].id = cudaLaunchAttributeProgrammaticStreamSerialization;
+  attr[0].val.programmaticStreamSerializationAllowed = 1;
+  cfg.attrs = attr;
+  cfg.numAttrs = dependent ? 1 : 0;
   if (down)
-    k_traverse<NM_ROUND_DOWN, MaxF><<<grid, block, smem, s>>>(w, m);
+    e = cudaLaunchKernelEx(&cfg, k_traverse<NM_ROUND_DOWN, MaxF>, w, m);
   else
-    k_traverse<NM_ROUND_NEAREST, MaxF><<<grid, block, smem, s>>>(w, m);
+    e = cudaLaunchKernelEx(&cfg, k_traverse<NM_ROUND_NEAREST, MaxF>, w, m);
+  if (e != cudaSuccess) return e;
   return cudaGetLastError();
 }
 
@@ -815,6 +836,7 @@ cudaError_t tile_order_reserve(TileOrderBuffers* b, uint32_t tiles, cudaStream_t
     return e;
   }
   b->capacity = cap;
+  b->pending = false;
   return cudaSuccess;
 }
 
@@ -831,33 +853,47 @@ float tile_order_scale(const TickWork<MaxF>& w) {
   return (float)kOrderBuckets / (longest * 1.7320508f + kSetupSteps);
 }
 
+namespace {
+cudaError_t clear_pending_counts(TileOrderBuffers* b, cudaStream_t s) {
+  if (!b->pending) return cudaSuccess;
+  const cudaError_t e = cudaMemsetAsync(b->counts, 0, kOrderBuckets * 4, s);
+  if (e == cudaSuccess) b->pending = false;
+  return e;
+}
+}  // namespace
+
 template <int MaxF>
-cudaError_t launch_tile_order(const TickWork<MaxF>& w, const TileOrderBuffers& b, cudaStream_t s) {
+cudaError_t launch_tile_order(const TickWork<MaxF>& w, TileOrderBuffers* b, cudaStream_t s) {
   if (w.total_tiles == 0) return cudaSuccess;
-  if (w.total_tiles > b.capacity) return cudaErrorInvalidValue;
-  cudaError_t e = cudaMemsetAsync(b.counts, 0, kOrderBuckets * 4, s);
+  if (w.total_tiles > b->capacity) return cudaErrorInvalidValue;
+  cudaError_t e = clear_pending_counts(b, s);
   if (e != cudaSuccess) return e;
-  k_tile_order<MaxF><<<order_grid(w.total_tiles), kOrderThreads, 0, s>>>(w, b);
-  return cudaGetLastError();
+  k_tile_order<MaxF><<<order_grid(w.total_tiles), kOrderThreads, 0, s>>>(w, *b);
+  e = cudaGetLastError();
+  if (e == cudaSuccess) b->pending = true;
+  return e;
 }
 
 cudaError_t launch_tile_order_dev(const TickWork<kMaxTickFrames>* d_work, uint32_t total_tiles,
-                                  const TileOrderBuffers& b, cudaStream_t s) {
+                                  TileOrderBuffers* b, cudaStream_t s) {
   if (total_tiles == 0) return cudaSuccess;
-  if (total_tiles > b.capacity) return cudaErrorInvalidValue;
-  cudaError_t e = cudaMemsetAsync(b.counts, 0, kOrderBuckets * 4, s);
+  if (total_tiles > b->capacity) return cudaErrorInvalidValue;
+  cudaError_t e = clear_pending_counts(b, s);
   if (e != cudaSuccess) return e;
-  k_tile_order_dev<<<order_grid(total_tiles), kOrderThreads, 0, s>>>(d_work, b);
-  return cudaGetLastError();
+  k_tile_order_dev<<<order_grid(total_tiles), kOrderThreads, 0, s>>>(d_work, *b);
+  e = cudaGetLastError();
+  if (e == cudaSuccess) b->pending = true;
+  return e;
 }
 
 template float tile_order_scale<1>(const TickWork<1>&);
 template float tile_order_scale<kMaxTickFrames>(const TickWork<kMaxTickFrames>&);
-template cudaError_t launch_tile_order<1>(const TickWork<1>&, const TileOrderBuffers&, cudaStream_t);
+template cudaError_t launch_tile_order<1>(const TickWork<1>&, TileOrderBuffers*, cudaStream_t);
 template cudaError_t launch_tile_order<kMaxTickFrames>(const TickWork<kMaxTickFrames>&,
-                                                       const TileOrderBuffers&, cudaStream_t);
-template cudaError_t launch_traverse_labels<1>(const TickWork<1>&, const MapView&, int, cudaStream_t);
+                                                       TileOrderBuffers*, cudaStream_t);
+template cudaError_t launch_traverse_labels<1>(const TickWork<1>&, const MapView&, int, cudaStream_t,
+                                               bool);
 template cudaError_t launch_traverse_labels<kMaxTickFrames>(const TickWork<kMaxTickFrames>&,
-                                                            const MapView&, int, cudaStream_t);
+                                                            const MapView&, int, cudaStream_t, bool);
 
 }  // namespace nm
