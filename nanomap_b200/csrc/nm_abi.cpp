@@ -382,16 +382,16 @@ int do_integrate(nm_map m, cudaStream_t s, bool dependent) {
 }
 
 int check_device_errors(nm_map m, cudaStream_t s) {
-  // leaf_count, touched_count and error_flags are adjacent: one read
+  // leaf_count and error_flags are adjacent: one read
   static_assert(offsetof(nm::MapCounters, error_flags) ==
-                    offsetof(nm::MapCounters, leaf_count) + 8, "counter layout");
+                    offsetof(nm::MapCounters, leaf_count) + 4, "counter layout");
   // one round trip: the status words are copied into page-locked memory on the map's
   // stream, then the stream is waited for
   unsigned int* w = m->h_status;
-  NM_CUDA(cudaMemcpyAsync(w, &m->d_ctr->leaf_count, 3 * sizeof(unsigned int),
+  NM_CUDA(cudaMemcpyAsync(w, &m->d_ctr->leaf_count, 2 * sizeof(unsigned int),
                           cudaMemcpyDeviceToHost, s));
   NM_CUDA(cudaStreamSynchronize(s));
-  const unsigned int lc = w[0], flags = w[2];
+  const unsigned int lc = w[0], flags = w[1];
   m->known_leaves = lc;
   m->pending_bound = 0;
   if (flags & nm::kErrProbe)

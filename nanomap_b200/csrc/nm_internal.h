@@ -43,10 +43,12 @@ struct MapCounters {
   unsigned long long unique_voxels;
   unsigned long long touched_total;
   unsigned int leaf_count;
-  unsigned int touched_count;
   unsigned int error_flags;
-  unsigned int frames;
+  // one 8-byte word: the integration reads the frame's count and takes its block ticket with
+  // one 64-bit atomic
+  unsigned int touched_count;
   unsigned int done_blocks;
+  unsigned int frames;
   unsigned int tile_queue;  // persistent traversal work counter (reset by its last reader)
   unsigned long long depth_visits;  // voxels visited by the expected-depth kernels
   unsigned int chunk_queue[kMaxChunks];  // work counters of concurrent chunk launches

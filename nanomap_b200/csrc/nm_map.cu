@@ -5,6 +5,7 @@
 // fp32 atomics, int8 quantisation) and the host map update of Handler.cpp:134-182.
 #include <atomic>
 #include <cfloat>
+#include <cstddef>
 #include <cstdint>
 
 #include "nm_device.cuh"
@@ -110,14 +111,28 @@ __device__ __forceinline__ float update_voxel(float v, uint32_t& abit, float tem
 }
 
 // The frame's touched-leaf count and the probe error bit, read once per block: every warp
-// reading the counter word itself queues thousands of requests on one L2 line.
-__device__ __forceinline__ void read_integrate_counters(const MapCounters* ctr, uint32_t* n,
+// reading the counter word itself queues thousands of requests on one L2 line.  Thread 0 reads
+// the count and takes the block's ticket in one 64-bit atomic on (touched_count, done_blocks);
+// the block with the last ticket knows that every block holds the count, so it resets the
+// per-frame list for the next frame and folds it into the totals.
+static_assert(offsetof(MapCounters, done_blocks) == offsetof(MapCounters, touched_count) + 4 &&
+                  offsetof(MapCounters, touched_count) % 8 == 0,
+              "touched_count and done_blocks form one 8-byte word");
+__device__ __forceinline__ void read_integrate_counters(MapCounters* ctr, uint32_t* n,
                                                         bool* fatal) {
   __shared__ uint32_t s_n, s_err;
   wait_prior_grid();  // the walk that fills the counters may still run at launch
   if (threadIdx.x == 0) {
-    s_n = *(const volatile unsigned int*)&ctr->touched_count;
+    unsigned long long* pair = reinterpret_cast<unsigned long long*>(&ctr->touched_count);
+    const unsigned long long old = atomicAdd(pair, 1ull << 32);
+    const uint32_t cnt = (uint32_t)old;
     s_err = *(const volatile unsigned int*)&ctr->error_flags;
+    if ((uint32_t)(old >> 32) == gridDim.x - 1) {
+      *pair = 0ull;  // touched_count = done_blocks = 0
+      ctr->touched_total += cnt;
+      ctr->frames += 1u;
+    }
+    s_n = cnt;
   }
   __syncthreads();
   *n = s_n;
@@ -130,29 +145,11 @@ __device__ __forceinline__ uint32_t integrate_warp() {
   return (threadIdx.x >> 5) * gridDim.x + blockIdx.x;
 }
 
-// The last CTA to finish resets the per-frame list and folds it into the totals.
-__device__ __forceinline__ void integrate_epilogue(MapCounters* ctr, uint32_t n_touched,
-                                                   unsigned long long uniq) {
-  __shared__ unsigned long long s_uniq;
-  __shared__ bool s_last;
-  if (threadIdx.x == 0) s_uniq = 0;
-  __syncthreads();
-  if (uniq) atomicAdd(&s_uniq, uniq);
-  __syncthreads();
-  if (threadIdx.x == 0) {
-    if (s_uniq) atomicAdd(&ctr->unique_voxels, s_uniq);
-    __threadfence();
-    const unsigned done = atomicAdd(&ctr->done_blocks, 1u);
-    s_last = (done == gridDim.x - 1);
-  }
-  __syncthreads();
-  if (s_last && threadIdx.x == 0) {
-    __threadfence();
-    ctr->touched_total += n_touched;
-    ctr->frames += 1u;
-    ctr->touched_count = 0u;
-    ctr->done_blocks = 0u;
-  }
+// Newly labelled voxels of the warp's leaves: one reduction per warp (called converged).
+__device__ __forceinline__ void add_unique(MapCounters* ctr, unsigned long long uniq) {
+#pragma unroll
+  for (int o = 16; o > 0; o >>= 1) uniq += __shfl_xor_sync(kFull, uniq, o);
+  if ((threadIdx.x & 31) == 0 && uniq) atomicAdd(&ctr->unique_voxels, uniq);
 }
 
 // One warp per touched leaf.  Lane i owns float4 i, i+32, i+64, i+96 of the leaf's 512
@@ -231,7 +228,7 @@ __global__ void __launch_bounds__(256) k_integrate_label(MapView m, IntegratePar
       if ((lane & 7) == 0 && any) act[q >> 3] = word;
     }
   }
-  integrate_epilogue(m.ctr, n, uniq);
+  add_unique(m.ctr, uniq);
 }
 
 template <int RM, bool Always>
@@ -267,7 +264,7 @@ __global__ void __launch_bounds__(256) k_integrate_count(MapView m, IntegratePar
       if (!fatal && __ballot_sync(kFull, t) != 0u && lane == 0) act[j] = word;
     }
   }
-  integrate_epilogue(m.ctr, n, uniq);
+  add_unique(m.ctr, uniq);
 }
 
 // ---- growth, export --------------------------------------------------------------------------

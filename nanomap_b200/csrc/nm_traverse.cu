@@ -248,7 +248,12 @@ __device__ __forceinline__ uint32_t walk_ray(const Ray& r, const TileTable& tt, 
     // miss label of the voxel being left
     const int wi = wbase + (l >> 5);
     if (wi != cw) {
-      if (acc) flush_word(tt.words, m, cw, acc, plane);
+      // acc holds at least the bit of the step that set cw (none only for the initial
+      // kLostWord, which flush_device_word drops)
+      if (cw >= 0)
+        atomicOr(&tt.words[cw], acc);
+      else
+        flush_device_word(m, cw, acc, plane);
       cw = wi;
       acc = 0u;
     }
@@ -503,18 +508,18 @@ __device__ __forceinline__ void traverse_body(const TickWork<MaxF>& work, const 
 // A frame's walk is bounded by its longest rays: a step costs a warp ~70 instructions issued
 // at one per ~11 cycles while the SM's other warps run, so a 350-step ray takes most of a
 // frame's traversal.  Claiming the tiles in decreasing order of their longest ray starts those
-// rays first.  One warp per tile takes the largest |R p|_1 / res over the tile's rays (the
+// rays first.  One CTA per tile takes the largest |R p|_1 / res over the tile's rays (the
 // DDA's step count up to rounding) plus kSetupSteps, scales it to one of kOrderBuckets
 // buckets, and appends the tile to that bucket's list (order inside a bucket is arbitrary).
 constexpr float kSetupSteps = 8.0f;
-constexpr int kOrderThreads = 256;
+constexpr int kOrderThreads = 128;
 
 template <int MaxF>
 __device__ __forceinline__ void tile_order_body(const TickWork<MaxF>& work, TileOrderBuffers b) {
   allow_dependent_launch();  // the walk's CTAs launch now and wait for this pass to finish
-  const int lane = threadIdx.x & 31;
-  const uint32_t tile = (blockIdx.x * blockDim.x + threadIdx.x) >> 5;
-  if (tile >= work.total_tiles) return;
+  // one CTA per tile, one thread per ray: every record load of the tile is in flight at once
+  const uint32_t tile = blockIdx.x;
+  const int tid = threadIdx.x, lane = tid & 31;
   const int nrays = work.tile_w * work.tile_h;
   int fi = 0;
   while (fi + 1 < work.n_frames && work.tile_start[fi + 1] <= tile) ++fi;
@@ -524,7 +529,7 @@ __device__ __forceinline__ void tile_order_body(const TickWork<MaxF>& work, Tile
   const int y0 = (int)(lt / (uint32_t)work.tiles_x[fi]) * work.tile_h;
   const float inv_res = (float)(1.0 / f.res_d);
   float longest = 0.0f;
-  for (int k = lane; k < nrays; k += 32) {
+  for (int k = tid; k < nrays; k += kOrderThreads) {
     const int px = x0 + k % work.tile_w, py = y0 + k / work.tile_w;
     float p[3];
     if (px < f.width && py < f.height && pixel_point(f, px, py, p)) {
@@ -539,7 +544,12 @@ __device__ __forceinline__ void tile_order_body(const TickWork<MaxF>& work, Tile
   }
 #pragma unroll
   for (int o = 16; o > 0; o >>= 1) longest = fmaxf(longest, __shfl_xor_sync(kFull, longest, o));
-  if (lane == 0) {
+  __shared__ float s_max[kOrderThreads / 32];
+  if (lane == 0) s_max[tid >> 5] = longest;
+  __syncthreads();
+  if (tid == 0) {
+#pragma unroll
+    for (int w = 1; w < kOrderThreads / 32; ++w) longest = fmaxf(longest, s_max[w]);
     const float q = longest * work.order_scale;
     const int bkt = kOrderBuckets - 1 - (q < (float)(kOrderBuckets - 1) ? (int)q : kOrderBuckets - 1);
     const uint32_t r = atomicAdd(&b.counts[bkt], 1u);
@@ -558,10 +568,7 @@ __global__ void __launch_bounds__(kOrderThreads) k_tile_order_dev(const TickWork
   tile_order_body<kMaxTickFrames>(*work, b);
 }
 
-int order_grid(uint32_t total_tiles) {
-  const uint32_t warps = kOrderThreads / 32;
-  return (int)((total_tiles + warps - 1) / warps);
-}
+int order_grid(uint32_t total_tiles) { return (int)total_tiles; }
 
 // Label sink of the wide-frame kernel: device-table lookups on leaf changes, one atomic per
 // new label bit.
