@@ -543,8 +543,31 @@ int run_frame_chunked(nm_map m, nm_sensor s, nm::FrameParams& f, const unsigned 
   return NM_OK;
 }
 
+// Order-pass sampling of input read over the host link: every 8th ray of a tile (a 16x16
+// tile: columns 0 and 8 of each row), 1/8 of the records read twice.
+constexpr uint32_t kHostOrderStride = 8;
+
+// Device alias of `bytes` of page-locked host memory at `p` (cudaHostAlloc / cudaMallocHost,
+// or cudaHostRegister with mapping), or null for pageable memory.  With the alias the
+// traversal reads the input over the host link itself, each record once, while it walks:
+// no copy to wait for.  Both ends of the range must map contiguously.
+const void* mapped_host(const void* p, size_t bytes) {
+  if (!p || bytes == 0) return nullptr;
+  void* d0 = nullptr;
+  void* d1 = nullptr;
+  const unsigned char* last = static_cast<const unsigned char*>(p) + bytes - 1;
+  if (cudaHostGetDevicePointer(&d0, const_cast<void*>(p), 0) != cudaSuccess ||
+      cudaHostGetDevicePointer(&d1, const_cast<unsigned char*>(last), 0) != cudaSuccess) {
+    cudaGetLastError();  // pageable memory: not an error of the call
+    return nullptr;
+  }
+  if (!d0 || static_cast<unsigned char*>(d1) != static_cast<unsigned char*>(d0) + bytes - 1)
+    return nullptr;
+  return d0;
+}
+
 int run_frame(nm_map m, nm_sensor s, nm::FrameParams& f, uint32_t flags, cudaStream_t s0,
-              uint64_t bound, const nm::SimRender* sim) {
+              uint64_t bound, const nm::SimRender* sim, uint32_t order_stride = 1) {
   int rc = ensure_capacity(m, bound, s0);
   if (rc != NM_OK) return rc;
   rc = set_plane_constants(m, 0, s);
@@ -582,6 +605,7 @@ int run_frame(nm_map m, nm_sensor s, nm::FrameParams& f, uint32_t flags, cudaStr
         if (ordered) {
           NM_CUDA(nm::tile_order_reserve(&m->tile_order, w.total_tiles, s0));
           w.order_scale = nm::tile_order_scale<1>(w);
+          w.order_stride = order_stride;
           NM_CUDA(nm::launch_tile_order<1>(w, &m->tile_order, s0));
           w.order_counts = m->tile_order.counts;
           w.order_lists = m->tile_order.lists;
@@ -837,6 +861,7 @@ int nm_map_reset(nm_map m) {
   m->pending_bound = 0;
   m->pending_labels = false;
   m->pending_planes = 0;
+  m->host_direct_frames = 0;
   return NM_OK;
 }
 
@@ -855,6 +880,7 @@ int nm_map_stats(nm_map m, nm_stats* out) {
   out->error_flags = c.error_flags;
   out->grow_count = m->grow_count;
   out->depth_visits = c.depth_visits;
+  out->host_direct_frames = m->host_direct_frames;
   m->known_leaves = c.leaf_count;
   m->pending_bound = 0;
   if (c.error_flags) NM_CUDA(cudaMemset(&m->d_ctr->error_flags, 0, 4));
@@ -881,10 +907,19 @@ int nm_map_insert_points(nm_map m, nm_sensor s, const nm_pose* pose, const void*
   f.input_kind = 0;
   f.step = step;
   const uint64_t bound = frame_leaf_bound(m, s, *pose, f.R, false, (uint64_t)n);
-  // host records of a label-mode insert: copy in chunks of tile rows, overlapped with the walk
+  // host records of a label-mode insert: page-locked ones are read by the walk itself over
+  // the host link; pageable ones are copied in chunks of tile rows, overlapped with the walk
   const int tiles_y = (height + m->tile_h - 1) / m->tile_h;
-  if ((flags & NM_INPUT_HOST) && m->desc.update_mode == NM_UPDATE_LABEL &&
-      !(flags & (NM_FILTER_MEAN | NM_FILTER_CENTRE)) && tiles_y >= 8) {
+  const bool direct = (flags & NM_INPUT_HOST) && m->desc.update_mode == NM_UPDATE_LABEL &&
+                      !(flags & (NM_FILTER_MEAN | NM_FILTER_CENTRE));
+  if (direct) {
+    if (const void* mapped = mapped_host(cloud, (size_t)n * step)) {
+      f.xyz = static_cast<const unsigned char*>(mapped);
+      m->host_direct_frames += 1;
+      return run_frame(m, s, f, flags, s0, bound, nullptr, kHostOrderStride);
+    }
+  }
+  if (direct && tiles_y >= 8) {
     rc = ensure_staging(m, (size_t)n * step);
     if (rc != NM_OK) return rc;
     f.xyz = m->staging;
@@ -914,13 +949,22 @@ int nm_map_insert_ranges(nm_map m, nm_sensor s, const nm_pose* pose, const float
   if (rc != NM_OK) return rc;
   const int64_t n = (int64_t)s->desc.hres * s->desc.vres;
   f.input_kind = 1;
+  const uint64_t bound = frame_leaf_bound(m, s, *pose, f.R, true, (uint64_t)n);
+  if ((flags & NM_INPUT_HOST) && m->desc.update_mode == NM_UPDATE_LABEL &&
+      !(flags & (NM_FILTER_MEAN | NM_FILTER_CENTRE))) {
+    // page-locked host ranges: read by the walk over the host link, each once
+    if (const void* mapped = mapped_host(ranges, (size_t)n * 4)) {
+      f.ranges = static_cast<const float*>(mapped);
+      m->host_direct_frames += 1;
+      return run_frame(m, s, f, flags, s0, bound, nullptr, kHostOrderStride);
+    }
+  }
   const void* dev = ranges;
   if (flags & NM_INPUT_HOST) {
     rc = stage_input(m, ranges, (size_t)n * 4, s0, &dev);
     if (rc != NM_OK) return rc;
   }
   f.ranges = static_cast<const float*>(dev);
-  const uint64_t bound = frame_leaf_bound(m, s, *pose, f.R, true, (uint64_t)n);
   if (flags & (NM_FILTER_MEAN | NM_FILTER_CENTRE)) {
     rc = apply_filter(m, f, flags, s0);
     if (rc != NM_OK) return rc;

@@ -51,7 +51,7 @@ struct nm_tick_plan_s {
   uint32_t captured_capacity = 0;
   unsigned long long* captured_keys = nullptr;
   int parity = 0;
-  int tile_w = 16, tile_h = 16, entries = 128;
+  int tile_w = 16, tile_h = 16, entries = 256;
   nm::IntegrateParams integ{};
   nm::TileOrderBuffers order{};  // claim order of the tick's tiles (fixed address per graph)
 };

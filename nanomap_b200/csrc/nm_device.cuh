@@ -154,7 +154,14 @@ __device__ __forceinline__ bool range_point(const FrameParams& f, int w, int h, 
 
 __device__ __forceinline__ bool xyz_point(const FrameParams& f, int w, int h, float p[3]) {
   const unsigned char* rec = f.xyz + ((size_t)h * f.width + w) * (size_t)f.step;
-  if ((((uintptr_t)rec) & 3u) == 0) {
+  // records of 16 bytes or a multiple, 16-byte aligned: one 16-byte load (within the record,
+  // so never past the input's end; one request where the input is read over the host link)
+  if (((f.step & 15) | (int)(((uintptr_t)rec) & 15u)) == 0) {
+    const float4 q = __ldg(reinterpret_cast<const float4*>(rec));
+    p[0] = q.x;
+    p[1] = q.y;
+    p[2] = q.z;
+  } else if ((((uintptr_t)rec) & 3u) == 0) {
     const float* q = reinterpret_cast<const float*>(rec);
     p[0] = __ldg(q);
     p[1] = __ldg(q + 1);

@@ -117,6 +117,7 @@ struct TickWork {
   const uint32_t* order_lists;
   uint32_t order_cap;
   float order_scale;      // buckets per walk step: kOrderBuckets / (longest possible walk)
+  uint32_t order_stride;  // the order pass reads every order_stride-th ray of a tile (0 = 1)
   uint32_t tile_start[MaxF + 1];
   int32_t tiles_x[MaxF];
   FrameParams fr[MaxF];

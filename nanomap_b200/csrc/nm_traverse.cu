@@ -307,7 +307,9 @@ __device__ __forceinline__ void traverse_body(const TickWork<MaxF>& work, const 
   uint32_t* s_tags = s_words + nent * kLabelWords;
   uint16_t* s_order = reinterpret_cast<uint16_t*>(s_tags + nent);
   uint8_t* s_bkt = reinterpret_cast<uint8_t*>(s_order + nrays);
-  float* s_rng = reinterpret_cast<float*>(s_bkt + nrays);  // Render: the tile's ranges
+  // the tile's sensor-frame points, read once (the input may be host memory read over the
+  // host link); x = NaN for a pixel without a point
+  float* s_pts = reinterpret_cast<float*>(s_bkt + nrays);
   __shared__ FrameParams s_f;
   __shared__ uint32_t s_tile;
   __shared__ int s_frame;
@@ -405,21 +407,28 @@ __device__ __forceinline__ void traverse_body(const TickWork<MaxF>& work, const 
     for (int k = tid; k < nrays; k += nthreads) {
       const int px = x0 + k % work.tile_w, py = y0 + k / work.tile_w;
       float rm = 0.0f;  // range in metres, 0 = no point
+      float p[3] = {__int_as_float(0x7fffffff), 0.0f, 0.0f};
       if (px < f.width && py < f.height) {
+        bool ok;
         if constexpr (Render) {
           float rr = sim_ray(sr->v, sr->rp, px, py);
           const long long i = (long long)py * f.width + px;
           if (sr->noise) rr = noisy(rr, sr->seed, i, sr->sigma_coef, sr->drop);
           if (sr->out) sr->out[i] = rr;
-          s_rng[k] = rr;
           rm = rr;
+          ok = range_point_r(f, px, py, rr, p);
         } else if (f.input_kind == 1) {
           rm = __ldg(&f.ranges[(size_t)py * f.width + px]);
+          ok = range_point_r(f, px, py, rm, p);
         } else {
-          float p[3];
-          if (pixel_point(f, px, py, p)) rm = sqrtf(p[0] * p[0] + p[1] * p[1] + p[2] * p[2]);
+          ok = pixel_point(f, px, py, p);
+          if (ok) rm = sqrtf(p[0] * p[0] + p[1] * p[1] + p[2] * p[2]);
         }
+        if (!ok) p[0] = __int_as_float(0x7fffffff);
       }
+      s_pts[3 * k] = p[0];
+      s_pts[3 * k + 1] = p[1];
+      s_pts[3 * k + 2] = p[2];
       const int b = range_bucket(rm, qs);
       s_bkt[k] = (uint8_t)b;
       const unsigned peers = __match_any_sync(kFull, b);
@@ -455,13 +464,9 @@ __device__ __forceinline__ void traverse_body(const TickWork<MaxF>& work, const 
       // alternate directions so every warp gets long and short rays
       const int pos = (j & 1) ? (j + 1) * nthreads - 1 - tid : j * nthreads + tid;
       const int k = s_order[pos];
-      const int px = x0 + k % work.tile_w, py = y0 + k / work.tile_w;
-      float p[3];
-      bool has_point = false;
-      if (px < f.width && py < f.height)
-        has_point = Render ? range_point_r(f, px, py, s_rng[k], p) : pixel_point(f, px, py, p);
+      const float p[3] = {s_pts[3 * k], s_pts[3 * k + 1], s_pts[3 * k + 2]};
       Ray r;
-      if (has_point && setup_ray<RM>(f, p, r)) {
+      if (!isnan(p[0]) && setup_ray<RM>(f, p, r)) {
         rays += 1;
         visits += walk_ray<RM>(r, tt, m, max_time, epoch, plane);
       }
@@ -511,6 +516,8 @@ __device__ __forceinline__ void traverse_body(const TickWork<MaxF>& work, const 
 // rays first.  One CTA per tile takes the largest |R p|_1 / res over the tile's rays (the
 // DDA's step count up to rounding) plus kSetupSteps, scales it to one of kOrderBuckets
 // buckets, and appends the tile to that bucket's list (order inside a bucket is arbitrary).
+// Input read over the host link is sampled (every order_stride-th ray of a tile): the walk
+// reads every record once, and the order only has to be roughly right.
 constexpr float kSetupSteps = 8.0f;
 constexpr int kOrderThreads = 128;
 
@@ -529,7 +536,8 @@ __device__ __forceinline__ void tile_order_body(const TickWork<MaxF>& work, Tile
   const int y0 = (int)(lt / (uint32_t)work.tiles_x[fi]) * work.tile_h;
   const float inv_res = (float)(1.0 / f.res_d);
   float longest = 0.0f;
-  for (int k = tid; k < nrays; k += kOrderThreads) {
+  const int stride = work.order_stride > 1u ? (int)work.order_stride : 1;
+  for (int k = tid * stride; k < nrays; k += kOrderThreads * stride) {
     const int px = x0 + k % work.tile_w, py = y0 + k / work.tile_w;
     float p[3];
     if (px < f.width && py < f.height && pixel_point(f, px, py, p)) {
@@ -722,7 +730,8 @@ bool work_is_wide(const FrameParams* fr, int n) {
 size_t traverse_smem_bytes(int tile_w, int tile_h, uint32_t smask, bool render) {
   const size_t nent = (size_t)smask + 1;
   const size_t nrays = (size_t)tile_w * tile_h;
-  return nent * (8 + kLabelWords * 4 + 4) + nrays * (2 + 1) + (render ? nrays * 4 : 0);
+  (void)render;
+  return nent * (8 + kLabelWords * 4 + 4) + nrays * (2 + 1 + 12);
 }
 
 template <int MaxF>
