@@ -116,8 +116,6 @@ typedef struct {
   uint32_t error_flags;    /* sticky device error bits, cleared by nm_map_stats */
   uint32_t grow_count;     /* table growths so far */
   uint64_t depth_visits;   /* voxels visited by expected-depth renders, adjoints, refinement */
-  uint64_t host_direct_frames; /* NM_INPUT_HOST inputs in page-locked memory, read in place by
-                                  the traversal over the host link (no staging copy) */
 } nm_stats;
 
 /* One frame of a batched tick. */
@@ -188,11 +186,7 @@ int nm_map_reset(nm_map m);
 int nm_map_stats(nm_map m, nm_stats* out);
 
 /* Insert one xyz point cloud: `width*height` records of `step` bytes, float x, y, z at byte
- * offsets 0, 4, 8, in the sensor frame.  Host input (NM_INPUT_HOST) in page-locked memory
- * (cudaHostAlloc, cudaMallocHost, or cudaHostRegister with mapping) is read in place by the
- * traversal, each record once, over the host link; pageable host input is copied to the
- * device first.  Either way host input must stay unchanged until the stream passes the call
- * (NM_SYNC: until it returns).  Replaces Manager::insertPointCloud (Manager.h:52-63)
+ * offsets 0, 4, 8, in the sensor frame.  Replaces Manager::insertPointCloud (Manager.h:52-63)
  * -> Handler::processPointCloud (Handler.cpp:237-284) -> filterCloud (filterCloud.cu:476)
  * + frustumCastCloud (frustumCastCloud.cu:311) + the host map update (Handler.cpp:134-182). */
 int nm_map_insert_points(nm_map m, nm_sensor s, const nm_pose* pose, const void* cloud,

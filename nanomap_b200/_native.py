@@ -79,7 +79,7 @@ class NmStats(C.Structure):
         ("unique_voxels", C.c_uint64), ("touched_leaves", C.c_uint64),
         ("leaf_count", C.c_uint64), ("leaf_capacity", C.c_uint64),
         ("error_flags", C.c_uint32), ("grow_count", C.c_uint32),
-        ("depth_visits", C.c_uint64), ("host_direct_frames", C.c_uint64),
+        ("depth_visits", C.c_uint64),
     ]
 
 

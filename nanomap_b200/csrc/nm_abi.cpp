@@ -466,108 +466,8 @@ int apply_filter(nm_map m, nm::FrameParams& f, uint32_t flags, cudaStream_t s0) 
   return NM_OK;
 }
 
-// One frame through traverse (+ integrate unless deferred).
-int ensure_chunk_streams(nm_context c) {
-  if (c->chunk_ready) return NM_OK;
-  NM_CUDA(cudaStreamCreateWithFlags(&c->copy_stream, cudaStreamNonBlocking));
-  NM_CUDA(cudaEventCreateWithFlags(&c->ev_prev, cudaEventDisableTiming));
-  for (int i = 0; i < kMaxChunks; ++i) {
-    NM_CUDA(cudaStreamCreateWithFlags(&c->chunk_stream[i], cudaStreamNonBlocking));
-    NM_CUDA(cudaEventCreateWithFlags(&c->ev_copied[i], cudaEventDisableTiming));
-    NM_CUDA(cudaEventCreateWithFlags(&c->ev_done[i], cudaEventDisableTiming));
-  }
-  c->chunk_ready = true;
-  return NM_OK;
-}
-
-// Label-mode insert of host xyz records with the copy overlapped: the records go to the
-// device in chunks of tile rows on the context's copy stream, and each chunk's traversal runs
-// on its own stream (and tile counter) as soon as its rows have arrived, so later chunks copy
-// while earlier ones are walked.  Tiles are those of the whole frame, so labels and map are
-// the same as one launch over the staged frame.
-int run_frame_chunked(nm_map m, nm_sensor s, nm::FrameParams& f, const unsigned char* host,
-                      uint32_t flags, cudaStream_t s0, uint64_t bound, int nchunks) {
-  nm_context c = m->ctx;
-  int rc = ensure_chunk_streams(c);
-  if (rc != NM_OK) return rc;
-  rc = ensure_capacity(m, bound, s0);
-  if (rc != NM_OK) return rc;
-  rc = set_plane_constants(m, 0, s);
-  if (rc != NM_OK) return rc;
-  f.epoch = m->epoch;
-  f.plane = 0;
-  const int tile_w = m->tile_w, tile_h = m->tile_h;
-  const int tiles_x = (f.width + tile_w - 1) / tile_w;
-  const int tiles_y = (f.height + tile_h - 1) / tile_h;
-  const int tiles_per_chunk = (tiles_y + nchunks - 1) / nchunks;
-  const size_t row_bytes = (size_t)f.width * (size_t)f.step;
-  unsigned char* dev = const_cast<unsigned char*>(f.xyz);
-  // everything before this call on s0 (earlier frames reading the staging buffer, a table
-  // growth) comes first
-  NM_CUDA(cudaEventRecord(c->ev_prev, s0));
-  NM_CUDA(cudaStreamWaitEvent(c->copy_stream, c->ev_prev, 0));
-  int used = 0;
-  for (int k = 0; k < nchunks; ++k) {
-    const int y0 = k * tiles_per_chunk * tile_h;
-    if (y0 >= f.height) break;
-    const int rows = std::min(f.height - y0, tiles_per_chunk * tile_h);
-    NM_CUDA(cudaMemcpyAsync(dev + (size_t)y0 * row_bytes, host + (size_t)y0 * row_bytes,
-                            (size_t)rows * row_bytes, cudaMemcpyHostToDevice, c->copy_stream));
-    NM_CUDA(cudaEventRecord(c->ev_copied[k], c->copy_stream));
-    NM_CUDA(cudaStreamWaitEvent(c->chunk_stream[k], c->ev_copied[k], 0));
-    nm::TickWork<1> w;
-    std::memset(&w, 0, sizeof(w));
-    w.n_frames = 1;
-    w.tile_w = tile_w;
-    w.tile_h = tile_h;
-    w.smask = (uint32_t)m->smem_entries - 1u;
-    w.queue = (uint32_t)k + 1u;
-    w.tiles_x[0] = tiles_x;
-    w.tile_start[0] = 0;
-    w.tile_start[1] = (uint32_t)(tiles_x * ((rows + tile_h - 1) / tile_h));
-    w.total_tiles = w.tile_start[1];
-    w.fr[0] = f;
-    w.fr[0].xyz = dev + (size_t)y0 * row_bytes;
-    w.fr[0].height = rows;
-    NM_CUDA(nm::launch_traverse_labels<1>(w, m->view, m->desc.rounding, c->chunk_stream[k]));
-    NM_CUDA(cudaEventRecord(c->ev_done[k], c->chunk_stream[k]));
-    used = k + 1;
-  }
-  for (int k = 0; k < used; ++k) NM_CUDA(cudaStreamWaitEvent(s0, c->ev_done[k], 0));
-  m->pending_labels = true;
-  if (!(flags & NM_DEFER_INTEGRATE)) {
-    rc = do_integrate(m, s0);
-    if (rc != NM_OK) return rc;
-  }
-  if (flags & NM_SYNC) return check_device_errors(m, s0);
-  return NM_OK;
-}
-
-// Order-pass sampling of input read over the host link: every 8th ray of a tile (a 16x16
-// tile: columns 0 and 8 of each row), 1/8 of the records read twice.
-constexpr uint32_t kHostOrderStride = 8;
-
-// Device alias of `bytes` of page-locked host memory at `p` (cudaHostAlloc / cudaMallocHost,
-// or cudaHostRegister with mapping), or null for pageable memory.  With the alias the
-// traversal reads the input over the host link itself, each record once, while it walks:
-// no copy to wait for.  Both ends of the range must map contiguously.
-const void* mapped_host(const void* p, size_t bytes) {
-  if (!p || bytes == 0) return nullptr;
-  void* d0 = nullptr;
-  void* d1 = nullptr;
-  const unsigned char* last = static_cast<const unsigned char*>(p) + bytes - 1;
-  if (cudaHostGetDevicePointer(&d0, const_cast<void*>(p), 0) != cudaSuccess ||
-      cudaHostGetDevicePointer(&d1, const_cast<unsigned char*>(last), 0) != cudaSuccess) {
-    cudaGetLastError();  // pageable memory: not an error of the call
-    return nullptr;
-  }
-  if (!d0 || static_cast<unsigned char*>(d1) != static_cast<unsigned char*>(d0) + bytes - 1)
-    return nullptr;
-  return d0;
-}
-
 int run_frame(nm_map m, nm_sensor s, nm::FrameParams& f, uint32_t flags, cudaStream_t s0,
-              uint64_t bound, const nm::SimRender* sim, uint32_t order_stride = 1) {
+              uint64_t bound, const nm::SimRender* sim) {
   int rc = ensure_capacity(m, bound, s0);
   if (rc != NM_OK) return rc;
   rc = set_plane_constants(m, 0, s);
@@ -605,7 +505,6 @@ int run_frame(nm_map m, nm_sensor s, nm::FrameParams& f, uint32_t flags, cudaStr
         if (ordered) {
           NM_CUDA(nm::tile_order_reserve(&m->tile_order, w.total_tiles, s0));
           w.order_scale = nm::tile_order_scale<1>(w);
-          w.order_stride = order_stride;
           NM_CUDA(nm::launch_tile_order<1>(w, &m->tile_order, s0));
           w.order_counts = m->tile_order.counts;
           w.order_lists = m->tile_order.lists;
@@ -635,17 +534,6 @@ void release(nm_context c) {
   cudaSetDevice(c->device);
   cudaStreamSynchronize(c->stream);
   cudaFree(c->render_staging);
-  if (c->chunk_ready) {
-    cudaStreamSynchronize(c->copy_stream);
-    cudaStreamDestroy(c->copy_stream);
-    cudaEventDestroy(c->ev_prev);
-    for (int i = 0; i < kMaxChunks; ++i) {
-      cudaStreamSynchronize(c->chunk_stream[i]);
-      cudaStreamDestroy(c->chunk_stream[i]);
-      cudaEventDestroy(c->ev_copied[i]);
-      cudaEventDestroy(c->ev_done[i]);
-    }
-  }
   delete c;
 }
 
@@ -861,7 +749,6 @@ int nm_map_reset(nm_map m) {
   m->pending_bound = 0;
   m->pending_labels = false;
   m->pending_planes = 0;
-  m->host_direct_frames = 0;
   return NM_OK;
 }
 
@@ -880,7 +767,6 @@ int nm_map_stats(nm_map m, nm_stats* out) {
   out->error_flags = c.error_flags;
   out->grow_count = m->grow_count;
   out->depth_visits = c.depth_visits;
-  out->host_direct_frames = m->host_direct_frames;
   m->known_leaves = c.leaf_count;
   m->pending_bound = 0;
   if (c.error_flags) NM_CUDA(cudaMemset(&m->d_ctr->error_flags, 0, 4));
@@ -907,25 +793,6 @@ int nm_map_insert_points(nm_map m, nm_sensor s, const nm_pose* pose, const void*
   f.input_kind = 0;
   f.step = step;
   const uint64_t bound = frame_leaf_bound(m, s, *pose, f.R, false, (uint64_t)n);
-  // host records of a label-mode insert: page-locked ones are read by the walk itself over
-  // the host link; pageable ones are copied in chunks of tile rows, overlapped with the walk
-  const int tiles_y = (height + m->tile_h - 1) / m->tile_h;
-  const bool direct = (flags & NM_INPUT_HOST) && m->desc.update_mode == NM_UPDATE_LABEL &&
-                      !(flags & (NM_FILTER_MEAN | NM_FILTER_CENTRE));
-  if (direct) {
-    if (const void* mapped = mapped_host(cloud, (size_t)n * step)) {
-      f.xyz = static_cast<const unsigned char*>(mapped);
-      m->host_direct_frames += 1;
-      return run_frame(m, s, f, flags, s0, bound, nullptr, kHostOrderStride);
-    }
-  }
-  if (direct && tiles_y >= 8) {
-    rc = ensure_staging(m, (size_t)n * step);
-    if (rc != NM_OK) return rc;
-    f.xyz = m->staging;
-    return run_frame_chunked(m, s, f, static_cast<const unsigned char*>(cloud), flags, s0,
-                             bound, 4);
-  }
   const void* dev = cloud;
   if (flags & NM_INPUT_HOST) {
     rc = stage_input(m, cloud, (size_t)n * step, s0, &dev);
@@ -949,22 +816,13 @@ int nm_map_insert_ranges(nm_map m, nm_sensor s, const nm_pose* pose, const float
   if (rc != NM_OK) return rc;
   const int64_t n = (int64_t)s->desc.hres * s->desc.vres;
   f.input_kind = 1;
-  const uint64_t bound = frame_leaf_bound(m, s, *pose, f.R, true, (uint64_t)n);
-  if ((flags & NM_INPUT_HOST) && m->desc.update_mode == NM_UPDATE_LABEL &&
-      !(flags & (NM_FILTER_MEAN | NM_FILTER_CENTRE))) {
-    // page-locked host ranges: read by the walk over the host link, each once
-    if (const void* mapped = mapped_host(ranges, (size_t)n * 4)) {
-      f.ranges = static_cast<const float*>(mapped);
-      m->host_direct_frames += 1;
-      return run_frame(m, s, f, flags, s0, bound, nullptr, kHostOrderStride);
-    }
-  }
   const void* dev = ranges;
   if (flags & NM_INPUT_HOST) {
     rc = stage_input(m, ranges, (size_t)n * 4, s0, &dev);
     if (rc != NM_OK) return rc;
   }
   f.ranges = static_cast<const float*>(dev);
+  const uint64_t bound = frame_leaf_bound(m, s, *pose, f.R, true, (uint64_t)n);
   if (flags & (NM_FILTER_MEAN | NM_FILTER_CENTRE)) {
     rc = apply_filter(m, f, flags, s0);
     if (rc != NM_OK) return rc;

@@ -33,10 +33,6 @@ constexpr uint32_t kErrProbe = 1u;     // leaf table probe limit reached: labels
 constexpr uint32_t kErrTimeout = 2u;   // a bounded wait gave up
 constexpr uint32_t kErrPlane = 4u;     // plane index outside the allocated planes
 
-// Host input copied in chunks of tile rows: one traversal launch per chunk, each on its own
-// stream and tile counter (MapCounters::chunk_queue), starting when its rows have arrived.
-constexpr int kMaxChunks = 8;
-
 struct MapCounters {
   unsigned long long rays;
   unsigned long long visits;
@@ -51,7 +47,6 @@ struct MapCounters {
   unsigned int frames;
   unsigned int tile_queue;  // persistent traversal work counter (reset by its last reader)
   unsigned long long depth_visits;  // voxels visited by the expected-depth kernels
-  unsigned int chunk_queue[kMaxChunks];  // work counters of concurrent chunk launches
 };
 
 struct MapView {
@@ -109,7 +104,6 @@ struct TickWork {
   int32_t tile_w, tile_h;
   uint32_t smask;         // shared-memory leaf table entries - 1 (power of two)
   uint32_t total_tiles;
-  uint32_t queue;         // 0: MapCounters::tile_queue; c + 1: chunk_queue[c]
   // claim order of the tiles (longest walks first; null = tile order): the number of tiles in
   // each of kOrderBuckets walk-length buckets, and bucket b's tiles at order_lists[b * order_cap];
   // the traversal zeroes the counts once every CTA has read them, for the next order pass
@@ -117,7 +111,6 @@ struct TickWork {
   const uint32_t* order_lists;
   uint32_t order_cap;
   float order_scale;      // buckets per walk step: kOrderBuckets / (longest possible walk)
-  uint32_t order_stride;  // the order pass reads every order_stride-th ray of a tile (0 = 1)
   uint32_t tile_start[MaxF + 1];
   int32_t tiles_x[MaxF];
   FrameParams fr[MaxF];

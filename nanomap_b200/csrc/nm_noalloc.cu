@@ -20,6 +20,7 @@
 // start at zero; calls that overlap on the GPU (different streams, or different host threads)
 // race on it and must be serialised by the caller.
 #include <cmath>
+#include <cstddef>
 #include <cstdint>
 #include <cstring>
 #include <mutex>
@@ -40,10 +41,11 @@ constexpr uint32_t kErrLeafLimit = 16u;  // more labelled leaves than kStaticLea
 struct StaticScratch {
   MapCounters ctr;
   unsigned long long keys[kStaticLeafSlots];
-  uint32_t labels[(size_t)kStaticLeafSlots * kLabelWords];
+  alignas(16) uint32_t labels[(size_t)kStaticLeafSlots * kLabelWords];  // cleared as uint4
   uint32_t epoch[kStaticLeafSlots];
   uint32_t touched[kStaticLeafSlots];
 };
+static_assert(offsetof(StaticScratch, labels) % 16 == 0, "labels are cleared with 16-byte stores");
 
 static __device__ __align__(256) StaticScratch g_static_scratch;
 

@@ -49,13 +49,6 @@ struct nm_context_s {
   cudaStream_t stream = nullptr;
   float* render_staging = nullptr;
   size_t render_staging_bytes = 0;
-  // chunked host input (created on first use): one copy stream, one stream per chunk launch
-  bool chunk_ready = false;
-  cudaStream_t copy_stream = nullptr;
-  cudaStream_t chunk_stream[nm::kMaxChunks] = {};
-  cudaEvent_t ev_prev = nullptr;
-  cudaEvent_t ev_copied[nm::kMaxChunks] = {};
-  cudaEvent_t ev_done[nm::kMaxChunks] = {};
 };
 
 struct nm_sensor_s {
@@ -88,7 +81,6 @@ struct nm_map_s {
   // 16x16 tiles, 256-entry leaf table: fastest or within a few percent on every frame kind
   // measured (one ray per thread; tiles of two or more rays per thread lose SIMT sharing)
   int tile_w = 16, tile_h = 16, smem_entries = 256;
-  uint64_t host_direct_frames = 0;  // host inputs read in place (page-locked memory)
   nm::FilterBuffers filter{};  // voxel-filter buffers, grown on first filtered insert
   nm::TileOrderBuffers tile_order{};  // claim order of traversal tiles, grown on demand
   double* depth_scratch = nullptr;  // expected-depth partial sums (grown on demand)

@@ -29,9 +29,6 @@
 // Frames whose reach exceeds the code's range (max_range / res >= kNarrowMaxTime) take
 // k_traverse_wide: one thread per ray with device-table lookups and label atomics.
 //
-// Host xyz records may arrive in chunks of tile rows: each chunk is then its own launch on
-// its own stream and tile counter (TickWork::queue), started when its rows have arrived.
-//
 // k_traverse_render renders each tile's ranges from the sim map into shared memory first
 // (nm_sim_insert), so one launch does the simulated frame and its insertion.
 #include <cfloat>
@@ -307,8 +304,8 @@ __device__ __forceinline__ void traverse_body(const TickWork<MaxF>& work, const 
   uint32_t* s_tags = s_words + nent * kLabelWords;
   uint16_t* s_order = reinterpret_cast<uint16_t*>(s_tags + nent);
   uint8_t* s_bkt = reinterpret_cast<uint8_t*>(s_order + nrays);
-  // the tile's sensor-frame points, read once (the input may be host memory read over the
-  // host link); x = NaN for a pixel without a point
+  // the tile's sensor-frame points, computed once by the range sort; x = NaN for a pixel
+  // without a point
   float* s_pts = reinterpret_cast<float*>(s_bkt + nrays);
   __shared__ FrameParams s_f;
   __shared__ uint32_t s_tile;
@@ -341,7 +338,7 @@ __device__ __forceinline__ void traverse_body(const TickWork<MaxF>& work, const 
 
   for (;;) {
     if (tid == 0) {
-      unsigned int* queue = work.queue ? &m.ctr->chunk_queue[work.queue - 1] : &m.ctr->tile_queue;
+      unsigned int* queue = &m.ctr->tile_queue;
       const uint32_t t = atomicAdd(queue, 1u);
       uint32_t tl = t;
       if (work.order_counts && t < s_pre[kOrderBuckets]) {
@@ -516,8 +513,6 @@ __device__ __forceinline__ void traverse_body(const TickWork<MaxF>& work, const 
 // rays first.  One CTA per tile takes the largest |R p|_1 / res over the tile's rays (the
 // DDA's step count up to rounding) plus kSetupSteps, scales it to one of kOrderBuckets
 // buckets, and appends the tile to that bucket's list (order inside a bucket is arbitrary).
-// Input read over the host link is sampled (every order_stride-th ray of a tile): the walk
-// reads every record once, and the order only has to be roughly right.
 constexpr float kSetupSteps = 8.0f;
 constexpr int kOrderThreads = 128;
 
@@ -536,8 +531,7 @@ __device__ __forceinline__ void tile_order_body(const TickWork<MaxF>& work, Tile
   const int y0 = (int)(lt / (uint32_t)work.tiles_x[fi]) * work.tile_h;
   const float inv_res = (float)(1.0 / f.res_d);
   float longest = 0.0f;
-  const int stride = work.order_stride > 1u ? (int)work.order_stride : 1;
-  for (int k = tid * stride; k < nrays; k += kOrderThreads * stride) {
+  for (int k = tid; k < nrays; k += kOrderThreads) {
     const int px = x0 + k % work.tile_w, py = y0 + k / work.tile_w;
     float p[3];
     if (px < f.width && py < f.height && pixel_point(f, px, py, p)) {

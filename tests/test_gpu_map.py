@@ -53,9 +53,9 @@ def test_labels_and_map_bit_exact_plain_small(ctx, small, rounding):
 @pytest.mark.parametrize("cut", [0, 13])
 def test_xyz_records_host_and_device_inputs(ctx, small, cut):
     """insertPointCloud-style input: width*height records of `step` bytes, xyz at 0/4/8.
-    Host records are copied in chunks of tile rows overlapped with the walk (four frames in a
-    row without a wait, so the staging buffer is reused while earlier frames run); `cut` drops
-    the last rows so that the last tile row is partial."""
+    Host records are staged by one copy (four frames in a row without a wait, so the staging
+    buffer is reused while earlier frames run); `cut` drops the last rows so that the last
+    tile row is partial."""
     spec, scene, desc, frames = small
     res = spec.map_res
     sensor = A.Sensor(ctx, desc)
@@ -76,54 +76,6 @@ def test_xyz_records_host_and_device_inputs(ctx, small, cut):
     oe = om.export()
     assert not compare_maps(m_host.export(), oe)
     assert not compare_maps(m_dev.export(), oe)
-
-
-@pytest.mark.parametrize("step,cut", [(16, 0), (20, 13)])
-def test_page_locked_host_input_is_read_in_place(ctx, small, step, cut):
-    """NM_INPUT_HOST records and ranges in page-locked memory are read by the traversal over
-    the host link (counted in host_direct_frames), each once, with the order pass sampling
-    every 8th ray; four frames in a row without a wait.  Maps and visit counts must equal
-    the oracle's and those of the device-input path; pageable records still take the copy."""
-    import torch
-    spec, scene, desc, frames = small
-    res = spec.map_res
-    sensor = A.Sensor(ctx, desc)
-    osen = O.Sensor.from_desc(desc)
-    m_pin = A.Map(ctx, A.map_desc(res=res))
-    m_rng = A.Map(ctx, A.map_desc(res=res))
-    m_dev = A.Map(ctx, A.map_desc(res=res))
-    m_page = A.Map(ctx, A.map_desc(res=res))
-    om = O.Map(res)
-    H, W = spec.height - cut, spec.width
-    keep = []  # page-locked inputs stay alive until the stream has passed them
-    for pose, ranges in frames[:4]:
-        pts = osen.points(ranges)[: H * W]
-        rec = np.zeros((H * W, step // 4), np.float32)
-        rec[:, :3] = pts
-        rec[:, 3] = 7.0
-        pinned = torch.from_numpy(rec).pin_memory()
-        pr = torch.from_numpy(np.ascontiguousarray(ranges, np.float32)).pin_memory()
-        keep += [pinned, pr]
-        m_pin.insert_points(sensor, pose, pinned, W, H, step)
-        m_dev.insert_points(sensor, pose, _torch(rec), W, H, step)
-        m_page.insert_points(sensor, pose, rec, W, H, step)
-        if cut == 0:
-            m_rng.insert_ranges(sensor, pose, pr)
-        R, eye, mt = oracle_frame(desc, pose, res, 1)
-        om.insert(R, eye, mt, desc.log_odds_hit, desc.log_odds_miss, pts)
-    torch.cuda.synchronize()
-    oe = om.export()
-    ost = om.stats()
-    maps = [m_pin, m_dev, m_page] + ([m_rng] if cut == 0 else [])
-    for m in maps:
-        errs = compare_maps(m.export(), oe)
-        assert not errs, "; ".join(errs[:5])
-        st = m.stats()
-        assert st["visits"] == ost["visits"] and st["rays"] == ost["rays"] and st["error_flags"] == 0
-    assert m_pin.stats()["host_direct_frames"] == 4
-    assert m_dev.stats()["host_direct_frames"] == 0 and m_page.stats()["host_direct_frames"] == 0
-    if cut == 0:
-        assert m_rng.stats()["host_direct_frames"] == 4
 
 
 @pytest.mark.parametrize("update_mode", [N.NM_UPDATE_LABEL, N.NM_UPDATE_ACCUMULATE])
