@@ -26,6 +26,7 @@ scaling, no collective on the data path); `value` = all ranks' voxel updates / m
 from __future__ import annotations
 
 import argparse
+import gc
 import json
 import math
 import os
@@ -352,15 +353,25 @@ def run_ours(args, rank, world, local):
         barrier()
         torch.cuda.synchronize()
         # each step: L2 flushed first (outside the timed call), then the synchronous insert of
-        # the host records, timed on the host clock from the call to its return
+        # the host records, timed on the host clock from the call to its return (the Python
+        # garbage collector paused over the loop: a collection inside a call is host noise
+        # that a C or C++ caller does not have)
         dt = 0.0
-        for k in range(args.e2e_steps):
-            i = (3 + k) % n_frames
-            flush.fill_(k & 0xFF)
-            torch.cuda.synchronize()
-            t0 = time.perf_counter()
-            m2.insert_points(sensor, poses[i], host_recs[i], W, H, 16, flags=N.NM_SYNC)
-            dt += time.perf_counter() - t0
+        calls = []
+        gc_was = gc.isenabled()
+        gc.disable()
+        try:
+            for k in range(args.e2e_steps):
+                i = (3 + k) % n_frames
+                flush.fill_(k & 0xFF)
+                torch.cuda.synchronize()
+                t0 = time.perf_counter()
+                m2.insert_points(sensor, poses[i], host_recs[i], W, H, 16, flags=N.NM_SYNC)
+                calls.append(time.perf_counter() - t0)
+        finally:
+            if gc_was:
+                gc.enable()
+        dt = sum(calls)
         barrier()
         e1 = m2.stats()
         dt = allreduce_max(dt)
@@ -379,6 +390,8 @@ def run_ours(args, rank, world, local):
         e2e = {"value": ev_all / dt, "unit": UNIT, "h2d_bytes_per_step": H * W * 16,
                "d2h_bytes_per_step": 8, "steps": args.e2e_steps,
                "ms_per_step": dt * 1e3 / args.e2e_steps,
+               "call_ms_median": statistics.median(calls) * 1e3,
+               "call_ms_max": max(calls) * 1e3,
                "path": "nm_map_insert_points(host xyz records, step 16, NM_SYNC)",
                "l2": "flushed before each step, outside the timed call",
                "host_link": {"copy_ms": link_ms, "gbs": H * W * 16 / (link_ms / 1e3) / 1e9,
