@@ -185,6 +185,15 @@ int nm_map_destroy(nm_map m);
 int nm_map_reset(nm_map m);
 int nm_map_stats(nm_map m, nm_stats* out);
 
+/* Non-blocking status read for pipelined use: enqueues on `stream` (after the work already on
+ * it) a copy of the map's status words into host_status[0..1]: the allocated leaf count and
+ * the sticky device error bits (1: leaf-table probe limit reached, 2: a bounded wait gave up;
+ * cleared by nm_map_stats).  host_status should be page-locked (the copy is then
+ * asynchronous); it is valid once the stream has passed this point, e.g. after an event
+ * recorded behind it has completed.  A caller feeding frames without NM_SYNC reads each
+ * frame's status this way while the next frame's host input is already being copied. */
+int nm_map_status_async(nm_map m, uint32_t* host_status, void* stream);
+
 /* Insert one xyz point cloud: `width*height` records of `step` bytes, float x, y, z at byte
  * offsets 0, 4, 8, in the sensor frame.  Replaces Manager::insertPointCloud (Manager.h:52-63)
  * -> Handler::processPointCloud (Handler.cpp:237-284) -> filterCloud (filterCloud.cu:476)

@@ -165,6 +165,7 @@ _SIGS = {
     "nm_map_destroy": (C.c_int, [_P]),
     "nm_map_reset": (C.c_int, [_P]),
     "nm_map_stats": (C.c_int, [_P, C.POINTER(NmStats)]),
+    "nm_map_status_async": (C.c_int, [_P, _P, _P]),
     "nm_map_insert_points": (C.c_int, [_P, _P, C.POINTER(NmPose), _P, _I32, _I32, _I32, _U32, _P]),
     "nm_sim_render_noisy": (C.c_int, [_P, _P, C.POINTER(NmPose), _P, _F, _F, _U64, _U32, _P]),
     "nm_sim_cast_rays": (C.c_int, [_P, _P, _P, _I64, _F, _P, _U32, _P]),

@@ -308,6 +308,14 @@ class Map:
             arr[i].agent = agent
         call("nm_map_tick", self.h, arr, len(frames), flags, _stream(stream))
 
+    def status_async(self, out, stream=None):
+        """Enqueue a copy of (leaf count, error bits) into `out` (2 x int32, page-locked host
+        tensor), valid once the stream has passed this point."""
+        p, host = _ptr(out)
+        if not host:
+            raise ValueError("status buffer must be host memory")
+        call("nm_map_status_async", self.h, p, _stream(stream))
+
     def stats(self) -> dict:
         s = N.NmStats()
         call("nm_map_stats", self.h, C.byref(s))

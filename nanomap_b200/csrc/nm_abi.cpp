@@ -402,26 +402,51 @@ int check_device_errors(nm_map m, cudaStream_t s) {
   return NM_OK;
 }
 
-int ensure_staging(nm_map m, size_t bytes) {
-  if (bytes > m->staging_bytes) {
-    // the old buffer may still be read by queued work: let it finish first
-    NM_CUDA(cudaDeviceSynchronize());
-    cudaFree(m->staging);
-    m->staging = nullptr;
-    m->staging_bytes = 0;
-    NM_CUDA(cudaMalloc((void**)&m->staging, bytes));
-    m->staging_bytes = bytes;
+// Host input goes to the device through two staging buffers used in turn.  Buffer b is filled
+// on the map's copy stream once the work that read it last has run (ev_free[b], recorded on
+// that work's stream when the call that staged it had enqueued everything), and the call's
+// stream waits for the copy (ev_staged[b]).  So with asynchronous calls frame k's copy runs
+// while frame k - 1 is walked; a synchronous call (NM_SYNC) is copy then work, as before.
+int stage_input(nm_map m, const void* src, size_t bytes, cudaStream_t s, const void** dev) {
+  if (!m->copy_stream) {
+    NM_CUDA(cudaStreamCreateWithFlags(&m->copy_stream, cudaStreamNonBlocking));
+    for (int i = 0; i < 2; ++i) {
+      NM_CUDA(cudaEventCreateWithFlags(&m->ev_staged[i], cudaEventDisableTiming));
+      NM_CUDA(cudaEventCreateWithFlags(&m->ev_free[i], cudaEventDisableTiming));
+    }
   }
+  const int b = m->staging_next;
+  if (bytes > m->staging_bytes[b]) {
+    // the old buffer may still be read by queued work: let that finish first
+    NM_CUDA(cudaEventSynchronize(m->ev_free[b]));
+    cudaFree(m->staging[b]);
+    m->staging[b] = nullptr;
+    m->staging_bytes[b] = 0;
+    NM_CUDA(cudaMalloc((void**)&m->staging[b], bytes));
+    m->staging_bytes[b] = bytes;
+  }
+  NM_CUDA(cudaStreamWaitEvent(m->copy_stream, m->ev_free[b], 0));
+  NM_CUDA(cudaMemcpyAsync(m->staging[b], src, bytes, cudaMemcpyHostToDevice, m->copy_stream));
+  NM_CUDA(cudaEventRecord(m->ev_staged[b], m->copy_stream));
+  NM_CUDA(cudaStreamWaitEvent(s, m->ev_staged[b], 0));
+  m->staging_next = b ^ 1;
+  m->staging_held = b;
+  *dev = m->staging[b];
   return NM_OK;
 }
 
-int stage_input(nm_map m, const void* src, size_t bytes, cudaStream_t s, const void** dev) {
-  const int rc = ensure_staging(m, bytes);
-  if (rc != NM_OK) return rc;
-  NM_CUDA(cudaMemcpyAsync(m->staging, src, bytes, cudaMemcpyHostToDevice, s));
-  *dev = m->staging;
-  return NM_OK;
-}
+// Marks the end of the current call's use of its staging buffer: every kernel reading it is
+// on `s` by now (on every return path of a call that staged input).
+struct StagingRelease {
+  nm_map m;
+  cudaStream_t s;
+  ~StagingRelease() {
+    if (m && m->staging_held >= 0) {
+      cudaEventRecord(m->ev_free[m->staging_held], s);
+      m->staging_held = -1;
+    }
+  }
+};
 
 int set_plane_constants(nm_map m, int plane, nm_sensor s) {
   const uint32_t bit = 1u << plane;
@@ -557,7 +582,12 @@ void release(nm_map m) {
   cudaFree(m->d_ctr);
   cudaFree(m->d_scratch_u32);
   cudaFreeHost(m->h_status);
-  cudaFree(m->staging);
+  for (int i = 0; i < 2; ++i) {
+    cudaFree(m->staging[i]);
+    if (m->ev_staged[i]) cudaEventDestroy(m->ev_staged[i]);
+    if (m->ev_free[i]) cudaEventDestroy(m->ev_free[i]);
+  }
+  if (m->copy_stream) cudaStreamDestroy(m->copy_stream);
   filter_release(&m->filter);
   nm::tile_order_release(&m->tile_order);
   cudaFree(m->depth_scratch);
@@ -752,6 +782,16 @@ int nm_map_reset(nm_map m) {
   return NM_OK;
 }
 
+int nm_map_status_async(nm_map m, uint32_t* host_status, void* stream) {
+  if (!m || !host_status) return fail(NM_ERR_ARG, "null argument");
+  static_assert(offsetof(nm::MapCounters, error_flags) ==
+                    offsetof(nm::MapCounters, leaf_count) + 4, "counter layout");
+  NM_CUDA(cudaSetDevice(m->ctx->device));
+  NM_CUDA(cudaMemcpyAsync(host_status, &m->d_ctr->leaf_count, 2 * sizeof(unsigned int),
+                          cudaMemcpyDeviceToHost, pick(m->ctx, stream)));
+  return NM_OK;
+}
+
 int nm_map_stats(nm_map m, nm_stats* out) {
   if (!m || !out) return fail(NM_ERR_ARG, "null argument");
   NM_CUDA(cudaDeviceSynchronize());
@@ -794,6 +834,7 @@ int nm_map_insert_points(nm_map m, nm_sensor s, const nm_pose* pose, const void*
   f.step = step;
   const uint64_t bound = frame_leaf_bound(m, s, *pose, f.R, false, (uint64_t)n);
   const void* dev = cloud;
+  StagingRelease staged{m, s0};
   if (flags & NM_INPUT_HOST) {
     rc = stage_input(m, cloud, (size_t)n * step, s0, &dev);
     if (rc != NM_OK) return rc;
@@ -817,6 +858,7 @@ int nm_map_insert_ranges(nm_map m, nm_sensor s, const nm_pose* pose, const float
   const int64_t n = (int64_t)s->desc.hres * s->desc.vres;
   f.input_kind = 1;
   const void* dev = ranges;
+  StagingRelease staged{m, s0};
   if (flags & NM_INPUT_HOST) {
     rc = stage_input(m, ranges, (size_t)n * 4, s0, &dev);
     if (rc != NM_OK) return rc;
@@ -915,6 +957,7 @@ int nm_map_filter_points(nm_map m, nm_sensor s, const nm_pose* pose, const void*
   if (np > 0 && !input) return fail(NM_ERR_ARG, "input is null");
   if (np == 0) return NM_OK;
   const void* dev = input;
+  StagingRelease staged{m, s0};
   if (flags & NM_INPUT_HOST) {
     rc = stage_input(m, input, (size_t)np * (step > 0 ? (size_t)step : 4u), s0, &dev);
     if (rc != NM_OK) return rc;

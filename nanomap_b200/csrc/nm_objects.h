@@ -74,8 +74,15 @@ struct nm_map_s {
   float pending_lh[nm::kMaxPlanes];
   float pending_lm[nm::kMaxPlanes];
   uint32_t pending_planes = 0;
-  unsigned char* staging = nullptr;  // device copy of host input
-  size_t staging_bytes = 0;
+  // host input staging: two device buffers used in turn, filled on the map's copy stream, so a
+  // frame's copy runs while the frame before it is walked (created on first host input)
+  unsigned char* staging[2] = {nullptr, nullptr};
+  size_t staging_bytes[2] = {0, 0};
+  int staging_next = 0;                            // buffer of the next host input
+  int staging_held = -1;                           // buffer the current call filled
+  cudaStream_t copy_stream = nullptr;
+  cudaEvent_t ev_staged[2] = {nullptr, nullptr};   // buffer filled (copy stream)
+  cudaEvent_t ev_free[2] = {nullptr, nullptr};     // work reading the buffer enqueued before it
   uint32_t* d_scratch_u32 = nullptr;  // export counters
   unsigned int* h_status = nullptr;   // page-locked copy of the map's status words
   // 16x16 tiles, 256-entry leaf table: fastest or within a few percent on every frame kind

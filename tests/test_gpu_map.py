@@ -78,6 +78,48 @@ def test_xyz_records_host_and_device_inputs(ctx, small, cut):
     assert not compare_maps(m_dev.export(), oe)
 
 
+def test_pipelined_host_frames_with_async_status(ctx, small):
+    """Host records in page-locked memory inserted without a wait: each frame's copy runs on
+    the map's copy stream while the frame before it is walked (two staging buffers used in
+    turn), and each frame is followed by nm_map_status_async.  The first frame has half the
+    rows, so both buffers grow between asynchronous frames.  The map equals the oracle's and
+    every status shows no error bits and a leaf count that never falls."""
+    import torch
+    spec, scene, desc, frames = small
+    res = spec.map_res
+    sensor = A.Sensor(ctx, desc)
+    osen = O.Sensor.from_desc(desc)
+    m = A.Map(ctx, A.map_desc(res=res))
+    om = O.Map(res)
+    H, W = spec.height, spec.width
+    stream = torch.cuda.current_stream()
+    reads, keep = [], []
+    for i, (pose, ranges) in enumerate(frames[:6]):
+        h = H // 2 if i == 0 else H
+        pts = osen.points(ranges)[: h * W]
+        rec = np.zeros((h * W, 4), np.float32)
+        rec[:, :3] = pts
+        pinned = torch.from_numpy(rec).pin_memory()
+        status = torch.zeros(2, dtype=torch.int32).pin_memory()
+        keep += [pinned, status]
+        m.insert_points(sensor, pose, pinned, W, h, 16, stream=stream)
+        m.status_async(status, stream=stream)
+        ev = torch.cuda.Event()
+        ev.record(stream)
+        reads.append((status, ev))
+        R, eye, mt = oracle_frame(desc, pose, res, 1)
+        om.insert(R, eye, mt, desc.log_odds_hit, desc.log_odds_miss, pts)
+    last = 0
+    for status, ev in reads:
+        ev.synchronize()
+        leaves, err = int(status[0]), int(status[1])
+        assert err == 0 and leaves >= last and leaves > 0, (leaves, err)
+        last = leaves
+    torch.cuda.synchronize()
+    errs = compare_maps(m.export(), om.export())
+    assert not errs, "; ".join(errs[:5])
+
+
 @pytest.mark.parametrize("update_mode", [N.NM_UPDATE_LABEL, N.NM_UPDATE_ACCUMULATE])
 @pytest.mark.parametrize("clamp_mode", [N.NM_CLAMP_ALWAYS, N.NM_CLAMP_ON_CROSSING])
 @pytest.mark.parametrize("thres", [(0.3, -0.2), (1.6, -1.1)])
