@@ -64,6 +64,15 @@ int finish_build(nm_context ctx, nm::SimBuild& b, nm_simmap sm, cudaStream_t s) 
   NM_CUDA(cudaMemsetAsync(d_nvox, 0, 8, s));
   NM_CUDA(cudaMemsetAsync(d_count, 0, 4, s));
   NM_CUDA(nm::launch_compact(b, v, d_count, 1, d_bbox, d_nvox, s));
+  // empty-space distances for the render (one byte per leaf of the leaf box, twice)
+  const size_t lprod = (size_t)b.ldim[0] * b.ldim[1] * b.ldim[2];
+  uint8_t* d_dist = nullptr;
+  NM_CUDA(cudaMalloc((void**)&d_dist, 2 * lprod));
+  const cudaError_t de = nm::launch_skip_distances(b, v, d_dist, d_dist + lprod, s);
+  if (de != cudaSuccess) {
+    cudaFree(d_dist);
+    return fail(NM_ERR_CUDA, "sim map distances: %s", cudaGetErrorString(de));
+  }
   unsigned long long nvox = 0;
   NM_CUDA(cudaMemcpyAsync(sm->bbox, d_bbox, 24, cudaMemcpyDeviceToHost, s));
   NM_CUDA(cudaMemcpyAsync(&nvox, d_nvox, 8, cudaMemcpyDeviceToHost, s));
@@ -71,6 +80,7 @@ int finish_build(nm_context ctx, nm::SimBuild& b, nm_simmap sm, cudaStream_t s) 
   cudaFree(d_count);
   cudaFree(d_bbox);
   cudaFree(d_nvox);
+  cudaFree(d_dist);
   if (!b.borrowed) cudaFree(b.dense);
   b.dense = nullptr;
   sm->leaves = nleaves;

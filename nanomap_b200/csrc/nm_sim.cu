@@ -235,6 +235,67 @@ __global__ void __launch_bounds__(256) k_compact(SimBuild b, SimMapView v, uint3
   }
 }
 
+// ---- empty-space distances (render acceleration) -----------------------------------------
+//
+// Every empty leaf of a non-empty brick gets its Chebyshev distance d, in leaves and capped at
+// kSkipCap, to the nearest leaf with active voxels, stored as -d in its brick_leaves entry (-1:
+// an empty leaf next to an occupied one, as before).  The render then skips the cube of
+// (2d - 1)^3 leaves around it, all empty, in one exact step.  The distances come from a
+// separable L-infinity distance transform over the build's leaf box: one pass per axis, each
+// the minimum over offsets |o| < kSkipCap of max(|o|, the previous value at p + o); leaves
+// outside the box count as empty.
+constexpr int kSkipCap = 8;
+
+__global__ void k_skip_init(SimBuild b, uint8_t* dist) {
+  const long long total = (long long)b.ldim[0] * b.ldim[1] * b.ldim[2];
+  const uint4* src = reinterpret_cast<const uint4*>(b.dense);
+  for (long long pos = (long long)blockIdx.x * blockDim.x + threadIdx.x; pos < total;
+       pos += (long long)gridDim.x * blockDim.x) {
+    uint32_t any = 0u;
+#pragma unroll
+    for (int i = 0; i < 4; ++i) {
+      const uint4 w = __ldg(&src[pos * 4 + i]);
+      any |= w.x | w.y | w.z | w.w;
+    }
+    dist[pos] = any ? 0 : (uint8_t)kSkipCap;
+  }
+}
+
+__global__ void k_skip_pass(const uint8_t* src, uint8_t* dst, int nx, int ny, int nz, int axis) {
+  const long long total = (long long)nx * ny * nz;
+  const long long step = axis == 0 ? (long long)ny * nz : (axis == 1 ? (long long)nz : 1);
+  const int n = axis == 0 ? nx : (axis == 1 ? ny : nz);
+  for (long long pos = (long long)blockIdx.x * blockDim.x + threadIdx.x; pos < total;
+       pos += (long long)gridDim.x * blockDim.x) {
+    const int c = (int)((pos / step) % n);
+    int best = src[pos];
+    for (int o = 1; o < best; ++o) {  // an offset >= best cannot lower it
+      if (c - o >= 0) best = min(best, max(o, (int)src[pos - o * step]));
+      if (c + o < n) best = min(best, max(o, (int)src[pos + o * step]));
+    }
+    dst[pos] = (uint8_t)best;
+  }
+}
+
+__global__ void k_skip_write(SimBuild b, SimMapView v, const uint8_t* dist) {
+  const long long total = (long long)b.ldim[0] * b.ldim[1] * b.ldim[2];
+  for (long long pos = (long long)blockIdx.x * blockDim.x + threadIdx.x; pos < total;
+       pos += (long long)gridDim.x * blockDim.x) {
+    const int d = dist[pos];
+    if (d == 0) continue;  // an occupied leaf keeps its index
+    const int lx = (int)(pos / ((long long)b.ldim[2] * b.ldim[1])) + b.llo[0];
+    const int ly = (int)((pos / b.ldim[2]) % b.ldim[1]) + b.llo[1];
+    const int lz = (int)(pos % b.ldim[2]) + b.llo[2];
+    const long long bpos =
+        ((long long)((lx >> 3) - v.blo[0]) * v.bdim[1] + ((ly >> 3) - v.blo[1])) * v.bdim[2] +
+        ((lz >> 3) - v.blo[2]);
+    const int32_t blk = v.brick_index[bpos];
+    if (blk < 0) continue;
+    const int e = ((lx & 7) << 6) | ((ly & 7) << 3) | (lz & 7);
+    v.brick_leaves[(size_t)blk * 512 + e] = -d;
+  }
+}
+
 __global__ void k_fill_i32(int32_t* p, long long n, int32_t v) {
   for (long long i = (long long)blockIdx.x * blockDim.x + threadIdx.x; i < n;
        i += (long long)gridDim.x * blockDim.x)
@@ -337,6 +398,16 @@ cudaError_t launch_set_voxels(const SimBuild& b, const int32_t* d_ijk, long long
 cudaError_t launch_compact(const SimBuild& b, const SimMapView& v, uint32_t* d_count, int pass2,
                            int32_t* d_bbox, unsigned long long* d_nvox, cudaStream_t s) {
   k_compact<<<1184, 256, 0, s>>>(b, v, d_count, pass2, d_bbox, d_nvox);
+  return cudaGetLastError();
+}
+
+cudaError_t launch_skip_distances(const SimBuild& b, const SimMapView& v, uint8_t* d_a,
+                                  uint8_t* d_b, cudaStream_t s) {
+  k_skip_init<<<1184, 256, 0, s>>>(b, d_a);
+  k_skip_pass<<<1184, 256, 0, s>>>(d_a, d_b, b.ldim[0], b.ldim[1], b.ldim[2], 0);
+  k_skip_pass<<<1184, 256, 0, s>>>(d_b, d_a, b.ldim[0], b.ldim[1], b.ldim[2], 1);
+  k_skip_pass<<<1184, 256, 0, s>>>(d_a, d_b, b.ldim[0], b.ldim[1], b.ldim[2], 2);
+  k_skip_write<<<1184, 256, 0, s>>>(b, v, d_b);
   return cudaGetLastError();
 }
 

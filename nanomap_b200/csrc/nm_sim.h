@@ -29,7 +29,8 @@ struct SimMapView {
   int32_t llo[3], ldim[3];   // leaf box
   int32_t blo[3], bdim[3];   // brick box (64^3-voxel bricks)
   int32_t* brick_index;      // bdim product entries: block of the brick, -1 = empty brick
-  int32_t* brick_leaves;     // 512 entries per block: compact leaf index, -1 = empty leaf
+  int32_t* brick_leaves;     // 512 entries per block: compact leaf index; an empty leaf -d, d
+                             // its Chebyshev distance in leaves (>= 1, capped) to an occupied one
   uint32_t* leaf_words;      // 16 words per non-empty leaf
   float box_lo[3], box_hi[3];  // active voxel box in index space, [amin, amax + 1]
 };
@@ -91,6 +92,11 @@ cudaError_t launch_set_voxels(const SimBuild& b, const int32_t* d_ijk, long long
 cudaError_t launch_compact(const SimBuild& b, const SimMapView& v, uint32_t* d_count, int pass2,
                            int32_t* d_bbox, unsigned long long* d_nvox, cudaStream_t s);
 cudaError_t launch_fill_i32(int32_t* p, long long n, int32_t val, cudaStream_t s);
+// After compaction, with the dense leaf buffer still there: the empty leaves' distances to the
+// nearest occupied leaf into v.brick_leaves (-d); d_a and d_b hold one byte per leaf of the
+// build's leaf box each.
+cudaError_t launch_skip_distances(const SimBuild& b, const SimMapView& v, uint8_t* d_a,
+                                  uint8_t* d_b, cudaStream_t s);
 cudaError_t launch_sim_render_noisy(const SimMapView& v, const SimRayParams& rp, float* out,
                                     float sigma_coef, float drop, uint64_t seed, cudaStream_t s);
 cudaError_t launch_sim_render(const SimMapView& v, const SimRayParams& rp, float* out,

@@ -51,7 +51,8 @@ __device__ __forceinline__ int advance_axis(int k, int far, int s, float e, floa
   return est;
 }
 
-// 2 = empty brick (or outside the map), 1 = empty leaf, 0 = leaf with bits (*leaf = index).
+// 2 = empty brick (or outside the map), 1 = empty leaf (*leaf = d >= 1: every leaf within
+// Chebyshev distance d - 1 of it is empty too), 0 = leaf with bits (*leaf = index).
 __device__ __forceinline__ int sim_level(const SimMapView& v, int x, int y, int z, int* leaf) {
   const int bx = (x >> 6) - v.blo[0], by = (y >> 6) - v.blo[1], bz = (z >> 6) - v.blo[2];
   if ((unsigned)bx >= (unsigned)v.bdim[0] || (unsigned)by >= (unsigned)v.bdim[1] ||
@@ -62,7 +63,10 @@ __device__ __forceinline__ int sim_level(const SimMapView& v, int x, int y, int 
   if (blk < 0) return 2;
   const int e = (((x >> 3) & 7) << 6) | (((y >> 3) & 7) << 3) | ((z >> 3) & 7);
   const int32_t li = __ldg(&v.brick_leaves[(size_t)blk * 512 + e]);
-  if (li < 0) return 1;
+  if (li < 0) {
+    *leaf = -li;
+    return 1;
+  }
   *leaf = li;
   return 0;
 }
@@ -161,7 +165,9 @@ __device__ __forceinline__ float sim_cast(const SimMapView& v, const float eye[3
         continue;  // left the leaf: the outer walk takes the next level
       }
       first = false;
-      const int S = lvl == 2 ? 64 : 8;
+      // the empty cube to leave: the brick (64^3 voxels), or the leaves within Chebyshev
+      // distance d - 1 of this empty leaf (all empty; d = 1: the leaf itself)
+      const int dc = lvl == 1 ? leaf : 0;
       int far[3];
       float T[3];
 #pragma unroll
@@ -170,19 +176,19 @@ __device__ __forceinline__ float sim_cast(const SimMapView& v, const float eye[3
           far[a] = k[a];
           T[a] = INFINITY;
         } else {
-          far[a] = st[a] > 0 ? (k[a] | (S - 1)) : (k[a] & ~(S - 1));
+          const int L = k[a] >> 3;
+          far[a] = lvl == 2 ? (st[a] > 0 ? (k[a] | 63) : (k[a] & ~63))
+                            : (st[a] > 0 ? (L + dc) * 8 - 1 : (L - dc + 1) * 8);
           T[a] = plane_time(st[a] > 0 ? far[a] + 1 : far[a], eye[a], inv[a]);
         }
       }
       const int ax = (T[0] < T[1]) ? ((T[0] < T[2]) ? 0 : 2) : ((T[1] < T[2]) ? 1 : 2);
       const float Tx = T[ax];
       if (!(Tx <= t_out)) break;
-      if (S > 1) {
 #pragma unroll
-        for (int a = 0; a < 3; ++a)
-          if (a != ax && st[a] != 0)
-            k[a] = advance_axis(k[a], far[a], st[a], eye[a], dir[a], inv[a], Tx, a > ax);
-      }
+      for (int a = 0; a < 3; ++a)
+        if (a != ax && st[a] != 0)
+          k[a] = advance_axis(k[a], far[a], st[a], eye[a], dir[a], inv[a], Tx, a > ax);
       k[ax] = far[ax] + st[ax];
       t = Tx;
     }
