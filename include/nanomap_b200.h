@@ -31,7 +31,7 @@ extern "C" {
 #define NM_ERR_TIMEOUT 4     /* a bounded device-side wait gave up */
 #define NM_ERR_STATE 5       /* call not valid in the object's current state */
 #define NM_ERR_IO 6          /* file could not be read or parsed */
-#define NM_ERR_UNSUPPORTED 7 /* input format or option this build does not handle */
+#define NM_ERR_UNSUPPORTED 7 /* input format or option this library does not handle */
 
 /* sensor types (SharedParameters::_type, SharedParameters.h:197) */
 #define NM_SENSOR_FRUSTUM 0
@@ -388,7 +388,7 @@ int nm_simmap_create_voxels(nm_context ctx, float res, const int32_t* ijk, int64
 /* From a voxel-list file: 8-byte magic "NMSIMv1", float res (m), int64 count, then count
  * triplets of int32 voxel coordinates (little endian).  Replaces SimManager::loadSimGrid /
  * loadGridFromFile (SimManager.h:171-213); OpenVDB .vdb files are refused with
- * NM_ERR_UNSUPPORTED (no OpenVDB reader in this build). */
+ * NM_ERR_UNSUPPORTED (no OpenVDB reader in this library). */
 int nm_simmap_load(nm_context ctx, const char* path, nm_simmap* out);
 int nm_simmap_destroy(nm_simmap sm);
 /* active bounding box (min xyz, max xyz, inclusive), active voxel count, leaf count */

@@ -307,7 +307,7 @@ int nm_simmap_load(nm_context ctx, const char* path, nm_simmap* out) {
   const size_t len = std::strlen(path);
   if (len >= 4 && std::strcmp(path + len - 4, ".vdb") == 0)
     return fail(NM_ERR_UNSUPPORTED,
-                "%s: OpenVDB .vdb grids cannot be read by this build; convert the active voxels to "
+                "%s: OpenVDB .vdb grids cannot be read by this library; convert the active voxels to "
                 "an NMSIMv1 voxel list", path);
   FILE* f = std::fopen(path, "rb");
   if (!f) return fail(NM_ERR_IO, "cannot open sim grid '%s'", path);
