@@ -5,7 +5,11 @@
  * (NM_OK or an NM_ERR_* code); nm_last_error() gives the message of the calling thread's
  * last failure.  All device memory belongs to the library; inputs are borrowed for the call;
  * outputs go to caller buffers.  `stream` arguments are cudaStream_t values passed as void*
- * (NULL = the CUDA default stream).  A context is used from one host thread at a time.
+ * (NULL = the context's own stream).  A context is used from one host thread at a time.
+ * The work given to one map is ordered: use one stream per map, or order the streams (an
+ * event), since a frame's kernels share the map's tables, counters and claim-order buffers.
+ * Calls return once their work is enqueued unless NM_SYNC is given; host input must then
+ * stay unchanged until the stream has passed the call.
  * No call changes the caller's floating-point environment.
  *
  * Reference interfaces each entry point replaces are cited as path:line within the
