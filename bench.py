@@ -742,14 +742,28 @@ def run_depth_section(ctx, m, sensor, sim, spec, poses, stream, hbm, reps=10):
     torch.cuda.synchronize()
     bwd_ms = (time.perf_counter() - t0) * 1e3 / reps
     v2 = m.stats()["depth_visits"]
+    depth = m.depth_render(sensor, pos, R, values=vals, scale=scale, bias=bias)
+    torch.cuda.synchronize()
+    v3 = m.stats()["depth_visits"]
+    t0 = time.perf_counter()
+    for _ in range(reps):
+        m.depth_backward(sensor, pos, R, gd, values=vals, grad_values=gvals, scale=scale, bias=bias,
+                         depth=depth)
+    torch.cuda.synchronize()
+    bwd1_ms = (time.perf_counter() - t0) * 1e3 / reps
+    v4 = m.stats()["depth_visits"]
     fv = (v1 - v0) / reps
     bv = (v2 - v1) / reps
+    bv1 = (v4 - v3) / reps
     # gathered bytes: one 4-byte log-odds per voxel visit, 4 B per pixel written (forward);
-    # the adjoint replays twice and scatters one 4-byte gradient per visit of the second replay
+    # the adjoint replays twice (once when given the forward's depths, read at 4 B per pixel)
+    # and scatters one 4-byte gradient per visit of its last replay
     fwd_bytes = 4 * fv + 4 * H * W
     bwd_bytes = 4 * bv + 4 * (bv / 2) + 4 * H * W
+    bwd1_bytes = 4 * bv1 + 4 * bv1 + 8 * H * W
     out = {
         "forward_ms": fwd_ms, "backward_ms_incl_host_sync": bwd_ms,
+        "backward_given_depth_ms_incl_host_sync": bwd1_ms,
         "rays_per_s_forward": H * W / (fwd_ms / 1e3),
         "voxel_visits_per_frame": fv,
         "roofline_forward": {"bound": "hbm", "achieved": fwd_bytes / (fwd_ms / 1e3) / 1e9, "peak": hbm,
@@ -757,6 +771,9 @@ def run_depth_section(ctx, m, sensor, sim, spec, poses, stream, hbm, reps=10):
                              "bytes": "4 B log-odds per voxel visit + 4 B depth per pixel"},
         "roofline_backward": {"bound": "hbm", "achieved": bwd_bytes / (bwd_ms / 1e3) / 1e9, "peak": hbm,
                               "unit": "GB/s", "frac": bwd_bytes / (bwd_ms / 1e3) / 1e9 / hbm},
+        "roofline_backward_given_depth": {
+            "bound": "hbm", "achieved": bwd1_bytes / (bwd1_ms / 1e3) / 1e9, "peak": hbm,
+            "unit": "GB/s", "frac": bwd1_bytes / (bwd1_ms / 1e3) / 1e9 / hbm},
         "occupancy": f"sigmoid({scale} * log-odds + {bias}) per voxel length",
     }
     return out

@@ -343,10 +343,13 @@ int nm_depth_render(nm_map m, nm_sensor s, const nm_ray_pose* pose, const float*
  * floats like `values`; may be NULL)
  * and writes sum_pixels grad_depth * dD/dxi to grad_pose (host; may be NULL) for the
  * world-frame pose increment xi = (rho, phi): position + rho, rotation exp([phi]x) R.
- * The traversal is replayed, not stored (memory independent of ray length). */
+ * The traversal is replayed, not stored (memory independent of ray length): twice per pixel,
+ * or once when `depth` (device, hres*vres floats; may be NULL) holds nm_depth_render's output
+ * for the same pose, values, scale and bias, which then stands in for the first replay. */
 int nm_depth_backward(nm_map m, nm_sensor s, const nm_ray_pose* pose, const float* values,
                       uint64_t n_floats, float scale, float bias, const float* grad_depth,
-                      float* grad_values, double grad_pose[6], void* stream);
+                      const float* depth, float* grad_values, double grad_pose[6],
+                      void* stream);
 
 /* Scan-to-map pose refinement: `steps` Adam steps (learning rates lr_position in metres,
  * lr_rotation in radians, decayed to zero over the steps by a cosine schedule) on the mean

@@ -175,8 +175,8 @@ _SIGS = {
     "nm_map_values_copy": (C.c_int, [_P, _P, _U64, _PU64, _P]),
     "nm_map_slot_origins": (C.c_int, [_P, _PI32, _U64, _PU64]),
     "nm_depth_render": (C.c_int, [_P, _P, C.POINTER(NmRayPose), _P, _U64, _F, _F, _P, _P]),
-    "nm_depth_backward": (C.c_int, [_P, _P, C.POINTER(NmRayPose), _P, _U64, _F, _F, _P, _P, _PD,
-                                    _P]),
+    "nm_depth_backward": (C.c_int, [_P, _P, C.POINTER(NmRayPose), _P, _U64, _F, _F, _P, _P, _P,
+                                    _PD, _P]),
     "nm_pose_refine": (C.c_int, [_P, _P, C.POINTER(NmRayPose), _P, _F, _F, _F, _I32, _F, _F,
                                  _PF]),
     "nm_pose_refine_desc": (C.c_int, [_P, _P, C.POINTER(NmRayPose), _P, C.POINTER(NmRefineDesc),

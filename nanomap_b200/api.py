@@ -260,9 +260,10 @@ class Map:
         return out
 
     def depth_backward(self, sensor: Sensor, position, rotation, grad_depth, values=None,
-                       grad_values=None, scale=1.0, bias=0.0):
+                       grad_values=None, scale=1.0, bias=0.0, depth=None):
         """Adds sum grad_depth * dD/dlog-odds into grad_values (slot layout) and returns
-        sum grad_depth * dD/dxi (6,) float64 for xi = (rho, phi)."""
+        sum grad_depth * dD/dxi (6,) float64 for xi = (rho, phi).  `depth`: depth_render's
+        output for the same pose, values, scale and bias (one traversal replay fewer)."""
         import torch
         rp = _ray_pose(position, rotation)
         g = np.zeros(6)
@@ -271,8 +272,9 @@ class Map:
         gv = C.c_void_p(grad_values.data_ptr()) if grad_values is not None else None
         sizes = [t.numel() for t in (values, grad_values) if t is not None]
         nv = min(sizes) if sizes else 0
+        dp = C.c_void_p(depth.contiguous().data_ptr()) if depth is not None else None
         call("nm_depth_backward", self.h, sensor.h, C.byref(rp), vp, nv, scale, bias,
-             C.c_void_p(gd.data_ptr()), gv, g.ctypes.data_as(N._PD),
+             C.c_void_p(gd.data_ptr()), dp, gv, g.ctypes.data_as(N._PD),
              _stream(torch.cuda.current_stream()))
         return g
 

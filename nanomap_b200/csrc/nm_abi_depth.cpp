@@ -178,7 +178,8 @@ int nm_depth_render(nm_map m, nm_sensor s, const nm_ray_pose* pose, const float*
 
 int nm_depth_backward(nm_map m, nm_sensor s, const nm_ray_pose* pose, const float* values,
                       uint64_t n_floats, float scale, float bias, const float* grad_depth,
-                      float* grad_values, double grad_pose[6], void* stream) {
+                      const float* depth, float* grad_values, double grad_pose[6],
+                      void* stream) {
   nm::DepthParams p;
   int rc = make_depth_params(m, s, pose, scale, bias, &p);
   if (rc != NM_OK) return rc;
@@ -192,7 +193,7 @@ int nm_depth_backward(nm_map m, nm_sensor s, const nm_ray_pose* pose, const floa
   cudaStream_t s0 = nm::pick(m->ctx, stream);
   double* out6 = m->depth_scratch + (size_t)nb * 6;
   NM_CUDA(nm::launch_depth_backward(p, m->view, values ? values : m->view.values, grad_depth,
-                                    grad_values, m->depth_scratch, out6, s0));
+                                    depth, grad_values, m->depth_scratch, out6, s0));
   if (grad_pose) {
     NM_CUDA(cudaMemcpyAsync(grad_pose, out6, 6 * sizeof(double), cudaMemcpyDeviceToHost, s0));
     NM_CUDA(cudaStreamSynchronize(s0));

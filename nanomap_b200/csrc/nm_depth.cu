@@ -199,6 +199,22 @@ __device__ __forceinline__ float expected_index_depth(const DepthParams& p, cons
   return (float)t1 + acc;
 }
 
+// The time of the ray's first voxel crossing (the t_in of walk()'s first visit, the same
+// operations), or t_max when the ray stays in its start voxel.
+__device__ __forceinline__ double first_crossing(const double e[3], const double d[3],
+                                                 double t_max) {
+  double t = CUDART_INF;
+#pragma unroll
+  for (int a = 0; a < 3; ++a) {
+    const int s = d[a] > 0.0 ? 1 : (d[a] < 0.0 ? -1 : 0);
+    if (!s) continue;
+    const int v = (int)floor(e[a]);
+    const double c = __dmul_rn(__dadd_rn((double)(v + (s > 0 ? 1 : 0)), -e[a]), __drcp_rn(d[a]));
+    t = c < t ? c : t;
+  }
+  return t < t_max ? t : t_max;
+}
+
 // Gradient replay of one ray: adds gd-weighted log-odds gradients into grad_vals (when given)
 // and returns the ray's pose gradient (6: rho, phi) times gd.
 __device__ __forceinline__ void replay_gradients(const DepthParams& p, const MapView& m,
@@ -300,9 +316,11 @@ __global__ void __launch_bounds__(kDepthTile * kDepthTile) k_depth_forward(Depth
   add_depth_visits(m, n);
 }
 
+// `depth` (may be null): the forward's output at this pose and these values; the ray's
+// expected depth is then taken from it instead of a first replay.
 __global__ void __launch_bounds__(kDepthTile * kDepthTile) k_depth_backward(
-    DepthParams p, MapView m, const float* vals, const float* grad_depth, float* grad_vals,
-    double* partials) {
+    DepthParams p, MapView m, const float* vals, const float* grad_depth, const float* depth,
+    float* grad_vals, double* partials) {
   const int w = blockIdx.x * kDepthTile + threadIdx.x;
   const int h = blockIdx.y * kDepthTile + threadIdx.y;
   double acc[6] = {0, 0, 0, 0, 0, 0};
@@ -312,8 +330,13 @@ __global__ void __launch_bounds__(kDepthTile * kDepthTile) k_depth_backward(
     if (gd != 0.0f) {
       double d[3];
       pixel_dir(p, w, h, d);
-      float t1;
-      const float D = expected_index_depth(p, m, vals, d, &t1, &n);
+      float t1, D;
+      if (depth) {
+        D = depth[(size_t)h * p.width + w] / (float)p.res;
+        t1 = (float)first_crossing(p.eye, d, p.t_max);
+      } else {
+        D = expected_index_depth(p, m, vals, d, &t1, &n);
+      }
       float g6[6];
       replay_gradients(p, m, vals, d, D, t1, gd, grad_vals, g6, &n);
 #pragma unroll
@@ -414,11 +437,11 @@ cudaError_t launch_depth_forward(const DepthParams& p, const MapView& m, const f
 }
 
 cudaError_t launch_depth_backward(const DepthParams& p, const MapView& m, const float* vals,
-                                  const float* grad_depth, float* grad_vals, double* partials,
-                                  double* out6, cudaStream_t s) {
+                                  const float* grad_depth, const float* depth, float* grad_vals,
+                                  double* partials, double* out6, cudaStream_t s) {
   const dim3 g = depth_grid(p);
-  k_depth_backward<<<g, dim3(kDepthTile, kDepthTile), 0, s>>>(p, m, vals, grad_depth, grad_vals,
-                                                              partials);
+  k_depth_backward<<<g, dim3(kDepthTile, kDepthTile), 0, s>>>(p, m, vals, grad_depth, depth,
+                                                              grad_vals, partials);
   cudaError_t e = cudaGetLastError();
   if (e != cudaSuccess) return e;
   k_sum_partials<<<1, 256, 0, s>>>(partials, (int)(g.x * g.y), 6, out6);

@@ -244,8 +244,8 @@ int depth_partial_blocks(const DepthParams& p);
 cudaError_t launch_depth_forward(const DepthParams& p, const MapView& m, const float* vals,
                                  float* depth, cudaStream_t s);
 cudaError_t launch_depth_backward(const DepthParams& p, const MapView& m, const float* vals,
-                                  const float* grad_depth, float* grad_vals, double* partials,
-                                  double* out6, cudaStream_t s);
+                                  const float* grad_depth, const float* depth, float* grad_vals,
+                                  double* partials, double* out6, cudaStream_t s);
 cudaError_t launch_depth_refine(const DepthParams& p, const MapView& m, const float* vals,
                                 const float* target, float max_residual, float surface_offset,
                                 float edge, double* partials, double* out8, cudaStream_t s);

@@ -50,17 +50,17 @@ class ExpectedDepth(torch.autograd.Function):
         R = so3_exp(x[3:]) @ np.asarray(rotation, np.float64)
         vals = values.detach().contiguous()
         depth = m.depth_render(sensor, pos, R, values=vals, scale=scale, bias=bias)
-        ctx.save_for_backward(vals)
+        ctx.save_for_backward(vals, depth)
         ctx.args = (m, sensor, pos, R, x, scale, bias)
         return depth
 
     @staticmethod
     def backward(ctx, grad_depth):
-        (vals,) = ctx.saved_tensors
+        vals, depth = ctx.saved_tensors
         m, sensor, pos, R, x, scale, bias = ctx.args
         gv = torch.zeros_like(vals) if ctx.needs_input_grad[0] else None
         g = m.depth_backward(sensor, pos, R, grad_depth.contiguous(), values=vals,
-                             grad_values=gv, scale=scale, bias=bias)
+                             grad_values=gv, scale=scale, bias=bias, depth=depth)
         # the adjoint differentiates with respect to a left increment at the evaluated pose;
         # chain through the exponential map to the coordinates of xi
         gx = np.concatenate([g[:3], so3_left_jacobian(x[3:]).T @ g[3:]])

@@ -70,7 +70,10 @@ def test_forward_matches_fp64(world, scale, bias):
     assert err.max() <= 1e-5 + 1e-5 * ref.max(), err.max()
 
 
-def test_adjoint_matches_fp64_gradient(world):
+@pytest.mark.parametrize("given_depth", [False, True])
+def test_adjoint_matches_fp64_gradient(world, given_depth):
+    """Both adjoint forms (two replays per pixel, or one with the forward's depths given)
+    against the FP64 gradient."""
     import torch
     w = world
     pos, R = w["pose"]
@@ -79,8 +82,10 @@ def test_adjoint_matches_fp64_gradient(world):
     gd = rng.choice([-1.0, 0.0, 1.0], 640 * 480).astype(np.float32)
     vals = w["m"].values_copy()
     gv = torch.zeros_like(vals)
+    depth = (w["m"].depth_render(w["cam"], pos, R, values=vals, scale=scale, bias=bias)
+             if given_depth else None)
     g = w["m"].depth_backward(w["cam"], pos, R, torch.from_numpy(gd).cuda().view(480, 640),
-                              values=vals, grad_values=gv, scale=scale, bias=bias)
+                              values=vals, grad_values=gv, scale=scale, bias=bias, depth=depth)
     _, dpose, _, ogv = O.depth(w["osen"], pos, R, w["res"], w["org"], w["val"], scale=scale,
                                bias=bias, grad_depth=gd.astype(np.float64))
     ref = (dpose * gd[:, None]).sum(axis=0)
