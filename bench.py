@@ -780,14 +780,18 @@ def run_depth_section(ctx, m, sensor, sim, spec, poses, stream, hbm, reps=10):
 
 
 def run_refine_section(local, trials=3):
-    """Config 4: the small world mapped at 0.1 m from its 100-frame walk (exact ray-box ranges
-    + N(0, 0.01 m), fp32 log-odds); one 640x480 87 x 58 deg camera at 5 m starts at a pose of
-    the walk perturbed by U(+-5 cm), U(+-2 deg); 50 Adam steps on the L1 residual against the
-    simulated depth of the 0.1 m sim grid at the ground truth.  Three settings: the surface at
-    the voxel face the ray enters (occupancy scale 4), the surface at the middle of the ending
-    voxel (scale 12, silhouettes left out) started perturbed and started at the ground truth
-    (the objective's own minimum), and a map-consistent scan (the map's expected depth at the
-    ground truth) as the target."""
+    """Config 4: one 640x480 87 x 58 deg camera at 5 m starts at a pose of the small world's
+    100-frame walk perturbed by U(+-5 cm), U(+-2 deg); 50 Adam steps on the L1 residual against
+    the simulated depth of the 0.1 m sim grid at the ground truth, over a 0.1 m map (fp32
+    log-odds) of the walk's frames.  Two maps.  Built from the simulated depth itself (the
+    walk's frames ray-cast from the 0.1 m sim grid + N(0, 0.01 m)): the noise puts half of each
+    surface's end points in the voxel before it, so the map's surface lies one voxel in front
+    of the sim grid's; the prediction adds one entry step (surface_offset 1), occupancy scale
+    12, silhouettes out, 30 steps truncated at 0.3 m then 20 at 0.1 m.  Built from exact ray-box
+    ranges + N(0, 0.01 m): the surface at the voxel face the ray enters (occupancy scale 4), at
+    the middle of the ending voxel (scale 12, silhouettes out), each started perturbed and at
+    the ground truth (the objective's own minimum), and a map-consistent scan (the map's
+    expected depth at the ground truth) as the target."""
     import torch
 
     from nanomap_b200 import api as A
@@ -814,6 +818,16 @@ def run_refine_section(local, trials=3):
     sim = A.SimMap(ctx, spec.sim_res, boxes=scene.boxes, cylinders=scene.cylinders,
                    vox_min=scene.vox_min, vox_max=scene.vox_max)
     target = torch.zeros(480, 640, device="cuda")
+    ms = A.Map(ctx, A.map_desc(res=spec.map_res, clamp_min=spec.clamp[0], clamp_max=spec.clamp[1]))
+    gen = torch.Generator(device="cuda")
+    gen.manual_seed(101)
+    rs = torch.zeros(spec.height, spec.width, device="cuda")
+    for pos, q in traj:
+        sim.render(sensor, A.Pose(pos, q), rs)
+        noise = torch.randn(rs.shape, generator=gen, device="cuda") * spec.noise_sigma
+        rn = torch.where(rs > 0, rs + noise, torch.zeros_like(rs))
+        ms.insert_ranges(sensor, A.Pose(pos, q), torch.where(rn > 0, rn, torch.zeros_like(rn)))
+    torch.cuda.synchronize()
 
     def gap(p0, R0, p1, R1):
         ang = math.degrees(math.acos(max(-1.0, min(1.0, (np.trace(R1 @ R0.T) - 1) / 2))))
@@ -821,9 +835,19 @@ def run_refine_section(local, trials=3):
 
     face = dict(steps=50, lr_position=0.01, lr_rotation=0.004, scale=4.0, bias=0.0, max_residual=0.3)
     mid = dict(face, scale=12.0, surface_offset=0.5, edge_threshold=0.15)
+    full1 = dict(steps=30, lr_position=0.01, lr_rotation=0.004, scale=12.0, bias=0.0,
+                 max_residual=0.3, surface_offset=1.0, edge_threshold=0.3)
+    full2 = dict(full1, steps=20, lr_position=0.005, lr_rotation=0.002, max_residual=0.1)
     out = {"workload": ("plain_small world mapped at 0.1 m from 100 frames; 640x480 camera at 5 m; "
                         "target = 0.1 m sim depth at the ground truth; 50 Adam steps from "
                         "U(+-5 cm), U(+-2 deg)"), "map_build_s": build_s, "trials": []}
+
+    def two_stage(p0, R0, tgt):
+        torch.cuda.synchronize()
+        t0 = time.perf_counter()
+        pa, Ra, la = ms.pose_refine(cam, p0, R0, tgt, **full1)
+        p1, R1, lb = ms.pose_refine(cam, pa, Ra, tgt, **full2)
+        return p1, R1, la, lb, (time.perf_counter() - t0) * 1e3 / 50
     for trial in range(trials):
         gt = A.Pose(*traj[10 + 20 * trial])
         gpos, gR = A.Map.ray_pose(cam, gt)
@@ -832,6 +856,15 @@ def run_refine_section(local, trials=3):
         R = so3_exp(np.radians(rr.uniform(-2.0, 2.0, 3))) @ gR
         sim.render(cam, gt, target)
         row = {"start_error": gap(gpos, gR, pos, R)}
+        sm = {}
+        for name, p0, R0 in (("perturbed", pos, R), ("from_truth", gpos, gR)):
+            p1, R1, la, lb, mps = two_stage(p0, R0, target)
+            te, ae = gap(gpos, gR, p1, R1)
+            sm[name] = {"final_error_m": te, "final_error_deg": ae, "loss_first": float(la[0]),
+                        "loss_last": float(lb[-1]), "ms_per_step": mps, "end": (p1, R1)}
+        g = gap(*sm["perturbed"].pop("end"), *sm["from_truth"].pop("end"))
+        sm["end_vs_minimum"] = {"m": g[0], "deg": g[1]}
+        row["sim_depth_map_full_voxel_two_stage"] = sm
         runs = [("sim_depth_face_scale4", pos, R, target, face),
                 ("sim_depth_mid_voxel", pos, R, target, mid),
                 ("sim_depth_mid_voxel_from_truth", gpos, gR, target, mid)]
@@ -854,6 +887,7 @@ def run_refine_section(local, trials=3):
         out["trials"].append(row)
     sim.close()
     cam.close()
+    ms.close()
     m.close()
     sensor.close()
     ctx.close()
