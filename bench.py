@@ -360,8 +360,9 @@ def run_ours(args, rank, world, local):
     # memory and copied inside each call, and each frame's status read back to the host.
     # Measured as a stream of frames (the primary number): every call asynchronous, each followed
     # by an asynchronous status read; before issuing frame k + 1 the host waits for frame k - 1's
-    # status, so frame k's copy (two staging buffers, the map's copy stream) runs while frame
-    # k - 1 is walked.  And as synchronous calls (NM_SYNC), one frame at a time.
+    # status, so frame k + 1's copy (two staging buffers, the map's copy stream) runs while frame
+    # k is walked (waiting for frame k - 2 instead measured 3 % slower).  And as synchronous
+    # calls (NM_SYNC), one frame at a time.
     e2e = None
     if args.e2e_steps > 0:
         # 32 distinct frames in turn (157 MB of records: more than L2; each call reads its
@@ -1332,7 +1333,7 @@ def main():
     ap.add_argument("--steps", type=int, default=50)
     ap.add_argument("--warmup", type=int, default=5)
     ap.add_argument("--impl", choices=["ours", "reference"], default="ours")
-    ap.add_argument("--e2e-steps", type=int, default=30)
+    ap.add_argument("--e2e-steps", type=int, default=100)
     ap.add_argument("--cpu-baseline-s", type=float, default=12.0)
     ap.add_argument("--batched-ticks", type=int, default=200,
                     help="ticks of the 16-agent batched comparison, warm-up included (0 = skip)")

@@ -215,6 +215,35 @@ __device__ __forceinline__ double first_crossing(const double e[3], const double
   return t < t_max ? t : t_max;
 }
 
+// Voxels nearer the eye than this (index units) take their log-odds gradient through
+// scatter_gradient: there the rays of a warp share voxels and thousands of rays add into the
+// same voxel.  Farther out lanes rarely share a voxel at the same step and a plain atomic is
+// cheaper (headline frame, given depths: 1.59 ms plain, 1.44 ms aggregated everywhere,
+// 1.09 ms aggregated within this span).
+constexpr double kGatherSpan = 48.0;
+
+// Adds x into grad_vals[slot * 512 + l] (nothing for slot < 0) with one atomic per voxel
+// among the warp's lanes at this call: lanes holding the same voxel (rays near the eye and
+// neighbouring rays walk the same voxels at the same step) are summed by a shuffle tree first,
+// in rounds that each fold every second remaining lane of a group into the one before it.
+__device__ __forceinline__ void scatter_gradient(float* grad_vals, int slot, int l, float x) {
+  const unsigned act = __activemask();
+  const int lane = (int)((threadIdx.y * blockDim.x + threadIdx.x) & 31u);
+  const unsigned long long key =
+      slot >= 0 ? (unsigned long long)slot * kLeafVoxels + (unsigned)l : ~0ull;
+  const unsigned peers = __match_any_sync(act, key);
+  int rank = __popc(peers & ((1u << lane) - 1u));  // position among the voxel's lanes
+  unsigned above = lane == 31 ? 0u : peers & (~0u << (lane + 1));
+  while (__any_sync(act, above != 0u)) {
+    const int nxt = __ffs(above);
+    const float y = __shfl_sync(act, x, nxt ? nxt - 1 : lane);
+    if (nxt) x += y;
+    above &= ~__ballot_sync(act, rank & 1);  // odd ranks have been folded into their left
+    rank >>= 1;
+  }
+  if (slot >= 0 && lane == __ffs(peers) - 1) atomicAdd(&grad_vals[key], x);
+}
+
 // Gradient replay of one ray: adds gd-weighted log-odds gradients into grad_vals (when given)
 // and returns the ray's pose gradient (6: rho, phi) times gd.
 __device__ __forceinline__ void replay_gradients(const DepthParams& p, const MapView& m,
@@ -251,9 +280,12 @@ __device__ __forceinline__ void replay_gradients(const DepthParams& p, const Map
     const float u = sg * Dk;
     const float em1 = expm1f(-u);
     const float Pn = P + T * (sg > 0.0f ? -em1 / sg : Dk);
-    if (grad_vals && slot >= 0) {
+    if (grad_vals) {
       const float dsig = T * Dk * Dk * seg_g(u, em1) - Dk * (tail0 - Pn);
-      atomicAdd(&grad_vals[(size_t)slot * kLeafVoxels + l], gv * dc.sig * dsig);
+      if (t_in < kGatherSpan)
+        scatter_gradient(grad_vals, slot, l, gv * dc.sig * dsig);
+      else if (slot >= 0)
+        atomicAdd(&grad_vals[(size_t)slot * kLeafVoxels + l], gv * dc.sig * dsig);
     }
     P = Pn;
     T *= 1.0f + em1;
