@@ -379,6 +379,84 @@ __global__ void __launch_bounds__(kDepthTile * kDepthTile) k_depth_backward(
   block_partials<6>(acc, partials);
 }
 
+// One walk giving the expected depth (as expected_index_depth, with the entry step) and the
+// ray's pose gradient for a unit depth gradient, for the refinement step.  replay_gradients'
+// crossing term is c (A - P) with c = (sigma_B - sigma_A) / d_a, P the transmittance integral
+// before the crossing and A the whole integral (D / res - t_1), so per axis the sums of c,
+// c P, c t and c t P (in double: A and P are close where c is large) give the gradient once
+// A is known at the end of the walk.  Returns D (index units); g6 as replay_gradients' for
+// gd = 1.
+__device__ __forceinline__ float depth_and_pose_gradient(const DepthParams& p, const MapView& m,
+                                                         const float* vals, const double d[3],
+                                                         uint32_t* visits, float* entry_step,
+                                                         float g6[6]) {
+  LeafCache c{kEmptyKey, -1};
+  DensityCache dc;
+  float T = 1.0f, acc = 0.0f, W = 0.0f, sg_prev = 0.0f;
+  double t1 = p.t_max;
+  bool first = true;
+  uint32_t n = 0;
+  const float step[3] = {(float)(1.0 / fabs(d[0])), (float)(1.0 / fabs(d[1])),
+                         (float)(1.0 / fabs(d[2]))};
+  const float inv_d[3] = {(float)(1.0 / d[0]), (float)(1.0 / d[1]), (float)(1.0 / d[2])};
+  double sc[3] = {0.0, 0.0, 0.0}, scp[3] = {0.0, 0.0, 0.0};
+  double sct[3] = {0.0, 0.0, 0.0}, sctp[3] = {0.0, 0.0, 0.0};
+  walk(p.eye, d, p.t_max, [&](const int v[3], double t_in, int a_in, double t_out, int) {
+    ++n;
+    int slot, l;
+    dc.at(p, voxel_logodds(m, vals, c, v, &slot, &l));
+    const float sg = dc.sg;
+    const float Dk = (float)(t_out - t_in);
+    if (first) {
+      t1 = t_in;
+      first = false;
+    }
+    if (sg != sg_prev) {
+      const double cd = (double)((sg - sg_prev) * (a_in == 0 ? inv_d[0] : (a_in == 1 ? inv_d[1] : inv_d[2])));
+      const double P = (double)acc, ti = (double)(float)t_in;
+      if (a_in == 0) {
+        sc[0] += cd;
+        scp[0] += cd * P;
+        sct[0] += cd * ti;
+        sctp[0] += cd * ti * P;
+      } else if (a_in == 1) {
+        sc[1] += cd;
+        scp[1] += cd * P;
+        sct[1] += cd * ti;
+        sctp[1] += cd * ti * P;
+      } else {
+        sc[2] += cd;
+        scp[2] += cd * P;
+        sct[2] += cd * ti;
+        sctp[2] += cd * ti * P;
+      }
+    }
+    const float em1 = expm1f(-sg * Dk);
+    acc += T * (sg > 0.0f ? -em1 / sg : Dk);
+    W -= T * em1 * step[a_in];
+    T *= 1.0f + em1;
+    sg_prev = sg;
+  });
+  *visits += n;
+  *entry_step = T < 1.0f ? W / (1.0f - T) : 0.0f;
+  const double A = (double)acc;
+  float ge[3], gdir[3];
+#pragma unroll
+  for (int a = 0; a < 3; ++a) {
+    ge[a] = (float)(scp[a] - A * sc[a]);
+    gdir[a] = (float)(sctp[a] - A * sct[a]);
+  }
+  const float r = (float)p.res;
+  const float dx = (float)d[0], dy = (float)d[1], dz = (float)d[2];
+  g6[0] = ge[0];
+  g6[1] = ge[1];
+  g6[2] = ge[2];
+  g6[3] = r * (dy * gdir[2] - dz * gdir[1]);
+  g6[4] = r * (dz * gdir[0] - dx * gdir[2]);
+  g6[5] = r * (dx * gdir[1] - dy * gdir[0]);
+  return (float)t1 + acc;
+}
+
 // Whether pixel (w, h) of the target lies on a silhouette: a 4-neighbour inside the image
 // without a return, or with a range more than `edge` metres away.
 __device__ __forceinline__ bool target_edge(const float* target, int W, int H, int w, int h,
@@ -414,19 +492,16 @@ __global__ void __launch_bounds__(kDepthTile * kDepthTile) k_depth_refine(
         !(edge > 0.0f && target_edge(target, p.width, p.height, w, h, r, edge))) {
       double d[3];
       pixel_dir(p, w, h, d);
-      float t1, step = 0.0f;
-      const float D = expected_index_depth(p, m, vals, d, &t1, &n,
-                                           surface_offset != 0.0f ? &step : nullptr);
+      float step, g6[6];
+      const float D = depth_and_pose_gradient(p, m, vals, d, &n, &step, g6);
       const float res = (D + surface_offset * step) * (float)p.res - r;
       const bool clipped = max_residual > 0.0f && fabsf(res) > max_residual;
       acc[0] = clipped ? (double)max_residual : fabs((double)res);
       acc[1] = 1.0;
       const float gd = clipped ? 0.0f : (res > 0.0f ? 1.0f : (res < 0.0f ? -1.0f : 0.0f));
       if (gd != 0.0f) {
-        float g6[6];
-        replay_gradients(p, m, vals, d, D, t1, gd, nullptr, g6, &n);
 #pragma unroll
-        for (int i = 0; i < 6; ++i) acc[2 + i] = (double)g6[i];
+        for (int i = 0; i < 6; ++i) acc[2 + i] = (double)(gd * g6[i]);
       }
     }
   }
