@@ -392,11 +392,25 @@ int nm_simmap_create_primitives(nm_context ctx, float res, const int32_t vox_min
 /* From a list of active voxel coordinates (3 ints each, host memory). */
 int nm_simmap_create_voxels(nm_context ctx, float res, const int32_t* ijk, int64_t n,
                             nm_simmap* out);
-/* From a voxel-list file: 8-byte magic "NMSIMv1", float res (m), int64 count, then count
- * triplets of int32 voxel coordinates (little endian).  Replaces SimManager::loadSimGrid /
- * loadGridFromFile (SimManager.h:171-213); OpenVDB .vdb files are refused with
- * NM_ERR_UNSUPPORTED (no OpenVDB reader in this library). */
+/* From a file.  Replaces SimManager::loadSimGrid / loadGridFromFile (SimManager.h:171-213).
+ * A path ending in ".vdb" is an OpenVDB file: the active voxels of its grid named "grid" (the
+ * file's first grid when none is), read by nm_vdb_active_voxels; the voxel size must be
+ * uniform and the translation a whole number of voxels.  Any other path is a voxel list:
+ * 8-byte magic "NMSIMv1", float res (m), int64 count, then count triplets of int32 voxel
+ * coordinates (little endian). */
 int nm_simmap_load(nm_context ctx, const char* path, nm_simmap* out);
+/* Active voxels of a grid in an OpenVDB .vdb file (no GPU used): file format versions
+ * 222-224 (OpenVDB 3 onwards), trees 5-4-3 of float (also saved as half) or double values,
+ * values stored raw, zip or blosc (only the tree topology is read: leaf value masks and
+ * active tiles, the latter expanded to their voxels; no decompression), transforms that are a
+ * scale and a translation.  `grid` names the grid (NULL: "grid", else the file's first grid).
+ * voxel_size and translation (3 doubles each, may be NULL) map index to world:
+ * world = index * voxel_size + translation, voxel (i, j, k) covering index [i, i + 1) etc.
+ * With ijk NULL only *n is set; else up to max_voxels triplets are written (more active
+ * voxels than that: NM_ERR_CAPACITY, *n the count).  Grids of more than 2^28 active voxels
+ * are refused (NM_ERR_CAPACITY). */
+int nm_vdb_active_voxels(const char* path, const char* grid, double voxel_size[3],
+                         double translation[3], int32_t* ijk, int64_t max_voxels, int64_t* n);
 int nm_simmap_destroy(nm_simmap sm);
 /* active bounding box (min xyz, max xyz, inclusive), active voxel count, leaf count */
 int nm_simmap_info(nm_simmap sm, int32_t bbox[6], uint64_t* active_voxels, uint64_t* leaves);

@@ -417,6 +417,21 @@ class TickPlan:
             pass
 
 
+def vdb_active_voxels(path: str, grid: str | None = None):
+    """nm_vdb_active_voxels: (voxel size (3,), translation (3,), active voxels (n, 3) int32) of
+    a grid in an OpenVDB .vdb file; host only."""
+    vs = np.zeros(3)
+    tr = np.zeros(3)
+    n = C.c_int64()
+    g = grid.encode() if grid is not None else None
+    call("nm_vdb_active_voxels", str(path).encode(), g, vs.ctypes.data_as(N._PD),
+         tr.ctypes.data_as(N._PD), None, 0, C.byref(n))
+    ijk = np.zeros((max(n.value, 1), 3), np.int32)
+    call("nm_vdb_active_voxels", str(path).encode(), g, vs.ctypes.data_as(N._PD),
+         tr.ctypes.data_as(N._PD), ijk.ctypes.data_as(N._PI32), n.value, C.byref(n))
+    return vs, tr, ijk[:n.value]
+
+
 class SimMap:
     """Device sim map (replaces the NanoVDB sim grid of SimHandler)."""
 
@@ -437,6 +452,13 @@ class SimMap:
             call("nm_simmap_create_primitives", ctx.h, C.c_float(res), lo, hi,
                  b.ctypes.data_as(N._PD), len(b), c.ctypes.data_as(N._PD), len(c), C.byref(h))
         self.h = h
+
+    @classmethod
+    def load(cls, ctx: Context, path: str) -> "SimMap":
+        """nm_simmap_load: an OpenVDB .vdb grid or an NMSIMv1 voxel list."""
+        h = C.c_void_p()
+        call("nm_simmap_load", ctx.h, str(path).encode(), C.byref(h))
+        return cls._adopt(ctx, None, h)
 
     def info(self):
         bb = (C.c_int32 * 6)()

@@ -305,10 +305,33 @@ int nm_simmap_load(nm_context ctx, const char* path, nm_simmap* out) {
   if (!ctx || !path || !out) return fail(NM_ERR_ARG, "null argument");
   *out = nullptr;
   const size_t len = std::strlen(path);
-  if (len >= 4 && std::strcmp(path + len - 4, ".vdb") == 0)
-    return fail(NM_ERR_UNSUPPORTED,
-                "%s: OpenVDB .vdb grids cannot be read by this library; convert the active voxels to "
-                "an NMSIMv1 voxel list", path);
+  if (len >= 4 && std::strcmp(path + len - 4, ".vdb") == 0) {
+    // the grid named "grid" (else the file's first grid), as SimManager::loadGridFromFile
+    // (SimManager.h:196-213) reads it: its active voxels, on a uniform voxel size, translated by
+    // whole voxels (world = (index + shift) * res)
+    double vs[3], tr[3];
+    int64_t n = 0;
+    int rc = nm_vdb_active_voxels(path, nullptr, vs, tr, nullptr, 0, &n);
+    if (rc != NM_OK) return rc;
+    if (!(vs[0] > 0.0) || std::fabs(vs[1] - vs[0]) > 1e-9 * vs[0] ||
+        std::fabs(vs[2] - vs[0]) > 1e-9 * vs[0])
+      return fail(NM_ERR_UNSUPPORTED, "%s: voxel size (%g, %g, %g) is not uniform", path, vs[0],
+                  vs[1], vs[2]);
+    int32_t shift[3];
+    for (int a = 0; a < 3; ++a) {
+      const double q = tr[a] / vs[0];
+      shift[a] = (int32_t)std::lround(q);
+      if (std::fabs(q - shift[a]) > 1e-6 || std::fabs(q) > 1e9)
+        return fail(NM_ERR_UNSUPPORTED, "%s: translation (%g, %g, %g) is not a whole number of voxels",
+                    path, tr[0], tr[1], tr[2]);
+    }
+    std::vector<int32_t> ijk((size_t)n * 3);
+    rc = nm_vdb_active_voxels(path, nullptr, vs, tr, ijk.data(), n, &n);
+    if (rc != NM_OK) return rc;
+    for (int64_t i = 0; i < n; ++i)
+      for (int a = 0; a < 3; ++a) ijk[3 * i + a] += shift[a];
+    return nm_simmap_create_voxels(ctx, (float)vs[0], ijk.data(), n, out);
+  }
   FILE* f = std::fopen(path, "rb");
   if (!f) return fail(NM_ERR_IO, "cannot open sim grid '%s'", path);
   char magic[8];

@@ -51,6 +51,38 @@ def test_voxel_list_constructor(ctx):
     assert g.info()[0] == o.bbox()[0]
 
 
+@pytest.mark.parametrize("collapse,compression", [(False, 0x3), (True, 0x6)])
+def test_vdb_sim_grid_loads_like_its_voxels(ctx, tmp_path, collapse, compression):
+    """A sim grid read from a .vdb file (nm_simmap_load) holds the file's active voxels: the
+    same sim map, and the same range images, as those voxels given directly; a translation of
+    whole voxels shifts them.  (The files come from the test-side writer: tests/vdb_files.py.)"""
+    from tests.vdb_files import write_vdb
+    sc, g, _ = _maps(ctx, "plain_small")
+    res = sc.spec.sim_res
+    vox = A.simmap_voxels(g)
+    p = write_vdb(tmp_path / "scene.vdb", vox, res=res, collapse=collapse, compression=compression,
+                  codes=(0, 6, 3))
+    loaded = A.SimMap.load(ctx, p)
+    assert np.array_equal(A.simmap_voxels(loaded), vox)
+    assert loaded.info() == g.info()
+    desc = camera_desc(sc.spec, hres=320, vres=240)
+    sensor = A.Sensor(ctx, desc)
+    traj = S.trajectory(sc, 3, seed=7)
+    for pos, q in traj:
+        a = np.zeros((240, 320), np.float32)
+        b = np.zeros((240, 320), np.float32)
+        g.render(sensor, A.Pose(pos, q), a)
+        loaded.render(sensor, A.Pose(pos, q), b)
+        assert np.array_equal(a, b)
+    t = write_vdb(tmp_path / "moved.vdb", vox, res=res, transform="UniformScaleTranslateMap",
+                  translation=(2 * res, -3 * res, 0.0))
+    moved = A.SimMap.load(ctx, t)
+    assert np.array_equal(A.simmap_voxels(moved), vox + np.array([2, -3, 0], np.int32))
+    for m in (loaded, moved, g):
+        m.close()
+    sensor.close()
+
+
 @pytest.mark.parametrize("name,n", [("plain_small", 6), ("sim_headline", 2)])
 def test_render_matches_oracle(ctx, name, n):
     import torch
