@@ -415,7 +415,8 @@ class Manager {
 
 class SimManager {
  public:
-  // Loads the sim grid named by the config's SimGrid: key (NMSIMv1 voxel list) and the agents.
+  // Loads the sim grid named by the config's SimGrid: key (a .vdb grid or an NMSIMv1 voxel
+  // list) and the agents.
   explicit SimManager(std::shared_ptr<config::Config> config) : config_(std::move(config)) {
     nm_simmap sm = nullptr;
     detail::check(nm_simmap_load(detail::context(), config_->simGrid().c_str(), &sm));
