@@ -303,7 +303,8 @@ class Agent {
     nm_agent_info a;
     detail::check(nm_config_agent(cfg.handle(), index, &a));
     if (a.spawn_random)
-      throw Error(NM_ERR_UNSUPPORTED, "nanomap_b200: random agent spawns need the OpenVDB sim grid");
+      throw Error(NM_ERR_UNSUPPORTED,
+                  "nanomap_b200: random agent spawns are not supported; give the agent a spawn pose");
     pose_.position = Vector3f(a.position[0], a.position[1], a.position[2]);
     pose_.orientation = Quaternionf(std::sqrt(0.5f), 0.f, 0.f, -std::sqrt(0.5f));
     num_obs_ = a.num_obs;
