@@ -71,6 +71,15 @@ __device__ __forceinline__ float seg_g(float u, float em1) {
   return (u * (1.0f + em1) + em1) / (u * u);
 }
 
+// Every walk of a ray (forward, adjoint replays, refinement) ends where its transmittance
+// falls below this: what the rest of the ray could add to the expected depth is at most
+// kStopTransmittance x its remaining length (< 1e-6 voxel lengths for rays up to 1000
+// voxels), each such FP32 term being below half an ulp of the running integral once that
+// exceeds 0.01 voxels, and the rest's gradients carry the factor T too (there, the FP32 tail
+// A - P is rounding noise).  The three walks compute T with the same operations, so they
+// stop at the same voxel.
+constexpr float kStopTransmittance = 1e-9f;
+
 // Density of a log-odds value, memoised on the last value seen: along a ray most voxels share
 // a few values (the clamp of observed free space, 0 for unknown space), so the softplus and
 // sigmoid are mostly reused and each visit costs one expm1.
@@ -89,9 +98,9 @@ struct DensityCache {
   }
 };
 
-// Visits every voxel of the ray after the start voxel: f(v, t_in, a_in, t_out, a_out), the
+// Visits the voxels of the ray after the start voxel: f(v, t_in, a_in, t_out, a_out), the
 // voxel entered at t_in < t_max across axis a_in and left at t_out = min(next crossing,
-// t_max) across a_out (-1 when clamped to t_max).  Crossings are (boundary - e) * (1 / d),
+// t_max) across a_out (-1 when clamped to t_max); f returns false to end the walk.  Crossings are (boundary - e) * (1 / d),
 // the reciprocal taken once per ray; per-axis state is kept in scalars (no local memory).
 template <class F>
 __device__ __forceinline__ void walk(const double e[3], const double d[3], double t_max, F&& f) {
@@ -141,10 +150,7 @@ __device__ __forceinline__ void walk(const double e[3], const double d[3], doubl
       t_out = tx;
     }
     const int v[3] = {vx, vy, vz};
-    if (t_out < t_max)
-      f(v, t_in, a_in, t_out, a_out);
-    else
-      f(v, t_in, a_in, t_max, -1);
+    if (!(t_out < t_max ? f(v, t_in, a_in, t_out, a_out) : f(v, t_in, a_in, t_max, -1))) break;
     a_in = a_out;
     t_in = t_out;
   }
@@ -192,6 +198,7 @@ __device__ __forceinline__ float expected_index_depth(const DepthParams& p, cons
     acc += T * (sg > 0.0f ? -em1 / sg : Dk);
     if (entry_step) W -= T * em1 * step[a_in];
     T *= 1.0f + em1;
+    return T >= kStopTransmittance;
   });
   *t1_out = (float)t1;
   *visits += n;
@@ -290,6 +297,7 @@ __device__ __forceinline__ void replay_gradients(const DepthParams& p, const Map
     P = Pn;
     T *= 1.0f + em1;
     sg_prev = sg;
+    return T >= kStopTransmittance;
   });
   *visits += n;
   const float r = gd * (float)p.res;
@@ -436,6 +444,7 @@ __device__ __forceinline__ float depth_and_pose_gradient(const DepthParams& p, c
     W -= T * em1 * step[a_in];
     T *= 1.0f + em1;
     sg_prev = sg;
+    return T >= kStopTransmittance;
   });
   *visits += n;
   *entry_step = T < 1.0f ? W / (1.0f - T) : 0.0f;
