@@ -121,10 +121,21 @@ def test_facade_matches_direct_abi(ctx, tmp_path):
     assert nd == 75
 
 
-def test_vdb_sim_grid_is_refused(ctx, tmp_path):
+def test_vdb_sim_grid_errors(ctx, tmp_path):
+    """nm_simmap_load on .vdb paths that are not OpenVDB files, or are files of a version or
+    transform the reader does not take: an error status, no sim map."""
     import ctypes as C
+
+    from tests.vdb_files import write_vdb
+    h = C.c_void_p()
     p = tmp_path / "grid.vdb"
     p.write_bytes(b"\0" * 16)
-    h = C.c_void_p()
-    rc = N.lib().nm_simmap_load(ctx.h, str(p).encode(), C.byref(h))
-    assert rc == N.NM_ERR_UNSUPPORTED and b"OpenVDB" in N.lib().nm_last_error()
+    assert N.lib().nm_simmap_load(ctx.h, str(p).encode(), C.byref(h)) == N.NM_ERR_IO
+    assert b"not an OpenVDB file" in N.lib().nm_last_error()
+    v = np.array([[0, 0, 0], [1, 2, 3]], np.int32)
+    for name, kw in (("old", dict(version=221)), ("rot", dict(transform="RotatedAffineMap")),
+                     ("half_voxel", dict(transform="UniformScaleTranslateMap",
+                                         translation=(0.05, 0.0, 0.0)))):
+        q = write_vdb(tmp_path / f"{name}.vdb", v, res=0.1, **kw)
+        assert N.lib().nm_simmap_load(ctx.h, str(q).encode(), C.byref(h)) == N.NM_ERR_UNSUPPORTED, name
+    assert not h.value
