@@ -76,26 +76,6 @@ int reserve_scratch(nm_map m, size_t n) {
   return NM_OK;
 }
 
-// exp([phi]x) R (Rodrigues), row-major, in place.
-void rotate_left(const double phi[3], double R[9]) {
-  const double th = std::sqrt(phi[0] * phi[0] + phi[1] * phi[1] + phi[2] * phi[2]);
-  double K[9] = {0, -phi[2], phi[1], phi[2], 0, -phi[0], -phi[1], phi[0], 0};
-  double E[9] = {1, 0, 0, 0, 1, 0, 0, 0, 1};
-  if (th > 0.0) {
-    const double a = std::sin(th) / th, b = (1.0 - std::cos(th)) / (th * th);
-    double K2[9];
-    for (int r = 0; r < 3; ++r)
-      for (int c = 0; c < 3; ++c)
-        K2[3 * r + c] = K[3 * r] * K[c] + K[3 * r + 1] * K[3 + c] + K[3 * r + 2] * K[6 + c];
-    for (int i = 0; i < 9; ++i) E[i] += a * K[i] + b * K2[i];
-  }
-  double out[9];
-  for (int r = 0; r < 3; ++r)
-    for (int c = 0; c < 3; ++c)
-      out[3 * r + c] = E[3 * r] * R[c] + E[3 * r + 1] * R[3 + c] + E[3 * r + 2] * R[6 + c];
-  std::memcpy(R, out, sizeof(out));
-}
-
 }  // namespace
 
 extern "C" {
@@ -233,41 +213,37 @@ int nm_pose_refine_desc(nm_map m, nm_sensor s, nm_ray_pose* pose, const float* t
   if (rc != NM_OK) return rc;
   NM_CUDA(cudaSetDevice(m->ctx->device));
   const int nb = nm::depth_partial_blocks(p);
-  rc = reserve_scratch(m, (size_t)nb * 8 + 8);
+  // partials, then the device state, then the losses
+  const size_t state_doubles = (sizeof(nm::RefineState) + 7) / 8;
+  rc = reserve_scratch(m, (size_t)nb * 8 + state_doubles + ((size_t)steps + 2) / 2);
   if (rc != NM_OK) return rc;
   cudaStream_t s0 = m->ctx->stream;
-  double* out8 = m->depth_scratch + (size_t)nb * 8;
-  // Adam on the left world-frame increment (rho, phi), re-linearised at every step, with the
-  // learning rates decayed to zero over the steps (cosine schedule).
-  const double b1 = 0.9, b2 = 0.999, eps = 1e-8;
-  double mom[6] = {0, 0, 0, 0, 0, 0}, var[6] = {0, 0, 0, 0, 0, 0};
-  nm_ray_pose cur = *pose;
-  for (int it = 0; it <= steps; ++it) {
-    rc = make_depth_params(m, s, &cur, scale, bias, &p);
-    if (rc != NM_OK) return rc;
+  nm::RefineState* d_st = reinterpret_cast<nm::RefineState*>(m->depth_scratch + (size_t)nb * 8);
+  float* d_losses = reinterpret_cast<float*>(m->depth_scratch + (size_t)nb * 8 + state_doubles);
+  nm::RefineState st{};
+  std::memcpy(st.position, pose->position, sizeof(st.position));
+  std::memcpy(st.R, pose->rotation, sizeof(st.R));
+  st.res = p.res;
+  st.t_max = p.t_max;
+  st.lr_position = lr_position;
+  st.lr_rotation = lr_rotation;
+  st.steps = steps;
+  NM_CUDA(cudaMemcpyAsync(d_st, &st, sizeof(st), cudaMemcpyHostToDevice, s0));
+  // every step queued at once: the kernels read the pose from d_st, the update kernel writes it
+  for (int it = 0; it <= steps; ++it)
     NM_CUDA(nm::launch_depth_refine(p, m->view, m->view.values, target, max_residual,
                                     desc->surface_offset, desc->edge_threshold,
-                                    m->depth_scratch, out8, s0));
-    double h[8];
-    NM_CUDA(cudaMemcpyAsync(h, out8, sizeof(h), cudaMemcpyDeviceToHost, s0));
-    NM_CUDA(cudaStreamSynchronize(s0));
-    if (h[1] < 1.0) return fail(NM_ERR_ARG, "target has no valid pixels");
-    if (losses) losses[it] = (float)(h[0] / h[1]);
-    if (it == steps) break;
-    const double t = (double)(it + 1);
-    const double decay = 0.5 * (1.0 + std::cos(3.14159265358979323846 * it / steps));
-    double step[6];
-    for (int i = 0; i < 6; ++i) {
-      const double g = h[2 + i] / h[1];
-      mom[i] = b1 * mom[i] + (1.0 - b1) * g;
-      var[i] = b2 * var[i] + (1.0 - b2) * g * g;
-      const double mh = mom[i] / (1.0 - std::pow(b1, t));
-      const double vh = var[i] / (1.0 - std::pow(b2, t));
-      step[i] = -decay * (i < 3 ? lr_position : lr_rotation) * mh / (std::sqrt(vh) + eps);
-    }
-    for (int a = 0; a < 3; ++a) cur.position[a] += step[a];
-    rotate_left(step + 3, cur.rotation);
-  }
+                                    m->depth_scratch, d_st, d_losses, it, s0));
+  NM_CUDA(cudaMemcpyAsync(&st, d_st, sizeof(st), cudaMemcpyDeviceToHost, s0));
+  NM_CUDA(cudaStreamSynchronize(s0));
+  if (st.error & nm::kRefineNoPixels) return fail(NM_ERR_ARG, "target has no valid pixels");
+  if (st.error & nm::kRefineOutOfRange)
+    return fail(NM_ERR_ARG, "pose left the map's addressable range (+-%d voxels)", 1 << 23);
+  if (losses)
+    NM_CUDA(cudaMemcpy(losses, d_losses, ((size_t)steps + 1) * sizeof(float), cudaMemcpyDeviceToHost));
+  nm_ray_pose cur = *pose;
+  std::memcpy(cur.position, st.position, sizeof(cur.position));
+  std::memcpy(cur.rotation, st.R, sizeof(cur.rotation));
   *pose = cur;
   return NM_OK;
 }

@@ -489,8 +489,14 @@ __device__ __forceinline__ bool target_edge(const float* target, int W, int H, i
 // for the gradient.  Silhouette pixels of the target are left out when edge > 0.  Partials:
 // loss, count, 6 gradients.
 __global__ void __launch_bounds__(kDepthTile * kDepthTile) k_depth_refine(
-    DepthParams p, MapView m, const float* vals, const float* target, float max_residual,
-    float surface_offset, float edge, double* partials) {
+    DepthParams p0, MapView m, const float* vals, const float* target, float max_residual,
+    float surface_offset, float edge, const RefineState* st, double* partials) {
+  // the pose of this step, from the device state (the eye as the host computes it)
+  DepthParams p = p0;
+#pragma unroll
+  for (int a = 0; a < 3; ++a) p.eye[a] = __ddiv_rn(st->position[a], p.res);
+#pragma unroll
+  for (int i = 0; i < 9; ++i) p.R[i] = st->R[i];
   const int w = blockIdx.x * kDepthTile + threadIdx.x;
   const int h = blockIdx.y * kDepthTile + threadIdx.y;
   double acc[8] = {0, 0, 0, 0, 0, 0, 0, 0};
@@ -516,6 +522,72 @@ __global__ void __launch_bounds__(kDepthTile * kDepthTile) k_depth_refine(
   }
   add_depth_visits(m, n);
   block_partials<8>(acc, partials);
+}
+
+// exp([phi]x) R (Rodrigues), row-major, in place.
+__device__ void rotate_left(const double phi[3], double R[9]) {
+  const double th = sqrt(phi[0] * phi[0] + phi[1] * phi[1] + phi[2] * phi[2]);
+  const double K[9] = {0, -phi[2], phi[1], phi[2], 0, -phi[0], -phi[1], phi[0], 0};
+  double E[9] = {1, 0, 0, 0, 1, 0, 0, 0, 1};
+  if (th > 0.0) {
+    const double a = sin(th) / th, b = (1.0 - cos(th)) / (th * th);
+    for (int r = 0; r < 3; ++r)
+      for (int c = 0; c < 3; ++c)
+        E[3 * r + c] += a * K[3 * r + c] +
+                        b * (K[3 * r] * K[c] + K[3 * r + 1] * K[3 + c] + K[3 * r + 2] * K[6 + c]);
+  }
+  double out[9];
+  for (int r = 0; r < 3; ++r)
+    for (int c = 0; c < 3; ++c)
+      out[3 * r + c] = E[3 * r] * R[c] + E[3 * r + 1] * R[3 + c] + E[3 * r + 2] * R[6 + c];
+  for (int i = 0; i < 9; ++i) R[i] = out[i];
+}
+
+// One block: the step's partials summed in a fixed order (loss, count, 6 gradients), then
+// thread 0 records the mean loss and, before the last step, applies Adam on the left
+// world-frame increment (rho, phi) with the learning rates cosine-decayed to zero.
+__global__ void k_refine_update(const double* partials, int n, RefineState* st, float* losses,
+                                int it) {
+  __shared__ double s[256];
+  __shared__ double h[8];
+  for (int c = 0; c < 8; ++c) {
+    double acc = 0.0;
+    for (int i = threadIdx.x; i < n; i += blockDim.x) acc += partials[(size_t)i * 8 + c];
+    s[threadIdx.x] = acc;
+    __syncthreads();
+    for (int k = blockDim.x / 2; k > 0; k >>= 1) {
+      if ((int)threadIdx.x < k) s[threadIdx.x] += s[threadIdx.x + k];
+      __syncthreads();
+    }
+    if (threadIdx.x == 0) h[c] = s[0];
+    __syncthreads();
+  }
+  if (threadIdx.x != 0 || st->error) return;
+  if (h[1] < 1.0) {
+    st->error |= kRefineNoPixels;
+    return;
+  }
+  losses[it] = (float)(h[0] / h[1]);
+  if (it >= st->steps) return;
+  const double b1 = 0.9, b2 = 0.999, eps = 1e-8;
+  const double t = (double)(it + 1);
+  const double decay = 0.5 * (1.0 + cos(CUDART_PI * it / st->steps));
+  double step[6];
+  for (int i = 0; i < 6; ++i) {
+    const double g = h[2 + i] / h[1];
+    st->mom[i] = b1 * st->mom[i] + (1.0 - b1) * g;
+    st->var[i] = b2 * st->var[i] + (1.0 - b2) * g * g;
+    const double mh = st->mom[i] / (1.0 - pow(b1, t));
+    const double vh = st->var[i] / (1.0 - pow(b2, t));
+    step[i] = -decay * (i < 3 ? st->lr_position : st->lr_rotation) * mh / (sqrt(vh) + eps);
+  }
+  for (int a = 0; a < 3; ++a)
+    if (fabs((st->position[a] + step[a]) / st->res) + st->t_max + 2.0 > (double)(1 << 23) - 16.0) {
+      st->error |= kRefineOutOfRange;
+      return;
+    }
+  for (int a = 0; a < 3; ++a) st->position[a] += step[a];
+  rotate_left(step + 3, st->R);
 }
 
 // Column sums of an (n, N) array of partials in a fixed order (deterministic).
@@ -566,13 +638,14 @@ cudaError_t launch_depth_backward(const DepthParams& p, const MapView& m, const 
 
 cudaError_t launch_depth_refine(const DepthParams& p, const MapView& m, const float* vals,
                                 const float* target, float max_residual, float surface_offset,
-                                float edge, double* partials, double* out8, cudaStream_t s) {
+                                float edge, double* partials, RefineState* st, float* losses,
+                                int it, cudaStream_t s) {
   const dim3 g = depth_grid(p);
   k_depth_refine<<<g, dim3(kDepthTile, kDepthTile), 0, s>>>(p, m, vals, target, max_residual,
-                                                            surface_offset, edge, partials);
+                                                            surface_offset, edge, st, partials);
   cudaError_t e = cudaGetLastError();
   if (e != cudaSuccess) return e;
-  k_sum_partials<<<1, 256, 0, s>>>(partials, (int)(g.x * g.y), 8, out8);
+  k_refine_update<<<1, 256, 0, s>>>(partials, (int)(g.x * g.y), st, losses, it);
   return cudaGetLastError();
 }
 

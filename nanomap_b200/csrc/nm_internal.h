@@ -246,9 +246,24 @@ cudaError_t launch_depth_forward(const DepthParams& p, const MapView& m, const f
 cudaError_t launch_depth_backward(const DepthParams& p, const MapView& m, const float* vals,
                                   const float* grad_depth, const float* depth, float* grad_vals,
                                   double* partials, double* out6, cudaStream_t s);
+// A refinement's pose and Adam state, kept on the device so that its steps queue without a
+// host round trip: each step's kernel reads the pose from it and the update kernel writes it.
+struct RefineState {
+  double position[3];  // metres
+  double R[9];         // world-from-sensor, row-major
+  double mom[6], var[6];
+  double res, t_max;   // to recompute the eye (index units) and check the addressable range
+  float lr_position, lr_rotation;
+  int32_t steps;
+  uint32_t error;  // kRefineNoPixels / kRefineOutOfRange; once set, the pose stays
+};
+constexpr uint32_t kRefineNoPixels = 1u, kRefineOutOfRange = 2u;
+// Step `it` of a refinement: the loss and pose gradient at st's pose (partials, then a fixed-
+// order sum), losses[it] = mean loss, and for it < steps the Adam update of st.
 cudaError_t launch_depth_refine(const DepthParams& p, const MapView& m, const float* vals,
                                 const float* target, float max_residual, float surface_offset,
-                                float edge, double* partials, double* out8, cudaStream_t s);
+                                float edge, double* partials, RefineState* st, float* losses,
+                                int it, cudaStream_t s);
 cudaError_t filter_reserve(FilterBuffers* b, int64_t n, cudaStream_t s);
 void filter_release(FilterBuffers* b);
 int filter_key_bits(float max_time);  // bits per axis of a filter key; 0 if out of range
