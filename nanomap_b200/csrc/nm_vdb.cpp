@@ -48,10 +48,18 @@ constexpr int64_t kMaxVoxels = int64_t(1) << 28;  // host list of 12 B per voxel
 struct Reader {
   FILE* f = nullptr;
   std::string err;
+  int code = NM_ERR_IO;  // status of the first error
   ~Reader() {
     if (f) std::fclose(f);
   }
   bool ok() const { return err.empty(); }
+  bool fail(int c, std::string msg) {
+    if (ok()) {
+      code = c;
+      err = std::move(msg);
+    }
+    return false;
+  }
   bool bytes(void* dst, size_t n) {
     if (!ok()) return false;
     if (n && std::fread(dst, 1, n, f) != n) err = "file ends early";
@@ -122,10 +130,7 @@ struct Grid {
 bool skip_values(Reader& r, const Grid& g, uint32_t count, uint32_t active, int log2dim) {
   const int8_t code = r.get<int8_t>();
   if (!r.ok()) return false;
-  if (code < 0 || code > 6) {
-    r.err = "bad value-compression code";
-    return false;
-  }
+  if (code < 0 || code > 6) return r.fail(NM_ERR_IO, "bad value-compression code");
   if (code == 2 || code == 4 || code == 5) r.skip((int64_t)g.value_size);  // inactive value 0
   if (code == 5) r.skip((int64_t)g.value_size);                            // inactive value 1
   if (code >= 3 && code <= 5) r.skip((int64_t)Mask(log2dim).w.size() * 8);  // selection mask
@@ -134,10 +139,8 @@ bool skip_values(Reader& r, const Grid& g, uint32_t count, uint32_t active, int 
   if (g.compression & (kCompressZip | kCompressBlosc)) {
     const int64_t stored = r.get<int64_t>();
     if (!r.ok()) return false;
-    if (stored <= 0 && -stored != raw) {
-      r.err = "uncompressed chunk of unexpected size";
-      return false;
-    }
+    if (stored <= 0 && -stored != raw)
+      return r.fail(NM_ERR_IO, "uncompressed chunk of unexpected size");
     return r.skip(stored <= 0 ? -stored : stored);
   }
   return r.skip(raw);
@@ -146,10 +149,8 @@ bool skip_values(Reader& r, const Grid& g, uint32_t count, uint32_t active, int 
 // Adds the active voxels of the cube [o, o + edge)^3.
 bool emit_cube(Reader& r, Grid& g, const int32_t o[3], int edge) {
   const int64_t n = (int64_t)edge * edge * edge;
-  if (g.n_voxels + n > kMaxVoxels) {
-    r.err = "more active voxels than this reader takes (2^28)";
-    return false;
-  }
+  if (g.n_voxels + n > kMaxVoxels)
+    return r.fail(NM_ERR_CAPACITY, "more active voxels than this reader takes (2^28)");
   if (g.out)
     for (int x = 0; x < edge; ++x)
       for (int y = 0; y < edge; ++y)
@@ -169,10 +170,8 @@ bool read_leaf(Reader& r, Grid& g, const int32_t o[3]) {
   if (!vm.load(r)) return false;
   for (uint32_t n = 0; n < 512; ++n) {
     if (!vm.on(n)) continue;
-    if (g.n_voxels + 1 > kMaxVoxels) {
-      r.err = "more active voxels than this reader takes (2^28)";
-      return false;
-    }
+    if (g.n_voxels + 1 > kMaxVoxels)
+      return r.fail(NM_ERR_CAPACITY, "more active voxels than this reader takes (2^28)");
     if (g.out && g.n_voxels < g.max_out) {
       int32_t* v = g.out + 3 * g.n_voxels;
       v[0] = o[0] + (int32_t)(n >> 6);
@@ -217,14 +216,11 @@ bool read_internal(Reader& r, Grid& g, const int32_t o[3], int log2dim, int chil
 
 bool read_topology(Reader& r, Grid& g) {
   const int32_t buffers = r.get<int32_t>();
-  if (r.ok() && buffers != 1) r.err = "multi-buffer tree";
+  if (r.ok() && buffers != 1) r.fail(NM_ERR_UNSUPPORTED, "multi-buffer tree");
   r.skip((int64_t)g.value_size);  // background
   const uint32_t tiles = r.get<uint32_t>(), children = r.get<uint32_t>();
   if (!r.ok()) return false;
-  if (tiles > (1u << 24) || children > (1u << 24)) {
-    r.err = "implausible root table";
-    return false;
-  }
+  if (tiles > (1u << 24) || children > (1u << 24)) return r.fail(NM_ERR_IO, "implausible root table");
   for (uint32_t i = 0; i < tiles && r.ok(); ++i) {
     int32_t c[3];
     r.bytes(c, 12);
@@ -268,17 +264,14 @@ bool read_transform(Reader& r, double vs[3], double tr[3]) {
     if (!r.bytes(m, sizeof(m))) return false;
     for (int i = 0; i < 3; ++i)
       for (int j = 0; j < 3; ++j)
-        if (i != j && m[4 * i + j] != 0.0) {
-          r.err = "rotated or sheared AffineMap";
-          return false;
-        }
+        if (i != j && m[4 * i + j] != 0.0)
+          return r.fail(NM_ERR_UNSUPPORTED, "rotated or sheared AffineMap");
     for (int a = 0; a < 3; ++a) {
       vs[a] = m[5 * a];
       tr[a] = m[12 + a];
     }
   } else {
-    r.err = "transform '" + type + "' is not a scale and translation";
-    return false;
+    return r.fail(NM_ERR_UNSUPPORTED, "transform '" + type + "' is not a scale and translation");
   }
   return r.ok();
 }
@@ -364,16 +357,10 @@ int nm_vdb_active_voxels(const char* path, const char* grid, double voxel_size[3
   g.compression = r.get<uint32_t>();
   r.skip_meta();
   double vs[3] = {0, 0, 0}, tr[3] = {0, 0, 0};
-  if (!r.ok() || !read_transform(r, vs, tr))
-    return nm::fail(r.err.find("transform") != std::string::npos || r.err.find("AffineMap") != std::string::npos
-                        ? NM_ERR_UNSUPPORTED : NM_ERR_IO,
-                    "%s: %s", path, r.err.c_str());
+  if (!r.ok() || !read_transform(r, vs, tr)) return nm::fail(r.code, "%s: %s", path, r.err.c_str());
   g.out = ijk;
   g.max_out = ijk ? max_voxels : 0;
-  if (!read_topology(r, g)) {
-    const bool cap = r.err.find("2^28") != std::string::npos;
-    return nm::fail(cap ? NM_ERR_CAPACITY : NM_ERR_IO, "%s: %s", path, r.err.c_str());
-  }
+  if (!read_topology(r, g)) return nm::fail(r.code, "%s: %s", path, r.err.c_str());
   if (voxel_size) std::memcpy(voxel_size, vs, sizeof(vs));
   if (translation) std::memcpy(translation, tr, sizeof(tr));
   *n = g.n_voxels;
