@@ -411,6 +411,12 @@ int nm_simmap_load(nm_context ctx, const char* path, nm_simmap* out);
  * are refused (NM_ERR_CAPACITY). */
 int nm_vdb_active_voxels(const char* path, const char* grid, double voxel_size[3],
                          double translation[3], int32_t* ijk, int64_t max_voxels, int64_t* n);
+/* Writes n active voxels (3 int32 each) as a float grid named `grid` (NULL: "grid") of an
+ * OpenVDB-layout file (format version 224, tree 5-4-3, uniform scale voxel_size, values 0
+ * stored raw with active-mask compression, grid class "unknown"), the layout
+ * nm_vdb_active_voxels reads. */
+int nm_vdb_write_active_voxels(const char* path, const char* grid, double voxel_size,
+                               const int32_t* ijk, int64_t n);
 int nm_simmap_destroy(nm_simmap sm);
 /* active bounding box (min xyz, max xyz, inclusive), active voxel count, leaf count */
 int nm_simmap_info(nm_simmap sm, int32_t bbox[6], uint64_t* active_voxels, uint64_t* leaves);
@@ -512,9 +518,11 @@ int nm_cave_cells(nm_cave c, int32_t* xyz, int64_t max_cells, int64_t* n);
  * dilate^half_width(M) minus erode^half_width(M) (half_width 3, closing 1 in the reference). */
 int nm_cave_simmap(nm_cave c, int32_t shell, int32_t half_width, int32_t closing,
                    nm_simmap* out);
-/* nm_cave_simmap written as an NMSIMv1 voxel list (the format nm_simmap_load reads) in
- * place of the reference's .vdb file; a path ending in ".vdb" is written with ".nmsim"
- * instead, and the name written is copied to written_path (may be NULL, 512 bytes). */
+/* nm_cave_simmap written to `path`, the reference's file_out (CaveGen.cpp:299-325): a path
+ * ending in ".vdb" gets the band's active voxels as the float grid "grid" of a .vdb file
+ * (nm_vdb_write_active_voxels; the reference writes the same active set as a level set), any
+ * other path an NMSIMv1 voxel list; both are what nm_simmap_load reads.  The name written is
+ * copied to written_path (may be NULL, 512 bytes). */
 int nm_cave_save(nm_cave c, int32_t shell, int32_t half_width, int32_t closing,
                  const char* path, char* written_path);
 

@@ -505,9 +505,10 @@ namespace mapgen {
 // nanomap::mapgen::CaveGen (CaveGen.h:32-68) over nm_cave_*: the same stages in the same
 // order give the same cave for the same #cavegenconfig file (the fill reproduces the
 // reference's srand/rand draws without changing the caller's rand() state).  The cells stay
-// on the device; invertAndSave / Save write an NMSIMv1 voxel list (a file_out ending in
-// ".vdb" is written as ".nmsim"; writtenPath() names it) that SimManager's sim grid loader
-// reads, and simMap() hands the cave to a SimManager without a file.
+// on the device; invertAndSave / Save write file_out (ending in ".vdb": the active band as the
+// float grid "grid" of a .vdb file, as the reference writes it; otherwise an NMSIMv1 voxel
+// list; writtenPath() names it) for SimManager's sim grid loader, and simMap() hands the cave
+// to a SimManager without a file.
 class CaveGen {
  public:
   explicit CaveGen(std::string config) { loadConfig(std::move(config)); }

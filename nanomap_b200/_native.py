@@ -160,6 +160,7 @@ _SIGS = {
     "nm_simmap_load": (C.c_int, [_P, C.c_char_p, C.POINTER(_P)]),
     "nm_vdb_active_voxels": (C.c_int, [C.c_char_p, C.c_char_p, _PD, _PD, _P, _I64,
                                        C.POINTER(_I64)]),
+    "nm_vdb_write_active_voxels": (C.c_int, [C.c_char_p, C.c_char_p, C.c_double, _P, _I64]),
     "nm_sensor_create": (C.c_int, [_P, C.POINTER(NmSensorDesc), C.POINTER(_P)]),
     "nm_sensor_destroy": (C.c_int, [_P]),
     "nm_sensor_params": (C.c_int, [_P, _PF]),

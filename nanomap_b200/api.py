@@ -432,6 +432,13 @@ def vdb_active_voxels(path: str, grid: str | None = None):
     return vs, tr, ijk[:n.value]
 
 
+def vdb_write_active_voxels(path: str, voxels, voxel_size: float, grid: str | None = None):
+    """nm_vdb_write_active_voxels: voxels ((n, 3) int) as a float grid of a .vdb file."""
+    v = np.ascontiguousarray(voxels, dtype=np.int32).reshape(-1, 3)
+    call("nm_vdb_write_active_voxels", str(path).encode(), grid.encode() if grid else None,
+         C.c_double(voxel_size), v.ctypes.data_as(N._PI32), len(v))
+
+
 class SimMap:
     """Device sim map (replaces the NanoVDB sim grid of SimHandler)."""
 

@@ -468,10 +468,9 @@ int nm_cave_simmap(nm_cave c, int32_t shell, int32_t half_width, int32_t closing
 int nm_cave_save(nm_cave c, int32_t shell, int32_t half_width, int32_t closing,
                  const char* path, char* written_path) {
   if (!c || !path) return fail(NM_ERR_ARG, "null argument");
-  std::string name(path);
-  if (name.size() >= 4 && name.compare(name.size() - 4, 4, ".vdb") == 0)
-    name = name.substr(0, name.size() - 4) + ".nmsim";
+  const std::string name(path);
   if (name.size() >= 512) return fail(NM_ERR_ARG, "output path too long");
+  const bool vdb = name.size() >= 4 && name.compare(name.size() - 4, 4, ".vdb") == 0;
   nm_simmap sm = nullptr;
   int rc = build_cave_simmap(c, shell, half_width, closing, &sm);
   if (rc != NM_OK) return rc;
@@ -491,6 +490,13 @@ int nm_cave_save(nm_cave c, int32_t shell, int32_t half_width, int32_t closing,
         ijk.push_back(origins[3 * q + 1] + ((l >> 3) & 7));
         ijk.push_back(origins[3 * q + 2] + (l & 7));
       }
+  if (vdb) {
+    rc = nm_vdb_write_active_voxels(name.c_str(), "grid", c->desc.grid_res, ijk.data(),
+                                    (int64_t)(ijk.size() / 3));
+    if (rc != NM_OK) return rc;
+    if (written_path) std::snprintf(written_path, 512, "%s", name.c_str());
+    return NM_OK;
+  }
   FILE* f = std::fopen(name.c_str(), "wb");
   if (!f) return fail(NM_ERR_IO, "cannot write '%s'", name.c_str());
   const char magic[8] = {'N', 'M', 'S', 'I', 'M', 'v', '1', '\0'};

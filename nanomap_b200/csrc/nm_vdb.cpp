@@ -28,10 +28,13 @@
 //            hold COMPRESS_ZIP (0x1) or COMPRESS_BLOSC (0x4) (a count <= 0: -count raw bytes)
 //   masks: 2^(3 log2dim) bits in 64-bit words; bit n of a node is local (x, y, z) with
 //            n = (x << 2 log2dim) | (y << log2dim) | z
+#include <algorithm>
+#include <array>
 #include <cmath>
 #include <cstdint>
 #include <cstdio>
 #include <cstring>
+#include <map>
 #include <memory>
 #include <string>
 #include <vector>
@@ -367,5 +370,154 @@ int nm_vdb_active_voxels(const char* path, const char* grid, double voxel_size[3
   if (ijk && g.n_voxels > max_voxels)
     return nm::fail(NM_ERR_CAPACITY, "%s: %lld active voxels, room for %lld", path,
                     (long long)g.n_voxels, (long long)max_voxels);
+  return NM_OK;
+}
+
+// ---- writer: the same layout, for sim grids of active voxels --------------------------------
+namespace {
+
+struct Out {
+  std::vector<unsigned char> b;
+  template <class T>
+  void put(const T& v) {
+    const unsigned char* p = reinterpret_cast<const unsigned char*>(&v);
+    b.insert(b.end(), p, p + sizeof(T));
+  }
+  void raw(const void* p, size_t n) {
+    const unsigned char* q = static_cast<const unsigned char*>(p);
+    b.insert(b.end(), q, q + n);
+  }
+  void str(const std::string& s) {
+    put<uint32_t>((uint32_t)s.size());
+    raw(s.data(), s.size());
+  }
+  void meta(const std::string& name, const std::string& type, const void* v, uint32_t n) {
+    str(name);
+    str(type);
+    put<uint32_t>(n);
+    raw(v, n);
+  }
+};
+
+struct LeafMask {
+  uint64_t w[8] = {0, 0, 0, 0, 0, 0, 0, 0};
+};
+
+// A node's values: code 0 (every inactive value is the background), then the active values
+// only (the grid is written with COMPRESS_ACTIVE_MASK), all 0.
+void put_values(Out& o, uint32_t active) {
+  o.put<int8_t>(0);
+  for (uint32_t i = 0; i < active; ++i) o.put<float>(0.0f);
+}
+
+}  // namespace
+
+int nm_vdb_write_active_voxels(const char* path, const char* grid, double voxel_size,
+                               const int32_t* ijk, int64_t n) {
+  if (!path || (n > 0 && !ijk) || n < 0) return nm::fail(NM_ERR_ARG, "invalid argument");
+  if (!(voxel_size > 0.0) || !std::isfinite(voxel_size))
+    return nm::fail(NM_ERR_ARG, "voxel size must be positive");
+  // leaves by origin; the tree's order below comes from sorting origins by the nodes' offsets
+  std::map<std::array<int32_t, 3>, LeafMask> leaves;
+  for (int64_t i = 0; i < n; ++i) {
+    const int32_t x = ijk[3 * i], y = ijk[3 * i + 1], z = ijk[3 * i + 2];
+    LeafMask& m = leaves[{x & ~7, y & ~7, z & ~7}];
+    const uint32_t bit = (uint32_t)(((x & 7) << 6) | ((y & 7) << 3) | (z & 7));
+    m.w[bit >> 6] |= uint64_t(1) << (bit & 63);
+  }
+  // root children (32^3 nodes, 4096 voxels) -> their 16^3 children by offset -> leaves by offset
+  std::map<std::array<int32_t, 3>, std::map<uint32_t, std::map<uint32_t, const LeafMask*>>> tree;
+  for (const auto& kv : leaves) {
+    const auto& o = kv.first;
+    const std::array<int32_t, 3> r = {o[0] & ~4095, o[1] & ~4095, o[2] & ~4095};
+    const uint32_t n5 = (uint32_t)((((o[0] - r[0]) >> 7) << 10) | (((o[1] - r[1]) >> 7) << 5) |
+                                   ((o[2] - r[2]) >> 7));
+    const int32_t i4[3] = {o[0] & ~127, o[1] & ~127, o[2] & ~127};
+    const uint32_t n4 = (uint32_t)((((o[0] - i4[0]) >> 3) << 8) | (((o[1] - i4[1]) >> 3) << 4) |
+                                   ((o[2] - i4[2]) >> 3));
+    tree[r][n5][n4] = &kv.second;
+  }
+  const uint32_t compression = kCompressActiveMask;
+  Out topo;
+  topo.put<int32_t>(1);     // buffer count
+  topo.put<float>(0.0f);    // background
+  topo.put<uint32_t>(0);    // root tiles
+  topo.put<uint32_t>((uint32_t)tree.size());
+  std::vector<const LeafMask*> order;  // leaves in the order the buffers follow
+  for (const auto& r : tree) {
+    topo.raw(r.first.data(), 12);
+    std::vector<uint64_t> cm5(512, 0);
+    for (const auto& c : r.second) cm5[c.first >> 6] |= uint64_t(1) << (c.first & 63);
+    topo.raw(cm5.data(), 4096);
+    std::vector<uint64_t> vm5(512, 0);
+    topo.raw(vm5.data(), 4096);
+    put_values(topo, 0);
+    for (const auto& c : r.second) {
+      std::vector<uint64_t> cm4(64, 0), vm4(64, 0);
+      for (const auto& l : c.second) cm4[l.first >> 6] |= uint64_t(1) << (l.first & 63);
+      topo.raw(cm4.data(), 512);
+      topo.raw(vm4.data(), 512);
+      put_values(topo, 0);
+      for (const auto& l : c.second) {
+        topo.raw(l.second->w, 64);
+        order.push_back(l.second);
+      }
+    }
+  }
+  Out buffers;
+  for (const LeafMask* m : order) {
+    buffers.raw(m->w, 64);
+    uint32_t active = 0;
+    for (uint64_t w : m->w) active += (uint32_t)__builtin_popcountll(w);
+    put_values(buffers, active);
+  }
+  const std::string name = grid ? grid : "grid";
+  Out head;
+  head.put<int64_t>(kVdbMagic);
+  head.put<uint32_t>(224);  // file format version
+  head.put<uint32_t>(0);    // library version major, minor: not written by the OpenVDB library
+  head.put<uint32_t>(0);
+  head.put<uint8_t>(1);     // grids stored with offsets
+  const char uuid[] = "6e6d2d62-3230-302d-7669-6d2d61637469";
+  head.raw(uuid, 36);
+  head.put<uint32_t>(0);  // no file metadata
+  head.put<int32_t>(1);   // one grid
+  head.str(name);
+  head.str("Tree_float_5_4_3");
+  head.str("");  // not an instance
+  Out sec;
+  sec.put<uint32_t>(compression);
+  const char cls[] = "unknown";
+  int32_t lo[3] = {0, 0, 0}, hi[3] = {0, 0, 0};
+  if (n > 0)
+    for (int a = 0; a < 3; ++a) {
+      lo[a] = hi[a] = ijk[a];
+      for (int64_t i = 1; i < n; ++i) {
+        lo[a] = std::min(lo[a], ijk[3 * i + a]);
+        hi[a] = std::max(hi[a], ijk[3 * i + a]);
+      }
+    }
+  sec.put<uint32_t>(3);
+  sec.meta("class", "string", cls, (uint32_t)std::strlen(cls));
+  sec.meta("file_bbox_min", "vec3i", lo, 12);
+  sec.meta("file_bbox_max", "vec3i", hi, 12);
+  sec.str("UniformScaleMap");
+  const double v = voxel_size, iv = 1.0 / voxel_size;
+  const double map[15] = {v, v, v, v, v, v, iv, iv, iv, iv * iv, iv * iv, iv * iv,
+                          iv / 2, iv / 2, iv / 2};
+  sec.raw(map, sizeof(map));
+  const int64_t grid_pos = (int64_t)head.b.size() + 24;
+  const int64_t block_pos = grid_pos + (int64_t)sec.b.size() + (int64_t)topo.b.size();
+  const int64_t end_pos = block_pos + (int64_t)buffers.b.size();
+  head.put<int64_t>(grid_pos);
+  head.put<int64_t>(block_pos);
+  head.put<int64_t>(end_pos);
+  FILE* f = std::fopen(path, "wb");
+  if (!f) return nm::fail(NM_ERR_IO, "cannot write '%s'", path);
+  bool ok = true;
+  for (const Out* part : {&head, &sec, &topo, &buffers})
+    ok = ok && (part->b.empty() || std::fwrite(part->b.data(), 1, part->b.size(), f) == part->b.size());
+  ok = (std::fclose(f) == 0) && ok;
+  if (!ok) return nm::fail(NM_ERR_IO, "short write to '%s'", path);
   return NM_OK;
 }

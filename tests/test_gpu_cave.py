@@ -116,19 +116,23 @@ def test_cave_empty_lattice(ctx):
     sm.close()
 
 
-def test_cave_save_and_load(ctx, tmp_path):
+@pytest.mark.parametrize("name", ["map1.vdb", "map1.nmsim"])
+def test_cave_save_and_load(ctx, tmp_path, name):
+    """The cave written to the reference's file_out (a .vdb grid "grid", or an NMSIMv1 list)
+    and loaded as a sim grid equals the cave's sim map."""
     g, o = make(ctx, CASES[0])
     g.populate()
     g.smooth()
     g.floor_ceil()
     g.keep_largest()
-    written = g.save(tmp_path / "map1.vdb")
-    assert written.endswith("map1.nmsim")
+    written = g.save(tmp_path / name)
+    assert written.endswith(name)
     h = C.c_void_p()
     N.call("nm_simmap_load", ctx.h, written.encode(), C.byref(h))
     loaded = A.SimMap._adopt(ctx, 0.1, h)
     sm = g.simmap()
     assert np.array_equal(A.simmap_voxels(loaded), A.simmap_voxels(sm))
+    assert loaded.info() == sm.info()
     loaded.close()
     sm.close()
 
@@ -154,18 +158,6 @@ def test_cave_raycast_from_inside(ctx):
     sm.close()
 
 
-def read_nmsim(path):
-    import struct
-    with open(path, "rb") as f:
-        magic = f.read(8)
-        res, = struct.unpack("<f", f.read(4))
-        n, = struct.unpack("<q", f.read(8))
-        v = np.frombuffer(f.read(12 * n), np.int32).reshape(n, 3)
-    assert magic == b"NMSIMv1\0"
-    idx = np.lexsort((v[:, 2], v[:, 1], v[:, 0]))
-    return res, v[idx]
-
-
 @pytest.mark.parametrize("mode", ["3d", "2d", "gen"])
 def test_cavegen_facade_program(ctx, tmp_path, mode):
     """The reference's generator mains, written against nanomap::mapgen::CaveGen, give the
@@ -186,7 +178,7 @@ def test_cavegen_facade_program(ctx, tmp_path, mode):
     out = subprocess.run([str(exe), str(cfg), mode], capture_output=True, text=True)
     assert out.returncode == 0, out.stderr
     written, n_regions, largest = out.stdout.split()
-    assert written == str(tmp_path / "map1.nmsim")
+    assert written == str(tmp_path / "map1.vdb")
     d = A.load_cave_config(cfg)
     o = O.Cave(list(d.map_size), d.grid_res, d.fill_percentage, d.smoothing_count,
                d.active_max, d.active_min, d.seed)
@@ -201,8 +193,9 @@ def test_cavegen_facade_program(ctx, tmp_path, mode):
     assert (int(n_regions), int(largest)) == o.regions()
     if mode != "gen":
         o.keep_largest()
-    res, v = read_nmsim(written)
-    assert res == np.float32(0.1)
+    vs, tr, v = A.vdb_active_voxels(written)
+    assert np.float32(vs[0]) == np.float32(0.1) and not tr.any()
+    v = v[np.lexsort((v[:, 2], v[:, 1], v[:, 0]))]
     assert np.array_equal(v, o.voxels(shell=True))
 
 

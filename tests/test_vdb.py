@@ -121,3 +121,16 @@ def test_refusals(tmp_path):
     rc = N.lib().nm_vdb_active_voxels(str(p).encode(), None, None, None,
                                       buf.ctypes.data_as(N._PI32), 5, C.byref(cnt))
     assert rc == N.NM_ERR_CAPACITY and cnt.value == len(v)
+
+
+@pytest.mark.parametrize("n", [0, 1, 3000])
+def test_writer_round_trip(tmp_path, n):
+    """nm_vdb_write_active_voxels (the caves' .vdb output) read back by nm_vdb_active_voxels."""
+    v = _voxels(seed=9, n=n)[:n] if n else np.zeros((0, 3), np.int32)
+    p = tmp_path / "w.vdb"
+    A.vdb_write_active_voxels(p, v, 0.05)
+    vs, tr, got = A.vdb_active_voxels(p)
+    assert np.allclose(vs, 0.05) and np.allclose(tr, 0.0)
+    assert np.array_equal(_sorted(got), _sorted(np.unique(v, axis=0)))
+    A.vdb_write_active_voxels(tmp_path / "named.vdb", v, 0.05, grid="cave")
+    assert len(A.vdb_active_voxels(tmp_path / "named.vdb", "cave")[2]) == len(np.unique(v, axis=0))
