@@ -134,3 +134,26 @@ def test_writer_round_trip(tmp_path, n):
     assert np.array_equal(_sorted(got), _sorted(np.unique(v, axis=0)))
     A.vdb_write_active_voxels(tmp_path / "named.vdb", v, 0.05, grid="cave")
     assert len(A.vdb_active_voxels(tmp_path / "named.vdb", "cave")[2]) == len(np.unique(v, axis=0))
+
+
+def test_corrupted_files_end_in_an_error_or_a_voxel_set(tmp_path):
+    """Bytes overwritten or the file cut short at seeded places: every read returns a status
+    (no crash, no out-of-bounds write); the voxel lists that come back fit the array."""
+    rng = np.random.default_rng(21)
+    v = _voxels(seed=4, n=500)
+    raw = write_vdb(tmp_path / "base.vdb", v, compression=ZIP | ACTIVE_MASK, codes=(0, 3, 5, 6),
+                    collapse=True, root_tiles=[(8192, 0, 0, 0)]).read_bytes()
+    p = tmp_path / "m.vdb"
+    for k in range(300):
+        b = bytearray(raw)
+        if k % 2:
+            b = b[: int(rng.integers(0, len(b)))]
+        else:
+            for _ in range(int(rng.integers(1, 6))):
+                b[int(rng.integers(0, len(b)))] = int(rng.integers(0, 256))
+        p.write_bytes(bytes(b))
+        try:
+            vs, tr, got = A.vdb_active_voxels(p)
+            assert got.ndim == 2 and got.shape[1] == 3
+        except N.NanomapError as e:
+            assert e.code in (N.NM_ERR_IO, N.NM_ERR_UNSUPPORTED, N.NM_ERR_ARG, N.NM_ERR_CAPACITY)
