@@ -857,6 +857,10 @@ def run_refine_section(local, trials=3):
         R = so3_exp(np.radians(rr.uniform(-2.0, 2.0, 3))) @ gR
         sim.render(cam, gt, target)
         row = {"start_error": gap(gpos, gR, pos, R)}
+        if trial == 0:
+            # untimed warm-up: the process's first refinement call carries one-time costs
+            # (about 0.1 s in a full bench run)
+            two_stage(pos, R, target)
         sm = {}
         for name, p0, R0 in (("perturbed", pos, R), ("from_truth", gpos, gR)):
             p1, R1, la, lb, mps = two_stage(p0, R0, target)
