@@ -91,6 +91,7 @@ def lib() -> C.CDLL:
         L.orc_voxel_filter.restype = C.c_int64
         L.orc_render_boxes.argtypes = [C.POINTER(OrcSensor), _PD, _PD, _PD, C.c_int, _PF]
         L.orc_sim_cast.argtypes = [C.c_void_p, _PF, _PF, C.c_int64, C.c_float, _PF]
+        L.orc_depth_set_stop.argtypes = [C.c_double]
         L.orc_depth.argtypes = [C.POINTER(OrcSensor), _PD, _PD, C.c_double, _PI32, _PF, C.c_int64,
                                 C.c_double, C.c_double, _PI32, C.c_int64, _PD, _PD,
                                 C.POINTER(C.c_uint64), _PD, _PD]
@@ -325,10 +326,12 @@ def voxel_filter(R, eye, res, max_time, rounding, points, centre=False):
 
 
 def depth(sensor: Sensor, pos, R, res, origins, values, scale=1.0, bias=0.0, pixels=None,
-          grad_depth=None, want_grad=True):
+          grad_depth=None, want_grad=True, stop_transmittance=0.0):
     """FP64 expected depth of the listed pixels (all when None) over a map given as leaf
     origins (n, 3) and values (n, 512).  Returns (depth (m), dpose (n_pix, 6): d/drho, d/dphi,
-    sequence hashes, grad_values (n, 512) of sum grad_depth * depth or None)."""
+    sequence hashes, grad_values (n, 512) of sum grad_depth * depth or None).
+    stop_transmittance > 0 leaves out each ray's voxels after its transmittance falls below
+    it (the definition walks to max range)."""
     s = sensor.s
     if pixels is None:
         pixels = np.arange(s.width * s.height, dtype=np.int32)
@@ -344,6 +347,7 @@ def depth(sensor: Sensor, pos, R, res, origins, values, scale=1.0, bias=0.0, pix
     if grad_depth is not None:
         gd = _d(grad_depth).reshape(-1)
         gv = np.zeros((len(origins), 512))
+    lib().orc_depth_set_stop(C.c_double(stop_transmittance))
     lib().orc_depth(C.byref(s), dp(_d(pos)), dp(_d(R).reshape(-1)), C.c_double(res),
                     origins.ctypes.data_as(_PI32), fp(values), len(origins), C.c_double(scale),
                     C.c_double(bias), pixels.ctypes.data_as(_PI32), n, dp(out),
