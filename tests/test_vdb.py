@@ -157,3 +157,14 @@ def test_corrupted_files_end_in_an_error_or_a_voxel_set(tmp_path):
             assert got.ndim == 2 and got.shape[1] == 3
         except N.NanomapError as e:
             assert e.code in (N.NM_ERR_IO, N.NM_ERR_UNSUPPORTED, N.NM_ERR_ARG, N.NM_ERR_CAPACITY)
+
+
+def test_writer_refusals(tmp_path):
+    v = np.array([[0, 0, 0]], np.int32)
+    for size in (0.0, -0.1, float("nan"), float("inf")):
+        with pytest.raises(N.NanomapError) as e:
+            A.vdb_write_active_voxels(tmp_path / "x.vdb", v, size)
+        assert e.value.code == N.NM_ERR_ARG, size
+    with pytest.raises(N.NanomapError) as e:
+        A.vdb_write_active_voxels(tmp_path / "missing_dir" / "x.vdb", v, 0.1)
+    assert e.value.code == N.NM_ERR_IO
