@@ -158,8 +158,12 @@ def write_vdb(path, voxels, *, res=0.1, translation=(0.0, 0.0, 0.0), transform="
         pos_at = len(body) + len(desc)
         grid_pos = pos_at + 24
         section = struct.pack("<I", compression)
+        # grid metadata as files carry it, including a binary entry of a type the reader does
+        # not know (skipped by its size)
         section += _meta([("class", "string", b"level set"), ("name", "string", name.encode()),
-                          ("file_bbox_min", "vec3i", struct.pack("<iii", 0, 0, 0))])
+                          ("file_bbox_min", "vec3i", struct.pack("<iii", 0, 0, 0)),
+                          ("file_voxel_count", "int64", struct.pack("<q", len(voxels))),
+                          ("file_delayed_load", "__delayedload", bytes(range(37)))])
         s = [res] * 3
         inv = [1.0 / res] * 3
         if transform == "UniformScaleMap":
